@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the neighbour-graph path (``pp.neighbors``) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload scale|plain|precision] [--precision bf16x3|fp16|bf16|fp32]
+
+A step = one full graph (exact kNN → distances CSR → UMAP connectivities) of the workload's
+synthetic embedding.  Default workload: 1,300,000 cells × 50 PCs, 200-cluster Gaussian mixture with
+lognormal sizes and 1% noise cells, euclidean, k=15, method='umap', BF16 tensor-core candidates
+(three-term split) + exact re-rank.
+
+value   cells/s with the embedding resident in HBM (whole job: N replicas × cells / max time);
+e2e     the same through the public call with host buffers: pinned host → device copy of the
+        embedding and device → host copy of both CSR matrices inside the timed region;
+roofline: the tensor-core candidate kernel, algorithmic 2·d·n² FLOP over its event-timed
+        duration, against the measured dense BF16 peak (MEASURED_PEAKS.json);
+cpu_baseline: the CPU oracle port on this host's cores, on a bounded sample of query rows.
+
+With --impl reference the CPU implementation alone runs (rank 0), on bounded samples.
+Multi-GPU (torchrun): every rank builds its own full graph (replicas; the path runs on one GPU).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT, ROOT / "metal-singlecell_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+import numpy as np
+
+METRIC = "kNN-graph cells/s at 1.3M×50 k=15, BF16+rerank vs FP32 GPU; serve p50/p99 ms"
+
+
+def workload(name: str):
+    from msc_b200 import synth
+    if name == "scale":
+        X, p = synth.scale_1m3()
+        return X, p, "scale: 1,300,000 cells x 50 PCs, 200 clusters (lognormal sizes), 1% noise"
+    if name == "plain":
+        X, p = synth.plain_10k()
+        return X, p, "plain: 10,000 cells x 50 PCs, 20 equal clusters"
+    if name == "precision":
+        X, p = synth.precision_200k()
+        return X, p, "precision: 200,000 cells x 50 PCs, 50 anisotropic clusters, cosine"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples of this GPU during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(X, k, metric, budget_s: float = 15.0):
+    """Oracle port on the host: exact kNN of a seeded sample of query rows against the whole
+    embedding, plus the per-row ρ/σ and membership stages; cells/s = rows / time."""
+    import oracle
+    cores = len(os.sched_getaffinity(0))
+    rng = np.random.default_rng(1234)
+    n = X.shape[0]
+    m = int(min(n, 256))
+    t_total, rows = 0.0, 0
+    while t_total < budget_s and rows < n:
+        q = np.sort(rng.choice(n, m, replace=False))
+        t0 = time.perf_counter()
+        idx, d2, dist = oracle.knn_exact(X, k, metric=metric, rows=q, threads=cores)
+        sigma, rho = oracle.smooth_knn_dist(dist, float(k))
+        oracle.membership_strengths(idx - q[:, None] + np.arange(m)[:, None], dist, sigma, rho)
+        t_total += time.perf_counter() - t0
+        rows += m
+        m = int(min(n, max(m, rows * 2)))  # grow the sample until the budget is spent
+        if t_total > budget_s * 0.5:
+            break
+    return {"value": rows / t_total, "unit": "cells/s", "cores": cores, "kind": "port",
+            "sample": f"{rows} seeded query rows of the {n}-cell embedding (exact kNN against all "
+                      f"{n} cells + rho/sigma + memberships), {t_total:.1f} s on {cores} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    X, p, desc = workload(args.workload)
+    k, metric = p["n_neighbors"], p["metric"]
+    for _ in range(args.warmup):
+        cpu_baseline(X, k, metric, budget_s=2.0)
+    vals, t0 = [], time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(X, k, metric, budget_s=args.ref_budget)["value"])
+    wall = time.perf_counter() - t0
+    cb = cpu_baseline.__doc__ and None
+    v = float(np.median(vals))
+    last = cpu_baseline(X, k, metric, budget_s=1.0)
+    line = {"metric": METRIC, "value": v, "unit": "cells/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "n_neighbors": k, "metric": metric,
+                       "method": p.get("method", "umap"), "impl": "CPU oracle port (NumPy/SciPy)"},
+            "cpu_baseline": {"value": v, "unit": "cells/s", "cores": last["cores"],
+                             "kind": "port", "sample": last["sample"]},
+            "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    del cb
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from msc_b200 import neighbors as nbm, _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    lib = _lib.load()
+
+    X, p, desc = workload(args.workload)
+    n, d = X.shape
+    k, metric = p["n_neighbors"], p["metric"]
+    method = p.get("method", "umap")
+    kprime = p.get("kprime", 0)
+    Xd = torch.from_numpy(X).to(dev)
+    ws = nbm.Workspace(dev)
+    out = {}
+
+    def step(precision=args.precision):
+        return nbm.neighbors_device(Xd, k, metric=metric, method=method, precision=precision,
+                                    kprime=kprime, workspace=ws, out=out)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    res = step()
+    torch.cuda.synchronize()
+    stats = res["stats"].cpu().numpy()
+    _lib.check_stats(stats)
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    st = torch.cuda.current_stream(dev)
+    launches0 = lib.msc_launch_count()
+    with ClockSampler(uuid) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        barrier()
+    launches = lib.msc_launch_count() - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = world * n / (ms / 1000.0)
+
+    # per-stage times of one profiled step (events on the launching stream)
+    lib.msc_profile_enable(1)
+    step()
+    torch.cuda.synchronize()
+    import ctypes
+    buf = (ctypes.c_float * 8)()
+    ns = lib.msc_profile_read(buf, 8)
+    lib.msc_profile_enable(0)
+    stage_names = ["prep", "candidates", "rerank_fp64", "csr_rho_sigma_membership", "union"]
+    stages = {stage_names[i]: round(buf[i], 3) for i in range(min(ns, len(stage_names)))}
+
+    pk, pk_kind = peaks()
+    cand_ms = stages.get("candidates")
+    alg_flop = 2.0 * d * float(n) * float(n)
+    achieved = alg_flop / (cand_ms / 1000.0) / 1e12 if cand_ms else None
+    peak = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops")
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(f"{args.workload}:{args.precision}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "knn_tc_kernel" if args.precision != "fp32" else "knn_fp32_kernel",
+                "algorithmic_flop_per_launch": alg_flop, "kernel_ms": cand_ms,
+                "peak_kind": f"{pk_kind} bf16 sustained (kernel timed inside a full step)",
+                "stage_ms": stages}
+
+    # e2e through the public call: pinned host in, both CSR matrices back to pinned host
+    Xh = torch.from_numpy(X).pin_memory()
+    m = k - 1
+    host = {"dist_indptr": torch.empty(n + 1, dtype=torch.int64).pin_memory(),
+            "dist_indices": torch.empty(n * m, dtype=torch.int32).pin_memory(),
+            "dist_data": torch.empty(n * m, dtype=torch.float32).pin_memory(),
+            "conn_indptr": torch.empty(n + 1, dtype=torch.int64).pin_memory(),
+            "conn_indices": torch.empty(2 * n * m, dtype=torch.int32).pin_memory(),
+            "conn_data": torch.empty(2 * n * m, dtype=torch.float32).pin_memory()}
+    Xe = torch.empty_like(Xd)
+
+    def e2e_step():
+        Xe.copy_(Xh, non_blocking=True)
+        r = nbm.neighbors_device(Xe, k, metric=metric, method=method, precision=args.precision,
+                                 kprime=kprime, workspace=ws, out=out)
+        nnz = int(r["conn_indptr"][n].item())          # device → host read of the result size
+        for key in ("dist_indptr", "conn_indptr"):
+            host[key].copy_(r[key], non_blocking=True)
+        host["dist_indices"][: n * m].copy_(r["dist_indices"][: n * m], non_blocking=True)
+        host["dist_data"][: n * m].copy_(r["dist_data"][: n * m], non_blocking=True)
+        host["conn_indices"][:nnz].copy_(r["conn_indices"][:nnz], non_blocking=True)
+        host["conn_data"][:nnz].copy_(r["conn_data"][:nnz], non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        return nnz
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nnzs = [e2e_step() for _ in range(args.steps)]
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    barrier()
+    h2d = X.nbytes
+    d2h = 8 + 2 * (n + 1) * 8 + n * m * 8 + nnzs[-1] * 8
+    e2e = {"value": world * n / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_s}
+
+    # the plain FP32 GPU form of the same graph (the comparison the metric names)
+    fp32 = None
+    if not args.skip_fp32 and args.precision != "fp32":
+        step("fp32")
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(st)
+        step("fp32")
+        f1.record(st)
+        torch.cuda.synchronize()
+        fms = max_over_ranks(f0.elapsed_time(f1))
+        fp32 = {"value": world * n / (fms / 1000.0), "unit": "cells/s", "ms_per_step": fms,
+                "speedup_of_headline": fms / ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(X, k, metric, budget_s=args.ref_budget)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": desc, "n_neighbors": k, "metric": metric,
+                           "method": method, "precision": args.precision,
+                           "kprime": int(kprime) or "auto",
+                           "l2": "inputs larger than L2 (embedding 260 MB + packed operands)",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+                "cpu_baseline": cpu, "fp32_form": fp32,
+                "stats": {"certified": int(stats[_lib.STAT_CERTIFIED]),
+                          "rescanned": int(stats[_lib.STAT_RESCANNED]),
+                          "fp64_boundary_recomputes": int(stats[_lib.STAT_FP64_TIES]),
+                          "conn_nnz": int(stats[_lib.STAT_CONN_NNZ])},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="scale", choices=["scale", "plain", "precision"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp16", "bf16", "fp32"])
+    ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=15.0)
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * msc_b200 — C ABI of the B200 neighbour-graph library (the `msc.pp.neighbors` hot path).
+ *
+ * Every entry point is stream-ordered: it enqueues work on `stream` (a cudaStream_t passed as
+ * void*, NULL = legacy default stream) and returns without waiting.  Pointers named *_dev are
+ * device pointers; nothing is allocated inside the library — scratch memory is the caller's
+ * `workspace`, sized by the matching *_workspace_bytes() query.  Errors come back as an int status
+ * (never as an exception across the ABI); msc_last_error() gives the message of the calling
+ * thread's last failure.  Errors that can only be seen on the device (non-finite input, a timed-out
+ * wait) are counted in the int64 `stats_dev` block (MSC_STAT_*) that the caller reads after the
+ * stream completes.
+ *
+ * Conventions shared by all calls (the reference's, metalsinglecell `neighbors.py`):
+ *   X          n×d float32, row-major, one cell per row (the PCA embedding).
+ *   knn_idx    n×k int32, row i = [i, then the k-1 nearest other cells by (distance, index)].
+ *   knn_dist   n×k float32, the matching distances (column 0 is 0).
+ *   CSR        int64 indptr (n+1), int32 indices (column-sorted per row), float32 data.
+ */
+#ifndef MSC_B200_H
+#define MSC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MSC_OK                  0
+#define MSC_ERR_INVALID_ARG     1   /* bad shape, k, pointer or option (Python: ValueError)      */
+#define MSC_ERR_WORKSPACE       2   /* workspace smaller than *_workspace_bytes() (MemoryError) */
+#define MSC_ERR_TIMEOUT         3   /* a device-side wait hit its bound (RuntimeError)          */
+#define MSC_ERR_CUDA            4   /* a CUDA runtime call failed (RuntimeError)                */
+#define MSC_ERR_UNSUPPORTED     5   /* valid request this build does not handle (NotImplemented)*/
+
+/* metric (the reference accepts only euclidean, pp.py:768-769) */
+#define MSC_METRIC_EUCLIDEAN    0
+#define MSC_METRIC_COSINE       1
+
+/* candidate precision of the distance + top-k stage */
+#define MSC_PREC_FP32           0   /* plain FP32 SIMT Gram form                                 */
+#define MSC_PREC_BF16X3         1   /* tcgen05 BF16, 3-term split (hi·hi + hi·lo + lo·hi)        */
+#define MSC_PREC_FP16           2   /* tcgen05 FP16, one term (the reference ranks on fp16)      */
+#define MSC_PREC_BF16           3   /* tcgen05 BF16, one term                                    */
+
+/* connectivity method */
+#define MSC_METHOD_UMAP         0
+#define MSC_METHOD_GAUSS        1
+
+/* indices into the int64 stats block (MSC_STATS_LEN entries, zeroed by the call) */
+#define MSC_STAT_NONFINITE      0   /* non-finite input values seen                              */
+#define MSC_STAT_TIMEOUT        1   /* device waits that gave up                                 */
+#define MSC_STAT_CERTIFIED      2   /* rows whose candidate set was proven to hold the exact kNN */
+#define MSC_STAT_REFINED        3   /* rows re-run through the BF16x3 candidate stage            */
+#define MSC_STAT_RESCANNED      4   /* rows finished by the exact FP64 full scan                 */
+#define MSC_STAT_FP64_TIES      5   /* candidates re-ranked in FP64 at the k-th boundary         */
+#define MSC_STAT_CONN_NNZ       6   /* nnz of the connectivities CSR                              */
+#define MSC_STAT_PRECISION      7   /* candidate precision actually used (FP32 when the operand
+                                       row is too wide for the tensor-core tile; -1: FP64 scan) */
+#define MSC_STATS_LEN           8
+
+#define MSC_MAX_K               129 /* largest n_neighbors (above 65 every row takes the FP64 scan) */
+#define MSC_MAX_D               128 /* largest representation width                             */
+
+int         msc_version(void);
+const char* msc_last_error(void);
+
+/* Instrumentation (no counterpart in the reference).
+ *   msc_launch_count   kernels this library has launched in this process;
+ *   msc_profile_enable process-wide switch: record CUDA events between pipeline stages
+ *                      (prep | candidates | re-rank + FP64 scan | CSR + rho/sigma + memberships |
+ *                      fuzzy union) of the following calls — not for concurrent callers;
+ *   msc_profile_read   waits for the last profiled call's events and writes its stage times in ms;
+ *                      returns the number of stages written. */
+long long msc_launch_count(void);
+int       msc_profile_enable(int on);
+int       msc_profile_read(float* ms_out, int max_stages);
+
+/* ---------------------------------------------------------------------------------------------
+ * Whole graph — replaces metalsinglecell `neighbors.neighbors` (neighbors.py:727-760), itself
+ * called by `pp.neighbors` (pp.py:774).
+ *   dist_*  : the distances CSR of neighbors.py:755-759 (k-1 entries per row, indptr i·(k-1)).
+ *   conn_*  : the connectivities CSR (capacity 2·n·(k-1) entries); its nnz is written to
+ *             stats_dev[MSC_STAT_CONN_NNZ] and conn_indptr[n].
+ *   kprime  : candidates kept per row by the tensor-core stage (0 = automatic).
+ * ------------------------------------------------------------------------------------------- */
+size_t msc_neighbors_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric,
+                                     int32_t method, int32_t precision, int32_t kprime);
+int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+                  int32_t method, int32_t precision, int32_t kprime,
+                  int32_t* knn_idx_dev, float* knn_dist_dev,
+                  int64_t* dist_indptr_dev, int32_t* dist_indices_dev, float* dist_data_dev,
+                  int64_t* conn_indptr_dev, int32_t* conn_indices_dev, float* conn_data_dev,
+                  int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Exact kNN — replaces `_knn` / `_knn_gpu` (neighbors.py:698-724, 82-132): the fp16 Gram
+ * distance (neighbors.py:117-118), the register top-k kernel `topk_rows` (neighbors.py:25-79),
+ * the fp32 recompute (neighbors.py:122-123) and the host sort (neighbors.py:129-131), as one fused
+ * candidate kernel + exact re-rank.  Self first; ties by index.
+ * ------------------------------------------------------------------------------------------- */
+size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, int32_t precision,
+                               int32_t kprime);
+int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+            int32_t precision, int32_t kprime, int32_t* knn_idx_dev, float* knn_dist_dev,
+            int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Many independent samples in one persistent launch: sample s is rows [offsets[s], offsets[s+1])
+ * of X and its neighbours are searched only among its own rows.  `offsets_host` has n_samples+1
+ * entries; every sample needs at least k cells.  New in this library (the reference loops in
+ * Python over per-batch brute-force calls, neighbors.py:516-539).
+ *   msc_batched_prepare  writes the sample table into the workspace and waits for that copy;
+ *   msc_batched_knn      only enqueues kernels (capturable in a CUDA graph); call it with the
+ *                        same offsets / shapes as the prepare call.
+ * tile_config: 0 = automatic, else bn | stages<<12 | cb<<20 (key tile rows, pipeline depth,
+ * selector buffer) as chosen by the Python autotuner. */
+size_t msc_batched_workspace_bytes(const int64_t* offsets_host, int32_t n_samples, int32_t d,
+                                   int32_t k, int32_t metric, int32_t precision, int32_t kprime);
+int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t d, int32_t k,
+                        int32_t metric, int32_t precision, int32_t kprime, void* workspace,
+                        size_t workspace_bytes, void* stream);
+int msc_batched_knn(const float* X_dev, const int64_t* offsets_host, int32_t n_samples, int32_t d,
+                    int32_t k, int32_t metric, int32_t precision, int32_t kprime,
+                    int32_t tile_config, int32_t* knn_idx_dev, float* knn_dist_dev,
+                    int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * UMAP fuzzy simplicial set pieces — replace umap-learn 0.5.12 `fuzzy_simplicial_set` as the
+ * reference calls it (neighbors.py:742-753: set_op_mix_ratio=1, local_connectivity=1).
+ * ------------------------------------------------------------------------------------------- */
+/* per-row rho / sigma by bisection (umap-learn smooth_knn_dist); workspace >= 64 bytes */
+int msc_smooth_knn_dist(const float* knn_dist_dev, int64_t n, int32_t k,
+                        float local_connectivity, float* sigma_dev, float* rho_dev,
+                        void* workspace, size_t workspace_bytes, void* stream);
+/* memberships w_ij (umap-learn compute_membership_strengths); self -> 0 */
+int msc_membership(const int32_t* knn_idx_dev, const float* knn_dist_dev, const float* sigma_dev,
+                   const float* rho_dev, int64_t n, int32_t k, float* w_dev, void* stream);
+/* P = A + A^T - A∘A^T as CSR (zeros of A eliminated first), bit-exact float32 arithmetic */
+size_t msc_fuzzy_union_workspace_bytes(int64_t n, int32_t k);
+int msc_fuzzy_union(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, int32_t k,
+                    int64_t* indptr_dev, int32_t* indices_dev, float* data_dev, int64_t* nnz_dev,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* method='gauss' connectivities (scanpy's locally scaled Gaussian kernel; not in the reference) */
+size_t msc_gauss_workspace_bytes(int64_t n, int32_t k);
+int msc_gauss_connectivities(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                             int32_t k, int64_t* indptr_dev, int32_t* indices_dev,
+                             float* data_dev, int64_t* nnz_dev, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* distances CSR exactly as neighbors.py:755-759 builds it (explicit zeros kept) */
+int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                      int32_t k, int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSC_B200_H */

@@ -1,0 +1,588 @@
+// C ABI of the library: argument checks, workspace layout and the stream-ordered pipelines.
+//
+//   msc_neighbors  = kNN + distances CSR + connectivities   (metalsinglecell neighbors.py:727-760)
+//   msc_knn        = kNN only                                (neighbors.py:698-724 / 82-132)
+//   msc_batched_*  = kNN of many samples in one persistent launch
+//   msc_smooth_knn_dist / msc_membership / msc_fuzzy_union / msc_gauss_connectivities /
+//   msc_distances_csr = the individual graph stages
+//
+// Nothing here allocates device memory: every buffer is carved out of the caller's workspace.
+#include <mutex>
+#include <vector>
+#include <algorithm>
+#include <unordered_map>
+
+#include "kernels.cuh"
+
+namespace msc {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+const char* last_error() { return g_err.c_str(); }
+
+std::atomic<long long> g_launch_count{0};
+
+// ---- stage timing: events recorded between pipeline stages when enabled ----
+namespace {
+constexpr int MAX_MARKS = 16;
+struct StageTimer {
+  bool on = false;
+  cudaEvent_t ev[MAX_MARKS] = {};
+  int last = -1;           // highest mark recorded in the current call
+  std::mutex mu;
+};
+StageTimer& timer() {
+  static StageTimer t;
+  return t;
+}
+}  // namespace
+
+void stage_mark(cudaStream_t st, int stage) {
+  StageTimer& t = timer();
+  if (!t.on || stage < 0 || stage >= MAX_MARKS) return;
+  if (!t.ev[stage] && cudaEventCreate(&t.ev[stage]) != cudaSuccess) return;
+  cudaEventRecord(t.ev[stage], st);
+  if (stage == 0) t.last = 0;
+  else t.last = std::max(t.last, stage);
+}
+
+int num_sms() {
+  static std::mutex mu;
+  static std::unordered_map<int, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int v = 148;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 148;
+  cache[dev] = v;
+  return v;
+}
+
+namespace {
+
+constexpr int COLMEAN_NB = 256;
+
+struct Problem {
+  int64_t n = 0;          // total cells
+  int d = 0, k = 0, metric = 0, prec = 0, kprime = 0;
+  int nseg = 1;
+  int64_t npacked = 0;    // packed rows
+  int64_t ntiles = 0;     // 128-row query tiles
+  int64_t max_seg = 0;
+  bool candidates = true; // false: every row takes the FP64 scan (k-1 > 64)
+  OpLayout L{};
+  int dpad = 0;
+};
+
+struct KnnWs {
+  Ctl* ctl;
+  KeyMax* km;
+  SegDesc* seg;
+  WorkItem* items;
+  double* mean;
+  double* partial;
+  float* Xn;
+  void* Aop;
+  void* Bop;
+  float* A32;
+  float* sq32;
+  QStat* qs;
+  int32_t* cand_idx;
+  float* cand_thr;
+  int32_t* fail_rows;
+};
+
+int default_kprime(int prec, int k) {
+  if (prec == PREC_FP32) return std::min(64, std::max(k - 1, k + 7));
+  return std::min(64, std::max(48, k + 15));
+}
+
+int check_common(int64_t n, int d, int k, int metric, int prec, int kprime) {
+  if (n < 1 || n >= (int64_t(1) << 30)) { set_error("n=%lld out of range", (long long)n); return MSC_ERR_INVALID_ARG; }
+  if (d < 1 || d > MSC_MAX_D) { set_error("d=%d must be in [1, %d]", d, MSC_MAX_D); return MSC_ERR_INVALID_ARG; }
+  if (k < 1 || k > MSC_MAX_K) { set_error("n_neighbors=%d must be in [1, %d]", k, MSC_MAX_K); return MSC_ERR_INVALID_ARG; }
+  if (metric != MSC_METRIC_EUCLIDEAN && metric != MSC_METRIC_COSINE) { set_error("unknown metric %d", metric); return MSC_ERR_INVALID_ARG; }
+  if (prec < 0 || prec > 3) { set_error("unknown precision %d", prec); return MSC_ERR_INVALID_ARG; }
+  if (kprime != 0 && (kprime < k - 1 || kprime > 64)) {
+    set_error("kprime=%d must be 0 or in [n_neighbors-1=%d, 64]", kprime, k - 1);
+    return MSC_ERR_INVALID_ARG;
+  }
+  return MSC_OK;
+}
+
+int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int kprime,
+                 const int64_t* offsets, int nseg) {
+  MSC_TRY(check_common(n, d, k, metric, prec, kprime));
+  P.n = n; P.d = d; P.k = k; P.metric = metric; P.prec = prec;
+  P.kprime = kprime ? kprime : default_kprime(prec, k);
+  P.candidates = (k - 1) <= 64;
+  if (P.candidates) P.kprime = std::max(P.kprime, k - 1);
+  P.nseg = nseg;
+  P.L = op_layout(prec, d);
+  P.dpad = int(round_up(d, 4));
+  if (offsets) {
+    if (offsets[0] != 0 || offsets[nseg] != n) { set_error("offsets must run from 0 to n"); return MSC_ERR_INVALID_ARG; }
+    P.npacked = 0; P.ntiles = 0; P.max_seg = 0;
+    for (int s = 0; s < nseg; ++s) {
+      const int64_t ns = offsets[s + 1] - offsets[s];
+      if (ns < k) { set_error("sample %d has %lld cells < n_neighbors=%d", s, (long long)ns, k); return MSC_ERR_INVALID_ARG; }
+      P.npacked += round_up(ns, SEG_PAD);
+      P.ntiles += ceil_div(ns, QTILE);
+      P.max_seg = std::max(P.max_seg, ns);
+    }
+  } else {
+    if (n < k) { set_error("n_neighbors=%d > n=%lld", k, (long long)n); return MSC_ERR_INVALID_ARG; }
+    P.npacked = round_up(n, SEG_PAD);
+    P.ntiles = ceil_div(n, QTILE);
+    P.max_seg = n;
+  }
+  if (P.npacked >= (int64_t(1) << 31)) { set_error("too many packed rows"); return MSC_ERR_UNSUPPORTED; }
+  if (P.candidates && prec != PREC_FP32) {
+    TcConfig c = tc_default_config(prec, d, P.kprime);
+    if (!tc_config_ok(c, P.L.kp, P.kprime)) {
+      // the operand row is too wide for a resident query tile at this precision: the FP32
+      // candidate kernel takes over (the result is exact either way; MSC_STAT_PRECISION says)
+      P.prec = PREC_FP32;
+      P.kprime = kprime ? kprime : default_kprime(PREC_FP32, k);
+      P.kprime = std::max(P.kprime, k - 1);
+      P.L = op_layout(PREC_FP32, d);
+    }
+  }
+  return MSC_OK;
+}
+
+KnnWs carve_knn(Carver& c, const Problem& P) {
+  KnnWs w{};
+  w.ctl = c.take<Ctl>(1);
+  w.km = c.take<KeyMax>(1);
+  w.seg = c.take<SegDesc>(P.nseg);
+  w.items = c.take<WorkItem>(P.ntiles);
+  w.mean = c.take<double>(size_t(P.nseg) * P.d);
+  w.partial = c.take<double>(colmean_partial_elems(P.nseg, P.d, COLMEAN_NB));
+  w.Xn = P.metric == MSC_METRIC_COSINE ? c.take<float>(size_t(P.n) * P.d) : nullptr;
+  if (P.prec == PREC_FP32) {
+    w.A32 = c.take<float>(size_t(P.npacked) * P.dpad);
+    w.sq32 = c.take<float>(P.npacked);
+  } else {
+    w.Aop = c.take<uint16_t>(size_t(P.npacked) * P.L.kp);
+    w.Bop = c.take<uint16_t>(size_t(P.npacked) * P.L.kp);
+  }
+  w.qs = c.take<QStat>(P.npacked);
+  w.cand_idx = c.take<int32_t>(size_t(P.n) * P.kprime);
+  w.cand_thr = c.take<float>(P.n);
+  w.fail_rows = c.take<int32_t>(P.n);
+  return w;
+}
+
+int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
+  cfg = tc_default_config(P.prec, P.d, P.kprime);
+  if (code == 0) return MSC_OK;
+  TcConfig c{code & 0xfff, (code >> 12) & 0xff, P.kprime <= 32 ? 32 : 64, (code >> 20) & 0xff};
+  if (!tc_config_ok(c, P.L.kp, P.kprime)) {
+    set_error("tile_config 0x%x (bn=%d stages=%d cb=%d) is not valid here", code, c.bn, c.stages, c.cb);
+    return MSC_ERR_INVALID_ARG;
+  }
+  cfg = c;
+  return MSC_OK;
+}
+
+int launch_set_stat(Ctl* ctl, int idx, int64_t v, cudaStream_t st);
+
+// The kNN pipeline after the sample table (w.seg) is in place.
+int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, float* knn_dist,
+            int32_t tile_code, cudaStream_t st) {
+  stage_mark(st, 0);
+  MSC_CUDA_TRY(cudaMemsetAsync(w.ctl, 0, sizeof(Ctl), st));
+  MSC_CUDA_TRY(cudaMemsetAsync(w.km, 0, sizeof(KeyMax), st));
+  MSC_TRY(launch_set_stat(w.ctl, MSC_STAT_PRECISION, P.candidates ? P.prec : -1, st));
+  const bool cosine = P.metric == MSC_METRIC_COSINE;
+  const float* Xu = X;
+  if (cosine) {
+    MSC_TRY(launch_normalize(X, w.Xn, P.n, P.d, &w.ctl->stats[MSC_STAT_NONFINITE], st));
+    Xu = w.Xn;
+  }
+  MSC_TRY(launch_build_items(w.seg, P.nseg, P.ntiles, w.items, w.ctl, st));
+  if (!P.candidates) {
+    MSC_TRY(launch_all_rows_fail(w.seg, P.nseg, P.npacked, w.fail_rows, w.ctl, st));
+    MSC_TRY(launch_fp64_scan(Xu, P.d, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine, knn_idx,
+                             knn_dist, w.ctl, st));
+    return MSC_OK;
+  }
+  MSC_TRY(launch_colmean(Xu, w.seg, P.nseg, P.max_seg, P.d, w.partial, COLMEAN_NB, w.mean,
+                         cosine ? nullptr : &w.ctl->stats[MSC_STAT_NONFINITE], st));
+  if (P.k > 1) {
+    if (P.prec == PREC_FP32) {
+      MSC_TRY(launch_pack_fp32(Xu, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked, w.A32, w.sq32,
+                               w.qs, w.km, st));
+      stage_mark(st, 1);
+      MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.ctl, P.kprime,
+                              w.cand_idx, w.cand_thr, P.kprime, st));
+    } else {
+      if (P.prec == PREC_FP16)
+        MSC_TRY(launch_maxnorm(Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.ctl, st));
+      MSC_TRY(launch_pack_tc(P.prec, Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.Aop, w.Bop,
+                             w.qs, w.km, w.ctl, st));
+      TcConfig cfg;
+      MSC_TRY(decode_tile_config(tile_code, P, cfg));
+      stage_mark(st, 1);
+      MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
+                            w.items, P.ntiles, w.ctl, P.kprime, w.cand_idx, w.cand_thr,
+                            P.kprime, st));
+    }
+  }
+  stage_mark(st, 2);
+  MSC_TRY(launch_rerank(Xu, P.d, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr, P.kprime,
+                        P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx, knn_dist,
+                        w.fail_rows, w.ctl, st));
+  MSC_TRY(launch_fp64_scan(Xu, P.d, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine, knn_idx,
+                           knn_dist, w.ctl, st));
+  stage_mark(st, 3);
+  return MSC_OK;
+}
+
+int copy_stats(const KnnWs& w, int64_t* stats_dev, cudaStream_t st) {
+  if (stats_dev)
+    MSC_CUDA_TRY(cudaMemcpyAsync(stats_dev, w.ctl->stats, sizeof(int64_t) * MSC_STATS_LEN,
+                                 cudaMemcpyDeviceToDevice, st));
+  return MSC_OK;
+}
+
+struct GraphWs {
+  float* sigma;
+  float* rho;
+  float* w;
+  double* gsum;
+  double* sig2;
+  void* uws;
+  size_t uws_bytes;
+};
+
+GraphWs carve_graph(Carver& c, int64_t n, int k, int method) {
+  GraphWs g{};
+  if (method == MSC_METHOD_UMAP) {
+    g.sigma = c.take<float>(n);
+    g.rho = c.take<float>(n);
+    g.w = c.take<float>(size_t(n) * k);
+    g.gsum = c.take<double>(1 + 1024);
+  } else {
+    g.sig2 = c.take<double>(n);
+  }
+  g.uws_bytes = union_workspace_bytes(n, k);
+  g.uws = c.take<unsigned char>(g.uws_bytes);
+  return g;
+}
+
+__global__ void set_stat_kernel(Ctl* ctl, int idx, int64_t v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctl->stats[idx] = v;
+}
+int launch_set_stat(Ctl* ctl, int idx, int64_t v, cudaStream_t st) {
+  set_stat_kernel<<<1, 32, 0, st>>>(ctl, idx, v);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+__global__ void store_nnz_kernel(const int64_t* __restrict__ indptr, int64_t n, Ctl* ctl) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctl->stats[MSC_STAT_CONN_NNZ] = indptr[n];
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+bool bad_ptr(const void* p, const char* name) {
+  if (p) return false;
+  set_error("%s is NULL", name);
+  return true;
+}
+
+}  // namespace
+}  // namespace msc
+
+using namespace msc;
+
+extern "C" {
+
+int msc_version(void) { return 10000; }
+const char* msc_last_error(void) { return msc::last_error(); }
+
+long long msc_launch_count(void) { return msc::g_launch_count.load(); }
+
+int msc_profile_enable(int on) {
+  timer().on = on != 0;
+  timer().last = -1;
+  return MSC_OK;
+}
+
+int msc_profile_read(float* ms_out, int max_stages) {
+  StageTimer& t = timer();
+  if (!ms_out || max_stages < 1) { set_error("ms_out/max_stages invalid"); return -MSC_ERR_INVALID_ARG; }
+  int n = 0;
+  for (int s = 1; s <= t.last && n < max_stages; ++s, ++n) {
+    float ms = -1.f;
+    if (t.ev[s] && t.ev[s - 1]) {
+      cudaEventSynchronize(t.ev[s]);
+      if (cudaEventElapsedTime(&ms, t.ev[s - 1], t.ev[s]) != cudaSuccess) ms = -1.f;
+    }
+    ms_out[n] = ms;
+  }
+  return n;
+}
+
+size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, int32_t precision,
+                               int32_t kprime) {
+  Problem P;
+  if (make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1) != MSC_OK) return 0;
+  Carver c(nullptr);
+  carve_knn(c, P);
+  return c.bytes();
+}
+
+int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+            int32_t precision, int32_t kprime, int32_t* knn_idx_dev, float* knn_dist_dev,
+            int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  Problem P;
+  MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
+  if (bad_ptr(X_dev, "X") || bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  Carver c(workspace);
+  KnnWs w = carve_knn(c, P);
+  if (c.bytes() > workspace_bytes) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, c.bytes());
+    return MSC_ERR_WORKSPACE;
+  }
+  cudaStream_t st = as_stream(stream);
+  MSC_TRY(launch_single_segment(w.seg, n, st));
+  MSC_TRY(run_knn(P, w, X_dev, knn_idx_dev, knn_dist_dev, 0, st));
+  return copy_stats(w, stats_dev, st);
+}
+
+size_t msc_neighbors_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric,
+                                     int32_t method, int32_t precision, int32_t kprime) {
+  Problem P;
+  if (make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1) != MSC_OK) return 0;
+  if (method != MSC_METHOD_UMAP && method != MSC_METHOD_GAUSS) return 0;
+  Carver c(nullptr);
+  carve_knn(c, P);
+  carve_graph(c, n, k, method);
+  return c.bytes();
+}
+
+int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+                  int32_t method, int32_t precision, int32_t kprime, int32_t* knn_idx_dev,
+                  float* knn_dist_dev, int64_t* dist_indptr_dev, int32_t* dist_indices_dev,
+                  float* dist_data_dev, int64_t* conn_indptr_dev, int32_t* conn_indices_dev,
+                  float* conn_data_dev, int64_t* stats_dev, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+  Problem P;
+  MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
+  if (method != MSC_METHOD_UMAP && method != MSC_METHOD_GAUSS) {
+    set_error("unknown method %d", method);
+    return MSC_ERR_INVALID_ARG;
+  }
+  if (bad_ptr(X_dev, "X") || bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(dist_indptr_dev, "dist_indptr") || bad_ptr(dist_indices_dev, "dist_indices") ||
+      bad_ptr(dist_data_dev, "dist_data") || bad_ptr(conn_indptr_dev, "conn_indptr") ||
+      bad_ptr(conn_indices_dev, "conn_indices") || bad_ptr(conn_data_dev, "conn_data") ||
+      bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  Carver c(workspace);
+  KnnWs w = carve_knn(c, P);
+  GraphWs g = carve_graph(c, n, k, method);
+  if (c.bytes() > workspace_bytes) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, c.bytes());
+    return MSC_ERR_WORKSPACE;
+  }
+  cudaStream_t st = as_stream(stream);
+  MSC_TRY(launch_single_segment(w.seg, n, st));
+  MSC_TRY(run_knn(P, w, X_dev, knn_idx_dev, knn_dist_dev, 0, st));
+  MSC_TRY(launch_distances_csr(knn_idx_dev, knn_dist_dev, n, k, dist_indptr_dev, dist_indices_dev,
+                               dist_data_dev, st));
+  if (method == MSC_METHOD_UMAP) {
+    MSC_TRY(launch_smooth_knn(knn_dist_dev, n, k, 1.0f, g.sigma, g.rho, g.gsum, st));
+    MSC_TRY(launch_membership(knn_idx_dev, knn_dist_dev, g.sigma, g.rho, n, k, g.w, st));
+    stage_mark(st, 4);
+    MSC_TRY(launch_union(0, knn_idx_dev, g.w, nullptr, n, k, conn_indptr_dev, conn_indices_dev,
+                         conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
+  } else {
+    MSC_TRY(launch_gauss_sigma(knn_dist_dev, n, k, g.sig2, st));
+    stage_mark(st, 4);
+    MSC_TRY(launch_union(1, knn_idx_dev, knn_dist_dev, g.sig2, n, k, conn_indptr_dev,
+                         conn_indices_dev, conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
+  }
+  store_nnz_kernel<<<1, 32, 0, st>>>(conn_indptr_dev, n, w.ctl);
+  MSC_LAUNCH_CHECK();
+  stage_mark(st, 5);
+  return copy_stats(w, stats_dev, st);
+}
+
+size_t msc_batched_workspace_bytes(const int64_t* offsets_host, int32_t n_samples, int32_t d,
+                                   int32_t k, int32_t metric, int32_t precision, int32_t kprime) {
+  if (!offsets_host || n_samples < 1) return 0;
+  Problem P;
+  if (make_problem(P, offsets_host[n_samples], d, k, metric, precision, kprime, offsets_host,
+                   n_samples) != MSC_OK)
+    return 0;
+  Carver c(nullptr);
+  carve_knn(c, P);
+  return c.bytes();
+}
+
+int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t d, int32_t k,
+                        int32_t metric, int32_t precision, int32_t kprime, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+  if (!offsets_host || n_samples < 1) { set_error("offsets/n_samples invalid"); return MSC_ERR_INVALID_ARG; }
+  Problem P;
+  MSC_TRY(make_problem(P, offsets_host[n_samples], d, k, metric, precision, kprime, offsets_host,
+                       n_samples));
+  if (bad_ptr(workspace, "workspace")) return MSC_ERR_INVALID_ARG;
+  Carver c(workspace);
+  KnnWs w = carve_knn(c, P);
+  if (c.bytes() > workspace_bytes) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, c.bytes());
+    return MSC_ERR_WORKSPACE;
+  }
+  // samples packed largest first: the persistent kernels hand out query tiles round-robin, and
+  // starting with the longest tiles balances the work across SMs
+  std::vector<int> order(n_samples);
+  for (int s = 0; s < n_samples; ++s) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return offsets_host[a + 1] - offsets_host[a] > offsets_host[b + 1] - offsets_host[b];
+  });
+  std::vector<SegDesc> segs(n_samples);
+  int64_t poff = 0, tile = 0;
+  for (int r = 0; r < n_samples; ++r) {
+    const int s = order[r];
+    SegDesc sd{};
+    sd.off = offsets_host[s];
+    sd.n = offsets_host[s + 1] - offsets_host[s];
+    sd.poff = poff;
+    sd.padlen = round_up(sd.n, SEG_PAD);
+    sd.tile0 = tile;
+    sd.ntiles = ceil_div(sd.n, QTILE);
+    segs[r] = sd;
+    poff += sd.padlen;
+    tile += sd.ntiles;
+  }
+  cudaStream_t st = as_stream(stream);
+  MSC_CUDA_TRY(cudaMemcpyAsync(w.seg, segs.data(), sizeof(SegDesc) * n_samples,
+                               cudaMemcpyHostToDevice, st));
+  MSC_CUDA_TRY(cudaStreamSynchronize(st));
+  return MSC_OK;
+}
+
+int msc_batched_knn(const float* X_dev, const int64_t* offsets_host, int32_t n_samples, int32_t d,
+                    int32_t k, int32_t metric, int32_t precision, int32_t kprime,
+                    int32_t tile_config, int32_t* knn_idx_dev, float* knn_dist_dev,
+                    int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!offsets_host || n_samples < 1) { set_error("offsets/n_samples invalid"); return MSC_ERR_INVALID_ARG; }
+  Problem P;
+  MSC_TRY(make_problem(P, offsets_host[n_samples], d, k, metric, precision, kprime, offsets_host,
+                       n_samples));
+  if (bad_ptr(X_dev, "X") || bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  Carver c(workspace);
+  KnnWs w = carve_knn(c, P);
+  if (c.bytes() > workspace_bytes) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, c.bytes());
+    return MSC_ERR_WORKSPACE;
+  }
+  cudaStream_t st = as_stream(stream);
+  MSC_TRY(run_knn(P, w, X_dev, knn_idx_dev, knn_dist_dev, tile_config, st));
+  return copy_stats(w, stats_dev, st);
+}
+
+int msc_smooth_knn_dist(const float* knn_dist_dev, int64_t n, int32_t k,
+                        float local_connectivity, float* sigma_dev, float* rho_dev,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || k < 1 || k > MSC_MAX_K) { set_error("bad n/k"); return MSC_ERR_INVALID_ARG; }
+  if (!(local_connectivity >= 0.f)) { set_error("local_connectivity must be >= 0"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_dist_dev, "knn_dist") || bad_ptr(sigma_dev, "sigma") || bad_ptr(rho_dev, "rho") ||
+      bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (workspace_bytes < sizeof(double) * 1025) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, sizeof(double) * 1025);
+    return MSC_ERR_WORKSPACE;
+  }
+  return launch_smooth_knn(knn_dist_dev, n, k, local_connectivity, sigma_dev, rho_dev,
+                           static_cast<double*>(workspace), as_stream(stream));
+}
+
+int msc_membership(const int32_t* knn_idx_dev, const float* knn_dist_dev, const float* sigma_dev,
+                   const float* rho_dev, int64_t n, int32_t k, float* w_dev, void* stream) {
+  if (n < 1 || k < 1 || k > MSC_MAX_K) { set_error("bad n/k"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(sigma_dev, "sigma") || bad_ptr(rho_dev, "rho") || bad_ptr(w_dev, "w"))
+    return MSC_ERR_INVALID_ARG;
+  return launch_membership(knn_idx_dev, knn_dist_dev, sigma_dev, rho_dev, n, k, w_dev,
+                           as_stream(stream));
+}
+
+size_t msc_fuzzy_union_workspace_bytes(int64_t n, int32_t k) {
+  if (n < 1 || k < 1) return 0;
+  return union_workspace_bytes(n, k);
+}
+
+int msc_fuzzy_union(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, int32_t k,
+                    int64_t* indptr_dev, int32_t* indices_dev, float* data_dev, int64_t* nnz_dev,
+                    void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || k < 1 || k > MSC_MAX_K) { set_error("bad n/k"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(w_dev, "w") || bad_ptr(indptr_dev, "indptr") ||
+      bad_ptr(indices_dev, "indices") || bad_ptr(data_dev, "data") || bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  return launch_union(0, knn_idx_dev, w_dev, nullptr, n, k, indptr_dev, indices_dev, data_dev,
+                      nnz_dev, workspace, workspace_bytes, as_stream(stream));
+}
+
+size_t msc_gauss_workspace_bytes(int64_t n, int32_t k) {
+  if (n < 1 || k < 1) return 0;
+  Carver c(nullptr);
+  c.take<double>(n);
+  c.take<unsigned char>(union_workspace_bytes(n, k));
+  return c.bytes();
+}
+
+int msc_gauss_connectivities(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                             int32_t k, int64_t* indptr_dev, int32_t* indices_dev,
+                             float* data_dev, int64_t* nnz_dev, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  if (n < 1 || k < 1 || k > MSC_MAX_K) { set_error("bad n/k"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(indptr_dev, "indptr") || bad_ptr(indices_dev, "indices") ||
+      bad_ptr(data_dev, "data") || bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (workspace_bytes < msc_gauss_workspace_bytes(n, k)) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, msc_gauss_workspace_bytes(n, k));
+    return MSC_ERR_WORKSPACE;
+  }
+  Carver c(workspace);
+  double* sig2 = c.take<double>(n);
+  const size_t ub = union_workspace_bytes(n, k);
+  void* uws = c.take<unsigned char>(ub);
+  cudaStream_t st = as_stream(stream);
+  MSC_TRY(launch_gauss_sigma(knn_dist_dev, n, k, sig2, st));
+  return launch_union(1, knn_idx_dev, knn_dist_dev, sig2, n, k, indptr_dev, indices_dev, data_dev,
+                      nnz_dev, uws, ub, st);
+}
+
+int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                      int32_t k, int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
+                      void* stream) {
+  if (n < 1 || k < 1 || k > MSC_MAX_K) { set_error("bad n/k"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(indptr_dev, "indptr") || bad_ptr(indices_dev, "indices") || bad_ptr(data_dev, "data"))
+    return MSC_ERR_INVALID_ARG;
+  return launch_distances_csr(knn_idx_dev, knn_dist_dev, n, k, indptr_dev, indices_dev, data_dev,
+                              as_stream(stream));
+}
+
+}  // extern "C"

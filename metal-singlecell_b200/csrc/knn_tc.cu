@@ -1,0 +1,510 @@
+// Fused pairwise-distance + per-row top-k' on the Blackwell tensor cores (sm_100a).
+//
+// Reference counterpart: metalsinglecell neighbors.py:114-119 — an fp16 Gram tile
+// `sq_i + sq_j − 2·X_i·X_jᵀ` materialised as a block×n matrix in device memory, then the
+// `topk_rows` register kernel (neighbors.py:25-79) scanning it.  Here the n×n matrix never leaves
+// the SM: a 128-row query tile stays in shared memory, key tiles stream through a TMA pipeline,
+// one thread issues tcgen05.mma into a double-buffered FP32 accumulator in tensor memory, and four
+// epilogue warps read the accumulator (TMEM lane i = query row i) straight into the per-row
+// selector while the next tile's MMAs run.  The key norms are folded into the key operand, so the
+// accumulator already holds the ranking value v = |y|² − 2x·y.
+//
+// Roles (256 threads, one CTA per SM, persistent over 128-row query tiles):
+//   warp 0  TMA producer      A tile once per query tile, then the key tiles of its sample
+//   warp 1  MMA issuer        KSTEPS × tcgen05.mma (M=128, N=BN, K=16) per key tile
+//   warp 2  TMEM allocator    2·BN columns for two accumulators
+//   warps 4-7 epilogue        tcgen05.ld 32x32b → filter → selector; release the accumulator
+// Every mbarrier wait is bounded (wall-clock, via %globaltimer); a wait that gives up raises an
+// abort flag that every role polls, the kernel records MSC_STAT_TIMEOUT and all roles leave their
+// loops, so a fault in the pipeline returns an error instead of hanging the GPU.
+#include <cuda.h>
+
+#include "kernels.cuh"
+#include "msc_select.cuh"
+
+namespace msc {
+
+namespace {
+
+constexpr int TC_THREADS = 256;
+constexpr int EPI_WARP0 = 4;
+constexpr int BM = 128;
+constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
+constexpr size_t SMEM_LIMIT = 232448;               // 227 KB opt-in per block
+
+// ------------------------------------------------------------------------------------------------
+// PTX wrappers
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of `parity` to complete.  false = gave up (abort raised).
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if ((it & 255) == 0 && globaltimer() - t0 > WAIT_LIMIT_NS) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+// Teardown wait for work this thread itself started (copies, MMAs): ignores the abort flag
+// because such work completes on its own, but is still bounded in time.
+__device__ __noinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 255) == 255 && globaltimer() - t0 > WAIT_LIMIT_NS) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst)),
+               "r"(ncols));
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= uint64_t((saddr & 0x3FFFFu) >> 4);       // start address
+  d |= uint64_t(1) << 16;                        // leading byte offset (unused for SW128 K-major)
+  d |= uint64_t(1024 >> 4) << 32;                // stride byte offset
+  d |= uint64_t(1) << 46;                        // descriptor version (sm_100)
+  d |= uint64_t(2) << 61;                        // SWIZZLE_128B
+  return d;
+}
+// Instruction descriptor, kind::f16: F32 accumulate, A/B f16 or bf16, both K-major, M×N.
+__host__ __device__ constexpr uint32_t idesc_f16(bool bf16, int m, int n) {
+  return (1u << 4) | ((bf16 ? 1u : 0u) << 7) | ((bf16 ? 1u : 0u) << 10) |
+         (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+struct TcParams {
+  int kb;           // 64-element K atoms per row
+  int ksteps;       // K=16 MMA steps per tile
+  int bn;           // key tile rows
+  int stages;       // key tile pipeline depth
+  int na;           // query tile buffers
+  int kprime;
+  int cand_stride;
+  int bf16;
+  int n_items;
+  uint32_t idesc;
+};
+
+struct SmemPlan {
+  size_t a_off, b_off, sel_off, bar_off, total;
+};
+template <int KPL, int CB>
+__host__ __device__ inline SmemPlan smem_plan(int kb, int bn, int stages, int na) {
+  SmemPlan p;
+  p.a_off = 0;
+  p.b_off = p.a_off + size_t(na) * kb * BM * 128;
+  p.sel_off = p.b_off + size_t(stages) * kb * bn * 128;
+  p.bar_off = p.sel_off + RowSelect<KPL, CB, BM>::smem_bytes();
+  p.total = p.bar_off + 256 + 1024;          // barriers + slack for 1024-byte alignment
+  return p;
+}
+
+template <int KPL, int CB>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              const TcParams P, const WorkItem* __restrict__ items, Ctl* __restrict__ ctl,
+              int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
+  extern __shared__ unsigned char smem_dyn[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
+  const SmemPlan sp = smem_plan<KPL, CB>(P.kb, P.bn, P.stages, P.na);
+  unsigned char* Asm = smem + sp.a_off;
+  unsigned char* Bsm = smem + sp.b_off;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + sp.bar_off);
+  uint64_t* a_full = bars;                 // [2]
+  uint64_t* a_empty = bars + 2;            // [2]
+  uint64_t* acc_full = bars + 4;           // [2]
+  uint64_t* acc_empty = bars + 6;          // [2]
+  uint64_t* done_bar = bars + 8;           // [1]
+  uint64_t* b_full = bars + 9;             // [stages <= 6]
+  uint64_t* b_empty = bars + 15;           // [stages <= 6]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 22);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 23);
+
+  const int warp = warp_id(), lane = lane_id();
+  const size_t a_bytes = size_t(P.kb) * BM * 128;
+  const size_t b_bytes = size_t(P.kb) * P.bn * 128;
+  const uint32_t tmem_cols = uint32_t(2 * P.bn);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&a_full[i], 1);
+      mbar_init(&a_empty[i], 1);
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 4);
+    }
+    mbar_init(done_bar, 1);
+    for (int s = 0; s < P.stages; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    tmem_alloc(tmem_slot, tmem_cols);
+    tmem_relinquish();
+  }
+  if (warp == 0 && lane == 0) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int stage = 0, abuf = 0;
+      uint32_t sphase = 0, aphase = 0;
+      bool ok = true;
+      for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+        const WorkItem w = items[it];
+        ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
+        if (!ok) break;
+        mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
+        for (int kb = 0; kb < P.kb; ++kb)
+          tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
+                      w.qrow0);
+        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
+        for (int kt = 0; kt < nkt; ++kt) {
+          ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+          if (!ok) break;
+          mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
+          for (int kb = 0; kb < P.kb; ++kb)
+            tma_load_2d(Bsm + stage * b_bytes + size_t(kb) * P.bn * 128, &tmB, &b_full[stage],
+                        kb * 64, w.key0 + kt * P.bn);
+          if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+        }
+      }
+      // drain: every load this thread armed completes on its own; wait for them (bounded)
+      for (int s = 0; s < P.stages; ++s) {
+        // stages armed in the current lap have parity sphase for indices < stage
+        const uint32_t par = s < stage ? sphase : (sphase ^ 1);
+        (void)mbar_drain(&b_full[s], par);
+      }
+      for (int a = 0; a < P.na; ++a) {
+        const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
+        (void)mbar_drain(&a_full[a], par);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      int stage = 0, abuf = 0, acc = 0;
+      uint32_t sphase = 0, aphase = 0, accphase = 0;
+      bool ok = true, issued = false;
+      for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+        const WorkItem w = items[it];
+        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+        if (!ok) break;
+        const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
+        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
+        for (int kt = 0; kt < nkt; ++kt) {
+          ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+          if (!ok) break;
+          ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
+          const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
+          for (int ks = 0; ks < P.ksteps; ++ks) {
+            const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
+            const uint32_t bo = uint32_t((ks >> 2) * P.bn * 128 + (ks & 3) * 32);
+            umma_f16(d_tmem, sdesc(a_base + ao), sdesc(b_base + bo), P.idesc, ks > 0 ? 1u : 0u);
+          }
+          issued = true;
+          umma_commit(&b_empty[stage]);
+          umma_commit(&acc_full[acc]);
+          if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+          if (++acc == 2) { acc = 0; accphase ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(&a_empty[abuf]);
+        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+      }
+      if (issued) umma_commit(done_bar);
+      else mbar_arrive(done_bar);
+    }
+  } else if (warp >= EPI_WARP0) {
+    // ------------------------------------------------------------------ epilogue
+    const int q = warp - EPI_WARP0;               // TMEM lane quarter
+    const int row = q * 32 + lane;
+    RowSelect<KPL, CB, BM> sel;
+    sel.bind(smem + sp.sel_off, row, P.kprime);
+    int acc = 0;
+    uint32_t accphase = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+      const WorkItem w = items[it];
+      sel.reset();
+      __syncwarp();
+      const int self = w.qorig0 + row;
+      const int limit = w.orig_off + w.nkeys;
+      const int nkt = (w.nkeys + P.bn - 1) / P.bn;
+      for (int kt = 0; kt < nkt; ++kt) {
+        ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t t0 = tmem_base + uint32_t(acc * P.bn) + (uint32_t(q * 32) << 16);
+        const int col_base = w.orig_off + kt * P.bn;
+        const int nch = P.bn / 32;
+        for (int c = 0; c < nch; ++c) {
+          float v[32];
+          tmem_ld32(t0 + uint32_t(c * 32), v);
+          if (c == nch - 1) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+          }
+          sel.push32(v, col_base + c * 32, self, limit);
+        }
+        if (++acc == 2) { acc = 0; accphase ^= 1; }
+      }
+      if (!ok) break;
+      const int wrow0 = q * 32;
+      const int nvalid = min(32, w.nq - wrow0);
+      if (nvalid > 0)
+        sel.finish(cand_idx, cand_thr, P.cand_stride, int64_t(w.qorig0) + wrow0, nvalid,
+                   P.kprime);
+      else
+        sel.compact();
+    }
+  }
+
+  __syncthreads();
+  if (warp == 2) {
+    // the MMA warp's last commit marks the end of every tensor-core write to TMEM
+    (void)mbar_drain(done_bar, 0);
+    tc_fence_after();
+    tmem_dealloc(tmem_base, tmem_cols);
+  }
+  if (threadIdx.x == 0 && *abort_flag) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_TIMEOUT]), 1ull);
+    atomicExch(&ctl->timeout_flag, 1);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+int make_map(CUtensorMap* m, const void* base, int64_t rows, int kp, int box_rows, bool bf16) {
+  EncodeTiledFn enc = get_encode();
+  if (!enc) { set_error("cuTensorMapEncodeTiled unavailable"); return MSC_ERR_CUDA; }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) {
+    set_error("operand base not 16-byte aligned");
+    return MSC_ERR_INVALID_ARG;
+  }
+  cuuint64_t dims[2] = {cuuint64_t(kp), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(kp) * 2};
+  cuuint32_t box[2] = {64u, cuuint32_t(box_rows)};
+  cuuint32_t estr[2] = {1u, 1u};
+  CUresult r = enc(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                   const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", int(r));
+    return MSC_ERR_CUDA;
+  }
+  return MSC_OK;
+}
+
+template <int KPL, int CB>
+size_t smem_total(const TcConfig& c, int kb, int na) {
+  return smem_plan<KPL, CB>(kb, c.bn, c.stages, na).total;
+}
+
+size_t config_smem(const TcConfig& c, int kb, int na) {
+  if (c.kpl == 32 && c.cb == 16) return smem_total<32, 16>(c, kb, na);
+  if (c.kpl == 32 && c.cb == 32) return smem_total<32, 32>(c, kb, na);
+  if (c.kpl == 64 && c.cb == 16) return smem_total<64, 16>(c, kb, na);
+  if (c.kpl == 64 && c.cb == 32) return smem_total<64, 32>(c, kb, na);
+  return SIZE_MAX;
+}
+
+int pick_na(const TcConfig& c, int kb) {
+  return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1;
+}
+
+template <int KPL, int CB>
+int launch_tc_t(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
+                const CUtensorMap& mb, const WorkItem* items, Ctl* ctl, int32_t* cand_idx,
+                float* cand_thr, cudaStream_t st) {
+  const size_t smem = smem_plan<KPL, CB>(P.kb, P.bn, P.stages, P.na).total;
+  auto kern = knn_tc_kernel<KPL, CB>;
+  MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int grid = std::max(1, std::min(P.n_items, num_sms()));
+  kern<<<grid, TC_THREADS, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
+  MSC_LAUNCH_CHECK();
+  (void)cfg;
+  return MSC_OK;
+}
+
+}  // namespace
+
+bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
+  if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;
+  if (c.stages < 2 || c.stages > 6) return false;
+  if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 64)) return false;
+  if (c.cb != 16 && c.cb != 32) return false;
+  const int kb = kp / 64;
+  return config_smem(c, kb, 1) <= SMEM_LIMIT;
+}
+
+TcConfig tc_default_config(int prec, int d, int kprime) {
+  const OpLayout L = op_layout(prec, d);
+  const int kpl = kprime <= 32 ? 32 : 64;
+  // widest key tile, deepest pipeline and largest buffer that fit
+  const int bns[4] = {256, 128, 64, 32};
+  for (int bn : bns)
+    for (int stages = 4; stages >= 2; --stages)
+      for (int cb : {32, 16}) {
+        TcConfig c{bn, stages, kpl, cb};
+        if (tc_config_ok(c, L.kp, kprime)) return c;
+      }
+  return TcConfig{64, 2, kpl, 16};
+}
+
+int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
+                  int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
+                  int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
+                  int cand_stride, cudaStream_t st) {
+  if (!tc_config_ok(cfg, kp, kprime)) {
+    set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d) does not fit", cfg.bn,
+              cfg.stages, cfg.kpl, cfg.cb);
+    return MSC_ERR_INVALID_ARG;
+  }
+  const bool bf16 = prec != PREC_FP16;
+  CUtensorMap ma, mb;
+  MSC_TRY(make_map(&ma, Aop, a_rows, kp, BM, bf16));
+  MSC_TRY(make_map(&mb, Bop, b_rows, kp, cfg.bn, bf16));
+  TcParams P;
+  P.kb = kp / 64;
+  P.ksteps = kmma / 16;
+  P.bn = cfg.bn;
+  P.stages = cfg.stages;
+  P.na = pick_na(cfg, P.kb);
+  P.kprime = kprime;
+  P.cand_stride = cand_stride;
+  P.bf16 = bf16;
+  P.n_items = int(n_items);
+  P.idesc = idesc_f16(bf16, BM, cfg.bn);
+  if (cfg.kpl == 32 && cfg.cb == 16)
+    return launch_tc_t<32, 16>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 32 && cfg.cb == 32)
+    return launch_tc_t<32, 32>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 64 && cfg.cb == 16)
+    return launch_tc_t<64, 16>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  return launch_tc_t<64, 32>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+}
+
+}  // namespace msc

@@ -1,0 +1,339 @@
+// Exact re-rank of the candidates and the certificate that they contain the true neighbours.
+//
+// Reference counterpart: the fp32 direct-difference recompute of the selected neighbours
+// (metalsinglecell neighbors.py:120-123) and the host sort by distance with self first
+// (neighbors.py:129-131; ties by index as in neighbors.py:457-461).  The reference ranks on fp16
+// and accepts ~0.99 recall; here every row is either proven exact or re-scanned exactly:
+//
+//   1. FP32 direct differences Σ(x_t − y_t)² for all k' candidates (one lane per candidate);
+//   2. warp bitonic sort by FP32 distance; the (k−1)-th value B bounds the answer;
+//   3. candidates within B·(1+3δ) (δ = (d+4)·2⁻²⁴, the FP32 sum's relative error bound) are
+//      recomputed in FP64 and ordered by (FP64 distance, index) — FP64 only breaks ties at the
+//      k-th boundary, and gives the returned distances float32(sqrt(d²₆₄));
+//   4. certificate: every key outside the candidate list has approximate value v̂ ≥ T (the
+//      k'-th smallest kept), so its true squared distance is ≥ (|z_x|² + T − ε)/f² where ε
+//      bounds |v̂ − v| from the operand residual norms recorded by the packing kernel.  If the
+//      (k−1)-th FP64 distance is strictly below that, the row is exact; otherwise the row goes
+//      to the FP64 full scan below.
+#include "kernels.cuh"
+#include "msc_select.cuh"
+
+namespace msc {
+
+namespace {
+
+constexpr int RR_WARPS = 8;
+
+struct DKey {
+  double v;
+  int i;
+};
+__device__ __forceinline__ bool dless(double av, int ai, double bv, int bi) {
+  return av < bv || (av == bv && ai < bi);
+}
+__device__ __forceinline__ void cmpx_d(double& v, int& i, int j, bool keep_min) {
+  double ov = __shfl_xor_sync(FULL, v, j);
+  int oi = __shfl_xor_sync(FULL, i, j);
+  bool take = keep_min ? dless(ov, oi, v, i) : dless(v, i, ov, oi);
+  if (take) { v = ov; i = oi; }
+}
+__device__ __forceinline__ void warp_sort32_d(double& v, int& i) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) cmpx_d(v, i, j, ((lane & j) == 0) == ((lane & k) == 0));
+}
+__device__ __forceinline__ void warp_merge32_d(double& v, int& i) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) cmpx_d(v, i, j, (lane & j) == 0);
+}
+// lo/hi := elementwise min/max of a and reversed b (both ascending), lexicographic
+__device__ __forceinline__ void min_rev_d(double av, int ai, double bv, int bi, double& lv, int& li,
+                                          double& hv, int& hi) {
+  const int lane = lane_id();
+  double rv = __shfl_sync(FULL, bv, 31 - lane);
+  int ri = __shfl_sync(FULL, bi, 31 - lane);
+  if (dless(rv, ri, av, ai)) { lv = rv; li = ri; hv = av; hi = ai; }
+  else { lv = av; li = ai; hv = rv; hi = ri; }
+}
+// sort 64 pairs held as (v0,i0) lane-slot 0 and (v1,i1) lane-slot 1
+__device__ __forceinline__ void warp_sort64_d(double& v0, int& i0, double& v1, int& i1) {
+  warp_sort32_d(v0, i0);
+  warp_sort32_d(v1, i1);
+  double lv, hv; int li, hi;
+  min_rev_d(v0, i0, v1, i1, lv, li, hv, hi);
+  warp_merge32_d(lv, li);
+  warp_merge32_d(hv, hi);
+  v0 = lv; i0 = li; v1 = hv; i1 = hi;
+}
+
+__device__ __forceinline__ double d2_f64(const float* xs, const float* __restrict__ y, int d) {
+  double acc = 0.0;
+  for (int t = 0; t < d; ++t) {
+    double df = double(xs[t]) - double(y[t]);
+    acc += df * df;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ float d2_f32(const float* xs, const float* __restrict__ y, int d) {
+  float acc = 0.f;
+  for (int t = 0; t < d; ++t) {
+    float df = xs[t] - y[t];
+    acc = fmaf(df, df, acc);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ float out_dist(double d2, int cosine) {
+  return cosine ? __double2float_rn(d2 * 0.5) : __double2float_rn(sqrt(d2));
+}
+
+__global__ void __launch_bounds__(RR_WARPS * 32)
+rerank_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ seg, int nseg,
+              int64_t npacked, const int32_t* __restrict__ cand_idx,
+              const float* __restrict__ cand_thr, int cand_stride, int kprime,
+              const QStat* __restrict__ qs, const KeyMax* __restrict__ km, Ctl* __restrict__ ctl,
+              int prec, int kmma, int k, int cosine, int32_t* __restrict__ knn_idx,
+              float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows) {
+  __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
+  const int lane = lane_id(), wib = warp_id();
+  float* xs = xs_all[wib];
+  const int kk = k - 1;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  // key-side maxima and the scale
+  const double Kh = __uint_as_float(km->hi), Kl = __uint_as_float(km->lo);
+  const double Kr = __uint_as_float(km->res), Kn = __uint_as_float(km->nerr);
+  const double Ks = __uint_as_float(km->sq);
+  double f = 1.0;
+  if (prec == PREC_FP16) {
+    float mx = __uint_as_float(ctl->max_sq_bits);
+    if (mx > 0.f) {
+      int e = int(floor(0.5 * log2(16384.0 / double(mx))));
+      e = max(-60, min(60, e));
+      f = ldexp(1.0, e);
+    }
+  }
+  const double f2 = f * f;
+  const double delta = double(d + 4) * 0x1p-24;
+  int64_t n_cert = 0, n_ties = 0;
+  for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
+       p += nwarps) {
+    const int s = find_seg(seg, nseg, p);
+    const int64_t j = p - seg[s].poff;
+    if (j >= seg[s].n) continue;                        // warp-uniform
+    const int64_t i = seg[s].off + j;                   // original row
+    const int64_t ns = seg[s].n;
+    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
+    __syncwarp();
+    if (kk == 0) {
+      if (lane == 0) { knn_idx[i * k] = int32_t(i); knn_dist[i * k] = 0.f; ++n_cert; }
+      continue;
+    }
+    // 1. FP32 distances of the candidates (lane: slots lane and lane+32)
+    int c0 = lane < kprime ? cand_idx[i * cand_stride + lane] : -1;
+    int c1 = lane + 32 < kprime ? cand_idx[i * cand_stride + lane + 32] : -1;
+    float e0 = c0 >= 0 ? d2_f32(xs, X + int64_t(c0) * d, d) : __int_as_float(0x7f800000);
+    float e1 = c1 >= 0 ? d2_f32(xs, X + int64_t(c1) * d, d) : __int_as_float(0x7f800000);
+    // 2. sort by (FP32 distance, index)
+    {
+      double v0 = e0, v1 = e1;
+      int i0 = c0 >= 0 ? c0 : INT32_MAX, i1 = c1 >= 0 ? c1 : INT32_MAX;
+      warp_sort64_d(v0, i0, v1, i1);
+      e0 = float(v0); e1 = float(v1); c0 = i0; c1 = i1;
+    }
+    const float B = __shfl_sync(FULL, kk - 1 < 32 ? e0 : e1, (kk - 1) & 31);
+    // 3. FP64 for the window
+    const double lim = double(B) * (1.0 + 3.0 * delta) + 1e-300;
+    const bool w0 = c0 != INT32_MAX && double(e0) <= lim;
+    const bool w1 = c1 != INT32_MAX && double(e1) <= lim;
+    double g0 = w0 ? d2_f64(xs, X + int64_t(c0) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
+    double g1 = w1 ? d2_f64(xs, X + int64_t(c1) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
+    const int m = __popc(__ballot_sync(FULL, w0)) + __popc(__ballot_sync(FULL, w1));
+    int h0 = c0, h1 = c1;
+    warp_sort64_d(g0, h0, g1, h1);
+    const double Dk = __shfl_sync(FULL, kk - 1 < 32 ? g0 : g1, (kk - 1) & 31);
+    // 4. certificate
+    bool cert;
+    const int nvalid = int(min64(ns - 1, kprime));
+    if (ns - 1 <= kprime) {
+      cert = true;                                      // every key is a candidate
+    } else {
+      const QStat q = qs[p];
+      const double qh = q.hi, ql = q.lo, qr = q.res;
+      const double dot_err = ql * Kl + (qh + ql) * Kr + qr * (Kh + Kl) + qr * Kr;
+      double acc_err;
+      if (prec == PREC_FP32)
+        acc_err = 0x1p-23 * ((2.0 * d + 4.0) * qh * Kh + 2.0 * Ks);
+      else
+        acc_err = double(kmma) * 0x1p-22 * (2.0 * (qh + ql) * (Kh + Kl) + Ks);
+      const double eps = 2.0 * dot_err + Kn + acc_err + 0x1p-40 * (q.sq + Ks);
+      const double T = double(cand_thr[i]);
+      cert = f2 * Dk < q.sq + T - eps;
+    }
+    (void)nvalid;
+    // outputs
+    if (lane == 0) {
+      knn_idx[i * k] = int32_t(i);
+      knn_dist[i * k] = 0.f;
+    }
+    // a slot without a valid candidate (only possible with non-finite input) is filled with the
+    // row itself so that every index stays in range for the graph stages
+    if (lane < kk) {
+      knn_idx[i * k + 1 + lane] = h0 == INT32_MAX ? int32_t(i) : h0;
+      knn_dist[i * k + 1 + lane] = out_dist(g0, cosine);
+    }
+    if (lane + 32 < kk) {
+      knn_idx[i * k + 33 + lane] = h1 == INT32_MAX ? int32_t(i) : h1;
+      knn_dist[i * k + 33 + lane] = out_dist(g1, cosine);
+    }
+    if (lane == 0) {
+      n_ties += m - kk;
+      if (cert) ++n_cert;
+      else {
+        int slot = atomicAdd(&ctl->n_fail, 1);
+        fail_rows[slot] = int32_t(p);                   // packed row
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (n_cert) atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_CERTIFIED]),
+                          (unsigned long long)n_cert);
+    if (n_ties) atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_FP64_TIES]),
+                          (unsigned long long)n_ties);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP64 full scan of one row per warp: all keys of the row's sample, ordered by (d², index), with
+// a warp-distributed sorted list of 128 (four slots per lane) merged 32 keys at a time.
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(RR_WARPS * 32)
+fp64_scan_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ seg, int nseg,
+                 const int32_t* __restrict__ fail_rows, Ctl* __restrict__ ctl, int k, int cosine,
+                 int32_t* __restrict__ knn_idx, float* __restrict__ knn_dist) {
+  __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
+  const int lane = lane_id(), wib = warp_id();
+  float* xs = xs_all[wib];
+  const int kk = k - 1;
+  const int nfail = ctl->n_fail;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const double INF = __longlong_as_double(0x7ff0000000000000ll);
+  int64_t done = 0;
+  for (int64_t w = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; w < nfail; w += nwarps) {
+    const int64_t p = fail_rows[w];                      // packed row
+    const int sg = find_seg(seg, nseg, p);
+    const int64_t off = seg[sg].off, ns = seg[sg].n;
+    const int64_t i = off + (p - seg[sg].poff);          // original row
+    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
+    __syncwarp();
+    double a[4];
+    int ai[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) { a[s] = INF; ai[s] = INT32_MAX; }
+    double thr = INF;
+    int thri = INT32_MAX;
+    for (int64_t base = 0; base < ns; base += 32) {
+      const int64_t jj = base + lane;
+      double v = INF;
+      int vi = INT32_MAX;
+      if (jj < ns && off + jj != i) {
+        v = d2_f64(xs, X + (off + jj) * d, d);
+        vi = int(off + jj);
+      }
+      if (!__any_sync(FULL, dless(v, vi, thr, thri))) continue;
+      warp_sort32_d(v, vi);
+      double z, u; int zi, ui;
+      min_rev_d(a[3], ai[3], v, vi, z, zi, u, ui);
+      warp_merge32_d(z, zi);
+      // cascade: (a2, z) -> (w2, slot3), (a1, w2) -> (w1, slot2), (a0, w1) -> (slot0, slot1)
+      double lw, hw; int lwi, hwi;
+      min_rev_d(a[2], ai[2], z, zi, lw, lwi, hw, hwi);
+      warp_merge32_d(lw, lwi); warp_merge32_d(hw, hwi);
+      a[3] = hw; ai[3] = hwi;
+      double lw1, hw1; int lwi1, hwi1;
+      min_rev_d(a[1], ai[1], lw, lwi, lw1, lwi1, hw1, hwi1);
+      warp_merge32_d(lw1, lwi1); warp_merge32_d(hw1, hwi1);
+      a[2] = hw1; ai[2] = hwi1;
+      double lw0, hw0; int lwi0, hwi0;
+      min_rev_d(a[0], ai[0], lw1, lwi1, lw0, lwi0, hw0, hwi0);
+      warp_merge32_d(lw0, lwi0); warp_merge32_d(hw0, hwi0);
+      a[0] = lw0; ai[0] = lwi0; a[1] = hw0; ai[1] = hwi0;
+      const int slot = (kk - 1) >> 5, src = (kk - 1) & 31;
+      double tv = slot == 0 ? a[0] : slot == 1 ? a[1] : slot == 2 ? a[2] : a[3];
+      int ti = slot == 0 ? ai[0] : slot == 1 ? ai[1] : slot == 2 ? ai[2] : ai[3];
+      thr = __shfl_sync(FULL, tv, src);
+      thri = __shfl_sync(FULL, ti, src);
+    }
+    if (lane == 0) { knn_idx[i * k] = int32_t(i); knn_dist[i * k] = 0.f; }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int r = s * 32 + lane;
+      if (r < kk) {
+        knn_idx[i * k + 1 + r] = ai[s] == INT32_MAX ? int32_t(i) : ai[s];
+        knn_dist[i * k + 1 + r] = out_dist(a[s], cosine);
+      }
+    }
+    ++done;
+    __syncwarp();
+  }
+  if (lane == 0 && done)
+    atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_RESCANNED]),
+              (unsigned long long)done);
+}
+
+// every valid packed row goes to the FP64 scan (n_neighbors beyond the candidate kernels)
+__global__ void all_rows_fail_kernel(const SegDesc* __restrict__ seg, int nseg, int64_t npacked,
+                                     int32_t* __restrict__ fail_rows, Ctl* __restrict__ ctl) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    const int s = find_seg(seg, nseg, p);
+    if (p - seg[s].poff < seg[s].n) fail_rows[atomicAdd(&ctl->n_fail, 1)] = int32_t(p);
+  }
+}
+
+}  // namespace
+
+int launch_all_rows_fail(const SegDesc* seg, int nseg, int64_t npacked, int32_t* fail_rows,
+                         Ctl* ctl, cudaStream_t st) {
+  int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
+  all_rows_fail_kernel<<<std::max(blocks, 1), 256, 0, st>>>(seg, nseg, npacked, fail_rows, ctl);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_rerank(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
+                  const int32_t* cand_idx, const float* cand_thr, int cand_stride, int kprime,
+                  const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
+                  int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
+                  cudaStream_t st) {
+  if (kprime > 64 || k - 1 > 64) {
+    set_error("rerank: kprime=%d / k=%d beyond 64", kprime, k);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  int blocks = int(std::min<int64_t>(ceil_div(npacked, RR_WARPS), int64_t(num_sms()) * 8));
+  rerank_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
+      X, d, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
+      kmma, k, cosine, knn_idx, knn_dist, fail_rows);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_fp64_scan(const float* X, int d, const SegDesc* seg, int nseg,
+                     const int32_t* fail_rows, int64_t max_rows, int k, int cosine,
+                     int32_t* knn_idx, float* knn_dist, Ctl* ctl, cudaStream_t st) {
+  if (k - 1 > 128) {
+    set_error("fp64 scan: k=%d beyond 129", k);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  int blocks = int(std::min<int64_t>(ceil_div(max_rows, RR_WARPS), int64_t(num_sms()) * 8));
+  fp64_scan_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
+      X, d, seg, nseg, fail_rows, ctl, k, cosine, knn_idx, knn_dist);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+}  // namespace msc

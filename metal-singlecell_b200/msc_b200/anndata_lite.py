@@ -1,0 +1,38 @@
+"""A minimal AnnData stand-in: the slots ``pp.neighbors`` reads and writes.
+
+``pp.neighbors`` works on any object exposing ``X``, ``n_obs``, ``n_vars``, ``obsm``, ``obsp``,
+``uns`` and ``copy()`` — a real ``anndata.AnnData`` included.  This class provides exactly that
+for environments without anndata.
+"""
+
+from __future__ import annotations
+
+import copy as _copy
+
+
+class AnnDataLite:
+    def __init__(self, X=None, *, obsm=None, obsp=None, uns=None, n_obs=None, n_vars=None):
+        self.X = X
+        self.obsm = dict(obsm or {})
+        self.obsp = dict(obsp or {})
+        self.uns = dict(uns or {})
+        if n_obs is None:
+            if X is not None:
+                n_obs = X.shape[0]
+            elif self.obsm:
+                n_obs = next(iter(self.obsm.values())).shape[0]
+            else:
+                n_obs = 0
+        self.n_obs = int(n_obs)
+        self.n_vars = int(n_vars if n_vars is not None else (X.shape[1] if X is not None else 0))
+
+    @property
+    def shape(self):
+        return (self.n_obs, self.n_vars)
+
+    def copy(self):
+        return _copy.deepcopy(self)
+
+    def __repr__(self):
+        return (f"AnnDataLite(n_obs={self.n_obs}, n_vars={self.n_vars}, obsm={list(self.obsm)}, "
+                f"obsp={list(self.obsp)}, uns={list(self.uns)})")

@@ -1,0 +1,85 @@
+"""The C-ABI library loads and exports every entry point ``include/msc_b200.h`` declares; host-side
+argument checks answer with the documented status codes.  No compute calls: runs without a GPU."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from msc_b200 import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "msc_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(msc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in msc_b200.h but not exported"
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_version_and_constants():
+    lib = _lib.load()
+    assert lib.msc_version() >= 10000
+    text = HEADER.read_text()
+    for name, val in [("MSC_STATS_LEN", _lib.STATS_LEN), ("MSC_MAX_K", _lib.MAX_K),
+                      ("MSC_MAX_D", _lib.MAX_D), ("MSC_STAT_CONN_NNZ", _lib.STAT_CONN_NNZ)]:
+        assert re.search(rf"#define {name}\s+{val}\b", text), name
+
+
+@pytest.mark.parametrize("n,d,k,metric,prec,kprime,code", [
+    (10, 5, 11, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),      # k > n
+    (10, 0, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # d = 0
+    (10, 129, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),     # d > MSC_MAX_D
+    (10, 5, 0, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # k = 0
+    (10, 5, 3, 7, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # metric
+    (10, 5, 3, 0, 9, 0, _lib.MSC_ERR_INVALID_ARG),       # precision
+    (100, 5, 30, 0, 1, 20, _lib.MSC_ERR_INVALID_ARG),    # kprime < k-1
+    (100, 5, 3, 0, 1, 65, _lib.MSC_ERR_INVALID_ARG),     # kprime > 64
+    (10, 5, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # NULL pointers
+])
+def test_argument_checks(n, d, k, metric, prec, kprime, code):
+    lib = _lib.load()
+    rc = lib.msc_knn(None, n, d, k, metric, prec, kprime, None, None, None, None, 0, None)
+    assert rc == code
+    assert _lib.last_error()
+    with pytest.raises((ValueError, NotImplementedError)):
+        _lib.check(rc)
+
+
+def test_workspace_queries_are_host_only():
+    lib = _lib.load()
+    a = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 1, 0)
+    b = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 2, 0)
+    c = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 0, 0)
+    assert a > b > c > 0
+    assert a < 4e9            # the whole scale workload fits a few GB of the 180 GB
+    assert lib.msc_neighbors_workspace_bytes(10, 5, 11, 0, 0, 1, 0) == 0
+    off = (ctypes.c_int64 * 4)(0, 100, 300, 350)
+    assert lib.msc_batched_workspace_bytes(off, 3, 30, 15, 0, 1, 0) > 0
+    bad = (ctypes.c_int64 * 3)(0, 10, 300)             # sample 0 smaller than k
+    assert lib.msc_batched_workspace_bytes(bad, 2, 30, 15, 0, 1, 0) == 0
+    assert lib.msc_fuzzy_union_workspace_bytes(1000, 15) > 0
+
+
+def test_status_mapping():
+    with pytest.raises(ValueError):
+        _lib.check(_lib.MSC_ERR_INVALID_ARG)
+    with pytest.raises(MemoryError):
+        _lib.check(_lib.MSC_ERR_WORKSPACE)
+    with pytest.raises(NotImplementedError):
+        _lib.check(_lib.MSC_ERR_UNSUPPORTED)
+    with pytest.raises(RuntimeError):
+        _lib.check(_lib.MSC_ERR_TIMEOUT)
+    with pytest.raises(RuntimeError):
+        _lib.check_stats([0, 1, 0, 0, 0, 0, 0, 0])
+    with pytest.raises(ValueError):
+        _lib.check_stats([3, 0, 0, 0, 0, 0, 0, 0])
