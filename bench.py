@@ -41,11 +41,12 @@ import numpy as np
 METRIC = "kNN-graph cells/s at 1.3M×50 k=15, BF16+rerank vs FP32 GPU; serve p50/p99 ms"
 
 
-def workload(name: str):
+def workload(name: str, n: int | None = None):
     from msc_b200 import synth
     if name == "scale":
-        X, p = synth.scale_1m3()
-        return X, p, "scale: 1,300,000 cells x 50 PCs, 200 clusters (lognormal sizes), 1% noise"
+        X, p = synth.scale_1m3(n=n or 1_300_000)
+        return X, p, (f"scale: {X.shape[0]:,} cells x 50 PCs, 200 clusters (lognormal sizes), "
+                      "1% noise")
     if name == "plain":
         X, p = synth.plain_10k()
         return X, p, "plain: 10,000 cells x 50 PCs, 20 equal clusters"
@@ -151,7 +152,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    X, p, desc = workload(args.workload)
+    X, p, desc = workload(args.workload, args.n)
     k, metric = p["n_neighbors"], p["metric"]
     for _ in range(args.warmup):
         cpu_baseline(X, k, metric, budget_s=2.0)
@@ -159,7 +160,6 @@ def run_reference(args):
     for _ in range(args.steps):
         vals.append(cpu_baseline(X, k, metric, budget_s=args.ref_budget)["value"])
     wall = time.perf_counter() - t0
-    cb = cpu_baseline.__doc__ and None
     v = float(np.median(vals))
     last = cpu_baseline(X, k, metric, budget_s=1.0)
     line = {"metric": METRIC, "value": v, "unit": "cells/s", "impl": "reference",
@@ -172,7 +172,6 @@ def run_reference(args):
                              "kind": "port", "sample": last["sample"]},
             "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    del cb
     print(json.dumps(line), flush=True)
 
 
@@ -191,7 +190,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     lib = _lib.load()
 
-    X, p, desc = workload(args.workload)
+    X, p, desc = workload(args.workload, args.n)
     n, d = X.shape
     k, metric = p["n_neighbors"], p["metric"]
     method = p.get("method", "umap")
@@ -363,6 +362,7 @@ def main(argv=None):
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=15.0)
+    ap.add_argument("--n", type=int, default=None, help="cells of the scale workload (profiling)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)

@@ -77,6 +77,12 @@ long long msc_launch_count(void);
 int       msc_profile_enable(int on);
 int       msc_profile_read(float* ms_out, int max_stages);
 
+/* Self-test of the bounded device waits that every pipeline wait uses (no counterpart in the
+ * reference): one kernel waits on a barrier that nothing arrives at, gives up after limit_ns
+ * (1 us .. 10 s) and returns normally.  out_dev (int32[3]) = {1 if it gave up, abort flag,
+ * elapsed ms}.  Nothing faults or hangs; the context stays usable. */
+int       msc_selftest_wait_timeout(int64_t limit_ns, int32_t* out_dev, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Whole graph — replaces metalsinglecell `neighbors.neighbors` (neighbors.py:727-760), itself
  * called by `pp.neighbors` (pp.py:774).

@@ -336,6 +336,14 @@ int msc_profile_read(float* ms_out, int max_stages) {
   return n;
 }
 
+int msc_selftest_wait_timeout(int64_t limit_ns, int32_t* out_dev, void* stream) {
+  if (limit_ns < 1000 || limit_ns > int64_t(10) * 1000000000ll || !out_dev) {
+    set_error("limit_ns must be in [1 us, 10 s] and out_dev non-NULL");
+    return MSC_ERR_INVALID_ARG;
+  }
+  return launch_wait_selftest(uint64_t(limit_ns), out_dev, as_stream(stream));
+}
+
 size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, int32_t precision,
                                int32_t kprime) {
   Problem P;

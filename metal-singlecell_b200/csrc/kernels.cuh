@@ -85,6 +85,7 @@ struct TcConfig {
   int cb;        // selector buffer (8 / 16 / 32)
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
+int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st);
 TcConfig tc_default_config(int prec, int d, int kprime);
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,

@@ -140,7 +140,7 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       if (nvalid > 0)
         sel.finish(cand_idx, cand_thr, cand_stride, int64_t(w.qorig0) + wrow0, nvalid, kprime);
       else
-        sel.compact();
+        sel.flush();
     }
     __syncthreads();
   }

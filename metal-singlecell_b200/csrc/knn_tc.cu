@@ -66,17 +66,23 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of `parity` to complete.  false = gave up (abort raised).
-__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  if (mbar_test(bar, parity)) return true;
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
+                                            volatile int* abort_flag,
+                                            uint64_t limit_ns = WAIT_LIMIT_NS) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_test(bar, parity)) return true;
     if (*abort_flag) return false;
-    if ((it & 255) == 0 && globaltimer() - t0 > WAIT_LIMIT_NS) {
+    if ((it & 255) == 0 && globaltimer() - t0 > limit_ns) {
       *abort_flag = 1;
       return false;
     }
   }
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          volatile int* abort_flag) {
+  if (mbar_test(bar, parity)) return true;
+  return mbar_wait_slow(bar, parity, abort_flag);
 }
 // Teardown wait for work this thread itself started (copies, MMAs): ignores the abort flag
 // because such work completes on its own, but is still bounded in time.
@@ -125,6 +131,32 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
           smem_u32(bar))
       : "memory");
+}
+// tcgen05.ld of 32 columns of this warp's 32 lanes; completes at the next tmem_wait
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+// wait for this thread's outstanding tcgen05.ld; the registers of the load are operands so that
+// no use of them can be scheduled before the wait
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
@@ -339,15 +371,33 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         const uint32_t t0 = tmem_base + uint32_t(acc * P.bn) + (uint32_t(q * 32) << 16);
         const int col_base = w.orig_off + kt * P.bn;
         const int nch = P.bn / 32;
-        for (int c = 0; c < nch; ++c) {
-          float v[32];
-          tmem_ld32(t0 + uint32_t(c * 32), v);
-          if (c == nch - 1) {
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        // two register buffers: the next chunk's TMEM load is in flight while the current
+        // chunk is filtered; the accumulator is released right after its last load completes
+        uint32_t ra[32], rb[32];
+        auto release = [&]() {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[acc]);
+        };
+        tmem_ld32_async(t0, ra);
+        tmem_wait(ra);
+        if (nch == 1) release();
+        for (int c = 0; c < nch; c += 2) {
+          const bool more = c + 1 < nch;
+          if (more) tmem_ld32_async(t0 + uint32_t((c + 1) * 32), rb);
+          sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
+          if (more) {
+            tmem_wait(rb);
+            if (c + 1 == nch - 1) release();
+            const bool more2 = c + 2 < nch;
+            if (more2) tmem_ld32_async(t0 + uint32_t((c + 2) * 32), ra);
+            sel.push32(reinterpret_cast<const float(&)[32]>(rb), col_base + (c + 1) * 32, self,
+                       limit);
+            if (more2) {
+              tmem_wait(ra);
+              if (c + 2 == nch - 1) release();
+            }
           }
-          sel.push32(v, col_base + c * 32, self, limit);
         }
         if (++acc == 2) { acc = 0; accphase ^= 1; }
       }
@@ -358,7 +408,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         sel.finish(cand_idx, cand_thr, P.cand_stride, int64_t(w.qorig0) + wrow0, nvalid,
                    P.kprime);
       else
-        sel.compact();
+        sel.flush();
     }
   }
 
@@ -372,6 +422,26 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   if (threadIdx.x == 0 && *abort_flag) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_TIMEOUT]), 1ull);
     atomicExch(&ctl->timeout_flag, 1);
+  }
+}
+
+// Self-test of the bounded wait: an mbarrier that nothing ever arrives at.  The wait must give
+// up after `limit_ns`, raise the abort flag and let the kernel return normally.
+__global__ void wait_selftest_kernel(uint64_t limit_ns, int32_t* out) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint64_t t0 = globaltimer();
+    const bool ok = mbar_wait_slow(&bar, 0, &abort_flag, limit_ns);
+    out[0] = ok ? 0 : 1;                                  // 1 = gave up as designed
+    out[1] = abort_flag;
+    out[2] = int32_t((globaltimer() - t0) / 1000000ull);  // elapsed ms
   }
 }
 
@@ -450,6 +520,12 @@ int launch_tc_t(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
 }
 
 }  // namespace
+
+int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st) {
+  wait_selftest_kernel<<<1, 32, 0, st>>>(limit_ns, out);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
 
 bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;

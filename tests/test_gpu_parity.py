@@ -134,3 +134,19 @@ def test_errors():
     torch.cuda.synchronize()
     with pytest.raises(ValueError):
         _lib.check_stats(res["stats"].cpu().numpy())
+
+
+def test_bounded_wait_gives_up_without_hanging():
+    """Failure detection without a GPU fault: a device wait on a barrier nothing arrives at gives
+    up after its bound, the kernel returns an error status, and the context stays usable."""
+    import torch
+    lib = _lib.load()
+    out = torch.zeros(3, dtype=torch.int32, device="cuda")
+    _lib.check(lib.msc_selftest_wait_timeout(50_000_000, out.data_ptr(),
+                                             torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    gave_up, flag, ms = out.cpu().tolist()
+    assert gave_up == 1 and flag == 1 and 40 <= ms < 5000
+    # the context still works
+    X = synth.gaussian_mixture(2000, 20, 5, seed=3)
+    check_against_oracle(X, 10, precision="bf16x3")
