@@ -148,6 +148,23 @@ int msc_fuzzy_union(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, i
                     int64_t* indptr_dev, int32_t* indices_dev, float* data_dev, int64_t* nnz_dev,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* The fuzzy union without caller-provided scratch.  No counterpart in the reference: it is for
+ * callers that cannot give the library device memory — code under a memory manager that owns all
+ * of the GPU's memory (a framework's caching allocator, a serving process that reserves its HBM
+ * at start-up and offers plug-ins no allocator) or a hot loop where cudaMalloc/cudaFree, which may
+ * synchronise the device, are not acceptable.  It allocates nothing: its scratch is a fixed 20 MiB
+ * array in the library's own device memory (held on every GPU that loads the library until the
+ * process exits), so it accepts only n <= MSC_NOALLOC_MAX_CELLS and n*k <= MSC_NOALLOC_MAX_ENTRIES
+ * and answers MSC_ERR_INVALID_ARG beyond that.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and corrupt each other's results — serialise them. */
+#define MSC_NOALLOC_MAX_CELLS   65536
+#define MSC_NOALLOC_MAX_ENTRIES 1048576
+int msc_fuzzy_union_noalloc(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, int32_t k,
+                            int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
+                            int64_t* nnz_dev, void* stream);
+
 /* method='gauss' connectivities (scanpy's locally scaled Gaussian kernel; not in the reference) */
 size_t msc_gauss_workspace_bytes(int64_t n, int32_t k);
 int msc_gauss_connectivities(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,

@@ -51,6 +51,7 @@ SIGNATURES = {
     "msc_membership": (I32, [P, P, P, P, I64, I32, P, P]),
     "msc_fuzzy_union_workspace_bytes": (SZ, [I64, I32]),
     "msc_fuzzy_union": (I32, [P, P, I64, I32, P, P, P, P, P, SZ, P]),
+    "msc_fuzzy_union_noalloc": (I32, [P, P, I64, I32, P, P, P, P, P]),
     "msc_gauss_workspace_bytes": (SZ, [I64, I32]),
     "msc_gauss_connectivities": (I32, [P, P, I64, I32, P, P, P, P, P, SZ, P]),
     "msc_distances_csr": (I32, [P, P, I64, I32, P, P, P, P]),
