@@ -1,0 +1,106 @@
+"""Generate golden vectors by running the reference's own code (metalsinglecell) on the CPU.
+
+The reference needs Apple's `mlx`, which cannot exist here.  The parts of its neighbour path that
+use only array arithmetic are run under a small NumPy stand-in for ``mlx.core`` (the module below
+maps every ``mx.*`` call those functions make onto its NumPy equivalent):
+
+* ``neighbors._knn_gpu`` (neighbors.py:82-132) for k = 33 and 50 on the reference's own test
+  input (tests/test_postfix_fixes.py:108-121: 500×20 N(0,1), default_rng(0)).  For k > 32 the
+  reference selects with ``mx.argpartition`` (neighbors.py:66-68), so every step it takes —
+  fp16 rescaled Gram ranking, argpartition, fp32 direct-difference recompute, host sort — is the
+  reference's code.  (k ≤ 32 goes through a Metal kernel and is not run.)
+* the vendored mlx-vis ``UMAP._fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271) on an
+  exact kNN graph: the per-row ρ and the bisection σ are captured from its ``mx.eval`` calls.
+
+Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
+Writes tests/golden/reference_knn_500x20.npz and tests/golden/reference_rho_sigma.npz.
+"""
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+REF = Path("/root/reference/src")
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+sys.path.insert(0, str(Path(__file__).resolve().parents[2] / "metal-singlecell_b200"))
+
+
+def numpy_mlx():
+    """A stand-in ``mlx.core`` backed by NumPy; ``captured`` records every ``eval`` argument."""
+    mx = types.ModuleType("mlx.core")
+    mx.captured = []
+    mx.float16, mx.float32, mx.int32, mx.uint32, mx.int64 = (np.float16, np.float32, np.int32,
+                                                              np.uint32, np.int64)
+
+    def array(x, dtype=None):
+        a = np.array(x)
+        if dtype is not None:
+            a = a.astype(dtype)
+        elif a.dtype == np.float64:
+            a = a.astype(np.float32)             # MLX's default float type
+        return a
+
+    def eval_(*args):
+        mx.captured.append([np.array(a) for a in args])
+
+    mx.array = array
+    mx.eval = eval_
+    mx.sum = lambda a, axis=None: np.sum(a, axis=axis, dtype=a.dtype)
+    mx.max = lambda a, axis=None: np.max(a, axis=axis)
+    mx.min = lambda a, axis=None: np.min(a, axis=axis)
+    mx.maximum = lambda a, b: np.maximum(a, np.asarray(b, dtype=np.asarray(a).dtype))
+    mx.where = lambda c, a, b: np.where(c, a, b).astype(np.result_type(
+        np.asarray(a).dtype, np.asarray(b).dtype) if np.asarray(a).dtype != np.float64
+        else np.float32)
+    mx.full = lambda shape, v: np.full(shape, v, dtype=np.float32)
+    mx.ones = lambda shape: np.ones(shape, dtype=np.float32)
+    mx.exp = np.exp
+    mx.abs = np.abs
+    mx.all = np.all
+    mx.argpartition = lambda a, kth, axis=-1: np.argpartition(a, kth, axis=axis)
+    mx.argsort = lambda a, axis=-1: np.argsort(a, axis=axis)
+    mx.compile = lambda f: f                     # decorators in the vendored module
+    pkg = types.ModuleType("mlx")
+    pkg.core = mx
+    sys.modules["mlx"] = pkg
+    sys.modules["mlx.core"] = mx
+    return mx
+
+
+def main():
+    mx = numpy_mlx()
+    sys.path.insert(0, str(REF))
+    from metalsinglecell import neighbors as ref_nb
+    from metalsinglecell._vendor.mlx_vis.umap import UMAP as RefUMAP
+
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((500, 20)).astype(np.float32)
+    out = {"X": X}
+    for k in (33, 50):
+        idx, dist = ref_nb._knn_gpu(X, k)
+        out[f"idx_k{k}"] = np.asarray(idx, np.int64)
+        out[f"dist_k{k}"] = np.asarray(dist, np.float32)
+    np.savez_compressed(OUT / "reference_knn_500x20.npz", **out)
+
+    import oracle
+    from msc_b200 import synth
+    Xg = synth.gaussian_mixture(400, 12, 6, seed=17)
+    k = 15
+    idx, d2, dist = oracle.knn_exact(Xg, k)
+    self = types.SimpleNamespace(n_neighbors=k, n_epochs=200)
+    mx.captured.clear()
+    try:
+        RefUMAP._fuzzy_simplicial_set(self, idx.astype(np.int32), dist, Xg.shape[0])
+    except Exception:
+        pass            # only the captured ρ and σ are needed; the later symmetrisation may not run
+    rho = np.asarray(mx.captured[0][0], np.float32)
+    sigma = np.asarray([c[0] for c in mx.captured if c[0].shape == rho.shape][-1], np.float32)
+    np.savez_compressed(OUT / "reference_rho_sigma.npz", X=Xg, knn_idx=idx, knn_dist=dist,
+                        rho=rho, sigma=sigma, k=k)
+    print("wrote", sorted(p.name for p in OUT.glob("reference_*.npz")))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,45 @@
+"""The oracle against golden vectors produced by the reference's own code
+(tests/golden/make_golden.py runs metalsinglecell's NumPy-expressible neighbour functions).
+
+* ``_knn_gpu`` (neighbors.py:82-132) at k = 33, 50 on the reference's test input: the reference
+  ranks on fp16 (recall ~0.99 by its own test), then recomputes fp32 distances.  The exact oracle
+  must contain it (recall ≥ 0.99, self first) and agree to fp32 precision on every neighbour both
+  place at the same position.
+* mlx-vis ``_fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271): ρ must be identical and σ
+  within the bisection tolerance (1e-5 relative on the sum ⇒ ~1e-5 on σ), wherever that function
+  and umap-learn share semantics (ρ > 1e-8, no mean-distance floor).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+
+G = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("k", [33, 50])
+def test_oracle_vs_reference_knn(k):
+    g = np.load(G / "reference_knn_500x20.npz")
+    X, ri, rd = g["X"], g[f"idx_k{k}"], g[f"dist_k{k}"]
+    idx, d2, dist = oracle.knn_exact(X, k)
+    assert (ri[:, 0] == np.arange(500)).all() and (idx[:, 0] == np.arange(500)).all()
+    recall = np.mean([len(set(idx[i]) & set(ri[i])) / k for i in range(500)])
+    assert recall >= 0.99
+    same = idx == ri
+    assert same.mean() >= 0.99
+    rel = np.abs(dist[same] - rd[same]) / np.maximum(rd[same], 1e-30)
+    assert rel.max() < 1e-6
+    # the reference's lists are ascending, like the oracle's
+    assert (np.diff(rd, axis=1) >= 0).all()
+
+
+def test_oracle_vs_reference_rho_sigma():
+    g = np.load(G / "reference_rho_sigma.npz")
+    sigma, rho = oracle.smooth_knn_dist(g["knn_dist"], float(g["k"]))
+    ok = g["rho"] > 1e-8
+    assert ok.all()
+    assert np.array_equal(rho, g["rho"])
+    rel = np.abs(sigma - g["sigma"]) / g["sigma"]
+    assert rel.max() < 1e-5
