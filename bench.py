@@ -194,7 +194,7 @@ def run_ours(args):
     n, d = X.shape
     k, metric = p["n_neighbors"], p["metric"]
     method = p.get("method", "umap")
-    kprime = p.get("kprime", 0)
+    kprime = args.kprime or p.get("kprime", 0)
     Xd = torch.from_numpy(X).to(dev)
     ws = nbm.Workspace(dev)
     out = {}
@@ -253,6 +253,14 @@ def run_ours(args):
     lib.msc_profile_enable(0)
     stage_names = ["prep", "candidates", "rerank_fp64", "csr_rho_sigma_membership", "union"]
     stages = {stage_names[i]: round(buf[i], 3) for i in range(min(ns, len(stage_names)))}
+    cnt = (ctypes.c_ulonglong * 16)()
+    lib.msc_profile_counters(cnt, 16)
+    ctas = max(int(cnt[9]), 1)
+    pipeline = {"producer_wait_stage": cnt[0] / ctas, "mma_wait_keys": cnt[1] / ctas,
+                "mma_wait_accumulator": cnt[2] / ctas, "epilogue_wait_accumulator": cnt[3] / ctas / 4,
+                "epilogue_loop": cnt[4] / ctas / 4, "kernel": cnt[5] / ctas,
+                "hot_chunks_per_warp": cnt[6] / ctas / 4, "compactions_per_thread": cnt[7] / ctas / 128,
+                "appends_per_row": cnt[8] / max(n, 1), "ctas": ctas}
 
     pk, pk_kind = peaks()
     cand_ms = stages.get("candidates")
@@ -271,7 +279,7 @@ def run_ours(args):
                 "kernel": "knn_tc_kernel" if args.precision != "fp32" else "knn_fp32_kernel",
                 "algorithmic_flop_per_launch": alg_flop, "kernel_ms": cand_ms,
                 "peak_kind": f"{pk_kind} bf16 sustained (kernel timed inside a full step)",
-                "stage_ms": stages}
+                "stage_ms": stages, "pipeline_cycles_per_cta": pipeline}
 
     # e2e through the public call: pinned host in, both CSR matrices back to pinned host
     Xh = torch.from_numpy(X).pin_memory()
@@ -351,19 +359,121 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """Batching workload: 256 samples (~4M cells, 30 PCs, k=15) in one persistent launch under a
+    captured CUDA graph with autotuned tiles, against a per-sample launch loop."""
+    import torch
+    from msc_b200 import batch, synth, _lib
+    torch.cuda.set_device(0)
+    X, offsets, p = synth.batch_samples(args.samples, seed=3, d=30)
+    n, d = X.shape
+    k = p["n_neighbors"]
+    Xd = torch.from_numpy(X).cuda()
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    loop_out = batch.per_sample_loop(Xd, offsets, k)
+    loop_ms = timed(lambda: batch.per_sample_loop(Xd, offsets, k, out=loop_out), args.steps)
+    bk = batch.BatchedKnn(offsets, d, k)
+    batched_ms = timed(lambda: bk.run(Xd), args.steps)
+    tune = batch.autotune(Xd, offsets, k, reps=1, use_cache=False)
+    bt = batch.BatchedKnn(offsets, d, k, tile_config=tune["tile_config"])
+    bt.capture(Xd)
+    graph_ms = timed(bt.replay, args.steps)
+    stats = bt.check()
+    same = bool(torch.equal(bt.idx, loop_out[0]) and torch.equal(bt.dist, loop_out[1]))
+    sizes = np.diff(offsets)
+    line = {"metric": "batching: kNN cells/s, one persistent launch + CUDA graph vs per-sample "
+                      "launch loop", "value": n / (graph_ms / 1000), "unit": "cells/s",
+            "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": f"{len(sizes)} samples, {n:,} cells (min {sizes.min()}, "
+                                   f"max {sizes.max()}), 30 PCs, k=15, euclidean",
+                       "precision": "bf16x3", "tile": batch.decode_tile_code(tune["tile_config"])},
+            "graph_ms": graph_ms, "batched_ms": batched_ms, "per_sample_loop_ms": loop_ms,
+            "speedup_vs_loop": loop_ms / graph_ms, "identical_to_loop": same,
+            "autotune_table": [(batch.decode_tile_code(c), round(ms, 3))
+                               for c, ms in tune.get("table", [])],
+            "certified": int(stats[_lib.STAT_CERTIFIED]),
+            "rescanned": int(stats[_lib.STAT_RESCANNED]),
+            "algorithmic_tflops": 2.0 * d * float((sizes.astype(np.float64) ** 2).sum())
+                                  / (graph_ms / 1000) / 1e12}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Serving workload: Poisson arrivals of graph requests (1k-500k cells, 30/50/100 PCs,
+    k in {10,15,30}, euclidean/cosine); p50/p99 latency and cells/s at swept arrival rates
+    against the batched-offline throughput of the same requests."""
+    import torch
+    from msc_b200 import serve, synth
+    torch.cuda.set_device(0)
+    spec = synth.serving_requests(1.0, args.requests, seed=5)
+    data = [synth.request_embedding(r) for r in spec]
+    total_cells = sum(x.shape[0] for x in data)
+    budget = int(args.hbm_budget_gb * (1 << 30))
+
+    def fresh():
+        return [serve.Request(X=x, n_neighbors=r["k"], metric=r["metric"])
+                for x, r in zip(data, spec)]
+
+    serve.run_offline(fresh()[: min(8, len(data))], budget, args.slots)     # warm-up
+    off = serve.run_offline(fresh(), budget, args.slots)
+    sweep = []
+    mean_cells = total_cells / len(data)
+    for frac in args.load_fracs:
+        rate = frac * off["cells_per_s"] / mean_cells
+        rng = np.random.default_rng(7)
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(data))).tolist()
+        rep = serve.run_trace(fresh(), arr, budget, args.slots)
+        rep.update({"load_frac_of_offline": frac, "rate_req_per_s": rate,
+                    "throughput_frac_of_offline": rep["cells_per_s"] / off["cells_per_s"]})
+        sweep.append(rep)
+    best = max((r for r in sweep if r["failed"] == 0), key=lambda r: r["cells_per_s"],
+               default=None)
+    line = {"metric": "serving: p50/p99 ms and cells/s vs batched offline throughput",
+            "value": best["p99_ms"] if best else None, "unit": "ms (p99 at highest load swept)",
+            "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+            "config": {"requests": len(data), "cells_total": total_cells,
+                       "slots": args.slots, "hbm_budget_gb": args.hbm_budget_gb,
+                       "distribution": "cells LogNormal(ln 20000, 1) clipped 1k-500k; PCs {30,50,100}; "
+                                       "k {10,15,30}; metric {euclidean, cosine}"},
+            "offline": off, "sweep": sweep}
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scale", choices=["scale", "plain", "precision"])
+    ap.add_argument("--workload", default="scale",
+                    choices=["scale", "plain", "precision", "batch", "serve"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp16", "bf16", "fp32"])
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--n", type=int, default=None, help="cells of the scale workload (profiling)")
+    ap.add_argument("--samples", type=int, default=256, help="batch workload: samples")
+    ap.add_argument("--requests", type=int, default=120, help="serve workload: requests")
+    ap.add_argument("--slots", type=int, default=8, help="serve workload: concurrent slots")
+    ap.add_argument("--hbm-budget-gb", type=float, default=64.0)
+    ap.add_argument("--kprime", type=int, default=0, help="over-fetch k' (0: the library default)")
+    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.5, 0.7, 0.9])
     args = ap.parse_args(argv)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.impl == "reference":
         run_reference(args)
     else:

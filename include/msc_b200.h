@@ -76,6 +76,10 @@ const char* msc_last_error(void);
 long long msc_launch_count(void);
 int       msc_profile_enable(int on);
 int       msc_profile_read(float* ms_out, int max_stages);
+/* pipeline counters of the tensor-core candidate kernel summed over CTAs since the last
+ * msc_profile_enable(1) (cycles waiting / busy per role, hot chunks, compactions, appends, CTAs);
+ * synchronizes the device. */
+int       msc_profile_counters(unsigned long long* out, int max_counters);
 
 /* Self-test of the bounded device waits that every pipeline wait uses (no counterpart in the
  * reference): one kernel waits on a barrier that nothing arrives at, gives up after limit_ns
@@ -119,8 +123,9 @@ int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
  *   msc_batched_prepare  writes the sample table into the workspace and waits for that copy;
  *   msc_batched_knn      only enqueues kernels (capturable in a CUDA graph); call it with the
  *                        same offsets / shapes as the prepare call.
- * tile_config: 0 = automatic, else bn | stages<<12 | cb<<20 (key tile rows, pipeline depth,
- * selector buffer) as chosen by the Python autotuner. */
+ * tile_config: 0 = automatic, else bn | stages<<12 | cb<<20 | atmem<<27 (key tile rows,
+ * pipeline depth, selector buffer, query operand in tensor memory) as chosen by the Python
+ * autotuner. */
 size_t msc_batched_workspace_bytes(const int64_t* offsets_host, int32_t n_samples, int32_t d,
                                    int32_t k, int32_t metric, int32_t precision, int32_t kprime);
 int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t d, int32_t k,

@@ -45,6 +45,8 @@ StageTimer& timer() {
 }
 }  // namespace
 
+bool profiling_enabled() { return timer().on; }
+
 void stage_mark(cudaStream_t st, int stage) {
   StageTimer& t = timer();
   if (!t.on || stage < 0 || stage >= MAX_MARKS) return;
@@ -103,7 +105,12 @@ struct KnnWs {
 };
 
 int default_kprime(int prec, int k) {
-  if (prec == PREC_FP32) return std::min(64, std::max(k - 1, k + 7));
+  // over-fetch sized to each precision's certificate.  FP32 and the three-term BF16 split have
+  // error bounds far below typical neighbour gaps, but the k'-th candidate must still clear the
+  // k-th neighbour by the bound: at 1.3M cells k' = k+8 left ~0.04% of the rows to the FP64 scan,
+  // k' = 32 none.  One-term FP16/BF16 need a wider margin.
+  if (prec == PREC_FP32) return std::min(64, std::max(k - 1, k + 8));
+  if (prec == PREC_BF16X3) return std::min(64, std::max(32, k + 8));
   return std::min(64, std::max(48, k + 15));
 }
 
@@ -187,7 +194,8 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
 int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
   cfg = tc_default_config(P.prec, P.d, P.kprime);
   if (code == 0) return MSC_OK;
-  TcConfig c{code & 0xfff, (code >> 12) & 0xff, P.kprime <= 32 ? 32 : 64, (code >> 20) & 0xff};
+  TcConfig c{code & 0xfff, (code >> 12) & 0xff, P.kprime <= 32 ? 32 : 64, (code >> 20) & 0x7f,
+             (code >> 27) & 1};
   if (!tc_config_ok(c, P.L.kp, P.kprime)) {
     set_error("tile_config 0x%x (bn=%d stages=%d cb=%d) is not valid here", code, c.bn, c.stages, c.cb);
     return MSC_ERR_INVALID_ARG;
@@ -318,7 +326,14 @@ long long msc_launch_count(void) { return msc::g_launch_count.load(); }
 int msc_profile_enable(int on) {
   timer().on = on != 0;
   timer().last = -1;
+  if (on) return tc_counters_clear();
   return MSC_OK;
+}
+
+int msc_profile_counters(unsigned long long* out, int max_counters) {
+  if (!out || max_counters < 1) { set_error("out/max_counters invalid"); return MSC_ERR_INVALID_ARG; }
+  MSC_CUDA_TRY(cudaDeviceSynchronize());
+  return tc_counters(out, max_counters);
 }
 
 int msc_profile_read(float* ms_out, int max_stages) {

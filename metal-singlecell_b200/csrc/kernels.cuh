@@ -79,13 +79,17 @@ int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const 
 
 // ---- knn_tc.cu ----
 struct TcConfig {
-  int bn;        // key tile rows (64, 128, 256)
+  int bn;        // key tile rows (32, 64, 128, 256)
   int stages;    // smem pipeline depth of the key tiles
   int kpl;       // selector list length (32 / 64)
-  int cb;        // selector buffer (8 / 16 / 32)
+  int cb;        // selector buffer (16 / 32)
+  int atmem;     // 1: query operand in tensor memory, 0: in shared memory
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
 int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st);
+int tc_counters(unsigned long long* out, int max);
+int tc_counters_clear();
+bool profiling_enabled();
 TcConfig tc_default_config(int prec, int d, int kprime);
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,

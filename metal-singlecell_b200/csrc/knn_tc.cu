@@ -126,6 +126,30 @@ __device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
+// same, with the A operand in tensor memory (M lanes × K columns, two 16-bit elements per column)
+__device__ __forceinline__ void umma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -157,6 +181,17 @@ __device__ __forceinline__ void tmem_wait(uint32_t (&r)[32]) {
                  "+r"(r[30]), "+r"(r[31])
                :
                : "memory");
+}
+// orders later uses of r after a preceding tmem_wait (the statement is empty; the registers are
+// declared modified, and volatile asm is never moved across the wait)
+__device__ __forceinline__ void tmem_dep(uint32_t (&r)[32]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31]));
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
@@ -202,7 +237,18 @@ struct TcParams {
   int bf16;
   int n_items;
   uint32_t idesc;
+  int prof;         // accumulate the pipeline counters below
+  int a_tmem;       // 1: the query tile lives in tensor memory (loaded by the epilogue warps)
+  const uint32_t* a_glob;   // packed query operand (A-in-TMEM mode): rows of kp 16-bit elements
+  int kp;           // elements per packed row
 };
+
+// Pipeline counters (cycles / events summed over CTAs), filled when profiling is enabled:
+//   0 producer waiting for a free key stage     1 MMA waiting for a loaded key tile
+//   2 MMA waiting for a free accumulator         3 epilogue waiting for an accumulator
+//   4 epilogue cycles in its tile loops          5 kernel cycles (thread 0)
+//   6 hot chunks (any row below its threshold)   7 compactions   8 appends   9 CTAs
+__device__ unsigned long long g_tc_prof[16];
 
 struct SmemPlan {
   size_t a_off, b_off, sel_off, bar_off, total;
@@ -212,7 +258,7 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int bn, int stages, int na
   SmemPlan p;
   p.a_off = 0;
   p.b_off = p.a_off + size_t(na) * kb * BM * 128;
-  p.sel_off = p.b_off + size_t(stages) * kb * bn * 128;
+  p.sel_off = p.b_off + size_t(stages) * bn * 128;
   p.bar_off = p.sel_off + RowSelect<KPL, CB, BM>::smem_bytes();
   p.total = p.bar_off + 256 + 1024;          // barriers + slack for 1024-byte alignment
   return p;
@@ -235,19 +281,19 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   uint64_t* acc_full = bars + 4;           // [2]
   uint64_t* acc_empty = bars + 6;          // [2]
   uint64_t* done_bar = bars + 8;           // [1]
-  uint64_t* b_full = bars + 9;             // [stages <= 6]
-  uint64_t* b_empty = bars + 15;           // [stages <= 6]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 22);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 23);
+  uint64_t* b_full = bars + 9;             // [stages <= 8]
+  uint64_t* b_empty = bars + 17;           // [stages <= 8]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 25);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 26);   // 27 x 8 B < 256 B
 
   const int warp = warp_id(), lane = lane_id();
   const size_t a_bytes = size_t(P.kb) * BM * 128;
-  const size_t b_bytes = size_t(P.kb) * P.bn * 128;
-  const uint32_t tmem_cols = uint32_t(2 * P.bn);
+  const size_t b_bytes = size_t(P.bn) * 128;            // one K atom of a key tile
+  const uint32_t tmem_cols = P.a_tmem ? 512u : uint32_t(2 * P.bn);
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2; ++i) {
-      mbar_init(&a_full[i], 1);
+      mbar_init(&a_full[i], P.a_tmem ? 4 : 1);
       mbar_init(&a_empty[i], 1);
       mbar_init(&acc_full[i], 1);
       mbar_init(&acc_empty[i], 4);
@@ -272,6 +318,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  const long long t_kernel0 = clock64();
 
   if (warp == 0) {
     // ------------------------------------------------------------------ TMA producer
@@ -279,33 +326,39 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       int stage = 0, abuf = 0;
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
+      long long c_wait = 0;
       for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
         const WorkItem w = items[it];
-        ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
-        if (!ok) break;
-        mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
-        for (int kb = 0; kb < P.kb; ++kb)
-          tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
-                      w.qrow0);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        for (int kt = 0; kt < nkt; ++kt) {
-          ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+        if (!P.a_tmem) {
+          ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
           if (!ok) break;
-          mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
+          mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
           for (int kb = 0; kb < P.kb; ++kb)
-            tma_load_2d(Bsm + stage * b_bytes + size_t(kb) * P.bn * 128, &tmB, &b_full[stage],
-                        kb * 64, w.key0 + kt * P.bn);
-          if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf],
+                        kb * 64, w.qrow0);
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        }
+        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
+        for (int kt = 0; kt < nkt && ok; ++kt) {
+          for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
+            const long long tw = P.prof ? clock64() : 0;
+            ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+            if (P.prof) c_wait += clock64() - tw;
+            if (!ok) break;
+            mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
+            tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64, w.key0 + kt * P.bn);
+            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+          }
         }
       }
+      if (P.prof) atomicAdd(&g_tc_prof[0], (unsigned long long)c_wait);
       // drain: every load this thread armed completes on its own; wait for them (bounded)
       for (int s = 0; s < P.stages; ++s) {
         // stages armed in the current lap have parity sphase for indices < stage
         const uint32_t par = s < stage ? sphase : (sphase ^ 1);
         (void)mbar_drain(&b_full[s], par);
       }
-      for (int a = 0; a < P.na; ++a) {
+      for (int a = 0; a < P.na && !P.a_tmem; ++a) {
         const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
         (void)mbar_drain(&a_full[a], par);
       }
@@ -316,37 +369,57 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       int stage = 0, abuf = 0, acc = 0;
       uint32_t sphase = 0, aphase = 0, accphase = 0;
       bool ok = true, issued = false;
+      long long c_b = 0, c_acc = 0;
       for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
         const WorkItem w = items[it];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (!ok) break;
-        const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
+        const uint32_t a_base = P.a_tmem ? 0u : smem_u32(Asm + abuf * a_bytes);
+        const uint32_t a_tcol = tmem_base + uint32_t(2 * P.bn);   // A columns in TMEM
         const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        for (int kt = 0; kt < nkt; ++kt) {
-          ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-          if (!ok) break;
+        for (int kt = 0; kt < nkt && ok; ++kt) {
+          const long long t2 = P.prof ? clock64() : 0;
           ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+          if (P.prof) c_acc += clock64() - t2;
           if (!ok) break;
           tc_fence_after();
-          const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
           const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
-          for (int ks = 0; ks < P.ksteps; ++ks) {
-            const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
-            const uint32_t bo = uint32_t((ks >> 2) * P.bn * 128 + (ks & 3) * 32);
-            umma_f16(d_tmem, sdesc(a_base + ao), sdesc(b_base + bo), P.idesc, ks > 0 ? 1u : 0u);
+          for (int kb = 0; kb < P.kb; ++kb) {
+            const long long t1 = P.prof ? clock64() : 0;
+            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+            if (P.prof) c_b += clock64() - t1;
+            if (!ok) break;
+            const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
+            const int ks1 = min(P.ksteps, 4 * kb + 4);
+            for (int ks = 4 * kb; ks < ks1; ++ks) {
+              const uint32_t bo = uint32_t((ks & 3) * 32);
+              if (P.a_tmem) {
+                umma_f16_ts(d_tmem, a_tcol + uint32_t(ks * 8), sdesc(b_base + bo), P.idesc,
+                            ks > 0 ? 1u : 0u);
+              } else {
+                const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
+                umma_f16(d_tmem, sdesc(a_base + ao), sdesc(b_base + bo), P.idesc,
+                         ks > 0 ? 1u : 0u);
+              }
+            }
+            umma_commit(&b_empty[stage]);
+            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
+          if (!ok) break;
           issued = true;
-          umma_commit(&b_empty[stage]);
           umma_commit(&acc_full[acc]);
-          if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           if (++acc == 2) { acc = 0; accphase ^= 1; }
         }
         if (!ok) break;
         umma_commit(&a_empty[abuf]);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        if (++abuf == (P.a_tmem ? 1 : P.na)) { abuf = 0; aphase ^= 1; }
       }
       if (issued) umma_commit(done_bar);
       else mbar_arrive(done_bar);
+      if (P.prof) {
+        atomicAdd(&g_tc_prof[1], (unsigned long long)c_b);
+        atomicAdd(&g_tc_prof[2], (unsigned long long)c_acc);
+      }
     }
   } else if (warp >= EPI_WARP0) {
     // ------------------------------------------------------------------ epilogue
@@ -357,22 +430,50 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     int acc = 0;
     uint32_t accphase = 0;
     bool ok = true;
+    long long c_ew = 0, c_loop = 0;
+    uint32_t aphase_e = 0;
     for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
       const WorkItem w = items[it];
+      const long long tl = P.prof ? clock64() : 0;
+      if (P.a_tmem) {
+        // the query rows of this tile into TMEM: this thread's lane holds its row; the MMAs of
+        // the previous tile must be done reading the old rows first
+        ok = __all_sync(FULL, mbar_wait(&a_empty[0], aphase_e ^ 1, abort_flag));
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t* src = P.a_glob + (int64_t(w.qrow0) + row) * (P.kp / 2);
+        const uint32_t a_t = tmem_base + uint32_t(2 * P.bn) + (uint32_t(q * 32) << 16);
+        for (int c = 0; c < P.kp / 2; c += 32) {
+          uint32_t r[32];
+#pragma unroll
+          for (int e = 0; e < 32; e += 4) {
+            const uint4 v4 = *reinterpret_cast<const uint4*>(src + c + e);
+            r[e] = v4.x; r[e + 1] = v4.y; r[e + 2] = v4.z; r[e + 3] = v4.w;
+          }
+          tmem_st32(a_t + uint32_t(c), r);
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&a_full[0]);
+        aphase_e ^= 1;
+      }
       sel.reset();
       __syncwarp();
       const int self = w.qorig0 + row;
       const int limit = w.orig_off + w.nkeys;
       const int nkt = (w.nkeys + P.bn - 1) / P.bn;
       for (int kt = 0; kt < nkt; ++kt) {
+        const long long te = P.prof ? clock64() : 0;
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
+        if (P.prof) c_ew += clock64() - te;
         if (!ok) break;
         tc_fence_after();
         const uint32_t t0 = tmem_base + uint32_t(acc * P.bn) + (uint32_t(q * 32) << 16);
         const int col_base = w.orig_off + kt * P.bn;
         const int nch = P.bn / 32;
-        // two register buffers: the next chunk's TMEM load is in flight while the current
-        // chunk is filtered; the accumulator is released right after its last load completes
+        // two register buffers: the next chunk's TMEM load is in flight while the current chunk
+        // is filtered; the accumulator is released right after its last load completes
         uint32_t ra[32], rb[32];
         auto release = [&]() {
           tc_fence_before();
@@ -409,6 +510,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                    P.kprime);
       else
         sel.flush();
+      if (P.prof) c_loop += clock64() - tl;
+    }
+    if (P.prof) {
+      if (lane == 0) {
+        atomicAdd(&g_tc_prof[3], (unsigned long long)c_ew);
+        atomicAdd(&g_tc_prof[4], (unsigned long long)c_loop);
+        atomicAdd(&g_tc_prof[6], (unsigned long long)sel.n_hot);
+      }
+      atomicAdd(&g_tc_prof[7], (unsigned long long)sel.n_compact);
+      atomicAdd(&g_tc_prof[8], (unsigned long long)sel.n_append);
     }
   }
 
@@ -418,6 +529,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     (void)mbar_drain(done_bar, 0);
     tc_fence_after();
     tmem_dealloc(tmem_base, tmem_cols);
+  }
+  if (P.prof && threadIdx.x == 0) {
+    atomicAdd(&g_tc_prof[5], (unsigned long long)(clock64() - t_kernel0));
+    atomicAdd(&g_tc_prof[9], 1ull);
   }
   if (threadIdx.x == 0 && *abort_flag) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_TIMEOUT]), 1ull);
@@ -502,6 +617,7 @@ size_t config_smem(const TcConfig& c, int kb, int na) {
 }
 
 int pick_na(const TcConfig& c, int kb) {
+  if (c.atmem) return 0;
   return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1;
 }
 
@@ -521,6 +637,18 @@ int launch_tc_t(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
 
 }  // namespace
 
+int tc_counters(unsigned long long* out, int max) {
+  unsigned long long buf[16];
+  MSC_CUDA_TRY(cudaMemcpyFromSymbol(buf, g_tc_prof, sizeof(buf)));
+  for (int i = 0; i < max && i < 16; ++i) out[i] = buf[i];
+  return MSC_OK;
+}
+int tc_counters_clear() {
+  unsigned long long z[16] = {};
+  MSC_CUDA_TRY(cudaMemcpyToSymbol(g_tc_prof, z, sizeof(z)));
+  return MSC_OK;
+}
+
 int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st) {
   wait_selftest_kernel<<<1, 32, 0, st>>>(limit_ns, out);
   MSC_LAUNCH_CHECK();
@@ -529,25 +657,30 @@ int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st) {
 
 bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;
-  if (c.stages < 2 || c.stages > 6) return false;
+  if (c.stages < 2 || c.stages > 8) return false;
   if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 64)) return false;
   if (c.cb != 16 && c.cb != 32) return false;
   const int kb = kp / 64;
+  if (c.atmem) {
+    if (2 * c.bn + kp / 2 > 512) return false;        // accumulators + query rows in TMEM
+    return config_smem(c, kb, 0) <= SMEM_LIMIT;
+  }
   return config_smem(c, kb, 1) <= SMEM_LIMIT;
 }
 
 TcConfig tc_default_config(int prec, int d, int kprime) {
   const OpLayout L = op_layout(prec, d);
   const int kpl = kprime <= 32 ? 32 : 64;
-  // widest key tile, deepest pipeline and largest buffer that fit
-  const int bns[4] = {256, 128, 64, 32};
-  for (int bn : bns)
-    for (int stages = 4; stages >= 2; --stages)
-      for (int cb : {32, 16}) {
-        TcConfig c{bn, stages, kpl, cb};
-        if (tc_config_ok(c, L.kp, kprime)) return c;
-      }
-  return TcConfig{64, 2, kpl, 16};
+  // N=256 key tiles first (one MMA costs the same ~186 cycles at N = 64..256, so only N=256
+  // reaches the tensor peak), then the deepest K-atom pipeline and the largest buffer that fit
+  for (int bn : {256, 128, 64, 32})
+    for (int atmem : {0, 1})
+      for (int stages = 6; stages >= 2; --stages)
+        for (int cb : {32, 16}) {
+          TcConfig c{bn, stages, kpl, cb, atmem};
+          if (tc_config_ok(c, L.kp, kprime)) return c;
+        }
+  return TcConfig{64, 2, kpl, 16, 0};
 }
 
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
@@ -564,8 +697,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   MSC_TRY(make_map(&ma, Aop, a_rows, kp, BM, bf16));
   MSC_TRY(make_map(&mb, Bop, b_rows, kp, cfg.bn, bf16));
   TcParams P;
-  P.kb = kp / 64;
   P.ksteps = kmma / 16;
+  P.kb = (P.ksteps + 3) / 4;                           // K atoms the MMAs read
   P.bn = cfg.bn;
   P.stages = cfg.stages;
   P.na = pick_na(cfg, P.kb);
@@ -574,6 +707,11 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.bf16 = bf16;
   P.n_items = int(n_items);
   P.idesc = idesc_f16(bf16, BM, cfg.bn);
+  P.prof = profiling_enabled() ? 1 : 0;
+  P.kp = kp;
+  P.a_tmem = cfg.atmem;
+  P.a_glob = static_cast<const uint32_t*>(Aop);
+  if (P.a_tmem) P.na = 0;
   if (cfg.kpl == 32 && cfg.cb == 16)
     return launch_tc_t<32, 16>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
   if (cfg.kpl == 32 && cfg.cb == 32)

@@ -13,7 +13,7 @@
 #include <cstdio>
 #include <string>
 
-#include "../../include/msc_b200.h"
+#include "msc_b200.h"          // include/ is on the include path
 
 namespace msc {
 

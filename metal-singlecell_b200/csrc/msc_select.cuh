@@ -43,6 +43,7 @@ struct RowSelect {
   int kp;         // k'
   float thr;
   int cnt;
+  int n_hot = 0, n_compact = 0, n_append = 0;   // counters for the pipeline profile
 
   __device__ void bind(void* smem, int row_, int kprime) {
     lv = static_cast<float*>(smem);
@@ -67,12 +68,14 @@ struct RowSelect {
     bv[cnt * ROWS + row] = v;
     bi[cnt * ROWS + row] = col;
     ++cnt;
+    ++n_append;
   }
 
   // This thread's row only (no warp collectives): merge the buffer into the sorted list.
   __device__ __noinline__ void compact_own() {
     const int n = cnt;
     if (n == 0) return;
+    ++n_compact;
     float* B = bv + row;
     int* BI = bi + row;
     float* L = lv + row;
@@ -130,6 +133,7 @@ struct RowSelect {
     const float n2 = min3f(g[6], g[7], g[8]), n3 = fminf(g[9], g[10]);
     const float mn = fminf(min3f(n0, n1, n2), n3);
     if (!__any_sync(FULL, mn < thr)) return;
+    ++n_hot;
 #pragma unroll
     for (int q = 0; q < 11; ++q) {
       if (__any_sync(FULL, g[q] < thr)) {

@@ -38,6 +38,7 @@ SIGNATURES = {
     "msc_launch_count": (ctypes.c_longlong, []),
     "msc_profile_enable": (I32, [I32]),
     "msc_profile_read": (I32, [P, I32]),
+    "msc_profile_counters": (I32, [P, I32]),
     "msc_selftest_wait_timeout": (I32, [I64, P, P]),
     "msc_neighbors_workspace_bytes": (SZ, [I64, I32, I32, I32, I32, I32, I32]),
     "msc_neighbors": (I32, [P, I64, I32, I32, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P, P,

@@ -28,12 +28,13 @@ from .neighbors import _torch, _ids, knn_device, Workspace, DEFAULT_PRECISION
 _TILE_CACHE: dict[str, int] = {}
 
 
-def tile_code(bn: int, stages: int, cb: int) -> int:
-    return int(bn) | (int(stages) << 12) | (int(cb) << 20)
+def tile_code(bn: int, stages: int, cb: int, atmem: int = 0) -> int:
+    return int(bn) | (int(stages) << 12) | (int(cb) << 20) | (int(atmem) << 27)
 
 
 def decode_tile_code(code: int):
-    return {"bn": code & 0xFFF, "stages": (code >> 12) & 0xFF, "cb": (code >> 20) & 0xFF}
+    return {"bn": code & 0xFFF, "stages": (code >> 12) & 0xFF, "cb": (code >> 20) & 0x7F,
+            "atmem": (code >> 27) & 1}
 
 
 class BatchedKnn:
@@ -166,8 +167,8 @@ def autotune(X, offsets, n_neighbors: int = 15, *, metric: str = "euclidean",
             except Exception:
                 pass
     if configs is None:
-        configs = [tile_code(bn, st, cb) for bn in (256, 128, 64, 32) for st in (2, 3, 4)
-                   for cb in (16, 32)]
+        configs = [tile_code(bn, st, cb, am) for am in (1, 0) for bn in (256, 128, 64, 32)
+                   for st in (2, 3, 4) for cb in (16, 32)]
     table = []
     for code in configs:
         try:

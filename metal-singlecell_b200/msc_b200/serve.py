@@ -1,0 +1,223 @@
+"""Continuous-batching request loop for neighbour-graph jobs.
+
+Requests (an embedding plus n_neighbors / metric / method) arrive at any time.  A single scheduler
+thread admits them as soon as an execution slot is free and their device memory fits the HBM
+budget.  Admitted requests run on their own CUDA streams, so the work of requests that arrive
+while others are on the GPU overlaps on the device: small graphs share the SMs, and a large one
+yields slots as its neighbours finish.  Embeddings are uploaded once and results stay in HBM as
+device CSR tensors, ready for GPU consumers; a host copy is optional.
+
+Every request's result is the exact graph, so it does not depend on what else was running
+(``tests/test_gpu_serve.py`` checks alone-vs-mixed equality).  ``run_trace`` replays a Poisson
+arrival trace and reports p50/p99 latency (arrival → result complete on the device) and cells/s;
+``run_offline`` pushes the same requests back to back at full concurrency, the batched-offline
+throughput that the served throughput is compared against.
+"""
+
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .neighbors import _torch, _ids, DEFAULT_PRECISION
+
+
+@dataclass
+class Request:
+    X: object                      # host numpy (n, d) float32, or a CUDA tensor
+    n_neighbors: int = 15
+    metric: str = "euclidean"
+    method: str = "umap"
+    precision: str = DEFAULT_PRECISION
+    to_host: bool = False
+    arrival: float = 0.0           # seconds on the server clock (set by submit)
+    rid: int = -1
+    # filled in by the server
+    admitted: float = 0.0
+    done: float = 0.0
+    result: dict = field(default_factory=dict)
+    error: BaseException | None = None
+    event: threading.Event = field(default_factory=threading.Event)
+
+    @property
+    def n(self) -> int:
+        return int(self.X.shape[0])
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def request_bytes(lib, n, d, k, metric, method, precision) -> int:
+    """Device bytes one request holds while in flight: workspace + input + outputs."""
+    mid, meth, pid = _ids(metric, method, precision)
+    ws = lib.msc_neighbors_workspace_bytes(n, d, k, mid, meth, pid, 0)
+    if ws == 0:
+        return -1
+    m = max(k - 1, 0)
+    outs = n * k * 8 + 2 * (n + 1) * 8 + n * m * 8 + 2 * n * m * 8 + 64
+    return int(ws + n * d * 4 + outs)
+
+
+class GraphServer:
+    """Admission by HBM budget and free slots; one CUDA stream per slot."""
+
+    def __init__(self, hbm_budget: int, slots: int = 8, device=None, poll_s: float = 2e-4):
+        torch = _torch()
+        self.torch = torch
+        self.lib = _lib.load()
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        self.budget = int(hbm_budget)
+        self.slots = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
+        self.free_slots = collections.deque(range(slots))
+        self.pending: collections.deque[Request] = collections.deque()
+        self.inflight: dict[int, tuple[Request, object, int]] = {}
+        self.in_use = 0
+        self.lock = threading.Lock()
+        self.t0 = time.perf_counter()
+        self.completed: list[Request] = []
+        self._next_id = 0
+        self._stop = False
+        self.peak_in_use = 0
+        self.peak_inflight = 0
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def submit(self, req: Request) -> Request:
+        with self.lock:
+            req.arrival = self.now()
+            req.rid = self._next_id
+            self._next_id += 1
+            self.pending.append(req)
+        return req
+
+    def close(self):
+        self._stop = True
+        self._thread.join()
+
+    # -- scheduler ------------------------------------------------------------------------------
+
+    def _start(self, req: Request, slot: int, need: int):
+        torch = self.torch
+        st = self.slots[slot]
+        from .neighbors import neighbors_device
+        with torch.cuda.stream(st):
+            X = req.X
+            if not isinstance(X, torch.Tensor):
+                X = torch.from_numpy(np.ascontiguousarray(X, np.float32))
+            Xd = X.to(self.device, non_blocking=True) if not X.is_cuda else X
+            res = neighbors_device(Xd, req.n_neighbors, metric=req.metric, method=req.method,
+                                   precision=req.precision)
+            res["X"] = Xd
+            if req.to_host:
+                res["host_stats"] = res["stats"].to("cpu", non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        req.result = res
+        req.admitted = self.now()
+        self.inflight[slot] = (req, ev, need)
+
+    def _finish(self, slot: int):
+        req, ev, need = self.inflight.pop(slot)
+        req.done = self.now()
+        try:
+            stats = req.result["stats"].cpu().numpy()
+            _lib.check_stats(stats)
+            if req.to_host:
+                from .neighbors import graph_to_host
+                req.result["host"] = graph_to_host(req.result, req.n, req.n_neighbors)
+        except BaseException as e:      # report per request, keep serving
+            req.error = e
+        self.in_use -= need
+        self.free_slots.append(slot)
+        self.completed.append(req)
+        req.event.set()
+
+    def _loop(self):
+        torch = self.torch
+        torch.cuda.set_device(self.device)
+        while not self._stop or self.pending or self.inflight:
+            progressed = False
+            for slot in list(self.inflight):
+                if self.inflight[slot][1].query():
+                    self._finish(slot)
+                    progressed = True
+            while self.free_slots:
+                with self.lock:
+                    if not self.pending:
+                        break
+                    req = self.pending[0]
+                need = request_bytes(self.lib, req.n, int(req.X.shape[1]), req.n_neighbors,
+                                     req.metric, req.method, req.precision)
+                if need < 0 or need > self.budget:
+                    with self.lock:
+                        self.pending.popleft()
+                    req.error = ValueError(f"request needs {need} bytes > budget {self.budget}")
+                    req.done = self.now()
+                    self.completed.append(req)
+                    req.event.set()
+                    continue
+                if self.in_use + need > self.budget:
+                    break                      # wait for memory to free up (FIFO admission)
+                with self.lock:
+                    self.pending.popleft()
+                slot = self.free_slots.popleft()
+                self.in_use += need
+                self.peak_in_use = max(self.peak_in_use, self.in_use)
+                try:
+                    self._start(req, slot, need)
+                except BaseException as e:
+                    self.in_use -= need
+                    self.free_slots.append(slot)
+                    req.error = e
+                    req.done = self.now()
+                    self.completed.append(req)
+                    req.event.set()
+                    continue
+                self.peak_inflight = max(self.peak_inflight, len(self.inflight))
+                progressed = True
+            if not progressed:
+                time.sleep(2e-4)
+
+
+def _percentile(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else float("nan")
+
+
+def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots: int = 8,
+              device=None) -> dict:
+    """Submit ``reqs`` at ``arrivals`` (seconds from start); wait for all; report latency and
+    throughput."""
+    srv = GraphServer(hbm_budget, slots, device)
+    t_start = srv.now()
+    for r, a in zip(reqs, arrivals):
+        delay = a - (srv.now() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        srv.submit(r)
+    for r in reqs:
+        r.event.wait()
+    srv.close()
+    ok = [r for r in reqs if r.error is None]
+    lat = [r.latency * 1e3 for r in ok]
+    makespan = max(r.done for r in reqs) - t_start
+    cells = sum(r.n for r in ok)
+    return {"requests": len(reqs), "failed": len(reqs) - len(ok),
+            "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
+            "mean_ms": float(np.mean(lat)) if lat else float("nan"),
+            "cells_per_s": cells / makespan, "makespan_s": makespan,
+            "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_in_use}
+
+
+def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None) -> dict:
+    """All requests available at t=0: the batched-offline throughput."""
+    return run_trace(reqs, [0.0] * len(reqs), hbm_budget, slots, device)
