@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <unordered_map>
 
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace msc {
@@ -80,6 +82,7 @@ struct Problem {
   int nseg = 1;
   int64_t npacked = 0;    // packed rows
   int64_t ntiles = 0;     // 128-row query tiles
+  int64_t nptiles = 0;    // 256-row query tiles (CTA-pair work items)
   int64_t max_seg = 0;
   bool candidates = true; // false: every row takes the FP64 scan (k-1 > 64)
   OpLayout L{};
@@ -102,6 +105,9 @@ struct KnnWs {
   int32_t* cand_idx;
   float* cand_thr;
   int32_t* fail_rows;
+  int32_t* perm;          // packed row -> original row (-1: padding)
+  void* order_ws;
+  size_t order_ws_bytes;
 };
 
 int default_kprime(int prec, int k) {
@@ -139,18 +145,20 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
   P.dpad = int(round_up(d, 4));
   if (offsets) {
     if (offsets[0] != 0 || offsets[nseg] != n) { set_error("offsets must run from 0 to n"); return MSC_ERR_INVALID_ARG; }
-    P.npacked = 0; P.ntiles = 0; P.max_seg = 0;
+    P.npacked = 0; P.ntiles = 0; P.nptiles = 0; P.max_seg = 0;
     for (int s = 0; s < nseg; ++s) {
       const int64_t ns = offsets[s + 1] - offsets[s];
       if (ns < k) { set_error("sample %d has %lld cells < n_neighbors=%d", s, (long long)ns, k); return MSC_ERR_INVALID_ARG; }
       P.npacked += round_up(ns, SEG_PAD);
       P.ntiles += ceil_div(ns, QTILE);
+      P.nptiles += ceil_div(ns, 2 * QTILE);
       P.max_seg = std::max(P.max_seg, ns);
     }
   } else {
     if (n < k) { set_error("n_neighbors=%d > n=%lld", k, (long long)n); return MSC_ERR_INVALID_ARG; }
     P.npacked = round_up(n, SEG_PAD);
     P.ntiles = ceil_div(n, QTILE);
+    P.nptiles = ceil_div(n, 2 * QTILE);
     P.max_seg = n;
   }
   if (P.npacked >= (int64_t(1) << 31)) { set_error("too many packed rows"); return MSC_ERR_UNSUPPORTED; }
@@ -188,16 +196,38 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
   w.cand_idx = c.take<int32_t>(size_t(P.n) * P.kprime);
   w.cand_thr = c.take<float>(P.n);
   w.fail_rows = c.take<int32_t>(P.n);
+  w.perm = c.take<int32_t>(P.npacked);
+  w.order_ws_bytes = order_workspace_bytes(P.npacked);
+  w.order_ws = c.take<unsigned char>(w.order_ws_bytes);
   return w;
+}
+
+// Levels of the locality tree (order.cu) for the tensor-core path: enough halvings to bring the
+// largest sample to leaves of ORDER_LEAF rows, plus slack for uneven splits.  The FP32 SIMT kernel
+// scans keys in plain order, so it keeps the identity order.  MSC_B200_ORDER=0 turns it off.
+constexpr int ORDER_LEAF = 256;
+int order_levels(const Problem& P, bool tc) {
+  if (!tc || P.max_seg <= 2 * ORDER_LEAF) return 0;
+  const char* env = std::getenv("MSC_B200_ORDER");
+  if (env && *env == '0') return 0;
+  int l = 0;
+  while ((int64_t(ORDER_LEAF) << l) < P.max_seg) ++l;
+  return std::min(28, l + 4);
 }
 
 int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
   cfg = tc_default_config(P.prec, P.d, P.kprime);
+  if (code == 0) {
+    // tuning override for the automatic choice (same encoding as tile_config)
+    const char* env = std::getenv("MSC_B200_TILE_CONFIG");
+    if (env && *env) code = int32_t(std::strtol(env, nullptr, 0));
+  }
   if (code == 0) return MSC_OK;
   TcConfig c{code & 0xfff, (code >> 12) & 0xff, P.kprime <= 32 ? 32 : 64, (code >> 20) & 0x7f,
-             (code >> 27) & 1};
+             (code >> 27) & 1 ? 8 : 4, (code >> 28) & 1};
   if (!tc_config_ok(c, P.L.kp, P.kprime)) {
-    set_error("tile_config 0x%x (bn=%d stages=%d cb=%d) is not valid here", code, c.bn, c.stages, c.cb);
+    set_error("tile_config 0x%x (bn=%d stages=%d cb=%d epi=%d pair=%d) is not valid here", code,
+              c.bn, c.stages, c.cb, c.epi, c.pair);
     return MSC_ERR_INVALID_ARG;
   }
   cfg = c;
@@ -219,41 +249,47 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
     MSC_TRY(launch_normalize(X, w.Xn, P.n, P.d, &w.ctl->stats[MSC_STAT_NONFINITE], st));
     Xu = w.Xn;
   }
-  MSC_TRY(launch_build_items(w.seg, P.nseg, P.ntiles, w.items, w.ctl, st));
+  const bool tc = P.candidates && P.k > 1 && P.prec != PREC_FP32;
+  TcConfig cfg{};
+  if (tc) MSC_TRY(decode_tile_config(tile_code, P, cfg));
+  const bool pair_items = tc && cfg.pair;
+  const int64_t n_items = pair_items ? P.nptiles : P.ntiles;
+  MSC_TRY(launch_build_items(w.seg, P.nseg, n_items, pair_items ? 2 * QTILE : QTILE, w.items, w.ctl,
+                             st));
+  MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc), ORDER_LEAF,
+                       w.perm, w.order_ws, w.order_ws_bytes, st));
   if (!P.candidates) {
-    MSC_TRY(launch_all_rows_fail(w.seg, P.nseg, P.npacked, w.fail_rows, w.ctl, st));
-    MSC_TRY(launch_fp64_scan(Xu, P.d, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine, knn_idx,
-                             knn_dist, w.ctl, st));
+    MSC_TRY(launch_all_rows_fail(w.perm, P.npacked, w.fail_rows, w.ctl, st));
+    MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
+                             knn_idx, knn_dist, w.ctl, st));
     return MSC_OK;
   }
   MSC_TRY(launch_colmean(Xu, w.seg, P.nseg, P.max_seg, P.d, w.partial, COLMEAN_NB, w.mean,
                          cosine ? nullptr : &w.ctl->stats[MSC_STAT_NONFINITE], st));
   if (P.k > 1) {
     if (P.prec == PREC_FP32) {
-      MSC_TRY(launch_pack_fp32(Xu, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked, w.A32, w.sq32,
-                               w.qs, w.km, st));
+      MSC_TRY(launch_pack_fp32(Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked, w.A32,
+                               w.sq32, w.qs, w.km, st));
       stage_mark(st, 1);
-      MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.ctl, P.kprime,
-                              w.cand_idx, w.cand_thr, P.kprime, st));
+      MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
+                              P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
     } else {
       if (P.prec == PREC_FP16)
         MSC_TRY(launch_maxnorm(Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.ctl, st));
-      MSC_TRY(launch_pack_tc(P.prec, Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.Aop, w.Bop,
-                             w.qs, w.km, w.ctl, st));
-      TcConfig cfg;
-      MSC_TRY(decode_tile_config(tile_code, P, cfg));
+      MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked, w.Aop,
+                             w.Bop, w.qs, w.km, w.ctl, st));
       stage_mark(st, 1);
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
-                            w.items, P.ntiles, w.ctl, P.kprime, w.cand_idx, w.cand_thr,
+                            w.items, n_items, w.perm, w.ctl, P.kprime, w.cand_idx, w.cand_thr,
                             P.kprime, st));
     }
   }
   stage_mark(st, 2);
-  MSC_TRY(launch_rerank(Xu, P.d, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr, P.kprime,
-                        P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx, knn_dist,
-                        w.fail_rows, w.ctl, st));
-  MSC_TRY(launch_fp64_scan(Xu, P.d, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine, knn_idx,
-                           knn_dist, w.ctl, st));
+  MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
+                        P.kprime, P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx,
+                        knn_dist, w.fail_rows, w.ctl, st));
+  MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
+                           knn_idx, knn_dist, w.ctl, st));
   stage_mark(st, 3);
   return MSC_OK;
 }
@@ -481,7 +517,7 @@ int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t 
     return offsets_host[a + 1] - offsets_host[a] > offsets_host[b + 1] - offsets_host[b];
   });
   std::vector<SegDesc> segs(n_samples);
-  int64_t poff = 0, tile = 0;
+  int64_t poff = 0, tile = 0, ptile = 0;
   for (int r = 0; r < n_samples; ++r) {
     const int s = order[r];
     SegDesc sd{};
@@ -490,10 +526,12 @@ int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t 
     sd.poff = poff;
     sd.padlen = round_up(sd.n, SEG_PAD);
     sd.tile0 = tile;
+    sd.ptile0 = ptile;
     sd.ntiles = ceil_div(sd.n, QTILE);
     segs[r] = sd;
     poff += sd.padlen;
     tile += sd.ntiles;
+    ptile += ceil_div(sd.n, 2 * QTILE);
   }
   cudaStream_t st = as_stream(stream);
   MSC_CUDA_TRY(cudaMemcpyAsync(w.seg, segs.data(), sizeof(SegDesc) * n_samples,

@@ -430,4 +430,10 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
   return MSC_OK;
 }
 
+// exclusive scan of n int32 values into n + 1 int64 values (out[n] = total), deterministic
+size_t scan_i32_scratch_elems(int64_t n) { return scan_scratch_elems(n); }
+int scan_excl_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream_t st) {
+  return scan_excl<int32_t>(in, n, out, scratch, st);
+}
+
 }  // namespace msc

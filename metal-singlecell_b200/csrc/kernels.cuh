@@ -24,7 +24,8 @@ struct SegDesc {
   int64_t padlen;   // packed rows (n rounded up to SEG_PAD)
   int64_t tile0;    // index of the sample's first 128-row query tile
   int64_t ntiles;   // query tiles of the sample
-  int64_t pad0, pad1;
+  int64_t ptile0;   // index of the sample's first 256-row query tile (CTA-pair work items)
+  int64_t pad1;
 };
 
 __device__ __forceinline__ int find_seg(const SegDesc* seg, int nseg, int64_t p) {
@@ -62,20 +63,29 @@ int launch_colmean(const float* X, const SegDesc* seg, int nseg, int64_t max_seg
 size_t colmean_partial_elems(int nseg, int d, int nb);
 int launch_maxnorm(const float* X, const SegDesc* seg, int nseg, const double* mean, int d,
                    int64_t npacked, Ctl* ctl, cudaStream_t st);
-int launch_pack_tc(int prec, const float* X, const SegDesc* seg, int nseg, const double* mean,
-                   int d, int64_t npacked, void* Aop, void* Bop, QStat* qs, KeyMax* km,
-                   const Ctl* ctl, cudaStream_t st);
-int launch_pack_fp32(const float* X, const SegDesc* seg, int nseg, const double* mean, int d,
-                     int dpad, int64_t npacked, float* A32, float* sq32, QStat* qs, KeyMax* km,
-                     cudaStream_t st);
+// packed row p holds original row perm[p] (-1: padding) of the sample seg[find_seg(p)]
+int launch_pack_tc(int prec, const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
+                   const double* mean, int d, int64_t npacked, void* Aop, void* Bop, QStat* qs,
+                   KeyMax* km, const Ctl* ctl, cudaStream_t st);
+int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
+                     const double* mean, int d, int dpad, int64_t npacked, float* A32, float* sq32,
+                     QStat* qs, KeyMax* km, cudaStream_t st);
+// locality order (order.cu): perm[p] for every packed row, cells of a sample permuted so that
+// near cells are near in packed order; levels = 0 gives the identity order
+size_t order_workspace_bytes(int64_t npacked);
+int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
+                 int leaf, int32_t* perm, void* ws, size_t ws_bytes, cudaStream_t st);
+size_t scan_i32_scratch_elems(int64_t n);
+int scan_excl_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream_t st);
 int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st);
-int launch_build_items(const SegDesc* seg, int nseg, int64_t ntiles_total, WorkItem* items,
+// one work item per `rows` (128 or 256) query rows of every sample
+int launch_build_items(const SegDesc* seg, int nseg, int64_t n_items, int rows, WorkItem* items,
                        Ctl* ctl, cudaStream_t st);
 
 // ---- knn_fp32.cu ----
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
-                    int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
-                    int cand_stride, cudaStream_t st);
+                    int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
+                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
 
 // ---- knn_tc.cu ----
 struct TcConfig {
@@ -83,7 +93,8 @@ struct TcConfig {
   int stages;    // smem pipeline depth of the key tiles
   int kpl;       // selector list length (32 / 64)
   int cb;        // selector buffer (16 / 32)
-  int atmem;     // 1: query operand in tensor memory, 0: in shared memory
+  int epi;       // epilogue warps: 4 (one per TMEM lane quarter) or 8 (two, splitting the columns)
+  int pair;      // 1: CTA pairs (cta_group::2, M=256, each CTA stages half of every key tile)
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
 int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st);
@@ -93,18 +104,19 @@ bool profiling_enabled();
 TcConfig tc_default_config(int prec, int d, int kprime);
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
-                  int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
-                  int cand_stride, cudaStream_t st);
+                  int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
+                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
 
 // ---- rerank.cu ----
-int launch_rerank(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
+int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
+                  int64_t npacked,
                   const int32_t* cand_idx, const float* cand_thr, int cand_stride, int kprime,
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
                   cudaStream_t st);
-int launch_all_rows_fail(const SegDesc* seg, int nseg, int64_t npacked, int32_t* fail_rows,
-                         Ctl* ctl, cudaStream_t st);
-int launch_fp64_scan(const float* X, int d, const SegDesc* seg, int nseg,
+int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
+                         cudaStream_t st);
+int launch_fp64_scan(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
                      const int32_t* fail_rows, int64_t max_rows, int k, int cosine,
                      int32_t* knn_idx, float* knn_dist, Ctl* ctl, cudaStream_t st);
 

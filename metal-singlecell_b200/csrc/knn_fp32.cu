@@ -33,8 +33,9 @@ struct FpSmem {
 template <int KPL, int CB>
 __global__ void __launch_bounds__(F_THREADS, 1)
 knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, int dpad,
-                const WorkItem* __restrict__ items, Ctl* __restrict__ ctl, int kprime,
-                int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr, int cand_stride) {
+                const WorkItem* __restrict__ items, const int32_t* __restrict__ perm,
+                Ctl* __restrict__ ctl, int kprime, int32_t* __restrict__ cand_idx,
+                float* __restrict__ cand_thr, int cand_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* As = reinterpret_cast<float*>(smem_raw);
   float* Bs = As + size_t(dpad) * F_BM;
@@ -85,8 +86,9 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
     };
     if (tid >= F_BM) load_b(0, 0);
     __syncthreads();
-    const int self_base = w.qorig0;
-    const int limit = w.orig_off + w.nkeys;
+    // neighbour ids are packed positions here; finish() maps them to original rows
+    const int self_base = w.qrow0;
+    const int limit = w.key0 + w.nkeys;
     for (int kt = 0; kt < nkt; ++kt) {
       const int buf = kt & 1;
       const float* B = Bs + size_t(buf) * dpad * F_BN;
@@ -118,7 +120,7 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       }
       __syncthreads();
       if (selector) {
-        const int col0 = w.orig_off + kt * F_BN;
+        const int col0 = w.key0 + kt * F_BN;
 #pragma unroll
         for (int h = 0; h < F_BN; h += 32) {
           float v[32];
@@ -138,7 +140,7 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       const int wrow0 = tid & ~31;
       const int nvalid = min(32, w.nq - wrow0);
       if (nvalid > 0)
-        sel.finish(cand_idx, cand_thr, cand_stride, int64_t(w.qorig0) + wrow0, nvalid, kprime);
+        sel.finish(cand_idx, cand_thr, cand_stride, perm, int64_t(w.qrow0) + wrow0, nvalid, kprime);
       else
         sel.flush();
     }
@@ -148,15 +150,15 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
 
 template <int KPL, int CB>
 int launch_fp32_t(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
-                  int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
-                  int cand_stride, cudaStream_t st) {
+                  int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime, int32_t* cand_idx,
+                  float* cand_thr, int cand_stride, cudaStream_t st) {
   (void)d;
   const size_t smem = FpSmem<KPL, CB>::bytes(dpad);
   auto kern = knn_fp32_kernel<KPL, CB>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(smem)));
   int grid = int(std::min<int64_t>(n_items, num_sms()));
-  kern<<<std::max(grid, 1), F_THREADS, smem, st>>>(A32, sq32, dpad, items, ctl, kprime,
+  kern<<<std::max(grid, 1), F_THREADS, smem, st>>>(A32, sq32, dpad, items, perm, ctl, kprime,
                                                    cand_idx, cand_thr, cand_stride);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
@@ -165,13 +167,13 @@ int launch_fp32_t(const float* A32, const float* sq32, int d, int dpad, const Wo
 }  // namespace
 
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
-                    int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
-                    int cand_stride, cudaStream_t st) {
+                    int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
+                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st) {
   if (kprime <= 32)
-    return launch_fp32_t<32, 32>(A32, sq32, d, dpad, items, n_items, ctl, kprime, cand_idx,
+    return launch_fp32_t<32, 32>(A32, sq32, d, dpad, items, n_items, perm, ctl, kprime, cand_idx,
                                  cand_thr, cand_stride, st);
   if (kprime <= 64)
-    return launch_fp32_t<64, 32>(A32, sq32, d, dpad, items, n_items, ctl, kprime, cand_idx,
+    return launch_fp32_t<64, 32>(A32, sq32, d, dpad, items, n_items, perm, ctl, kprime, cand_idx,
                                  cand_thr, cand_stride, st);
   set_error("kprime=%d > 64 is not supported by the candidate kernels", kprime);
   return MSC_ERR_UNSUPPORTED;

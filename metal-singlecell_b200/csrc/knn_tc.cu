@@ -4,16 +4,29 @@
 // `sq_i + sq_j − 2·X_i·X_jᵀ` materialised as a block×n matrix in device memory, then the
 // `topk_rows` register kernel (neighbors.py:25-79) scanning it.  Here the n×n matrix never leaves
 // the SM: a 128-row query tile stays in shared memory, key tiles stream through a TMA pipeline,
-// one thread issues tcgen05.mma into a double-buffered FP32 accumulator in tensor memory, and four
+// one thread issues tcgen05.mma into a double-buffered FP32 accumulator in tensor memory, and the
 // epilogue warps read the accumulator (TMEM lane i = query row i) straight into the per-row
 // selector while the next tile's MMAs run.  The key norms are folded into the key operand, so the
 // accumulator already holds the ranking value v = |y|² − 2x·y.
 //
-// Roles (256 threads, one CTA per SM, persistent over 128-row query tiles):
+// Roles (128 + 32·NEPI threads, one CTA per SM, persistent over query tiles):
 //   warp 0  TMA producer      A tile once per query tile, then the key tiles of its sample
-//   warp 1  MMA issuer        KSTEPS × tcgen05.mma (M=128, N=BN, K=16) per key tile
+//   warp 1  MMA issuer        KSTEPS × tcgen05.mma (K=16) per key tile
 //   warp 2  TMEM allocator    2·BN columns for two accumulators
-//   warps 4-7 epilogue        tcgen05.ld 32x32b → filter → selector; release the accumulator
+//   warp 3  relay (pairs)     forwards the odd CTA's completed loads to the even CTA
+//   warps 4.. epilogue        tcgen05.ld 32x32b → filter → selector; release the accumulator.
+//                             NEPI = 4: one warp per TMEM lane quarter reads all BN columns;
+//                             NEPI = 8: two warps per lane quarter read BN/2 columns each.
+//
+// CTA pairs (PAIR): a cluster of two CTAs computes a 256-row query tile against BN-key tiles with
+// tcgen05.mma.cta_group::2 (M=256).  Each CTA stages its own 128 query rows and HALF of every key
+// tile (BN/2 rows) in its own shared memory; the even CTA issues the MMAs, which read both halves,
+// and each CTA's tensor memory receives its 128 rows × BN accumulator.  Key bytes per SM and per
+// FLOP are halved, and the pipeline holds twice as many K-atom stages in the same shared memory.
+// Every TMA load signals a barrier of the CTA that issued it, so each CTA can drain its own
+// copies; the odd CTA's relay thread forwards those completions to the even CTA (remote mbarrier
+// arrive), and the even CTA's commits reach both CTAs through tcgen05.commit's CTA mask.
+//
 // Every mbarrier wait is bounded (wall-clock, via %globaltimer); a wait that gives up raises an
 // abort flag that every role polls, the kernel records MSC_STAT_TIMEOUT and all roles leave their
 // loops, so a fault in the pipeline returns an error instead of hanging the GPU.
@@ -26,7 +39,6 @@ namespace msc {
 
 namespace {
 
-constexpr int TC_THREADS = 256;
 constexpr int EPI_WARP0 = 4;
 constexpr int BM = 128;
 constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
@@ -126,30 +138,6 @@ __device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
-// same, with the A operand in tensor memory (M lanes × K columns, two 16-bit elements per column)
-__device__ __forceinline__ void umma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
-                                            uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
-      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
-      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
-      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
-      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
-      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
-      "r"(r[29]), "r"(r[30]), "r"(r[31])
-      : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -182,32 +170,103 @@ __device__ __forceinline__ void tmem_wait(uint32_t (&r)[32]) {
                :
                : "memory");
 }
-// orders later uses of r after a preceding tmem_wait (the statement is empty; the registers are
-// declared modified, and volatile asm is never moved across the wait)
-__device__ __forceinline__ void tmem_dep(uint32_t (&r)[32]) {
-  asm volatile(""
-               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
-                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
-                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
-                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
-                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
-                 "+r"(r[30]), "+r"(r[31]));
+
+// --- CTA-pair forms ------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
+// address of the same shared-memory variable in cluster CTA `rank`
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+// try_wait with cluster-scope acquire, for barriers that the partner CTA arrives at
+__device__ __forceinline__ bool mbar_test_cl(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __noinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
+                                               volatile int* abort_flag) {
+  const uint64_t t0 = globaltimer();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_test_cl(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if ((it & 255) == 0 && globaltimer() - t0 > WAIT_LIMIT_NS) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ bool mbar_wait_cl(uint64_t* bar, uint32_t parity,
+                                             volatile int* abort_flag) {
+  if (mbar_test_cl(bar, parity)) return true;
+  return mbar_wait_cl_slow(bar, parity, abort_flag);
+}
+template <bool PAIR>
+__device__ __forceinline__ void tmem_alloc_g(uint32_t* dst, uint32_t ncols) {
+  if (PAIR)
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(dst)),
+                 "r"(ncols));
+  else
+    tmem_alloc(dst, ncols);
+}
+template <bool PAIR>
+__device__ __forceinline__ void tmem_relinquish_g() {
+  if (PAIR) asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+  else tmem_relinquish();
+}
+template <bool PAIR>
+__device__ __forceinline__ void tmem_dealloc_g(uint32_t taddr, uint32_t ncols) {
+  if (PAIR)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+  else
+    tmem_dealloc(taddr, ncols);
+}
+template <bool PAIR>
+__device__ __forceinline__ void umma_f16_g(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate) {
+  if (PAIR)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+  else
+    umma_f16(tmem_d, adesc, bdesc, idesc, accumulate);
+}
+// commit: arrive at `bar` when the MMAs issued so far are complete — in a pair, at the barrier of
+// the same offset in both CTAs
+template <bool PAIR>
+__device__ __forceinline__ void umma_commit_g(uint64_t* bar) {
+  if (PAIR) {
+    const uint16_t both = 3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+        " [%0], %1;" ::"r"(smem_u32(bar)),
+        "h"(both)
+        : "memory");
+  } else {
+    umma_commit(bar);
+  }
 }
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
@@ -238,10 +297,28 @@ struct TcParams {
   int n_items;
   uint32_t idesc;
   int prof;         // accumulate the pipeline counters below
-  int a_tmem;       // 1: the query tile lives in tensor memory (loaded by the epilogue warps)
-  const uint32_t* a_glob;   // packed query operand (A-in-TMEM mode): rows of kp 16-bit elements
-  int kp;           // elements per packed row
+  const int32_t* perm;   // packed position -> original row (-1: padding)
 };
+
+// Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
+// around it (diag, diag+1, diag-1, diag+2, diag-2, clipped to the sample), then all other tiles
+// in plain order.  With the cells in locality order the near tiles hold most of the rows' true
+// neighbours, so the thresholds fall close to their final values at once; the plain sweep after
+// them is the same for every query tile, so the CTAs stream the keys through L2 together.
+constexpr int NEAR_SIDE = 2;
+__device__ __forceinline__ int key_tile_at(int j, int diag, int nkt) {
+  const int lo = max(0, diag - NEAR_SIDE), hi = min(nkt - 1, diag + NEAR_SIDE);
+  const int np = hi - lo + 1;
+  if (j >= np) {
+    const int t = j - np;
+    return t < lo ? t : t + np;
+  }
+  const int left = diag - lo, right = hi - diag;
+  const int m = min(left, right);
+  if (j == 0) return diag;
+  if (j <= 2 * m) return (j & 1) ? diag + ((j + 1) >> 1) : diag - (j >> 1);
+  return right > left ? diag + (j - m) : diag - (j - m);
+}
 
 // Pipeline counters (cycles / events summed over CTAs), filled when profiling is enabled:
 //   0 producer waiting for a free key stage     1 MMA waiting for a loaded key tile
@@ -251,64 +328,88 @@ struct TcParams {
 __device__ unsigned long long g_tc_prof[16];
 
 struct SmemPlan {
-  size_t a_off, b_off, sel_off, bar_off, total;
+  size_t a_off, b_off, sel_off, pub_off, bar_off, total;
 };
+// brows = key rows this CTA stages per tile (BN, or BN/2 in a CTA pair);
+// nh = column groups per TMEM lane quarter (1: four epilogue warps, 2: eight)
 template <int KPL, int CB>
-__host__ __device__ inline SmemPlan smem_plan(int kb, int bn, int stages, int na) {
+__host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int na, int nh) {
   SmemPlan p;
   p.a_off = 0;
   p.b_off = p.a_off + size_t(na) * kb * BM * 128;
-  p.sel_off = p.b_off + size_t(stages) * bn * 128;
-  p.bar_off = p.sel_off + RowSelect<KPL, CB, BM>::smem_bytes();
-  p.total = p.bar_off + 256 + 1024;          // barriers + slack for 1024-byte alignment
+  p.sel_off = p.b_off + size_t(stages) * brows * 128;
+  p.pub_off = p.sel_off + size_t(nh) * RowSelect<KPL, CB, BM>::smem_bytes();
+  p.bar_off = p.pub_off + (nh > 1 ? size_t(2) * BM * sizeof(float) : 0);
+  p.total = p.bar_off + 512 + 1024;          // barriers + slack for 1024-byte alignment
   return p;
 }
 
-template <int KPL, int CB>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+// NEPI epilogue warps: 4 (one per TMEM lane quarter, all columns of a tile) or 8 (two per lane
+// quarter, each filtering half of the columns into its own list; the two lists of a row share
+// their thresholds while filtering and are merged when the query tile is done).
+// PAIR: two-CTA clusters, 256-row work items (see the file comment).
+template <int KPL, int CB, int NEPI, bool PAIR>
+__global__ void __launch_bounds__(128 + 32 * NEPI, 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const TcParams P, const WorkItem* __restrict__ items, Ctl* __restrict__ ctl,
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
+  static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
+  constexpr int NH = NEPI / 4;
+  using Sel = RowSelect<KPL, CB, BM>;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
-  const SmemPlan sp = smem_plan<KPL, CB>(P.kb, P.bn, P.stages, P.na);
+  const int brows = PAIR ? P.bn / 2 : P.bn;            // key rows this CTA stages per tile
+  const SmemPlan sp = smem_plan<KPL, CB>(P.kb, brows, P.stages, P.na, NH);
   unsigned char* Asm = smem + sp.a_off;
   unsigned char* Bsm = smem + sp.b_off;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + sp.bar_off);
-  uint64_t* a_full = bars;                 // [2]
+  uint64_t* a_full = bars;                 // [2] this CTA's query rows landed
   uint64_t* a_empty = bars + 2;            // [2]
   uint64_t* acc_full = bars + 4;           // [2]
   uint64_t* acc_empty = bars + 6;          // [2]
   uint64_t* done_bar = bars + 8;           // [1]
-  uint64_t* b_full = bars + 9;             // [stages <= 8]
+  uint64_t* b_full = bars + 9;             // [stages <= 8] this CTA's key rows landed
   uint64_t* b_empty = bars + 17;           // [stages <= 8]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 25);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 26);   // 27 x 8 B < 256 B
+  uint64_t* qbar = bars + 25;              // [4] the two epilogue warps of a lane quarter
+  uint64_t* a_peer = bars + 29;            // [2] pair: the odd CTA's query rows landed
+  uint64_t* b_peer = bars + 31;            // [stages <= 8] pair: the odd CTA's key rows landed
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 39);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 40);   // 41 x 8 B < 512 B
+  float* pub = reinterpret_cast<float*>(smem + sp.pub_off);
 
   const int warp = warp_id(), lane = lane_id();
+  const uint32_t rank = PAIR ? cluster_ctarank() : 0u;
+  const bool leader = rank == 0;
+  const int unit = PAIR ? int(blockIdx.x >> 1) : int(blockIdx.x);
+  const int nunits = PAIR ? int(gridDim.x >> 1) : int(gridDim.x);
   const size_t a_bytes = size_t(P.kb) * BM * 128;
-  const size_t b_bytes = size_t(P.bn) * 128;            // one K atom of a key tile
-  const uint32_t tmem_cols = P.a_tmem ? 512u : uint32_t(2 * P.bn);
+  const size_t b_bytes = size_t(brows) * 128;           // one K atom of this CTA's key rows
+  const uint32_t tmem_cols = uint32_t(2 * P.bn);
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2; ++i) {
-      mbar_init(&a_full[i], P.a_tmem ? 4 : 1);
+      mbar_init(&a_full[i], 1);
       mbar_init(&a_empty[i], 1);
       mbar_init(&acc_full[i], 1);
-      mbar_init(&acc_empty[i], 4);
+      mbar_init(&acc_empty[i], PAIR ? 2 * NEPI : NEPI);
+      mbar_init(&a_peer[i], 1);
     }
     mbar_init(done_bar, 1);
     for (int s = 0; s < P.stages; ++s) {
       mbar_init(&b_full[s], 1);
       mbar_init(&b_empty[s], 1);
+      mbar_init(&b_peer[s], 1);
     }
+    for (int q = 0; q < 4; ++q) mbar_init(&qbar[q], 2);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (NH > 1)
+    for (int i = threadIdx.x; i < 2 * BM; i += blockDim.x) pub[i] = F_INF;
   if (warp == 2) {
-    tmem_alloc(tmem_slot, tmem_cols);
-    tmem_relinquish();
+    tmem_alloc_g<PAIR>(tmem_slot, tmem_cols);
+    tmem_relinquish_g<PAIR>();
   }
   if (warp == 0 && lane == 0) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
@@ -316,37 +417,39 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   }
   tc_fence_before();
   __syncthreads();
+  if (PAIR) cluster_sync();               // the partner's barriers exist before any remote arrive
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const long long t_kernel0 = clock64();
 
   if (warp == 0) {
-    // ------------------------------------------------------------------ TMA producer
+    // ------------------------------------------------------------------ TMA producer (each CTA)
     if (lane == 0) {
       int stage = 0, abuf = 0;
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
       long long c_wait = 0;
-      for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+      for (int it = unit; it < P.n_items && ok; it += nunits) {
         const WorkItem w = items[it];
-        if (!P.a_tmem) {
-          ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
-          if (!ok) break;
-          mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
-          for (int kb = 0; kb < P.kb; ++kb)
-            tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf],
-                        kb * 64, w.qrow0);
-          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        }
+        ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
+        if (!ok) break;
+        mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
+        for (int kb = 0; kb < P.kb; ++kb)
+          tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
+                      w.qrow0 + int(rank) * BM);
+        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
         const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        for (int kt = 0; kt < nkt && ok; ++kt) {
+        const int diag = (w.qrow0 - w.key0) / P.bn;
+        for (int j = 0; j < nkt && ok; ++j) {
+          const int kt = key_tile_at(j, diag, nkt);
           for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
             const long long tw = P.prof ? clock64() : 0;
             ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
             if (P.prof) c_wait += clock64() - tw;
             if (!ok) break;
             mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
-            tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64, w.key0 + kt * P.bn);
+            tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
+                        w.key0 + kt * P.bn + int(rank) * brows);
             if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
         }
@@ -358,28 +461,52 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         const uint32_t par = s < stage ? sphase : (sphase ^ 1);
         (void)mbar_drain(&b_full[s], par);
       }
-      for (int a = 0; a < P.na && !P.a_tmem; ++a) {
+      for (int a = 0; a < P.na; ++a) {
         const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
         (void)mbar_drain(&a_full[a], par);
       }
     }
+  } else if (warp == 3) {
+    // ------------------------------------------------------------------ relay (odd CTA of a pair)
+    if (PAIR && !leader && lane == 0) {
+      int stage = 0, abuf = 0;
+      uint32_t sphase = 0, aphase = 0;
+      bool ok = true;
+      for (int it = unit; it < P.n_items && ok; it += nunits) {
+        const WorkItem w = items[it];
+        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+        if (!ok) break;
+        mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
+        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
+        for (int kt = 0; kt < nkt && ok; ++kt) {
+          for (int kb = 0; kb < P.kb; ++kb) {
+            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+            if (!ok) break;
+            mbar_arrive_remote(mapa_shared(smem_u32(&b_peer[stage]), 0));
+            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+          }
+        }
+      }
+    }
   } else if (warp == 1) {
-    // ------------------------------------------------------------------ MMA issuer
-    if (lane == 0) {
+    // ------------------------------------------------------------------ MMA issuer (even CTA)
+    if (leader && lane == 0) {
       int stage = 0, abuf = 0, acc = 0;
       uint32_t sphase = 0, aphase = 0, accphase = 0;
       bool ok = true, issued = false;
       long long c_b = 0, c_acc = 0;
-      for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+      for (int it = unit; it < P.n_items && ok; it += nunits) {
         const WorkItem w = items[it];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+        if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
         if (!ok) break;
-        const uint32_t a_base = P.a_tmem ? 0u : smem_u32(Asm + abuf * a_bytes);
-        const uint32_t a_tcol = tmem_base + uint32_t(2 * P.bn);   // A columns in TMEM
+        const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
         const int nkt = (w.nkeys + P.bn - 1) / P.bn;
         for (int kt = 0; kt < nkt && ok; ++kt) {
           const long long t2 = P.prof ? clock64() : 0;
-          ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+          ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
+                    : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
           if (P.prof) c_acc += clock64() - t2;
           if (!ok) break;
           tc_fence_after();
@@ -387,98 +514,96 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           for (int kb = 0; kb < P.kb; ++kb) {
             const long long t1 = P.prof ? clock64() : 0;
             ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+            if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
             if (P.prof) c_b += clock64() - t1;
             if (!ok) break;
             const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
             const int ks1 = min(P.ksteps, 4 * kb + 4);
             for (int ks = 4 * kb; ks < ks1; ++ks) {
-              const uint32_t bo = uint32_t((ks & 3) * 32);
-              if (P.a_tmem) {
-                umma_f16_ts(d_tmem, a_tcol + uint32_t(ks * 8), sdesc(b_base + bo), P.idesc,
-                            ks > 0 ? 1u : 0u);
-              } else {
-                const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
-                umma_f16(d_tmem, sdesc(a_base + ao), sdesc(b_base + bo), P.idesc,
-                         ks > 0 ? 1u : 0u);
-              }
+              const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
+              umma_f16_g<PAIR>(d_tmem, sdesc(a_base + ao), sdesc(b_base + uint32_t((ks & 3) * 32)),
+                               P.idesc, ks > 0 ? 1u : 0u);
             }
-            umma_commit(&b_empty[stage]);
+            umma_commit_g<PAIR>(&b_empty[stage]);
             if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
           if (!ok) break;
           issued = true;
-          umma_commit(&acc_full[acc]);
+          umma_commit_g<PAIR>(&acc_full[acc]);
           if (++acc == 2) { acc = 0; accphase ^= 1; }
         }
         if (!ok) break;
-        umma_commit(&a_empty[abuf]);
-        if (++abuf == (P.a_tmem ? 1 : P.na)) { abuf = 0; aphase ^= 1; }
+        umma_commit_g<PAIR>(&a_empty[abuf]);
+        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
       }
-      if (issued) umma_commit(done_bar);
-      else mbar_arrive(done_bar);
+      if (issued) {
+        umma_commit_g<PAIR>(done_bar);
+      } else {
+        mbar_arrive(done_bar);
+        if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
+      }
       if (P.prof) {
         atomicAdd(&g_tc_prof[1], (unsigned long long)c_b);
         atomicAdd(&g_tc_prof[2], (unsigned long long)c_acc);
       }
     }
   } else if (warp >= EPI_WARP0) {
-    // ------------------------------------------------------------------ epilogue
-    const int q = warp - EPI_WARP0;               // TMEM lane quarter
+    // ------------------------------------------------------------------ epilogue (each CTA)
+    const int q = warp & 3;                        // TMEM lane quarter this warp may access
+    const int h = (warp - EPI_WARP0) >> 2;         // column group
     const int row = q * 32 + lane;
-    RowSelect<KPL, CB, BM> sel;
-    sel.bind(smem + sp.sel_off, row, P.kprime);
+    Sel sel;
+    sel.bind(smem + sp.sel_off + size_t(h) * Sel::smem_bytes(), row, P.kprime);
+    if (NH > 1) {
+      sel.pub_own = pub + h * BM + row;
+      sel.pub_other = pub + (1 - h) * BM + row;
+    }
+    sel.reset();
+    const int gcols = P.bn / NH;                   // accumulator columns of this group
+    const int nch = gcols / 32;
     int acc = 0;
-    uint32_t accphase = 0;
+    uint32_t accphase = 0, qphase = 0;
     bool ok = true;
     long long c_ew = 0, c_loop = 0;
-    uint32_t aphase_e = 0;
-    for (int it = blockIdx.x; it < P.n_items && ok; it += gridDim.x) {
+    // the two warps of a lane quarter meet here (bounded, abort-aware)
+    auto quarter_sync = [&]() -> bool {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&qbar[q]);
+      const bool r = __all_sync(FULL, mbar_wait(&qbar[q], qphase, abort_flag));
+      qphase ^= 1;
+      return r;
+    };
+    for (int it = unit; it < P.n_items && ok; it += nunits) {
       const WorkItem w = items[it];
       const long long tl = P.prof ? clock64() : 0;
-      if (P.a_tmem) {
-        // the query rows of this tile into TMEM: this thread's lane holds its row; the MMAs of
-        // the previous tile must be done reading the old rows first
-        ok = __all_sync(FULL, mbar_wait(&a_empty[0], aphase_e ^ 1, abort_flag));
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t* src = P.a_glob + (int64_t(w.qrow0) + row) * (P.kp / 2);
-        const uint32_t a_t = tmem_base + uint32_t(2 * P.bn) + (uint32_t(q * 32) << 16);
-        for (int c = 0; c < P.kp / 2; c += 32) {
-          uint32_t r[32];
-#pragma unroll
-          for (int e = 0; e < 32; e += 4) {
-            const uint4 v4 = *reinterpret_cast<const uint4*>(src + c + e);
-            r[e] = v4.x; r[e + 1] = v4.y; r[e + 2] = v4.z; r[e + 3] = v4.w;
-          }
-          tmem_st32(a_t + uint32_t(c), r);
-        }
-        tmem_wait_st();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&a_full[0]);
-        aphase_e ^= 1;
-      }
-      sel.reset();
-      __syncwarp();
-      const int self = w.qorig0 + row;
-      const int limit = w.orig_off + w.nkeys;
+      // neighbour ids are packed positions here; finish() maps them to original rows
+      const int nq = min(BM, w.nq - int(rank) * BM);   // this CTA's valid query rows (may be <= 0)
+      const int qrow = w.qrow0 + int(rank) * BM;
+      const int self = qrow + row;
+      const int limit = w.key0 + w.nkeys;
       const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-      for (int kt = 0; kt < nkt; ++kt) {
+      const int diag = (w.qrow0 - w.key0) / P.bn;
+      for (int j = 0; j < nkt; ++j) {
+        const int kt = key_tile_at(j, diag, nkt);
         const long long te = P.prof ? clock64() : 0;
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
         if (P.prof) c_ew += clock64() - te;
         if (!ok) break;
         tc_fence_after();
-        const uint32_t t0 = tmem_base + uint32_t(acc * P.bn) + (uint32_t(q * 32) << 16);
-        const int col_base = w.orig_off + kt * P.bn;
-        const int nch = P.bn / 32;
+        sel.refresh();
+        const uint32_t t0 =
+            tmem_base + uint32_t(acc * P.bn + h * gcols) + (uint32_t(q * 32) << 16);
+        const int col_base = w.key0 + kt * P.bn + h * gcols;
         // two register buffers: the next chunk's TMEM load is in flight while the current chunk
         // is filtered; the accumulator is released right after its last load completes
         uint32_t ra[32], rb[32];
         auto release = [&]() {
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[acc]);
+          if (lane == 0) {
+            if (PAIR && !leader) mbar_arrive_remote(mapa_shared(smem_u32(&acc_empty[acc]), 0));
+            else mbar_arrive(&acc_empty[acc]);
+          }
         };
         tmem_ld32_async(t0, ra);
         tmem_wait(ra);
@@ -504,12 +629,31 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       }
       if (!ok) break;
       const int wrow0 = q * 32;
-      const int nvalid = min(32, w.nq - wrow0);
-      if (nvalid > 0)
-        sel.finish(cand_idx, cand_thr, P.cand_stride, int64_t(w.qorig0) + wrow0, nvalid,
-                   P.kprime);
-      else
+      const int nvalid = min(32, nq - wrow0);
+      if (NH == 1) {
+        if (nvalid > 0)
+          sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, int64_t(qrow) + wrow0, nvalid,
+                     P.kprime);
+        else
+          sel.flush();
+      } else {
+        // both lists final and both published thresholds back to +inf (the partner may still be
+        // filtering this tile's columns; +inf only loosens its filter), then group 0 merges
         sel.flush();
+        *reinterpret_cast<volatile float*>(sel.pub_own) = F_INF;
+        ok = quarter_sync();
+        if (!ok) break;
+        if (h == 0) {
+          sel.merge_from(smem + sp.sel_off + Sel::smem_bytes());
+          if (nvalid > 0)
+            sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, int64_t(qrow) + wrow0, nvalid,
+                       P.kprime);
+        }
+        ok = quarter_sync();                       // the partner's list is read; reuse it
+        if (!ok) break;
+      }
+      sel.reset();
+      __syncwarp();
       if (P.prof) c_loop += clock64() - tl;
     }
     if (P.prof) {
@@ -525,11 +669,14 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
 
   __syncthreads();
   if (warp == 2) {
-    // the MMA warp's last commit marks the end of every tensor-core write to TMEM
+    // the even CTA's last commit marks the end of every tensor-core write to TMEM (in a pair it
+    // arrives at both CTAs)
     (void)mbar_drain(done_bar, 0);
     tc_fence_after();
-    tmem_dealloc(tmem_base, tmem_cols);
   }
+  // a pair leaves together: no remote arrive or MMA operand read can reach a CTA that has exited
+  if (PAIR) cluster_sync();
+  if (warp == 2) tmem_dealloc_g<PAIR>(tmem_base, tmem_cols);
   if (P.prof && threadIdx.x == 0) {
     atomicAdd(&g_tc_prof[5], (unsigned long long)(clock64() - t_kernel0));
     atomicAdd(&g_tc_prof[9], 1ull);
@@ -603,36 +750,62 @@ int make_map(CUtensorMap* m, const void* base, int64_t rows, int kp, int box_row
   return MSC_OK;
 }
 
-template <int KPL, int CB>
-size_t smem_total(const TcConfig& c, int kb, int na) {
-  return smem_plan<KPL, CB>(kb, c.bn, c.stages, na).total;
-}
-
 size_t config_smem(const TcConfig& c, int kb, int na) {
-  if (c.kpl == 32 && c.cb == 16) return smem_total<32, 16>(c, kb, na);
-  if (c.kpl == 32 && c.cb == 32) return smem_total<32, 32>(c, kb, na);
-  if (c.kpl == 64 && c.cb == 16) return smem_total<64, 16>(c, kb, na);
-  if (c.kpl == 64 && c.cb == 32) return smem_total<64, 32>(c, kb, na);
+  const int nh = c.epi / 4;
+  const int brows = c.pair ? c.bn / 2 : c.bn;
+  if (c.kpl == 32 && c.cb == 16) return smem_plan<32, 16>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 32 && c.cb == 32) return smem_plan<32, 32>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 64 && c.cb == 16) return smem_plan<64, 16>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 64 && c.cb == 32) return smem_plan<64, 32>(kb, brows, c.stages, na, nh).total;
   return SIZE_MAX;
 }
 
-int pick_na(const TcConfig& c, int kb) {
-  if (c.atmem) return 0;
-  return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1;
+int pick_na(const TcConfig& c, int kb) { return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1; }
+
+template <int KPL, int CB, int NEPI, bool PAIR>
+int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
+                const WorkItem* items, Ctl* ctl, int32_t* cand_idx, float* cand_thr,
+                cudaStream_t st) {
+  const int brows = PAIR ? P.bn / 2 : P.bn;
+  const size_t smem = smem_plan<KPL, CB>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
+  auto kern = knn_tc_kernel<KPL, CB, NEPI, PAIR>;
+  MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (!PAIR) {
+    const int grid = std::max(1, std::min(P.n_items, num_sms()));
+    kern<<<grid, 128 + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
+    MSC_LAUNCH_CHECK();
+    return MSC_OK;
+  }
+  // one two-CTA cluster per pair of SMs, persistent over the 256-row work items
+  const int pairs = std::max(1, std::min(P.n_items, num_sms() / 2));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(unsigned(2 * pairs));
+  lc.blockDim = dim3(unsigned(128 + 32 * NEPI));
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  MSC_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, ma, mb, P, items, ctl, cand_idx, cand_thr));
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
 }
 
-template <int KPL, int CB>
-int launch_tc_t(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
-                const CUtensorMap& mb, const WorkItem* items, Ctl* ctl, int32_t* cand_idx,
-                float* cand_thr, cudaStream_t st) {
-  const size_t smem = smem_plan<KPL, CB>(P.kb, P.bn, P.stages, P.na).total;
-  auto kern = knn_tc_kernel<KPL, CB>;
-  MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  const int grid = std::max(1, std::min(P.n_items, num_sms()));
-  kern<<<grid, TC_THREADS, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
-  MSC_LAUNCH_CHECK();
-  (void)cfg;
-  return MSC_OK;
+template <int NEPI, bool PAIR>
+int launch_tc_epi(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
+                  const CUtensorMap& mb, const WorkItem* items, Ctl* ctl, int32_t* cand_idx,
+                  float* cand_thr, cudaStream_t st) {
+  if (cfg.kpl == 32 && cfg.cb == 16)
+    return launch_tc_t<32, 16, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 32 && cfg.cb == 32)
+    return launch_tc_t<32, 32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 64 && cfg.cb == 16)
+    return launch_tc_t<64, 16, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  return launch_tc_t<64, 32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
 }
 
 }  // namespace
@@ -660,42 +833,46 @@ bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.stages < 2 || c.stages > 8) return false;
   if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 64)) return false;
   if (c.cb != 16 && c.cb != 32) return false;
-  const int kb = kp / 64;
-  if (c.atmem) {
-    if (2 * c.bn + kp / 2 > 512) return false;        // accumulators + query rows in TMEM
-    return config_smem(c, kb, 0) <= SMEM_LIMIT;
-  }
-  return config_smem(c, kb, 1) <= SMEM_LIMIT;
+  if (c.epi != 4 && c.epi != 8) return false;
+  if (c.epi == 8 && c.bn < 64) return false;         // each column group takes >= 32 columns
+  if (c.pair != 0 && c.pair != 1) return false;
+  if (c.pair && c.bn < 64) return false;             // each CTA stages >= 32 key rows
+  return config_smem(c, kp / 64, 1) <= SMEM_LIMIT;
 }
 
 TcConfig tc_default_config(int prec, int d, int kprime) {
   const OpLayout L = op_layout(prec, d);
   const int kpl = kprime <= 32 ? 32 : 64;
-  // N=256 key tiles first (one MMA costs the same ~186 cycles at N = 64..256, so only N=256
-  // reaches the tensor peak), then the deepest K-atom pipeline and the largest buffer that fit
-  for (int bn : {256, 128, 64, 32})
-    for (int atmem : {0, 1})
-      for (int stages = 6; stages >= 2; --stages)
-        for (int cb : {32, 16}) {
-          TcConfig c{bn, stages, kpl, cb, atmem};
-          if (tc_config_ok(c, L.kp, kprime)) return c;
-        }
-  return TcConfig{64, 2, kpl, 16, 0};
+  // Single CTAs first: CTA pairs halve the key bytes per SM and double the K-atom stages that
+  // fit, but measured slower at 1.3M × 50 (1057 vs 819 ms for the candidate stage), so they are
+  // taken only when nothing else fits.  N=256 key tiles (one MMA costs the same ~186 cycles at
+  // N = 64..256, so only N=256 reaches the tensor peak); eight epilogue warps (a warp's TMEM reads
+  // are serialised, so read bandwidth grows with the number of reading warps), else four; then
+  // the deepest K-atom pipeline and the largest selector buffer that fit
+  for (int pair : {0, 1})
+    for (int bn : {256, 128, 64, 32})
+      for (int epi : {8, 4})
+        for (int stages = 8; stages >= 2; --stages)
+          for (int cb : {32, 16}) {
+            TcConfig c{bn, stages, kpl, cb, epi, pair};
+            if (tc_config_ok(c, L.kp, kprime)) return c;
+          }
+  return TcConfig{64, 2, kpl, 16, 4, 0};
 }
 
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
-                  int64_t n_items, Ctl* ctl, int kprime, int32_t* cand_idx, float* cand_thr,
-                  int cand_stride, cudaStream_t st) {
+                  int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime, int32_t* cand_idx,
+                  float* cand_thr, int cand_stride, cudaStream_t st) {
   if (!tc_config_ok(cfg, kp, kprime)) {
-    set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d) does not fit", cfg.bn,
-              cfg.stages, cfg.kpl, cfg.cb);
+    set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
+              cfg.bn, cfg.stages, cfg.kpl, cfg.cb, cfg.epi, cfg.pair);
     return MSC_ERR_INVALID_ARG;
   }
   const bool bf16 = prec != PREC_FP16;
   CUtensorMap ma, mb;
   MSC_TRY(make_map(&ma, Aop, a_rows, kp, BM, bf16));
-  MSC_TRY(make_map(&mb, Bop, b_rows, kp, cfg.bn, bf16));
+  MSC_TRY(make_map(&mb, Bop, b_rows, kp, cfg.pair ? cfg.bn / 2 : cfg.bn, bf16));
   TcParams P;
   P.ksteps = kmma / 16;
   P.kb = (P.ksteps + 3) / 4;                           // K atoms the MMAs read
@@ -706,19 +883,17 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.cand_stride = cand_stride;
   P.bf16 = bf16;
   P.n_items = int(n_items);
-  P.idesc = idesc_f16(bf16, BM, cfg.bn);
+  P.idesc = idesc_f16(bf16, cfg.pair ? 2 * BM : BM, cfg.bn);
   P.prof = profiling_enabled() ? 1 : 0;
-  P.kp = kp;
-  P.a_tmem = cfg.atmem;
-  P.a_glob = static_cast<const uint32_t*>(Aop);
-  if (P.a_tmem) P.na = 0;
-  if (cfg.kpl == 32 && cfg.cb == 16)
-    return launch_tc_t<32, 16>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  if (cfg.kpl == 32 && cfg.cb == 32)
-    return launch_tc_t<32, 32>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  if (cfg.kpl == 64 && cfg.cb == 16)
-    return launch_tc_t<64, 16>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  return launch_tc_t<64, 32>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  P.perm = perm;
+  if (cfg.pair) {
+    if (cfg.epi == 8)
+      return launch_tc_epi<8, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+    return launch_tc_epi<4, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  }
+  if (cfg.epi == 8)
+    return launch_tc_epi<8, false>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  return launch_tc_epi<4, false>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
 }
 
 }  // namespace msc

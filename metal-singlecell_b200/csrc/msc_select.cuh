@@ -41,8 +41,14 @@ struct RowSelect {
   float* lv; int* li; float* bv; int* bi;
   int row;        // this thread's row within the ROWS rows
   int kp;         // k'
-  float thr;
+  float thr;      // this list's k'-th value
+  float thr_f;    // filter threshold: min(thr, the partner list's published thr)
   int cnt;
+  // When two selectors split one row's columns, each publishes its threshold here (shared memory)
+  // and filters against the smaller of the two: the k'-th smallest of the union is at most either
+  // list's k'-th value, so nothing it drops can belong to the union's k' smallest.
+  float* pub_own = nullptr;
+  const float* pub_other = nullptr;
   int n_hot = 0, n_compact = 0, n_append = 0;   // counters for the pipeline profile
 
   __device__ void bind(void* smem, int row_, int kprime) {
@@ -61,7 +67,13 @@ struct RowSelect {
       li[s * ROWS + row] = -1;
     }
     thr = F_INF;
+    thr_f = F_INF;
     cnt = 0;
+  }
+
+  // take the partner's latest published threshold
+  __device__ __forceinline__ void refresh() {
+    if (pub_other) thr_f = fminf(thr, *reinterpret_cast<const volatile float*>(pub_other));
   }
 
   __device__ __forceinline__ void append(float v, int col) {
@@ -120,6 +132,43 @@ struct RowSelect {
     }
     thr = L[(kp - 1) * ROWS];
     cnt = 0;
+    if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
+    thr_f = thr;
+    refresh();
+  }
+
+  // Merge another selector's sorted list for the same row (same layout, base `other`) into this
+  // one, keeping the k' smallest.  The buffer must be empty (after flush()).
+  __device__ void merge_from(const void* other) {
+    const float* O = static_cast<const float*>(other) + row;
+    const int* OI = reinterpret_cast<const int*>(static_cast<const float*>(other) + KPL * ROWS) + row;
+    float* L = lv + row;
+    int* LI = li + row;
+    int a = 0, b = 0;
+    float la = L[0], lb = O[0];
+    for (int p = 0; p < kp; ++p) {
+      if (lb < la) {
+        ++b;
+        lb = b < kp ? O[b * ROWS] : F_INF;
+      } else {
+        ++a;
+        la = a < kp ? L[a * ROWS] : F_INF;
+      }
+    }
+    int ia = a - 1, ib = b - 1;
+    for (int p = kp - 1; p >= 0; --p) {
+      if (ib >= 0 && (ia < 0 || O[ib * ROWS] > L[ia * ROWS])) {
+        L[p * ROWS] = O[ib * ROWS];
+        LI[p * ROWS] = OI[ib * ROWS];
+        --ib;
+      } else {
+        L[p * ROWS] = L[ia * ROWS];
+        LI[p * ROWS] = LI[ia * ROWS];
+        --ia;
+      }
+    }
+    thr = L[(kp - 1) * ROWS];
+    thr_f = thr;
   }
 
   // Offer 32 consecutive candidate columns col0..col0+31 of this row (warp-collective).
@@ -132,17 +181,17 @@ struct RowSelect {
     const float n0 = min3f(g[0], g[1], g[2]), n1 = min3f(g[3], g[4], g[5]);
     const float n2 = min3f(g[6], g[7], g[8]), n3 = fminf(g[9], g[10]);
     const float mn = fminf(min3f(n0, n1, n2), n3);
-    if (!__any_sync(FULL, mn < thr)) return;
+    if (!__any_sync(FULL, mn < thr_f)) return;
     ++n_hot;
 #pragma unroll
     for (int q = 0; q < 11; ++q) {
-      if (__any_sync(FULL, g[q] < thr)) {
+      if (__any_sync(FULL, g[q] < thr_f)) {
 #pragma unroll
         for (int t = 0; t < 3; ++t) {
           const int e = 3 * q + t;
           if (e < 32) {
             const int c = col0 + e;
-            if (v[e] < thr && c != self && c < limit) append(v[e], c);
+            if (v[e] < thr_f && c != self && c < limit) append(v[e], c);
           }
         }
         if (__any_sync(FULL, cnt > CB - 3)) compact_own();
@@ -152,15 +201,17 @@ struct RowSelect {
 
   // Offer one value (tails); warp-collective; keeps cnt <= CB-3.
   __device__ __forceinline__ void push1(float v, int c, int self, int limit) {
-    if (v < thr && c != self && c < limit) append(v, c);
+    if (v < thr_f && c != self && c < limit) append(v, c);
     if (__any_sync(FULL, cnt > CB - 3)) compact_own();
   }
 
   __device__ void flush() { compact_own(); }
 
   // warp-collective: flush and write the first `kout` list entries and the threshold value
-  // (list[k'-1]) of the warp's first `nvalid_rows` rows to global memory.
-  __device__ void finish(int* out_idx, float* out_thr, int out_stride, int64_t first_out_row,
+  // (list[k'-1]) of the warp's first `nvalid_rows` rows.  Rows and columns are packed positions;
+  // perm maps them to original rows (the output row and the stored neighbour ids).
+  __device__ void finish(int* out_idx, float* out_thr, int out_stride,
+                         const int32_t* __restrict__ perm, int64_t first_packed_row,
                          int nvalid_rows, int kout) {
     compact_own();
     __syncwarp();
@@ -168,8 +219,11 @@ struct RowSelect {
     const int row0 = row - lane;
     for (int r = 0; r < nvalid_rows; ++r) {
       const int rr = row0 + r;
-      const int64_t orow = first_out_row + r;
-      for (int s = lane; s < kout; s += 32) out_idx[orow * out_stride + s] = li[s * ROWS + rr];
+      const int64_t orow = perm[first_packed_row + r];
+      for (int s = lane; s < kout; s += 32) {
+        const int c = li[s * ROWS + rr];
+        out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
+      }
       if (lane == 0) out_thr[orow] = lv[(kp - 1) * ROWS + rr];
     }
     __syncwarp();

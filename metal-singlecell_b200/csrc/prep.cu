@@ -186,8 +186,8 @@ __device__ __forceinline__ void block_keymax(float (&m)[5], KeyMax* km) {
 }
 
 template <class T, int SPLIT>
-__global__ void pack_tc_kernel(const float* __restrict__ X, const SegDesc* __restrict__ seg,
-                               int nseg, const double* __restrict__ mean, int d, int kp, int prec,
+__global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
+                               const SegDesc* __restrict__ seg, int nseg, const double* __restrict__ mean, int d, int kp, int prec,
                                int64_t npacked, T* __restrict__ Aop, T* __restrict__ Bop,
                                QStat* __restrict__ qs, KeyMax* __restrict__ km,
                                const Ctl* __restrict__ ctl, double pad_term) {
@@ -202,9 +202,8 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const SegDesc* __res
   for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
        p += nwarps) {
     const int s = find_seg(seg, nseg, p);
-    const int64_t j = p - seg[s].poff;
-    const bool valid = j < seg[s].n;
-    const int64_t orow = seg[s].off + j;
+    const int64_t orow = perm[p];
+    const bool valid = orow >= 0;
     const double* c = mean + int64_t(s) * d;
     T* arow = Aop + p * kp;
     T* brow = Bop + p * kp;
@@ -266,26 +265,26 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const SegDesc* __res
   block_keymax(mx, km);
 }
 
-int launch_pack_tc(int prec, const float* X, const SegDesc* seg, int nseg, const double* mean,
-                   int d, int64_t npacked, void* Aop, void* Bop, QStat* qs, KeyMax* km,
-                   const Ctl* ctl, cudaStream_t st) {
+int launch_pack_tc(int prec, const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
+                   const double* mean, int d, int64_t npacked, void* Aop, void* Bop, QStat* qs,
+                   KeyMax* km, const Ctl* ctl, cudaStream_t st) {
   const OpLayout L = op_layout(prec, d);
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 8), int64_t(num_sms()) * 16));
   blocks = std::max(blocks, 1);
   switch (prec) {
     case PREC_BF16X3:
       pack_tc_kernel<__nv_bfloat16, 3><<<blocks, 256, 0, st>>>(
-          X, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
           static_cast<__nv_bfloat16*>(Bop), qs, km, ctl, PAD_NORM_TERM_BF16);
       break;
     case PREC_BF16:
       pack_tc_kernel<__nv_bfloat16, 1><<<blocks, 256, 0, st>>>(
-          X, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
           static_cast<__nv_bfloat16*>(Bop), qs, km, ctl, PAD_NORM_TERM_BF16);
       break;
     case PREC_FP16:
       pack_tc_kernel<__half, 1><<<blocks, 256, 0, st>>>(
-          X, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__half*>(Aop),
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__half*>(Aop),
           static_cast<__half*>(Bop), qs, km, ctl, PAD_NORM_TERM_FP16);
       break;
     default:
@@ -297,8 +296,8 @@ int launch_pack_tc(int prec, const float* X, const SegDesc* seg, int nseg, const
 }
 
 // FP32 SIMT operands: A32 = fp32(z) (row stride dpad, zero padded), sq32 = fp32(Σ z²)
-__global__ void pack_fp32_kernel(const float* __restrict__ X, const SegDesc* __restrict__ seg,
-                                 int nseg, const double* __restrict__ mean, int d, int dpad,
+__global__ void pack_fp32_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
+                                 const SegDesc* __restrict__ seg, int nseg, const double* __restrict__ mean, int d, int dpad,
                                  int64_t npacked, float* __restrict__ A32,
                                  float* __restrict__ sq32, QStat* __restrict__ qs,
                                  KeyMax* __restrict__ km) {
@@ -308,9 +307,8 @@ __global__ void pack_fp32_kernel(const float* __restrict__ X, const SegDesc* __r
   for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
        p += nwarps) {
     const int s = find_seg(seg, nseg, p);
-    const int64_t j = p - seg[s].poff;
-    const bool valid = j < seg[s].n;
-    const int64_t orow = seg[s].off + j;
+    const int64_t orow = perm[p];
+    const bool valid = orow >= 0;
     const double* c = mean + int64_t(s) * d;
     double sq = 0.0, nh = 0.0, nr = 0.0;
     for (int t = lane; t < dpad; t += 32) {
@@ -344,12 +342,12 @@ __global__ void pack_fp32_kernel(const float* __restrict__ X, const SegDesc* __r
   block_keymax(mx, km);
 }
 
-int launch_pack_fp32(const float* X, const SegDesc* seg, int nseg, const double* mean, int d,
-                     int dpad, int64_t npacked, float* A32, float* sq32, QStat* qs, KeyMax* km,
-                     cudaStream_t st) {
+int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
+                     const double* mean, int d, int dpad, int64_t npacked, float* A32, float* sq32,
+                     QStat* qs, KeyMax* km, cudaStream_t st) {
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 8), int64_t(num_sms()) * 16));
-  pack_fp32_kernel<<<std::max(blocks, 1), 256, 0, st>>>(X, seg, nseg, mean, d, dpad, npacked,
-                                                        A32, sq32, qs, km);
+  pack_fp32_kernel<<<std::max(blocks, 1), 256, 0, st>>>(X, perm, seg, nseg, mean, d, dpad,
+                                                        npacked, A32, sq32, qs, km);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
@@ -365,7 +363,8 @@ __global__ void single_segment_kernel(SegDesc* seg, int64_t n) {
   s.padlen = ((n + SEG_PAD - 1) / SEG_PAD) * SEG_PAD;
   s.tile0 = 0;
   s.ntiles = (n + QTILE - 1) / QTILE;
-  s.pad0 = s.pad1 = 0;
+  s.ptile0 = 0;
+  s.pad1 = 0;
   *seg = s;
 }
 
@@ -377,34 +376,39 @@ int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st) {
 
 // one work item per 128-row query tile; largest samples first so the persistent kernels'
 // dynamic scheduler ends with the short items
-__global__ void build_items_kernel(const SegDesc* __restrict__ seg, int nseg, int64_t ntiles,
-                                   WorkItem* __restrict__ items, Ctl* ctl) {
+__global__ void build_items_kernel(const SegDesc* __restrict__ seg, int nseg, int64_t n_items,
+                                   int rows, WorkItem* __restrict__ items, Ctl* ctl) {
   int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-  if (t == 0) ctl->n_items = int32_t(ntiles);
-  if (t >= ntiles) return;
-  // segment of tile t: last with tile0 <= t
+  if (t == 0) ctl->n_items = int32_t(n_items);
+  if (t >= n_items) return;
+  const bool pair = rows != QTILE;
+  // segment of item t: last with first item <= t
   int lo = 0, hi = nseg - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
-    if (seg[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+    if ((pair ? seg[mid].ptile0 : seg[mid].tile0) <= t) lo = mid; else hi = mid - 1;
   }
   const SegDesc s = seg[lo];
-  const int64_t q = t - s.tile0;
+  const int64_t q = t - (pair ? s.ptile0 : s.tile0);
   WorkItem w;
-  w.qrow0 = int32_t(s.poff + q * QTILE);
-  w.nq = int32_t(min64(QTILE, s.n - q * QTILE));
+  w.qrow0 = int32_t(s.poff + q * rows);
+  w.nq = int32_t(min64(rows, s.n - q * rows));
   w.key0 = int32_t(s.poff);
   w.nkeys = int32_t(s.n);
   w.orig_off = int32_t(s.off);
-  w.qorig0 = int32_t(s.off + q * QTILE);
+  w.qorig0 = int32_t(s.off + q * rows);
   w.pad0 = w.pad1 = 0;
   items[t] = w;
 }
 
-int launch_build_items(const SegDesc* seg, int nseg, int64_t ntiles_total, WorkItem* items,
+int launch_build_items(const SegDesc* seg, int nseg, int64_t n_items, int rows, WorkItem* items,
                        Ctl* ctl, cudaStream_t st) {
-  build_items_kernel<<<unsigned(std::max<int64_t>(1, ceil_div(ntiles_total, 256))), 256, 0, st>>>(
-      seg, nseg, ntiles_total, items, ctl);
+  if (rows != QTILE && rows != 2 * QTILE) {
+    set_error("work items of %d rows", rows);
+    return MSC_ERR_INVALID_ARG;
+  }
+  build_items_kernel<<<unsigned(std::max<int64_t>(1, ceil_div(n_items, 256))), 256, 0, st>>>(
+      seg, nseg, n_items, rows, items, ctl);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }

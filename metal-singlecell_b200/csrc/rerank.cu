@@ -92,7 +92,8 @@ __device__ __forceinline__ float out_dist(double d2, int cosine) {
 }
 
 __global__ void __launch_bounds__(RR_WARPS * 32)
-rerank_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ seg, int nseg,
+rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
+              const SegDesc* __restrict__ seg, int nseg,
               int64_t npacked, const int32_t* __restrict__ cand_idx,
               const float* __restrict__ cand_thr, int cand_stride, int kprime,
               const QStat* __restrict__ qs, const KeyMax* __restrict__ km, Ctl* __restrict__ ctl,
@@ -121,10 +122,9 @@ rerank_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ se
   int64_t n_cert = 0, n_ties = 0;
   for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
        p += nwarps) {
+    const int64_t i = perm[p];                          // original row
+    if (i < 0) continue;                                // padding (warp-uniform)
     const int s = find_seg(seg, nseg, p);
-    const int64_t j = p - seg[s].poff;
-    if (j >= seg[s].n) continue;                        // warp-uniform
-    const int64_t i = seg[s].off + j;                   // original row
     const int64_t ns = seg[s].n;
     for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
     __syncwarp();
@@ -212,7 +212,8 @@ rerank_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ se
 // a warp-distributed sorted list of 128 (four slots per lane) merged 32 keys at a time.
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(RR_WARPS * 32)
-fp64_scan_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__ seg, int nseg,
+fp64_scan_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
+                 const SegDesc* __restrict__ seg, int nseg,
                  const int32_t* __restrict__ fail_rows, Ctl* __restrict__ ctl, int k, int cosine,
                  int32_t* __restrict__ knn_idx, float* __restrict__ knn_dist) {
   __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
@@ -227,7 +228,7 @@ fp64_scan_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__
     const int64_t p = fail_rows[w];                      // packed row
     const int sg = find_seg(seg, nseg, p);
     const int64_t off = seg[sg].off, ns = seg[sg].n;
-    const int64_t i = off + (p - seg[sg].poff);          // original row
+    const int64_t i = perm[p];                           // original row
     for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
     __syncwarp();
     double a[4];
@@ -286,26 +287,25 @@ fp64_scan_kernel(const float* __restrict__ X, int d, const SegDesc* __restrict__
 }
 
 // every valid packed row goes to the FP64 scan (n_neighbors beyond the candidate kernels)
-__global__ void all_rows_fail_kernel(const SegDesc* __restrict__ seg, int nseg, int64_t npacked,
+__global__ void all_rows_fail_kernel(const int32_t* __restrict__ perm, int64_t npacked,
                                      int32_t* __restrict__ fail_rows, Ctl* __restrict__ ctl) {
   for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int s = find_seg(seg, nseg, p);
-    if (p - seg[s].poff < seg[s].n) fail_rows[atomicAdd(&ctl->n_fail, 1)] = int32_t(p);
-  }
+       p += int64_t(gridDim.x) * blockDim.x)
+    if (perm[p] >= 0) fail_rows[atomicAdd(&ctl->n_fail, 1)] = int32_t(p);
 }
 
 }  // namespace
 
-int launch_all_rows_fail(const SegDesc* seg, int nseg, int64_t npacked, int32_t* fail_rows,
-                         Ctl* ctl, cudaStream_t st) {
+int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
+                         cudaStream_t st) {
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
-  all_rows_fail_kernel<<<std::max(blocks, 1), 256, 0, st>>>(seg, nseg, npacked, fail_rows, ctl);
+  all_rows_fail_kernel<<<std::max(blocks, 1), 256, 0, st>>>(perm, npacked, fail_rows, ctl);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
 
-int launch_rerank(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
+int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
+                  int64_t npacked,
                   const int32_t* cand_idx, const float* cand_thr, int cand_stride, int kprime,
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
@@ -316,13 +316,13 @@ int launch_rerank(const float* X, int d, const SegDesc* seg, int nseg, int64_t n
   }
   int blocks = int(std::min<int64_t>(ceil_div(npacked, RR_WARPS), int64_t(num_sms()) * 8));
   rerank_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
-      X, d, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
+      X, d, perm, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
       kmma, k, cosine, knn_idx, knn_dist, fail_rows);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
 
-int launch_fp64_scan(const float* X, int d, const SegDesc* seg, int nseg,
+int launch_fp64_scan(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
                      const int32_t* fail_rows, int64_t max_rows, int k, int cosine,
                      int32_t* knn_idx, float* knn_dist, Ctl* ctl, cudaStream_t st) {
   if (k - 1 > 128) {
@@ -331,7 +331,7 @@ int launch_fp64_scan(const float* X, int d, const SegDesc* seg, int nseg,
   }
   int blocks = int(std::min<int64_t>(ceil_div(max_rows, RR_WARPS), int64_t(num_sms()) * 8));
   fp64_scan_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
-      X, d, seg, nseg, fail_rows, ctl, k, cosine, knn_idx, knn_dist);
+      X, d, perm, seg, nseg, fail_rows, ctl, k, cosine, knn_idx, knn_dist);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }

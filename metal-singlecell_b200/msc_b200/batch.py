@@ -28,13 +28,16 @@ from .neighbors import _torch, _ids, knn_device, Workspace, DEFAULT_PRECISION
 _TILE_CACHE: dict[str, int] = {}
 
 
-def tile_code(bn: int, stages: int, cb: int, atmem: int = 0) -> int:
-    return int(bn) | (int(stages) << 12) | (int(cb) << 20) | (int(atmem) << 27)
+def tile_code(bn: int, stages: int, cb: int, epi: int = 4, pair: int = 0) -> int:
+    """Candidate-kernel tile configuration: key tile rows, K-atom stages, selector buffer,
+    epilogue warps (4 or 8) and CTA pairs (1: two-CTA clusters, 256-row query tiles)."""
+    return (int(bn) | (int(stages) << 12) | (int(cb) << 20) | (int(epi == 8) << 27)
+            | (int(bool(pair)) << 28))
 
 
 def decode_tile_code(code: int):
     return {"bn": code & 0xFFF, "stages": (code >> 12) & 0xFF, "cb": (code >> 20) & 0x7F,
-            "atmem": (code >> 27) & 1}
+            "epi": 8 if (code >> 27) & 1 else 4, "pair": (code >> 28) & 1}
 
 
 class BatchedKnn:
@@ -167,8 +170,8 @@ def autotune(X, offsets, n_neighbors: int = 15, *, metric: str = "euclidean",
             except Exception:
                 pass
     if configs is None:
-        configs = [tile_code(bn, st, cb, am) for am in (1, 0) for bn in (256, 128, 64, 32)
-                   for st in (2, 3, 4) for cb in (16, 32)]
+        configs = [tile_code(bn, st, cb, ep, pr) for pr in (1, 0) for ep in (8, 4)
+                   for bn in (256, 128, 64) for st in (2, 3, 4, 6) for cb in (16, 32)]
     table = []
     for code in configs:
         try:

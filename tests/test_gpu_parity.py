@@ -150,3 +150,31 @@ def test_bounded_wait_gives_up_without_hanging():
     # the context still works
     X = synth.gaussian_mixture(2000, 20, 5, seed=3)
     check_against_oracle(X, 10, precision="bf16x3")
+
+
+def _tile(bn, stages, cb, epi, pair=0):
+    return bn | (stages << 12) | (cb << 20) | ((epi == 8) << 27) | (pair << 28)
+
+
+@pytest.mark.parametrize("precision,kprime", [("bf16x3", 0), ("fp16", 32), ("bf16x3", 48)])
+def test_candidate_tile_configs_agree(monkeypatch, precision, kprime):
+    """Every candidate-kernel configuration (key tile rows, K-atom stages, selector buffer, four or
+    eight epilogue warps, single CTAs or CTA pairs) gives the oracle's graph: 20,000 × 50, two
+    clusters of unequal size so that tiles are ragged."""
+    X = synth.gaussian_mixture(20000, 50, 2, seed=23)
+    ref = oracle.neighbors_graph(X, 15)
+    tried = 0
+    for code in (_tile(256, 4, 16, 4), _tile(256, 2, 16, 8), _tile(128, 4, 16, 8),
+                 _tile(64, 3, 32, 8), _tile(64, 2, 16, 4), _tile(256, 5, 16, 8, 1),
+                 _tile(256, 4, 32, 4, 1), _tile(128, 6, 16, 8, 1), _tile(64, 4, 16, 4, 1)):
+        monkeypatch.setenv("MSC_B200_TILE_CONFIG", hex(code))
+        try:
+            gi, gd, _, gconn, stats = run_graph(X, 15, precision=precision, kprime=kprime)
+        except ValueError:
+            continue                     # the configuration does not fit this operand width
+        tried += 1
+        assert int(stats[_lib.STAT_TIMEOUT]) == 0
+        np.testing.assert_array_equal(gi, ref["idx"].astype(np.int32), err_msg=hex(code))
+        np.testing.assert_array_equal(gd, ref["dist"], err_msg=hex(code))
+        assert_csr_equal(gconn, ref["connectivities"], f"connectivities {hex(code)}")
+    assert tried >= (5 if kprime <= 32 else 1)     # 64-entry lists fit fewer configurations
