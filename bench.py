@@ -2,7 +2,7 @@
 """Benchmark of the neighbour-graph path (``pp.neighbors``) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload scale|plain|precision] [--precision bf16x3|fp16|bf16|fp32]
+                    [--workload scale|plain|precision] [--precision fp16|bf16x3|bf16|fp32]
 
 A step = one full graph (exact kNN → distances CSR → UMAP connectivities) of the workload's
 synthetic embedding.  Default workload: 1,300,000 cells × 50 PCs, 200-cluster Gaussian mixture with
@@ -397,7 +397,8 @@ def run_batch(args):
             "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "data": "synthetic",
             "config": {"workload": f"{len(sizes)} samples, {n:,} cells (min {sizes.min()}, "
                                    f"max {sizes.max()}), 30 PCs, k=15, euclidean",
-                       "precision": "bf16x3", "tile": batch.decode_tile_code(tune["tile_config"])},
+                       "precision": batch.DEFAULT_PRECISION,
+                       "tile": batch.decode_tile_code(tune["tile_config"])},
             "graph_ms": graph_ms, "batched_ms": batched_ms, "per_sample_loop_ms": loop_ms,
             "speedup_vs_loop": loop_ms / graph_ms, "identical_to_loop": same,
             "autotune_table": [(batch.decode_tile_code(c), round(ms, 3))
@@ -458,7 +459,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="scale",
                     choices=["scale", "plain", "precision", "batch", "serve"])
-    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp16", "bf16", "fp32"])
+    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16x3", "bf16", "fp32"])
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=15.0)

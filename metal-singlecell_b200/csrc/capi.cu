@@ -87,6 +87,10 @@ struct Problem {
   bool candidates = true; // false: every row takes the FP64 scan (k-1 > 64)
   OpLayout L{};
   int dpad = 0;
+  // refine pass (one-term FP16/BF16 candidates): rows that fail the certificate re-run through
+  // the BF16x3 candidate kernel before the FP64 scan takes what is left
+  bool refine = false;
+  OpLayout L3{};
 };
 
 struct KnnWs {
@@ -108,6 +112,16 @@ struct KnnWs {
   int32_t* perm;          // packed row -> original row (-1: padding)
   void* order_ws;
   size_t order_ws_bytes;
+  // refine pass
+  int32_t* flags;         // per packed row: failed the first certificate
+  int64_t* S;             // scan of flags (npacked + 1)
+  int64_t* scan_scratch;
+  int32_t* qmap;          // refine query row -> packed row
+  WorkItem* items3;
+  void* A3;               // BF16x3 query operand of the listed rows
+  void* B3;               // BF16x3 key operand of every packed row
+  QStat* qs3;
+  KeyMax* km3;
 };
 
 int default_kprime(int prec, int k) {
@@ -173,6 +187,10 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
       P.L = op_layout(PREC_FP32, d);
     }
   }
+  if (P.candidates && k > 1 && (P.prec == PREC_FP16 || P.prec == PREC_BF16)) {
+    P.L3 = op_layout(PREC_BF16X3, d);
+    P.refine = tc_config_ok(tc_default_config(PREC_BF16X3, d, P.kprime), P.L3.kp, P.kprime);
+  }
   return MSC_OK;
 }
 
@@ -199,6 +217,17 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
   w.perm = c.take<int32_t>(P.npacked);
   w.order_ws_bytes = order_workspace_bytes(P.npacked);
   w.order_ws = c.take<unsigned char>(w.order_ws_bytes);
+  if (P.refine) {
+    w.flags = c.take<int32_t>(P.npacked);
+    w.S = c.take<int64_t>(P.npacked + 1);
+    w.scan_scratch = c.take<int64_t>(scan_i32_scratch_elems(P.npacked));
+    w.qmap = c.take<int32_t>(P.n);
+    w.items3 = c.take<WorkItem>(P.ntiles);
+    w.A3 = c.take<uint16_t>(size_t(P.n) * P.L3.kp);
+    w.B3 = c.take<uint16_t>(size_t(P.npacked) * P.L3.kp);
+    w.qs3 = c.take<QStat>(P.npacked);
+    w.km3 = c.take<KeyMax>(1);
+  }
   return w;
 }
 
@@ -276,18 +305,39 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
     } else {
       if (P.prec == PREC_FP16)
         MSC_TRY(launch_maxnorm(Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.ctl, st));
-      MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked, w.Aop,
-                             w.Bop, w.qs, w.km, w.ctl, st));
+      MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
+                             nullptr, nullptr, 0, w.Aop, w.Bop, w.qs, w.km, w.ctl, st));
       stage_mark(st, 1);
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
-                            w.items, n_items, w.perm, w.ctl, P.kprime, w.cand_idx, w.cand_thr,
-                            P.kprime, st));
+                            w.items, n_items, w.perm, nullptr, nullptr, w.ctl, P.kprime,
+                            w.cand_idx, w.cand_thr, P.kprime, st));
     }
   }
   stage_mark(st, 2);
+  if (P.refine) MSC_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * P.npacked, st));
   MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                         P.kprime, P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx,
-                        knn_dist, w.fail_rows, w.ctl, st));
+                        knn_dist, w.fail_rows, w.ctl, nullptr, nullptr, 0,
+                        P.refine ? w.flags : nullptr, st));
+  if (P.refine) {
+    // the rows the one-term candidates could not certify, again with the three-term split
+    MSC_TRY(launch_refine_plan(w.flags, P.npacked, w.seg, P.nseg, w.qmap, w.items3, w.S,
+                               w.scan_scratch, w.ctl, st));
+    MSC_CUDA_TRY(cudaMemsetAsync(w.km3, 0, sizeof(KeyMax), st));
+    MSC_TRY(launch_pack_tc(PREC_BF16X3, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
+                           nullptr, nullptr, 0, nullptr, w.B3, w.qs3, w.km3, w.ctl, st));
+    MSC_TRY(launch_pack_tc(PREC_BF16X3, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
+                           w.qmap, &w.ctl->n_refine, P.n, w.A3, nullptr, nullptr, nullptr, w.ctl,
+                           st));
+    const TcConfig cfg3 = tc_default_config(PREC_BF16X3, P.d, P.kprime);
+    MSC_TRY(launch_knn_tc(PREC_BF16X3, cfg3, w.A3, w.B3, P.n, P.npacked, P.L3.kp, P.L3.kmma,
+                          w.items3, P.ntiles, w.perm, w.qmap, &w.ctl->n_items_refine, w.ctl,
+                          P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
+    MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
+                          P.kprime, P.kprime, w.qs3, w.km3, PREC_BF16X3, P.L3.kmma, P.k, cosine,
+                          knn_idx, knn_dist, w.fail_rows, w.ctl, w.qmap, &w.ctl->n_refine, P.n,
+                          nullptr, st));
+  }
   MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
                            knn_idx, knn_dist, w.ctl, st));
   stage_mark(st, 3);

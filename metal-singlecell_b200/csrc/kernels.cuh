@@ -64,8 +64,11 @@ size_t colmean_partial_elems(int nseg, int d, int nb);
 int launch_maxnorm(const float* X, const SegDesc* seg, int nseg, const double* mean, int d,
                    int64_t npacked, Ctl* ctl, cudaStream_t st);
 // packed row p holds original row perm[p] (-1: padding) of the sample seg[find_seg(p)]
+// rows/nrows: pack only the listed packed rows (device count, at most max_rows) into output rows
+// 0..; null: every packed row.  Aop or Bop may be null; qs/km (key statistics) may be null.
 int launch_pack_tc(int prec, const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
-                   const double* mean, int d, int64_t npacked, void* Aop, void* Bop, QStat* qs,
+                   const double* mean, int d, int64_t npacked, const int32_t* rows,
+                   const int32_t* nrows, int64_t max_rows, void* Aop, void* Bop, QStat* qs,
                    KeyMax* km, const Ctl* ctl, cudaStream_t st);
 int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
                      const double* mean, int d, int dpad, int64_t npacked, float* A32, float* sq32,
@@ -104,8 +107,9 @@ bool profiling_enabled();
 TcConfig tc_default_config(int prec, int d, int kprime);
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
-                  int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
-                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
+                  int64_t n_items, const int32_t* perm, const int32_t* qmap,
+                  const int32_t* n_items_dev, Ctl* ctl, int kprime, int32_t* cand_idx,
+                  float* cand_thr, int cand_stride, cudaStream_t st);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
@@ -113,7 +117,13 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   const int32_t* cand_idx, const float* cand_thr, int cand_stride, int kprime,
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
-                  cudaStream_t st);
+                  const int32_t* rows, const int32_t* nrows, int64_t max_rows,
+                  int32_t* fail_flags, cudaStream_t st);
+// refine plan: compact the flagged packed rows (sorted) into qmap, count them (ctl->n_refine)
+// and cut them into per-sample query tiles (items, ctl->n_items_refine); S: npacked+1 int64
+int launch_refine_plan(const int32_t* flags, int64_t npacked, const SegDesc* seg, int nseg,
+                       int32_t* qmap, WorkItem* items, int64_t* S, int64_t* scan_scratch,
+                       Ctl* ctl, cudaStream_t st);
 int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
                          cudaStream_t st);
 int launch_fp64_scan(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

@@ -140,7 +140,8 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       const int wrow0 = tid & ~31;
       const int nvalid = min(32, w.nq - wrow0);
       if (nvalid > 0)
-        sel.finish(cand_idx, cand_thr, cand_stride, perm, int64_t(w.qrow0) + wrow0, nvalid, kprime);
+        sel.finish(cand_idx, cand_thr, cand_stride, perm, nullptr, int64_t(w.qrow0) + wrow0, nvalid,
+                   kprime);
       else
         sel.flush();
     }

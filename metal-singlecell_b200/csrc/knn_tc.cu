@@ -298,6 +298,8 @@ struct TcParams {
   uint32_t idesc;
   int prof;         // accumulate the pipeline counters below
   const int32_t* perm;   // packed position -> original row (-1: padding)
+  const int32_t* qmap;   // query row -> packed position (refine pass over a row list), or null
+  const int32_t* n_items_dev;   // work-item count in device memory (refine pass), or null
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -386,6 +388,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   const size_t a_bytes = size_t(P.kb) * BM * 128;
   const size_t b_bytes = size_t(brows) * 128;           // one K atom of this CTA's key rows
   const uint32_t tmem_cols = uint32_t(2 * P.bn);
+  const int n_items = P.n_items_dev ? *P.n_items_dev : P.n_items;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2; ++i) {
@@ -429,7 +432,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
       long long c_wait = 0;
-      for (int it = unit; it < P.n_items && ok; it += nunits) {
+      for (int it = unit; it < n_items && ok; it += nunits) {
         const WorkItem w = items[it];
         ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
         if (!ok) break;
@@ -439,7 +442,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                       w.qrow0 + int(rank) * BM);
         if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
         const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        const int diag = (w.qrow0 - w.key0) / P.bn;
+        const int diag = ((P.qmap ? P.qmap[w.qrow0] : w.qrow0) - w.key0) / P.bn;
         for (int j = 0; j < nkt && ok; ++j) {
           const int kt = key_tile_at(j, diag, nkt);
           for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
@@ -472,7 +475,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       int stage = 0, abuf = 0;
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
-      for (int it = unit; it < P.n_items && ok; it += nunits) {
+      for (int it = unit; it < n_items && ok; it += nunits) {
         const WorkItem w = items[it];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (!ok) break;
@@ -496,7 +499,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       uint32_t sphase = 0, aphase = 0, accphase = 0;
       bool ok = true, issued = false;
       long long c_b = 0, c_acc = 0;
-      for (int it = unit; it < P.n_items && ok; it += nunits) {
+      for (int it = unit; it < n_items && ok; it += nunits) {
         const WorkItem w = items[it];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
@@ -573,16 +576,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       qphase ^= 1;
       return r;
     };
-    for (int it = unit; it < P.n_items && ok; it += nunits) {
+    for (int it = unit; it < n_items && ok; it += nunits) {
       const WorkItem w = items[it];
       const long long tl = P.prof ? clock64() : 0;
       // neighbour ids are packed positions here; finish() maps them to original rows
       const int nq = min(BM, w.nq - int(rank) * BM);   // this CTA's valid query rows (may be <= 0)
       const int qrow = w.qrow0 + int(rank) * BM;
-      const int self = qrow + row;
+      const int self = P.qmap ? (row < nq ? P.qmap[qrow + row] : -1) : qrow + row;
       const int limit = w.key0 + w.nkeys;
       const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-      const int diag = (w.qrow0 - w.key0) / P.bn;
+      const int diag = ((P.qmap ? P.qmap[w.qrow0] : w.qrow0) - w.key0) / P.bn;
       for (int j = 0; j < nkt; ++j) {
         const int kt = key_tile_at(j, diag, nkt);
         const long long te = P.prof ? clock64() : 0;
@@ -632,8 +635,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       const int nvalid = min(32, nq - wrow0);
       if (NH == 1) {
         if (nvalid > 0)
-          sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, int64_t(qrow) + wrow0, nvalid,
-                     P.kprime);
+          sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
+                     nvalid, P.kprime);
         else
           sel.flush();
       } else {
@@ -646,8 +649,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         if (h == 0) {
           sel.merge_from(smem + sp.sel_off + Sel::smem_bytes());
           if (nvalid > 0)
-            sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, int64_t(qrow) + wrow0, nvalid,
-                       P.kprime);
+            sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
+                       nvalid, P.kprime);
         }
         ok = quarter_sync();                       // the partner's list is read; reuse it
         if (!ok) break;
@@ -862,7 +865,8 @@ TcConfig tc_default_config(int prec, int d, int kprime) {
 
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
-                  int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime, int32_t* cand_idx,
+                  int64_t n_items, const int32_t* perm, const int32_t* qmap,
+                  const int32_t* n_items_dev, Ctl* ctl, int kprime, int32_t* cand_idx,
                   float* cand_thr, int cand_stride, cudaStream_t st) {
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
@@ -886,6 +890,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.idesc = idesc_f16(bf16, cfg.pair ? 2 * BM : BM, cfg.bn);
   P.prof = profiling_enabled() ? 1 : 0;
   P.perm = perm;
+  P.qmap = qmap;
+  P.n_items_dev = n_items_dev;
   if (cfg.pair) {
     if (cfg.epi == 8)
       return launch_tc_epi<8, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);

@@ -115,7 +115,9 @@ struct Ctl {
   int32_t timeout_flag;
   double colsum_scale;      // scale factor f applied to the centred rows (power of two)
   unsigned max_sq_bits;     // max Σ z² over rows (before scaling), float bits
-  int32_t pad;
+  int32_t n_refine;         // rows compacted for the BF16x3 refine pass
+  int32_t n_items_refine;   // query tiles of the refine pass
+  int32_t pad[3];
 };
 
 // ------------------------------------------------------------------------------------------------

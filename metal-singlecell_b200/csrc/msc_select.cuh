@@ -208,18 +208,21 @@ struct RowSelect {
   __device__ void flush() { compact_own(); }
 
   // warp-collective: flush and write the first `kout` list entries and the threshold value
-  // (list[k'-1]) of the warp's first `nvalid_rows` rows.  Rows and columns are packed positions;
-  // perm maps them to original rows (the output row and the stored neighbour ids).
+  // (list[k'-1]) of the warp's first `nvalid_rows` rows.  Columns are packed positions; the
+  // warp's rows are query rows first_row.. (packed positions, or through qmap when the queries
+  // are a compacted row list); perm maps packed positions to original rows (the output row and
+  // the stored neighbour ids).
   __device__ void finish(int* out_idx, float* out_thr, int out_stride,
-                         const int32_t* __restrict__ perm, int64_t first_packed_row,
-                         int nvalid_rows, int kout) {
+                         const int32_t* __restrict__ perm, const int32_t* __restrict__ qmap,
+                         int64_t first_row, int nvalid_rows, int kout) {
     compact_own();
     __syncwarp();
     const int lane = lane_id();
     const int row0 = row - lane;
     for (int r = 0; r < nvalid_rows; ++r) {
       const int rr = row0 + r;
-      const int64_t orow = perm[first_packed_row + r];
+      const int64_t prow = qmap ? int64_t(qmap[first_row + r]) : first_row + r;
+      const int64_t orow = perm[prow];
       for (int s = lane; s < kout; s += 32) {
         const int c = li[s * ROWS + rr];
         out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;

@@ -185,12 +185,19 @@ __device__ __forceinline__ void block_keymax(float (&m)[5], KeyMax* km) {
   }
 }
 
+// Operand rows of the tensor-core candidate kernel.  Packed row p (original row perm[p]) goes to
+// output row p, or — with a row list — list entry q (packed row rows[q], q < *nrows) goes to
+// output row q.  Aop / Bop may each be null (that side is not written); the key-side statistics
+// (qs, km) are written with the key side.
 template <class T, int SPLIT>
 __global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
-                               const SegDesc* __restrict__ seg, int nseg, const double* __restrict__ mean, int d, int kp, int prec,
-                               int64_t npacked, T* __restrict__ Aop, T* __restrict__ Bop,
-                               QStat* __restrict__ qs, KeyMax* __restrict__ km,
-                               const Ctl* __restrict__ ctl, double pad_term) {
+                               const SegDesc* __restrict__ seg, int nseg,
+                               const double* __restrict__ mean, int d, int kp, int prec,
+                               int64_t npacked, const int32_t* __restrict__ rows,
+                               const int32_t* __restrict__ nrows, T* __restrict__ Aop,
+                               T* __restrict__ Bop, QStat* __restrict__ qs,
+                               KeyMax* __restrict__ km, const Ctl* __restrict__ ctl,
+                               double pad_term) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const double f = pack_scale(prec, ctl);
@@ -198,15 +205,17 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __res
   const T one = to_op<T>(1.0);
   const T padt = to_op<T>(pad_term);
   const int kd = SPLIT * d;                     // first column after the data terms
+  const int64_t count = rows ? int64_t(*nrows) : npacked;
   float mx[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
-       p += nwarps) {
+  for (int64_t q = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; q < count;
+       q += nwarps) {
+    const int64_t p = rows ? int64_t(rows[q]) : q;
     const int s = find_seg(seg, nseg, p);
     const int64_t orow = perm[p];
     const bool valid = orow >= 0;
     const double* c = mean + int64_t(s) * d;
-    T* arow = Aop + p * kp;
-    T* brow = Bop + p * kp;
+    T* arow = Aop ? Aop + q * kp : nullptr;
+    T* brow = Bop ? Bop + q * kp : nullptr;
     double sq = 0.0, nh = 0.0, nl = 0.0, nr = 0.0;
     for (int t = lane; t < d; t += 32) {
       double z = valid ? (double(X[orow * d + t]) - c[t]) * f : 0.0;
@@ -220,12 +229,14 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __res
       nl += lv * lv;
       nr += r * r;
       if (SPLIT == 3) {
-        arow[t] = hi; arow[d + t] = hi; arow[2 * d + t] = lo;
-        brow[t] = to_op<T>(-2.0 * hv); brow[d + t] = to_op<T>(-2.0 * lv);
-        brow[2 * d + t] = to_op<T>(-2.0 * hv);
+        if (arow) { arow[t] = hi; arow[d + t] = hi; arow[2 * d + t] = lo; }
+        if (brow) {
+          brow[t] = to_op<T>(-2.0 * hv); brow[d + t] = to_op<T>(-2.0 * lv);
+          brow[2 * d + t] = to_op<T>(-2.0 * hv);
+        }
       } else {
-        arow[t] = hi;
-        brow[t] = to_op<T>(-2.0 * hv);
+        if (arow) arow[t] = hi;
+        if (brow) brow[t] = to_op<T>(-2.0 * hv);
       }
     }
     sq = warp_sum_d(sq); nh = warp_sum_d(nh); nl = warp_sum_d(nl); nr = warp_sum_d(nr);
@@ -238,54 +249,60 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __res
     const double nerr = fabs(sq - s1 - s2 - s3);
     for (int col = kd + lane; col < kp; col += 32) {
       const int jj = col - kd;
-      arow[col] = (jj < 3 && valid) ? one : zero;
-      T v = zero;
-      if (jj == 0) v = valid ? t1 : padt;
-      if (jj == 1) v = valid ? t2 : padt;
-      if (jj == 2) v = valid ? t3 : padt;
-      brow[col] = v;
+      if (arow) arow[col] = (jj < 3 && valid) ? one : zero;
+      if (brow) {
+        T v = zero;
+        if (jj == 0) v = valid ? t1 : padt;
+        if (jj == 1) v = valid ? t2 : padt;
+        if (jj == 2) v = valid ? t3 : padt;
+        brow[col] = v;
+      }
     }
-    if (lane == 0) {
-      QStat q;
-      q.sq = sq;
-      q.hi = __double2float_ru(sqrt(nh));
-      q.lo = __double2float_ru(sqrt(nl));
-      q.res = __double2float_ru(sqrt(nr));
-      q.pad = 0.f;
-      qs[p] = q;
+    if (lane == 0 && qs) {
+      QStat qq;
+      qq.sq = sq;
+      qq.hi = __double2float_ru(sqrt(nh));
+      qq.lo = __double2float_ru(sqrt(nl));
+      qq.res = __double2float_ru(sqrt(nr));
+      qq.pad = 0.f;
+      qs[p] = qq;
       if (valid) {
-        mx[0] = fmaxf(mx[0], q.hi);
-        mx[1] = fmaxf(mx[1], q.lo);
-        mx[2] = fmaxf(mx[2], q.res);
+        mx[0] = fmaxf(mx[0], qq.hi);
+        mx[1] = fmaxf(mx[1], qq.lo);
+        mx[2] = fmaxf(mx[2], qq.res);
         mx[3] = fmaxf(mx[3], __double2float_ru(nerr));
         mx[4] = fmaxf(mx[4], __double2float_ru(sq));
       }
     }
   }
-  block_keymax(mx, km);
+  if (km) block_keymax(mx, km);
 }
 
 int launch_pack_tc(int prec, const float* X, const int32_t* perm, const SegDesc* seg, int nseg,
-                   const double* mean, int d, int64_t npacked, void* Aop, void* Bop, QStat* qs,
+                   const double* mean, int d, int64_t npacked, const int32_t* rows,
+                   const int32_t* nrows, int64_t max_rows, void* Aop, void* Bop, QStat* qs,
                    KeyMax* km, const Ctl* ctl, cudaStream_t st) {
   const OpLayout L = op_layout(prec, d);
-  int blocks = int(std::min<int64_t>(ceil_div(npacked, 8), int64_t(num_sms()) * 16));
+  const int64_t n_out = rows ? max_rows : npacked;
+  int blocks = int(std::min<int64_t>(ceil_div(n_out, 8), int64_t(num_sms()) * 16));
   blocks = std::max(blocks, 1);
   switch (prec) {
     case PREC_BF16X3:
       pack_tc_kernel<__nv_bfloat16, 3><<<blocks, 256, 0, st>>>(
-          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
-          static_cast<__nv_bfloat16*>(Bop), qs, km, ctl, PAD_NORM_TERM_BF16);
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, rows, nrows,
+          static_cast<__nv_bfloat16*>(Aop), static_cast<__nv_bfloat16*>(Bop), qs, km, ctl,
+          PAD_NORM_TERM_BF16);
       break;
     case PREC_BF16:
       pack_tc_kernel<__nv_bfloat16, 1><<<blocks, 256, 0, st>>>(
-          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__nv_bfloat16*>(Aop),
-          static_cast<__nv_bfloat16*>(Bop), qs, km, ctl, PAD_NORM_TERM_BF16);
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, rows, nrows,
+          static_cast<__nv_bfloat16*>(Aop), static_cast<__nv_bfloat16*>(Bop), qs, km, ctl,
+          PAD_NORM_TERM_BF16);
       break;
     case PREC_FP16:
       pack_tc_kernel<__half, 1><<<blocks, 256, 0, st>>>(
-          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, static_cast<__half*>(Aop),
-          static_cast<__half*>(Bop), qs, km, ctl, PAD_NORM_TERM_FP16);
+          X, perm, seg, nseg, mean, d, L.kp, prec, npacked, rows, nrows,
+          static_cast<__half*>(Aop), static_cast<__half*>(Bop), qs, km, ctl, PAD_NORM_TERM_FP16);
       break;
     default:
       set_error("pack_tc: bad precision %d", prec);

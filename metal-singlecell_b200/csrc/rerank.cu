@@ -98,7 +98,9 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
               const float* __restrict__ cand_thr, int cand_stride, int kprime,
               const QStat* __restrict__ qs, const KeyMax* __restrict__ km, Ctl* __restrict__ ctl,
               int prec, int kmma, int k, int cosine, int32_t* __restrict__ knn_idx,
-              float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows) {
+              float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows,
+              const int32_t* __restrict__ rows, const int32_t* __restrict__ nrows,
+              int32_t* __restrict__ fail_flags) {
   __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
@@ -120,8 +122,10 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
   const double f2 = f * f;
   const double delta = double(d + 4) * 0x1p-24;
   int64_t n_cert = 0, n_ties = 0;
-  for (int64_t p = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; p < npacked;
-       p += nwarps) {
+  const int64_t count = rows ? int64_t(*nrows) : npacked;
+  for (int64_t wq = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; wq < count;
+       wq += nwarps) {
+    const int64_t p = rows ? int64_t(rows[wq]) : wq;
     const int64_t i = perm[p];                          // original row
     if (i < 0) continue;                                // padding (warp-uniform)
     const int s = find_seg(seg, nseg, p);
@@ -191,10 +195,13 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     }
     if (lane == 0) {
       n_ties += m - kk;
-      if (cert) ++n_cert;
-      else {
+      if (cert) {
+        ++n_cert;
+      } else if (fail_flags) {
+        fail_flags[p] = 1;                              // to the refine pass
+      } else {
         int slot = atomicAdd(&ctl->n_fail, 1);
-        fail_rows[slot] = int32_t(p);                   // packed row
+        fail_rows[slot] = int32_t(p);                   // packed row, to the FP64 scan
       }
     }
     __syncwarp();
@@ -294,6 +301,44 @@ __global__ void all_rows_fail_kernel(const int32_t* __restrict__ perm, int64_t n
     if (perm[p] >= 0) fail_rows[atomicAdd(&ctl->n_fail, 1)] = int32_t(p);
 }
 
+// refine pass: the flagged rows, in packed order, as a compact query list
+__global__ void compact_flags_kernel(const int32_t* __restrict__ flags,
+                                     const int64_t* __restrict__ S, int64_t npacked,
+                                     int32_t* __restrict__ qmap, Ctl* __restrict__ ctl) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    if (flags[p]) qmap[S[p]] = int32_t(p);
+    if (p == 0) {
+      ctl->n_refine = int32_t(S[npacked]);
+      ctl->stats[MSC_STAT_REFINED] = S[npacked];
+    }
+  }
+}
+
+// query tiles of at most QTILE listed rows, never spanning two samples (one thread: the list is
+// short and the tile count is written once)
+__global__ void refine_items_kernel(const SegDesc* __restrict__ seg, int nseg,
+                                    const int64_t* __restrict__ S, WorkItem* __restrict__ items,
+                                    Ctl* __restrict__ ctl) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int32_t n = 0;
+  for (int s = 0; s < nseg; ++s) {
+    const int64_t cs = S[seg[s].poff], ce = S[seg[s].poff + seg[s].n];
+    for (int64_t q = cs; q < ce; q += QTILE) {
+      WorkItem w;
+      w.qrow0 = int32_t(q);
+      w.nq = int32_t(min64(QTILE, ce - q));
+      w.key0 = int32_t(seg[s].poff);
+      w.nkeys = int32_t(seg[s].n);
+      w.orig_off = int32_t(seg[s].off);
+      w.qorig0 = 0;
+      w.pad0 = w.pad1 = 0;
+      items[n++] = w;
+    }
+  }
+  ctl->n_items_refine = n;
+}
+
 }  // namespace
 
 int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
@@ -309,15 +354,29 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   const int32_t* cand_idx, const float* cand_thr, int cand_stride, int kprime,
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
-                  cudaStream_t st) {
+                  const int32_t* rows, const int32_t* nrows, int64_t max_rows,
+                  int32_t* fail_flags, cudaStream_t st) {
   if (kprime > 64 || k - 1 > 64) {
     set_error("rerank: kprime=%d / k=%d beyond 64", kprime, k);
     return MSC_ERR_UNSUPPORTED;
   }
-  int blocks = int(std::min<int64_t>(ceil_div(npacked, RR_WARPS), int64_t(num_sms()) * 8));
+  const int64_t n_work = rows ? max_rows : npacked;
+  int blocks = int(std::min<int64_t>(ceil_div(n_work, RR_WARPS), int64_t(num_sms()) * 8));
   rerank_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
       X, d, perm, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
-      kmma, k, cosine, knn_idx, knn_dist, fail_rows);
+      kmma, k, cosine, knn_idx, knn_dist, fail_rows, rows, nrows, fail_flags);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_refine_plan(const int32_t* flags, int64_t npacked, const SegDesc* seg, int nseg,
+                       int32_t* qmap, WorkItem* items, int64_t* S, int64_t* scan_scratch,
+                       Ctl* ctl, cudaStream_t st) {
+  MSC_TRY(scan_excl_i32(flags, npacked, S, scan_scratch, st));
+  int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
+  compact_flags_kernel<<<std::max(blocks, 1), 256, 0, st>>>(flags, S, npacked, qmap, ctl);
+  MSC_LAUNCH_CHECK();
+  refine_items_kernel<<<1, 32, 0, st>>>(seg, nseg, S, items, ctl);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }

@@ -57,11 +57,12 @@ def test_argument_checks(n, d, k, metric, prec, kprime, code):
 
 def test_workspace_queries_are_host_only():
     lib = _lib.load()
-    a = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 1, 0)
-    b = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 2, 0)
-    c = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 0, 0)
-    assert a > b > c > 0
-    assert a < 4e9            # the whole scale workload fits a few GB of the 180 GB
+    a = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 1, 0)     # BF16x3
+    b = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 2, 0)     # FP16 (+ refine)
+    c = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 0, 0)     # FP32
+    # FP16 carries the BF16x3 refine operands on top of its own, FP32 has the narrowest rows
+    assert b > a > c > 0
+    assert b < 4e9            # the whole scale workload fits a few GB of the 180 GB
     assert lib.msc_neighbors_workspace_bytes(10, 5, 11, 0, 0, 1, 0) == 0
     off = (ctypes.c_int64 * 4)(0, 100, 300, 350)
     assert lib.msc_batched_workspace_bytes(off, 3, 30, 15, 0, 1, 0) > 0

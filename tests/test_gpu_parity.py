@@ -178,3 +178,17 @@ def test_candidate_tile_configs_agree(monkeypatch, precision, kprime):
         np.testing.assert_array_equal(gd, ref["dist"], err_msg=hex(code))
         assert_csr_equal(gconn, ref["connectivities"], f"connectivities {hex(code)}")
     assert tried >= (5 if kprime <= 32 else 1)     # 64-entry lists fit fewer configurations
+
+
+@pytest.mark.parametrize("precision,kprime", [("fp16", 0), ("bf16", 14), ("fp16", 14)])
+def test_refine_pass(precision, kprime):
+    """One-term FP16/BF16 candidates: rows whose certificate fails re-run through the BF16x3
+    candidate kernel (MSC_STAT_REFINED), and only rows failing that too take the FP64 scan.
+    k' = k-1 (no over-fetch) sends many rows through the refine pass; the graph must still be
+    the oracle's, bit for bit."""
+    X = synth.gaussian_mixture(30000, 50, 12, seed=31, sizes="lognormal")
+    stats = check_against_oracle(X, 15, precision=precision, kprime=kprime)
+    refined = int(stats[_lib.STAT_REFINED])
+    assert int(stats[_lib.STAT_RESCANNED]) <= refined
+    if kprime == 14:
+        assert refined > 0
