@@ -309,7 +309,8 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                              nullptr, nullptr, 0, w.Aop, w.Bop, w.qs, w.km, w.ctl, st));
       stage_mark(st, 1);
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
-                            w.items, n_items, w.perm, nullptr, nullptr, w.ctl, P.kprime,
+                            w.items, n_items, w.perm, nullptr, nullptr, &w.ctl->tc_counter[0],
+                            w.ctl, P.kprime,
                             w.cand_idx, w.cand_thr, P.kprime, st));
     }
   }
@@ -331,7 +332,8 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                            st));
     const TcConfig cfg3 = tc_default_config(PREC_BF16X3, P.d, P.kprime);
     MSC_TRY(launch_knn_tc(PREC_BF16X3, cfg3, w.A3, w.B3, P.n, P.npacked, P.L3.kp, P.L3.kmma,
-                          w.items3, P.ntiles, w.perm, w.qmap, &w.ctl->n_items_refine, w.ctl,
+                          w.items3, P.ntiles, w.perm, w.qmap, &w.ctl->n_items_refine,
+                          &w.ctl->tc_counter[1], w.ctl,
                           P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
     MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                           P.kprime, P.kprime, w.qs3, w.km3, PREC_BF16X3, P.L3.kmma, P.k, cosine,

@@ -108,8 +108,8 @@ TcConfig tc_default_config(int prec, int d, int kprime);
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
                   int64_t n_items, const int32_t* perm, const int32_t* qmap,
-                  const int32_t* n_items_dev, Ctl* ctl, int kprime, int32_t* cand_idx,
-                  float* cand_thr, int cand_stride, cudaStream_t st);
+                  const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
+                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

@@ -41,6 +41,7 @@ namespace {
 
 constexpr int EPI_WARP0 = 4;
 constexpr int BM = 128;
+constexpr int ITEM_RING = 4;                        // claimed work items in flight per CTA
 constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
 constexpr size_t SMEM_LIMIT = 232448;               // 227 KB opt-in per block
 
@@ -300,6 +301,7 @@ struct TcParams {
   const int32_t* perm;   // packed position -> original row (-1: padding)
   const int32_t* qmap;   // query row -> packed position (refine pass over a row list), or null
   const int32_t* n_items_dev;   // work-item count in device memory (refine pass), or null
+  int32_t* counter;             // next unclaimed work item (zero at launch; single CTAs only)
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -377,7 +379,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   uint64_t* a_peer = bars + 29;            // [2] pair: the odd CTA's query rows landed
   uint64_t* b_peer = bars + 31;            // [stages <= 8] pair: the odd CTA's key rows landed
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 39);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 40);   // 41 x 8 B < 512 B
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 40);
+  uint64_t* item_full = bars + 41;         // [ITEM_RING] a claimed work item is in item_ring
+  uint64_t* item_empty = bars + 45;        // [ITEM_RING] every consumer has read it
+  int* item_ring = reinterpret_cast<int*>(bars + 49);   // [ITEM_RING]; 51 x 8 B < 512 B
   float* pub = reinterpret_cast<float*>(smem + sp.pub_off);
 
   const int warp = warp_id(), lane = lane_id();
@@ -405,6 +410,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       mbar_init(&b_peer[s], 1);
     }
     for (int q = 0; q < 4; ++q) mbar_init(&qbar[q], 2);
+    for (int r = 0; r < ITEM_RING; ++r) {
+      mbar_init(&item_full[r], 1);
+      mbar_init(&item_empty[r], 1 + NEPI);   // the MMA thread and every epilogue warp
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -425,6 +434,46 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   const uint32_t tmem_base = *tmem_slot;
   const long long t_kernel0 = clock64();
 
+  // Work distribution.  A single CTA claims work items dynamically: its producer thread takes the
+  // next item from a global counter and hands it to the MMA thread and the epilogue warps through
+  // a ring in shared memory, so query tiles of very different cost spread evenly over the SMs.
+  // CTA pairs keep a static round-robin assignment (both CTAs of a pair take the same items).
+  int r_slot = 0, s_next = unit;
+  uint32_t r_phase = 0;
+  // producer: claim the next item (-1: none left) and publish it; false = the kernel is aborting
+  auto claim = [&](int& it) -> bool {
+    if (PAIR) {
+      it = s_next < n_items ? s_next : -1;
+      s_next += nunits;
+      return true;
+    }
+    if (!mbar_wait(&item_empty[r_slot], r_phase ^ 1, abort_flag)) return false;
+    int v = atomicAdd(P.counter, 1);
+    if (v >= n_items) v = -1;
+    item_ring[r_slot] = v;
+    mbar_arrive(&item_full[r_slot]);         // release: the ring entry is visible to the waiters
+    if (++r_slot == ITEM_RING) { r_slot = 0; r_phase ^= 1; }
+    it = v;
+    return true;
+  };
+  // consumers: the next published item, by one thread or by a whole warp (warp_wide)
+  auto receive = [&](int& it, bool warp_wide) -> bool {
+    if (PAIR) {
+      it = s_next < n_items ? s_next : -1;
+      s_next += nunits;
+      return true;
+    }
+    bool got = mbar_wait(&item_full[r_slot], r_phase, abort_flag);
+    if (warp_wide) got = __all_sync(FULL, got);
+    if (!got) return false;
+    const int v = *reinterpret_cast<volatile int*>(&item_ring[r_slot]);
+    if (warp_wide) __syncwarp();
+    if (!warp_wide || lane_id() == 0) mbar_arrive(&item_empty[r_slot]);
+    if (++r_slot == ITEM_RING) { r_slot = 0; r_phase ^= 1; }
+    it = v;
+    return true;
+  };
+
   if (warp == 0) {
     // ------------------------------------------------------------------ TMA producer (each CTA)
     if (lane == 0) {
@@ -432,7 +481,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
       long long c_wait = 0;
-      for (int it = unit; it < n_items && ok; it += nunits) {
+      for (;;) {
+        int it;
+        if (!claim(it)) { ok = false; break; }
+        if (it < 0) break;
         const WorkItem w = items[it];
         ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
         if (!ok) break;
@@ -456,6 +508,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
         }
+        if (!ok) break;
       }
       if (P.prof) atomicAdd(&g_tc_prof[0], (unsigned long long)c_wait);
       // drain: every load this thread armed completes on its own; wait for them (bounded)
@@ -499,7 +552,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       uint32_t sphase = 0, aphase = 0, accphase = 0;
       bool ok = true, issued = false;
       long long c_b = 0, c_acc = 0;
-      for (int it = unit; it < n_items && ok; it += nunits) {
+      for (;;) {
+        int it;
+        if (!receive(it, false)) { ok = false; break; }
+        if (it < 0) break;
         const WorkItem w = items[it];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
@@ -576,7 +632,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       qphase ^= 1;
       return r;
     };
-    for (int it = unit; it < n_items && ok; it += nunits) {
+    for (;;) {
+      int it;
+      if (!receive(it, true)) { ok = false; break; }
+      if (it < 0) break;
       const WorkItem w = items[it];
       const long long tl = P.prof ? clock64() : 0;
       // neighbour ids are packed positions here; finish() maps them to original rows
@@ -866,8 +925,8 @@ TcConfig tc_default_config(int prec, int d, int kprime) {
 int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bop,
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
                   int64_t n_items, const int32_t* perm, const int32_t* qmap,
-                  const int32_t* n_items_dev, Ctl* ctl, int kprime, int32_t* cand_idx,
-                  float* cand_thr, int cand_stride, cudaStream_t st) {
+                  const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
+                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st) {
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
               cfg.bn, cfg.stages, cfg.kpl, cfg.cb, cfg.epi, cfg.pair);
@@ -892,6 +951,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.perm = perm;
   P.qmap = qmap;
   P.n_items_dev = n_items_dev;
+  P.counter = counter;
   if (cfg.pair) {
     if (cfg.epi == 8)
       return launch_tc_epi<8, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);

@@ -117,7 +117,7 @@ struct Ctl {
   unsigned max_sq_bits;     // max Σ z² over rows (before scaling), float bits
   int32_t n_refine;         // rows compacted for the BF16x3 refine pass
   int32_t n_items_refine;   // query tiles of the refine pass
-  int32_t pad[3];
+  int32_t tc_counter[3];    // item counters of the tensor-core launches (main, refine, near)
 };
 
 // ------------------------------------------------------------------------------------------------
