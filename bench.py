@@ -251,7 +251,8 @@ def run_ours(args):
     buf = (ctypes.c_float * 8)()
     ns = lib.msc_profile_read(buf, 8)
     lib.msc_profile_enable(0)
-    stage_names = ["prep", "candidates", "rerank_fp64", "csr_rho_sigma_membership", "union"]
+    stage_names = ["prep", "prune_plan", "candidates", "rerank_fp64", "csr_rho_sigma_membership",
+                   "union"]
     stages = {stage_names[i]: round(buf[i], 3) for i in range(min(ns, len(stage_names)))}
     cnt = (ctypes.c_ulonglong * 16)()
     lib.msc_profile_counters(cnt, 16)
@@ -261,6 +262,9 @@ def run_ours(args):
                 "epilogue_loop": cnt[4] / ctas / 4, "kernel": cnt[5] / ctas,
                 "hot_chunks_per_warp": cnt[6] / ctas / 4, "compactions_per_thread": cnt[7] / ctas / 128,
                 "appends_per_row": cnt[8] / max(n, 1), "ctas": ctas}
+    # key tiles beyond the near ones: kept by the pruning plan / all of them
+    pruning = {"far_tiles_visited": int(cnt[10]), "far_tiles_total": int(cnt[11]),
+               "visited_frac": (cnt[10] / cnt[11]) if cnt[11] else None}
 
     pk, pk_kind = peaks()
     cand_ms = stages.get("candidates")
@@ -279,7 +283,7 @@ def run_ours(args):
                 "kernel": "knn_tc_kernel" if args.precision != "fp32" else "knn_fp32_kernel",
                 "algorithmic_flop_per_launch": alg_flop, "kernel_ms": cand_ms,
                 "peak_kind": f"{pk_kind} bf16 sustained (kernel timed inside a full step)",
-                "stage_ms": stages, "pipeline_cycles_per_cta": pipeline}
+                "stage_ms": stages, "pipeline_cycles_per_cta": pipeline, "pruning": pruning}
 
     # e2e through the public call: pinned host in, both CSR matrices back to pinned host
     Xh = torch.from_numpy(X).pin_memory()

@@ -91,6 +91,9 @@ struct Problem {
   // the BF16x3 candidate kernel before the FP64 scan takes what is left
   bool refine = false;
   OpLayout L3{};
+  // key-tile pruning of the tensor-core scan (prune.cu): workspace carved, mask words per item
+  bool prune = false;
+  int prune_words = 0;
 };
 
 struct KnnWs {
@@ -122,6 +125,7 @@ struct KnnWs {
   void* B3;               // BF16x3 key operand of every packed row
   QStat* qs3;
   KeyMax* km3;
+  PruneWs pr;
 };
 
 int default_kprime(int prec, int k) {
@@ -146,6 +150,11 @@ int check_common(int64_t n, int d, int k, int metric, int prec, int kprime) {
   }
   return MSC_OK;
 }
+
+// key-tile pruning: samples from this size on, key tiles of this many rows, mask size cap
+constexpr int64_t PRUNE_MIN_CELLS = 4096;
+constexpr int PRUNE_BN = 256;
+constexpr int64_t PRUNE_MASK_MAX = int64_t(2) << 30;
 
 int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int kprime,
                  const int64_t* offsets, int nseg) {
@@ -191,8 +200,21 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
     P.L3 = op_layout(PREC_BF16X3, d);
     P.refine = tc_config_ok(tc_default_config(PREC_BF16X3, d, P.kprime), P.L3.kp, P.kprime);
   }
+  // Pruning pays once a sample spans many key tiles beyond the near ones; its mask (one bit per
+  // 256-key tile per 128-row query tile) is capped at 2 GB.  MSC_B200_PRUNE=0 turns it off.
+  if (P.candidates && k > 1 && P.prec != PREC_FP32 && P.max_seg >= PRUNE_MIN_CELLS) {
+    const char* env = std::getenv("MSC_B200_PRUNE");
+    const int words = prune_mask_words(P.max_seg, PRUNE_BN);
+    if (!(env && *env == '0') && double(P.ntiles) * words * 4.0 <= double(PRUNE_MASK_MAX)) {
+      P.prune = true;
+      P.prune_words = words;
+    }
+  }
   return MSC_OK;
 }
+
+// leaves of the locality tree (order.cu) hold at most this many rows
+constexpr int ORDER_LEAF = 256;
 
 KnnWs carve_knn(Carver& c, const Problem& P) {
   KnnWs w{};
@@ -215,7 +237,7 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
   w.cand_thr = c.take<float>(P.n);
   w.fail_rows = c.take<int32_t>(P.n);
   w.perm = c.take<int32_t>(P.npacked);
-  w.order_ws_bytes = order_workspace_bytes(P.npacked);
+  w.order_ws_bytes = order_workspace_bytes(P.npacked, P.d, ORDER_LEAF);
   w.order_ws = c.take<unsigned char>(w.order_ws_bytes);
   if (P.refine) {
     w.flags = c.take<int32_t>(P.npacked);
@@ -228,13 +250,13 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
     w.qs3 = c.take<QStat>(P.npacked);
     w.km3 = c.take<KeyMax>(1);
   }
+  if (P.prune) w.pr = carve_prune(c, P.npacked, P.nseg, P.d, P.ntiles, P.prune_words);
   return w;
 }
 
 // Levels of the locality tree (order.cu) for the tensor-core path: enough halvings to bring the
 // largest sample to leaves of ORDER_LEAF rows, plus slack for uneven splits.  The FP32 SIMT kernel
 // scans keys in plain order, so it keeps the identity order.  MSC_B200_ORDER=0 turns it off.
-constexpr int ORDER_LEAF = 256;
 int order_levels(const Problem& P, bool tc) {
   if (!tc || P.max_seg <= 2 * ORDER_LEAF) return 0;
   const char* env = std::getenv("MSC_B200_ORDER");
@@ -285,8 +307,10 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   const int64_t n_items = pair_items ? P.nptiles : P.ntiles;
   MSC_TRY(launch_build_items(w.seg, P.nseg, n_items, pair_items ? 2 * QTILE : QTILE, w.items, w.ctl,
                              st));
+  // pruning needs single-CTA work items over 256-key tiles
+  const bool prune = P.prune && tc && !cfg.pair && cfg.bn == PRUNE_BN;
   MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc), ORDER_LEAF,
-                       w.perm, w.order_ws, w.order_ws_bytes, st));
+                       w.perm, prune ? w.pr.leaf : nullptr, w.order_ws, w.order_ws_bytes, st));
   if (!P.candidates) {
     MSC_TRY(launch_all_rows_fail(w.perm, P.npacked, w.fail_rows, w.ctl, st));
     MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
@@ -300,6 +324,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       MSC_TRY(launch_pack_fp32(Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked, w.A32,
                                w.sq32, w.qs, w.km, st));
       stage_mark(st, 1);
+      stage_mark(st, 2);
       MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
                               P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
     } else {
@@ -308,13 +333,33 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
                              nullptr, nullptr, 0, w.Aop, w.Bop, w.qs, w.km, w.ctl, st));
       stage_mark(st, 1);
+      const uint32_t* mask = nullptr;
+      int words = 0;
+      if (prune) {
+        // near pass -> per-row radius -> outliers to the end of each sample -> operands of the
+        // new order -> balls and the visit mask of every query tile
+        MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp,
+                              P.L.kmma, w.items, n_items, w.perm, nullptr, nullptr,
+                              &w.ctl->tc_counter[2], w.ctl, P.kprime, w.cand_idx, w.cand_thr,
+                              P.kprime, st, nullptr, 0, true));
+        MSC_TRY(launch_prune_partition(Xu, P.d, w.seg, P.nseg, P.npacked, w.perm, w.cand_thr,
+                                       w.qs, w.km, P.prec, P.L.kmma, w.pr, st));
+        MSC_CUDA_TRY(cudaMemsetAsync(w.km, 0, sizeof(KeyMax), st));
+        MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
+                               nullptr, nullptr, 0, w.Aop, w.Bop, w.qs, w.km, w.ctl, st));
+        words = prune_mask_words(P.max_seg, cfg.bn);
+        MSC_TRY(launch_prune_plan(Xu, P.d, P.npacked, w.perm, w.items, n_items, cfg.bn, w.ctl,
+                                  P.prec, w.pr, words, st));
+        mask = w.pr.mask;
+      }
+      stage_mark(st, 2);
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
                             w.items, n_items, w.perm, nullptr, nullptr, &w.ctl->tc_counter[0],
-                            w.ctl, P.kprime,
-                            w.cand_idx, w.cand_thr, P.kprime, st));
+                            w.ctl, P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask, words,
+                            false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr));
     }
   }
-  stage_mark(st, 2);
+  stage_mark(st, 3);
   if (P.refine) MSC_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * P.npacked, st));
   MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                         P.kprime, P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx,
@@ -342,7 +387,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   }
   MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
                            knn_idx, knn_dist, w.ctl, st));
-  stage_mark(st, 3);
+  stage_mark(st, 4);
   return MSC_OK;
 }
 
@@ -414,14 +459,21 @@ long long msc_launch_count(void) { return msc::g_launch_count.load(); }
 int msc_profile_enable(int on) {
   timer().on = on != 0;
   timer().last = -1;
-  if (on) return tc_counters_clear();
+  if (on) {
+    MSC_TRY(tc_counters_clear());
+    return prune_counters_clear();
+  }
   return MSC_OK;
 }
 
 int msc_profile_counters(unsigned long long* out, int max_counters) {
   if (!out || max_counters < 1) { set_error("out/max_counters invalid"); return MSC_ERR_INVALID_ARG; }
   MSC_CUDA_TRY(cudaDeviceSynchronize());
-  return tc_counters(out, max_counters);
+  MSC_TRY(tc_counters(out, max_counters));
+  unsigned long long pt[2];
+  MSC_TRY(prune_counters(pt));
+  for (int i = 0; i < 2 && 10 + i < max_counters; ++i) out[10 + i] = pt[i];
+  return MSC_OK;
 }
 
 int msc_profile_read(float* ms_out, int max_stages) {
@@ -520,18 +572,18 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
   if (method == MSC_METHOD_UMAP) {
     MSC_TRY(launch_smooth_knn(knn_dist_dev, n, k, 1.0f, g.sigma, g.rho, g.gsum, st));
     MSC_TRY(launch_membership(knn_idx_dev, knn_dist_dev, g.sigma, g.rho, n, k, g.w, st));
-    stage_mark(st, 4);
+    stage_mark(st, 5);
     MSC_TRY(launch_union(0, knn_idx_dev, g.w, nullptr, n, k, conn_indptr_dev, conn_indices_dev,
                          conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
   } else {
     MSC_TRY(launch_gauss_sigma(knn_dist_dev, n, k, g.sig2, st));
-    stage_mark(st, 4);
+    stage_mark(st, 5);
     MSC_TRY(launch_union(1, knn_idx_dev, knn_dist_dev, g.sig2, n, k, conn_indptr_dev,
                          conn_indices_dev, conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
   }
   store_nnz_kernel<<<1, 32, 0, st>>>(conn_indptr_dev, n, w.ctl);
   MSC_LAUNCH_CHECK();
-  stage_mark(st, 5);
+  stage_mark(st, 6);
   return copy_stats(w, stats_dev, st);
 }
 

@@ -55,6 +55,35 @@ inline OpLayout op_layout(int prec, int d) {
   return L;
 }
 
+// operand scale f (a power of two): FP16 keeps max Σ z² at or below 2^14, the others use 1
+__device__ __forceinline__ double op_scale(int prec, const Ctl* ctl) {
+  if (prec != PREC_FP16) return 1.0;
+  float mx = __uint_as_float(ctl->max_sq_bits);
+  if (!(mx > 0.f)) return 1.0;
+  int e = int(floor(0.5 * log2(16384.0 / double(mx))));
+  e = max(-60, min(60, e));
+  return ldexp(1.0, e);
+}
+
+// Bound on |v̂ − v| for query row q against any key (z-space): v = |z_y|² − 2 z_x·z_y exactly, v̂
+// what the candidate kernel computes from the rounded operands.  Covers the operand residuals
+// (Cauchy–Schwarz), the norm-split error, the FP32 accumulation of kmma products (or of the FP32
+// SIMT dot product) and an FP64 slack.
+__device__ __forceinline__ double cert_eps(const QStat& q, const KeyMax& km, int prec, int kmma,
+                                           int d) {
+  const double Kh = __uint_as_float(km.hi), Kl = __uint_as_float(km.lo);
+  const double Kr = __uint_as_float(km.res), Kn = __uint_as_float(km.nerr);
+  const double Ks = __uint_as_float(km.sq);
+  const double qh = q.hi, ql = q.lo, qr = q.res;
+  const double dot_err = ql * Kl + (qh + ql) * Kr + qr * (Kh + Kl) + qr * Kr;
+  double acc_err;
+  if (prec == PREC_FP32)
+    acc_err = 0x1p-23 * ((2.0 * d + 4.0) * qh * Kh + 2.0 * Ks);
+  else
+    acc_err = double(kmma) * 0x1p-22 * (2.0 * (qh + ql) * (Kh + Kl) + Ks);
+  return 2.0 * dot_err + Kn + acc_err + 0x1p-40 * (q.sq + Ks);
+}
+
 // ---- prep.cu ----
 int launch_normalize(const float* X, float* Xn, int64_t n, int d, int64_t* nonfinite,
                      cudaStream_t st);
@@ -75,9 +104,11 @@ int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, in
                      QStat* qs, KeyMax* km, cudaStream_t st);
 // locality order (order.cu): perm[p] for every packed row, cells of a sample permuted so that
 // near cells are near in packed order; levels = 0 gives the identity order
-size_t order_workspace_bytes(int64_t npacked);
+// leaf_out (optional): per packed position, the first position of its leaf (-1: padding)
+size_t order_workspace_bytes(int64_t npacked, int d, int leaf);
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
-                 int leaf, int32_t* perm, void* ws, size_t ws_bytes, cudaStream_t st);
+                 int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
+                 cudaStream_t st);
 size_t scan_i32_scratch_elems(int64_t n);
 int scan_excl_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream_t st);
 int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st);
@@ -85,12 +116,50 @@ int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st);
 int launch_build_items(const SegDesc* seg, int nseg, int64_t n_items, int rows, WorkItem* items,
                        Ctl* ctl, cudaStream_t st);
 
+// ---- prune.cu ----
+constexpr int32_t OUTLIER_LEAF = -2;   // leaf id of the rows moved to the end of their sample
+struct PruneWs {
+  int32_t* leaf;      // locality-tree leaf per packed position (near-pass layout)
+  int32_t* leaf2;     // the same after the partition
+  int32_t* perm2;
+  int32_t* reg;
+  int64_t* S;
+  int64_t* scan_scratch;
+  double* rpos;       // R per packed position
+  double* rpos2;
+  double* mean;       // per sample
+  float *qc, *qr;     // 128-row balls: centres [npacked/128][d], radii
+  float *kc, *kr;     // 256-row balls
+  float *sc, *sr;     // two balls per 32-row block
+  double* rsub;       // max R per 32-row block
+  uint32_t* mask;     // visit bits per work item
+  float* seed;        // per packed row (final layout): bound on its final k'-th value
+};
+int prune_mask_words(int64_t max_seg, int bn);
+PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words);
+size_t prune_workspace_bytes(int64_t npacked, int nseg, int d, int64_t n_items, int words);
+// after the near pass: R per row, outliers to the end of each sample (perm is rewritten)
+int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
+                           int32_t* perm, const float* cand_thr, const QStat* qs,
+                           const KeyMax* km, int prec, int kmma, const PruneWs& w,
+                           cudaStream_t st);
+// balls of the final layout and the visit mask of every work item
+int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* perm,
+                      const WorkItem* items, int64_t n_items, int bn, const Ctl* ctl, int prec,
+                      const PruneWs& w, int words, cudaStream_t st);
+int prune_counters(unsigned long long* out);
+int prune_counters_clear();
+
 // ---- knn_fp32.cu ----
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
                     int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
                     int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
 
 // ---- knn_tc.cu ----
+// Work items are claimed dynamically by the persistent CTAs, in index order or (reverse) from the
+// last one down.  Batches pack their largest samples first, so index order starts the longest
+// items first; a single pruned sample keeps its costliest query tiles (the outlier rows, scanned
+// against every key) at its end, so it claims in reverse.
 struct TcConfig {
   int bn;        // key tile rows (32, 64, 128, 256)
   int stages;    // smem pipeline depth of the key tiles
@@ -109,7 +178,9 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
                   int64_t n_items, const int32_t* perm, const int32_t* qmap,
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
-                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
+                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
+                  const uint32_t* mask = nullptr, int mask_words = 0, bool near_only = false,
+                  bool reverse = false, const float* seed = nullptr);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

@@ -302,6 +302,11 @@ struct TcParams {
   const int32_t* qmap;   // query row -> packed position (refine pass over a row list), or null
   const int32_t* n_items_dev;   // work-item count in device memory (refine pass), or null
   int32_t* counter;             // next unclaimed work item (zero at launch; single CTAs only)
+  const uint32_t* mask;         // per work item: key tiles to visit beyond the near tiles, or null
+  int mask_words;               // mask words per work item
+  int near_only;                // near pass: the near tiles only
+  int reverse;                  // claim the work items from the last one down
+  const float* seed;            // per packed query row: bound on its final k'-th value, or null
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -323,6 +328,46 @@ __device__ __forceinline__ int key_tile_at(int j, int diag, int nkt) {
   if (j <= 2 * m) return (j & 1) ? diag + ((j + 1) >> 1) : diag - (j >> 1);
   return right > left ? diag + (j - m) : diag - (j - m);
 }
+
+// The key tiles of one work item in the order every role walks them: the near tiles
+// (key_tile_at), then all other tiles in plain order, or only those whose bit is set in the
+// item's visit mask (the pruned scan), or none (the near pass).  Every role of the CTA walks the
+// same sequence, so the tiles need no hand-off between them.
+struct KeyTileWalk {
+  int nkt, diag, np, j;
+  const uint32_t* mask;
+  int w, nw;
+  uint32_t cur, nxt;
+  bool near_only;
+  __device__ __forceinline__ void init(const WorkItem& item, int qref, int bn,
+                                       const uint32_t* m, int words, bool near) {
+    nkt = (item.nkeys + bn - 1) / bn;
+    diag = (qref - item.key0) / bn;
+    const int lo = max(0, diag - NEAR_SIDE), hi = min(nkt - 1, diag + NEAR_SIDE);
+    np = hi - lo + 1;
+    j = 0;
+    near_only = near;
+    mask = m;
+    w = 0;
+    nw = words;
+    cur = m ? m[0] : 0u;
+    nxt = (m && words > 1) ? m[1] : 0u;     // one word ahead: its load overlaps the near tiles
+  }
+  // the next key tile, or -1
+  __device__ __forceinline__ int next() {
+    if (j < np) return key_tile_at(j++, diag, nkt);
+    if (near_only) return -1;
+    if (!mask) return j < nkt ? key_tile_at(j++, diag, nkt) : -1;
+    while (cur == 0u) {
+      if (++w >= nw) return -1;
+      cur = nxt;
+      nxt = w + 1 < nw ? mask[w + 1] : 0u;
+    }
+    const int b = __ffs(cur) - 1;
+    cur &= cur - 1u;
+    return w * 32 + b;
+  }
+};
 
 // Pipeline counters (cycles / events summed over CTAs), filled when profiling is enabled:
 //   0 producer waiting for a free key stage     1 MMA waiting for a loaded key tile
@@ -449,7 +494,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
     if (!mbar_wait(&item_empty[r_slot], r_phase ^ 1, abort_flag)) return false;
     int v = atomicAdd(P.counter, 1);
-    if (v >= n_items) v = -1;
+    v = v < n_items ? (P.reverse ? n_items - 1 - v : v) : -1;
     item_ring[r_slot] = v;
     mbar_arrive(&item_full[r_slot]);         // release: the ring entry is visible to the waiters
     if (++r_slot == ITEM_RING) { r_slot = 0; r_phase ^= 1; }
@@ -493,10 +538,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
                       w.qrow0 + int(rank) * BM);
         if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        const int diag = ((P.qmap ? P.qmap[w.qrow0] : w.qrow0) - w.key0) / P.bn;
-        for (int j = 0; j < nkt && ok; ++j) {
-          const int kt = key_tile_at(j, diag, nkt);
+        KeyTileWalk walk;
+        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
+                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
+                  P.near_only != 0);
+        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
             const long long tw = P.prof ? clock64() : 0;
             ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
@@ -534,8 +580,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         if (!ok) break;
         mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
         if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        for (int kt = 0; kt < nkt && ok; ++kt) {
+        KeyTileWalk walk;
+        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
+                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
+                  P.near_only != 0);
+        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           for (int kb = 0; kb < P.kb; ++kb) {
             ok = mbar_wait(&b_full[stage], sphase, abort_flag);
             if (!ok) break;
@@ -561,8 +610,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
         if (!ok) break;
         const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
-        const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-        for (int kt = 0; kt < nkt && ok; ++kt) {
+        KeyTileWalk walk;
+        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
+                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
+                  P.near_only != 0);
+        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           const long long t2 = P.prof ? clock64() : 0;
           ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
                     : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
@@ -642,11 +694,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       const int nq = min(BM, w.nq - int(rank) * BM);   // this CTA's valid query rows (may be <= 0)
       const int qrow = w.qrow0 + int(rank) * BM;
       const int self = P.qmap ? (row < nq ? P.qmap[qrow + row] : -1) : qrow + row;
+      sel.set_seed((P.seed && row < nq) ? P.seed[qrow + row] : F_INF);
       const int limit = w.key0 + w.nkeys;
-      const int nkt = (w.nkeys + P.bn - 1) / P.bn;
-      const int diag = ((P.qmap ? P.qmap[w.qrow0] : w.qrow0) - w.key0) / P.bn;
-      for (int j = 0; j < nkt; ++j) {
-        const int kt = key_tile_at(j, diag, nkt);
+      KeyTileWalk walk;
+      walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
+                P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
+                P.near_only != 0);
+      for (int kt = walk.next(); kt >= 0; kt = walk.next()) {
         const long long te = P.prof ? clock64() : 0;
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
         if (P.prof) c_ew += clock64() - te;
@@ -926,7 +980,9 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int64_t a_rows, int64_t b_rows, int kp, int kmma, const WorkItem* items,
                   int64_t n_items, const int32_t* perm, const int32_t* qmap,
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
-                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st) {
+                  int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
+                  const uint32_t* mask, int mask_words, bool near_only, bool reverse,
+                  const float* seed) {
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
               cfg.bn, cfg.stages, cfg.kpl, cfg.cb, cfg.epi, cfg.pair);
@@ -952,6 +1008,15 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.qmap = qmap;
   P.n_items_dev = n_items_dev;
   P.counter = counter;
+  P.mask = mask;
+  P.mask_words = mask_words;
+  P.near_only = near_only ? 1 : 0;
+  P.reverse = reverse ? 1 : 0;
+  P.seed = seed;
+  if (cfg.pair && (mask || near_only)) {
+    set_error("pruned scans run on single CTAs only");
+    return MSC_ERR_INVALID_ARG;
+  }
   if (cfg.pair) {
     if (cfg.epi == 8)
       return launch_tc_epi<8, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);

@@ -42,7 +42,12 @@ struct RowSelect {
   int row;        // this thread's row within the ROWS rows
   int kp;         // k'
   float thr;      // this list's k'-th value
-  float thr_f;    // filter threshold: min(thr, the partner list's published thr)
+  float thr_f;    // filter threshold: min(thr, seed, the partner list's published thr)
+  // An upper bound on the row's final k'-th value known before the scan (from an earlier pass
+  // over a subset of its keys), +inf if none.  Values at or above it are never kept; the list's
+  // threshold reported by finish() is min(list[k'-1], seed), so every value not in the list is
+  // at least the reported threshold even if fewer than k' values passed the filter.
+  float seed = F_INF;
   int cnt;
   // When two selectors split one row's columns, each publishes its threshold here (shared memory)
   // and filters against the smaller of the two: the k'-th smallest of the union is at most either
@@ -68,12 +73,19 @@ struct RowSelect {
     }
     thr = F_INF;
     thr_f = F_INF;
+    seed = F_INF;
     cnt = 0;
+  }
+
+  __device__ __forceinline__ void set_seed(float s) {
+    seed = s;
+    thr_f = fminf(thr_f, s);
   }
 
   // take the partner's latest published threshold
   __device__ __forceinline__ void refresh() {
-    if (pub_other) thr_f = fminf(thr, *reinterpret_cast<const volatile float*>(pub_other));
+    thr_f = fminf(thr, seed);
+    if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
   }
 
   __device__ __forceinline__ void append(float v, int col) {
@@ -223,11 +235,12 @@ struct RowSelect {
       const int rr = row0 + r;
       const int64_t prow = qmap ? int64_t(qmap[first_row + r]) : first_row + r;
       const int64_t orow = perm[prow];
+      const float sd = __shfl_sync(FULL, seed, r);
       for (int s = lane; s < kout; s += 32) {
         const int c = li[s * ROWS + rr];
         out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
       }
-      if (lane == 0) out_thr[orow] = lv[(kp - 1) * ROWS + rr];
+      if (lane == 0) out_thr[orow] = fminf(lv[(kp - 1) * ROWS + rr], sd);
     }
     __syncwarp();
   }

@@ -1,21 +1,25 @@
-// Locality order of the cells: a deterministic bisection tree built on the GPU.
+// Locality order of the cells: a bisection tree built on the GPU.
 //
 // The candidate kernels filter every key against the row's running k'-th value.  With cells in
 // arbitrary order a row's list keeps improving through the whole scan (about k'·ln(n/k')
 // insertions per row), and a 32-row warp takes the slow path whenever any of its rows does.
 // Scanning first the keys that are near the query tile's rows brings every threshold close to its
-// final value within a few key tiles.  This file computes that order; the packed operands are
-// laid out in it, and each query tile scans its own key tile first and then outwards.  The
-// neighbour graph does not depend on the order (candidates are re-ranked exactly and certified).
+// final value within a few key tiles.  The order also decides how tight the bounding balls of the
+// tiles are, which is what lets whole tiles of keys be skipped.  This file computes that order;
+// the packed operands are laid out in it.  The neighbour graph does not depend on the order
+// (candidates are re-ranked exactly and certified).
 //
 // The tree: every node (a range of packed positions inside one sample) larger than LEAF rows is
-// split in two around two far-apart cells — a = the cell farthest from the node's first cell,
-// b = the cell farthest from a — each cell going to the side of the nearer of the two (ties to
-// a's side); a degenerate split (all on one side) halves the range instead.  Farthest-point
-// choices break distance ties by the lower position (64-bit atomicMax of distance bits and
-// inverted position), and the partition is stable, so the order is a pure function of the input.
-// A fixed number of levels runs without host synchronisation (graph-capturable); nodes at or
-// below LEAF rows are left as they are.
+// split in two by one step of 2-means.  It starts from two far-apart cells — a = the cell farthest
+// from the node's first cell, b = the cell farthest from a (distance ties to the lower position)
+// — assigns every cell to the nearer of the two (ties to a's side), then moves a and b to the
+// means of their sides and assigns again.  The second assignment follows the gaps between
+// clusters instead of the bisector of two extreme (often outlying) cells, so clusters stay whole.
+// A degenerate split (all on one side) halves the range instead; the partition is stable.  The
+// side means are summed with floating-point atomics, so a cell almost equidistant from both means
+// may fall on either side from run to run; the graph is the same either way.  A fixed number of
+// levels runs without host synchronisation (graph-capturable); nodes at or below LEAF rows are
+// left as they are and are the leaves of the tree.
 #include "kernels.cuh"
 
 namespace msc {
@@ -139,9 +143,107 @@ __global__ void scatter_kernel(int64_t npacked, int leaf, const int32_t* __restr
   }
 }
 
+// first position of every node that is split at this level
+__global__ void split_start_kernel(int64_t npacked, int leaf, const int32_t* __restrict__ ns,
+                                   const int32_t* __restrict__ ne, int32_t* __restrict__ flag) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x)
+    flag[p] = (ns[p] == p && ne[p] - ns[p] > leaf) ? 1 : 0;
+}
+
+// Per split node and side: Σ x and the count.  A warp walks 64 consecutive positions; lane t owns
+// dimensions t, t+32, ...; partial sums go out with one atomic per (node, side, dimension) each
+// time the node changes along the walk.  acc layout per node: [2][d] sums, then [2] counts.
+constexpr int SUM_RUN = 64;
+__global__ void side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+                                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+                                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
+                                const int32_t* __restrict__ side, double* __restrict__ acc) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int64_t nruns = (npacked + SUM_RUN - 1) / SUM_RUN;
+  const int per = (d + 31) / 32;            // dimensions per lane (d <= 128)
+  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < nruns; r += warps) {
+    const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
+    double s0[4] = {0, 0, 0, 0}, s1[4] = {0, 0, 0, 0};
+    double c0 = 0, c1 = 0;
+    int64_t cur = -1;                        // node id being accumulated
+    auto flush = [&]() {
+      if (cur < 0) return;
+      double* a = acc + cur * (2 * d + 2);
+      for (int j = 0; j < per; ++j) {
+        const int t = lane + 32 * j;
+        if (t < d) {
+          if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
+          if (s1[j] != 0.0) atomicAdd(&a[d + t], s1[j]);
+        }
+        s0[j] = 0; s1[j] = 0;
+      }
+      if (lane == 0) {
+        if (c0 != 0) atomicAdd(&a[2 * d], c0);
+        if (c1 != 0) atomicAdd(&a[2 * d + 1], c1);
+      }
+      c0 = 0; c1 = 0;
+    };
+    for (int64_t p = p0; p < p1; ++p) {
+      const int st = ns[p];
+      if (ne[p] - st <= leaf) continue;      // warp-uniform
+      const int64_t id = S[st];
+      if (id != cur) { flush(); cur = id; }
+      const float* x = X + int64_t(perm[p]) * d;
+      const bool one = side[p] != 0;
+      for (int j = 0; j < per; ++j) {
+        const int t = lane + 32 * j;
+        if (t < d) {
+          if (one) s1[j] += x[t]; else s0[j] += x[t];
+        }
+      }
+      if (one) c1 += 1.0; else c0 += 1.0;
+    }
+    flush();
+  }
+}
+
+// second assignment: the nearer of the two side means (ties to side 0); a side left empty by the
+// first assignment keeps it
+__global__ void reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+                                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+                                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
+                                const double* __restrict__ acc, int32_t* __restrict__ side) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    const int st = ns[p];
+    if (ne[p] - st <= leaf) continue;
+    const double* a = acc + S[st] * (2 * d + 2);
+    const double n0 = a[2 * d], n1 = a[2 * d + 1];
+    if (n0 == 0.0 || n1 == 0.0) continue;
+    const double i0 = 1.0 / n0, i1 = 1.0 / n1;
+    const float* x = X + int64_t(perm[p]) * d;
+    double d0 = 0.0, d1 = 0.0;
+    for (int t = 0; t < d; ++t) {
+      const double v = x[t];
+      const double u0 = v - a[t] * i0, u1 = v - a[d + t] * i1;
+      d0 += u0 * u0;
+      d1 += u1 * u1;
+    }
+    side[p] = d0 > d1 ? 1 : 0;
+  }
+}
+
+// leaf of every packed position: the first position of its final node (-1: padding rows)
+__global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm,
+                               const int32_t* __restrict__ ns, int32_t* __restrict__ leaf_out) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x)
+    leaf_out[p] = perm[p] >= 0 ? ns[p] : -1;
+}
+
 }  // namespace
 
-size_t order_workspace_bytes(int64_t npacked) {
+// split nodes at one level: each holds more than `leaf` rows
+inline int64_t max_split_nodes(int64_t npacked, int leaf) { return npacked / (leaf + 1) + 1; }
+
+size_t order_workspace_bytes(int64_t npacked, int d, int leaf) {
   Carver c(nullptr);
   c.take<int32_t>(npacked);                       // second permutation
   c.take<int32_t>(npacked);                       // node start, node end (two copies each)
@@ -154,13 +256,17 @@ size_t order_workspace_bytes(int64_t npacked) {
   c.take<int32_t>(npacked);                       // side
   c.take<int64_t>(npacked + 1);                   // scan of side
   c.take<int64_t>(scan_i32_scratch_elems(npacked));
+  c.take<int32_t>(npacked);                       // split-node starts
+  c.take<int64_t>(npacked + 1);                   // their scan: node ids
+  c.take<double>(size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2));   // side sums, counts
   return c.bytes();
 }
 
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
-                 int leaf, int32_t* perm, void* ws, size_t ws_bytes, cudaStream_t st) {
-  if (ws_bytes < order_workspace_bytes(npacked)) {
-    set_error("order: workspace %zu < %zu bytes", ws_bytes, order_workspace_bytes(npacked));
+                 int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
+                 cudaStream_t st) {
+  if (ws_bytes < order_workspace_bytes(npacked, d, leaf)) {
+    set_error("order: workspace %zu < %zu bytes", ws_bytes, order_workspace_bytes(npacked, d, leaf));
     return MSC_ERR_WORKSPACE;
   }
   Carver c(ws);
@@ -175,6 +281,10 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   int32_t* side = c.take<int32_t>(npacked);
   int64_t* S = c.take<int64_t>(npacked + 1);
   int64_t* scratch = c.take<int64_t>(scan_i32_scratch_elems(npacked));
+  int32_t* sflag = c.take<int32_t>(npacked);
+  int64_t* SN = c.take<int64_t>(npacked + 1);
+  const size_t acc_elems = size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2);
+  double* acc = c.take<double>(acc_elems);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(npacked, OR_T),
                                                               int64_t(num_sms()) * 8)));
   order_init_kernel<<<grid, OR_T, 0, st>>>(seg, nseg, npacked, perm, nsA, neA);
@@ -189,6 +299,15 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     MSC_LAUNCH_CHECK();
     side_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
     MSC_LAUNCH_CHECK();
+    // one 2-means step: side means, then the nearer mean
+    split_start_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, sc, ec, sflag);
+    MSC_LAUNCH_CHECK();
+    MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
+    MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
+    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    MSC_LAUNCH_CHECK();
+    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side);
+    MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(side, npacked, S, scratch, st));
     scatter_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, pc, sc, ec, side, S, pn, sn, en);
     MSC_LAUNCH_CHECK();
@@ -198,6 +317,10 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   }
   if (pc != perm)
     MSC_CUDA_TRY(cudaMemcpyAsync(perm, pc, sizeof(int32_t) * npacked, cudaMemcpyDeviceToDevice, st));
+  if (leaf_out) {
+    leaf_id_kernel<<<grid, OR_T, 0, st>>>(npacked, perm, sc, leaf_out);
+    MSC_LAUNCH_CHECK();
+  }
   return MSC_OK;
 }
 

@@ -156,15 +156,6 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// FP16 keeps max Σ z² at or below 2^14 with a power-of-two scale (exact); others use 1
-__device__ __forceinline__ double pack_scale(int prec, const Ctl* ctl) {
-  if (prec != PREC_FP16) return 1.0;
-  float mx = __uint_as_float(ctl->max_sq_bits);
-  if (!(mx > 0.f)) return 1.0;
-  int e = int(floor(0.5 * log2(16384.0 / double(mx))));
-  e = max(-60, min(60, e));
-  return ldexp(1.0, e);
-}
 
 // block-level max of 5 non-negative fields, then one atomicMax per field per block
 __device__ __forceinline__ void block_keymax(float (&m)[5], KeyMax* km) {
@@ -200,7 +191,7 @@ __global__ void pack_tc_kernel(const float* __restrict__ X, const int32_t* __res
                                double pad_term) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  const double f = pack_scale(prec, ctl);
+  const double f = op_scale(prec, ctl);
   const T zero = to_op<T>(0.0);
   const T one = to_op<T>(1.0);
   const T padt = to_op<T>(pad_term);

@@ -1,0 +1,458 @@
+// Key-tile pruning for the tensor-core candidate kernel: the pairs of (query tile, key tile) that
+// cannot contribute a candidate are never computed.
+//
+// The reference computes every distance of a row block (neighbors.py:114-119); so does the plain
+// form here.  An exact kNN does not need to: a key whose squared distance to row x is provably
+// above x's running k'-th value can never enter x's candidate list.  This file proves it per tile
+// pair with bounding balls:
+//
+//   1. near pass: the candidate kernel visits only the few key tiles around each query tile's own
+//      keys (the cells are in locality order) and returns every row's k'-th smallest value thr_x.
+//      R_x = thr_x + |z_x|² + 3·eps_x bounds, in the scaled space z of the operands, the squared
+//      distance below which x can still take a key (eps_x = the certificate's bound on the
+//      operand and accumulation error, see rerank.cu);
+//   2. outliers: rows whose R_x is far above their sample's mean R (cells in no dense region)
+//      move to the end of their sample, so that the balls of the tiles of regular rows stay
+//      tight; the order is otherwise kept (stable partition), and so are the locality-tree leaves;
+//   3. balls: every 32-row block of packed rows gets two balls (split at the first leaf boundary
+//      inside the block), every 128-row query tile and every 256-row block one ball; centres are
+//      float, radii are rounded up so that each ball holds all of its rows;
+//   4. plan: key tile K is skipped for query tile Q when every ball u of Q and every ball w of K
+//      are separated: |c_u − c_w| − r_u − r_w = L > 0 and f²·L² > max R over u's rows.  Then every
+//      (x, y) with x in Q, y in K has v(x,y) = |z_x − z_y|² − |z_x|² > thr_x + 3·eps_x, so the
+//      approximate value the kernel would compute is above thr_x + 2·eps_x; the k' keys behind
+//      thr_x are never skipped, so the final k'-th value T_x <= thr_x + 2·eps_x, and the
+//      certificate's premise (every key outside the list has approximate value >= T_x) holds for
+//      skipped keys exactly as for scanned ones.  Near tiles are always visited.
+//
+// Each query tile gets a bit mask over its sample's key tiles (set = visit, near tiles excluded);
+// the candidate kernel walks its near tiles first and then the set bits in ascending order.
+#include "kernels.cuh"
+
+namespace msc {
+
+namespace {
+
+constexpr int PR_T = 256;
+
+// key tiles visited beyond the near tiles, and all such tiles, summed over plans while profiling
+__device__ unsigned long long g_prune_tiles[2];
+constexpr int SUB = 32;          // rows per sub-block (two balls each)
+constexpr float NO_BALL = -1.f;  // radius of a ball without rows
+constexpr double OUTLIER_FACTOR = 4.0;
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// R per packed position of the near-pass layout (+inf where the row has no finite threshold;
+// padding rows get NaN and are never read as rows)
+__global__ void row_radius_kernel(const int32_t* __restrict__ perm, int64_t npacked,
+                                  const float* __restrict__ cand_thr,
+                                  const QStat* __restrict__ qs, const KeyMax* __restrict__ km,
+                                  int prec, int kmma, int d, double* __restrict__ rpos) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    const int32_t i = perm[p];
+    if (i < 0) { rpos[p] = __longlong_as_double(0x7ff8000000000000ll); continue; }
+    const double thr = cand_thr[i];
+    const QStat q = qs[p];
+    const double r = thr + q.sq + 3.0 * cert_eps(q, *km, prec, kmma, d);
+    rpos[p] = r < 1e300 ? r : __longlong_as_double(0x7ff0000000000000ll);
+  }
+}
+
+// mean of the finite R of every sample (one block per sample, fixed summation order)
+__global__ void sample_mean_kernel(const SegDesc* __restrict__ seg, const double* __restrict__ rpos,
+                                   double* __restrict__ mean_out) {
+  __shared__ double ssum[PR_T / 32], scnt[PR_T / 32];
+  const SegDesc s = seg[blockIdx.x];
+  double sum = 0.0, cnt = 0.0;
+  for (int64_t j = threadIdx.x; j < s.n; j += blockDim.x) {
+    const double r = rpos[s.poff + j];
+    if (r < 1e300) { sum += r; cnt += 1.0; }
+  }
+  sum = warp_sum_d(sum);
+  cnt = warp_sum_d(cnt);
+  if (lane_id() == 0) { ssum[warp_id()] = sum; scnt[warp_id()] = cnt; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) { a += ssum[w]; b += scnt[w]; }
+    mean_out[blockIdx.x] = b > 0.0 ? a / b : __longlong_as_double(0x7ff0000000000000ll);
+  }
+}
+
+__global__ void regular_flag_kernel(const int32_t* __restrict__ perm, int64_t npacked,
+                                    const SegDesc* __restrict__ seg, int nseg,
+                                    const double* __restrict__ rpos,
+                                    const double* __restrict__ mean, int32_t* __restrict__ reg) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    if (perm[p] < 0) { reg[p] = 0; continue; }
+    const double m = mean[find_seg(seg, nseg, p)];
+    reg[p] = rpos[p] > OUTLIER_FACTOR * m ? 0 : 1;        // NaN / inf mean: regular
+  }
+}
+
+// stable partition inside every sample: regular rows first, then the outliers (leaf OUTLIER_LEAF)
+// The seed of a row lies strictly above thr + 2·eps: the near pass's k' keys keep values at or
+// below thr + 2·eps in the scan of the new layout (the operands of a row are the same; each value is within eps of
+// the exact one), so the row's final k'-th value cannot exceed it.
+__global__ void partition_kernel(const int32_t* __restrict__ perm, const int32_t* __restrict__ leaf,
+                                 const double* __restrict__ rpos, int64_t npacked,
+                                 const SegDesc* __restrict__ seg, int nseg,
+                                 const int32_t* __restrict__ reg, const int64_t* __restrict__ S,
+                                 const float* __restrict__ cand_thr, const QStat* __restrict__ qs,
+                                 const KeyMax* __restrict__ km, int prec, int kmma, int d,
+                                 int32_t* __restrict__ perm2, int32_t* __restrict__ leaf2,
+                                 double* __restrict__ rpos2, float* __restrict__ seed2) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    const SegDesc s = seg[find_seg(seg, nseg, p)];
+    int64_t pos = p;
+    int32_t lf = leaf[p];
+    if (p < s.poff + s.n) {
+      const int64_t before = S[p] - S[s.poff];                 // regular rows before p
+      if (reg[p]) {
+        pos = s.poff + before;
+      } else {
+        const int64_t nreg = S[s.poff + s.n] - S[s.poff];
+        pos = s.poff + nreg + (p - s.poff) - before;
+        lf = OUTLIER_LEAF;
+      }
+    }
+    const int32_t i = perm[p];
+    float sd = F_INF;
+    if (i >= 0) {
+      const double t = double(cand_thr[i]) + 2.0 * cert_eps(qs[p], *km, prec, kmma, d);
+      if (t < 1e300) sd = nextafterf(__double2float_ru(t), F_INF);   // strictly above
+    }
+    perm2[pos] = i;
+    leaf2[pos] = lf;
+    rpos2[pos] = rpos[p];
+    seed2[pos] = sd;
+  }
+}
+
+// One ball per group of G packed rows (G = 128 or 256): centre = float(mean of the rows), radius =
+// max distance to that centre, rounded up.  One warp per group; lane t sums dimensions t, t+32, ...
+template <int G>
+__global__ void group_ball_kernel(const float* __restrict__ X, int d,
+                                  const int32_t* __restrict__ perm, int64_t ngroups,
+                                  float* __restrict__ centre, float* __restrict__ radius) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t g = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; g < ngroups;
+       g += warps) {
+    double s[4] = {0, 0, 0, 0};
+    int cnt = 0;
+    for (int r = 0; r < G; ++r) {
+      const int32_t i = perm[g * G + r];
+      if (i < 0) continue;
+      ++cnt;
+      for (int j = 0; j < 4; ++j) {
+        const int t = lane + 32 * j;
+        if (t < d) s[j] += X[int64_t(i) * d + t];
+      }
+    }
+    float c[4];
+    for (int j = 0; j < 4; ++j) {
+      const int t = lane + 32 * j;
+      c[j] = cnt ? float(s[j] / cnt) : 0.f;
+      if (t < d) centre[g * d + t] = c[j];
+    }
+    double mx = 0.0;
+    for (int r = 0; r < G; ++r) {
+      const int32_t i = perm[g * G + r];
+      if (i < 0) continue;
+      double a = 0.0;
+      for (int j = 0; j < 4; ++j) {
+        const int t = lane + 32 * j;
+        if (t < d) {
+          const double u = double(X[int64_t(i) * d + t]) - double(c[j]);
+          a += u * u;
+        }
+      }
+      mx = fmax(mx, warp_sum_d(a));
+    }
+    if (lane == 0)
+      radius[g] = cnt ? __double2float_ru(sqrt(mx) * (1.0 + 0x1p-40)) : NO_BALL;
+  }
+}
+
+// Two balls per 32-row block, split at the first row whose leaf differs from the block's first
+// row (rows of one leaf are close, rows of two leaves may lie in two clusters), and the block's
+// max R.  Ball 2b covers rows [0, m), ball 2b+1 rows [m, 32).
+__global__ void sub_ball_kernel(const float* __restrict__ X, int d,
+                                const int32_t* __restrict__ perm,
+                                const int32_t* __restrict__ leaf,
+                                const double* __restrict__ rpos, int64_t nsub,
+                                float* __restrict__ centre, float* __restrict__ radius,
+                                double* __restrict__ rsub) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t b = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; b < nsub; b += warps) {
+    const int64_t p0 = b * SUB;
+    const int32_t my_i = perm[p0 + lane];
+    const int32_t my_leaf = leaf[p0 + lane];
+    const int32_t leaf0 = __shfl_sync(FULL, my_leaf, 0);
+    const unsigned diff = __ballot_sync(FULL, my_leaf != leaf0);
+    const int m = diff ? __ffs(diff) - 1 : SUB;
+    // the block's max R over its rows (unknown radius = +inf)
+    double rv = 0.0;
+    if (my_i >= 0) {
+      const double r = rpos[p0 + lane];
+      rv = r < 1e300 ? r : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    rv = warp_max_d(rv);
+    if (lane == 0) rsub[b] = rv;
+    for (int h = 0; h < 2; ++h) {
+      const int r0 = h ? m : 0, r1 = h ? SUB : m;
+      double s[4] = {0, 0, 0, 0};
+      int cnt = 0;
+      for (int r = r0; r < r1; ++r) {
+        const int32_t i = __shfl_sync(FULL, my_i, r);
+        if (i < 0) continue;
+        ++cnt;
+        for (int j = 0; j < 4; ++j) {
+          const int t = lane + 32 * j;
+          if (t < d) s[j] += X[int64_t(i) * d + t];
+        }
+      }
+      float c[4];
+      float* cdst = centre + (2 * b + h) * d;
+      for (int j = 0; j < 4; ++j) {
+        const int t = lane + 32 * j;
+        c[j] = cnt ? float(s[j] / cnt) : 0.f;
+        if (t < d) cdst[t] = c[j];
+      }
+      double mx = 0.0;
+      for (int r = r0; r < r1; ++r) {
+        const int32_t i = __shfl_sync(FULL, my_i, r);
+        if (i < 0) continue;
+        double a = 0.0;
+        for (int j = 0; j < 4; ++j) {
+          const int t = lane + 32 * j;
+          if (t < d) {
+            const double u = double(X[int64_t(i) * d + t]) - double(c[j]);
+            a += u * u;
+          }
+        }
+        mx = fmax(mx, warp_sum_d(a));
+      }
+      if (lane == 0)
+        radius[2 * b + h] = cnt ? __double2float_ru(sqrt(mx) * (1.0 + 0x1p-40)) : NO_BALL;
+    }
+  }
+}
+
+// Are the balls (cu, ru) and (cw, rw) so far apart that no row of u can take a key of w?  R = max
+// R over u's rows (z-space), f2 = square of the operand scale.  An empty ball is separated from
+// everything; an unknown R (inf / NaN) from nothing.  The FP32 distance is lowered by its
+// rounding bound (d+8 units of 2^-23 relative) before the test.
+__device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru, double R,
+                                          const float* __restrict__ cw, float rw, int d,
+                                          double f2) {
+  if (ru < 0.f || rw < 0.f) return true;
+  if (!(R < 1e300)) return false;
+  float s = 0.f;
+  for (int t = 0; t < d; ++t) {
+    const float df = cu[t] - cw[t];
+    s = fmaf(df, df, s);
+  }
+  const double lo = double(s) * (1.0 - double(d + 8) * 0x1p-23);
+  const double L = sqrt(lo) - double(ru) - double(rw);
+  return L > 0.0 && f2 * L * L > R * (1.0 + 1e-9);
+}
+
+// One warp per query tile (work item); lane = key tile.  Level 1: the query tile's ball against
+// the 256-row ball holding the key tile; level 2: every ball pair of the two tiles.
+constexpr int PLAN_WARPS = 4;
+__global__ void __launch_bounds__(PLAN_WARPS * 32)
+plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, const Ctl* ctl,
+            int prec, const float* __restrict__ qc, const float* __restrict__ qr,
+            const float* __restrict__ kc, const float* __restrict__ kr,
+            const float* __restrict__ sc, const float* __restrict__ sr,
+            const double* __restrict__ rsub, int words, uint32_t* __restrict__ mask, int prof) {
+  extern __shared__ float sm[];
+  const int lane = lane_id(), wib = warp_id();
+  float* qball = sm + wib * (9 * d);            // [0]: the tile's ball, [1..8]: its sub-balls
+  const double f = op_scale(prec, ctl);
+  const double f2 = f * f;
+  const int64_t warps = int64_t(gridDim.x) * PLAN_WARPS;
+  long long nvis = 0, ntot = 0;
+  for (int64_t it = int64_t(blockIdx.x) * PLAN_WARPS + wib; it < n_items; it += warps) {
+    const WorkItem w = items[it];
+    const int64_t qt = w.qrow0 / QTILE;          // 128-row tile of packed rows
+    const int64_t sb0 = int64_t(w.qrow0) / SUB;  // its first 32-row block
+    __syncwarp();
+    for (int t = lane; t < d; t += 32) qball[t] = qc[qt * d + t];
+    for (int u = 0; u < 8; ++u)
+      for (int t = lane; t < d; t += 32) qball[(1 + u) * d + t] = sc[(2 * sb0 + u) * d + t];
+    __syncwarp();
+    const float rq = qr[qt];
+    double Rsb[4], Rq = 0.0;
+    for (int j = 0; j < 4; ++j) {
+      Rsb[j] = rsub[sb0 + j];
+      Rq = fmax(Rq, Rsb[j]);                      // NaN never occurs: rsub is >= 0 or +inf
+    }
+    float ru[8];
+    for (int u = 0; u < 8; ++u) ru[u] = sr[2 * sb0 + u];
+    const int nkt = (w.nkeys + bn - 1) / bn;
+    const int diag = (w.qrow0 - w.key0) / bn;
+    const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
+    uint32_t* out = mask + it * int64_t(words);
+    for (int base = 0; base < words * 32; base += 32) {
+      const int kt = base + lane;
+      bool visit = false;
+      if (kt < nkt && (kt < lo || kt > hi)) {
+        const int64_t k0 = int64_t(w.key0) + int64_t(kt) * bn;   // first packed key row
+        const int64_t g = k0 / 256;
+        const float* kcg = kc + g * d;
+        const float krg = kr[g];
+        visit = !separated(qball, rq, Rq, kcg, krg, d, f2);
+        if (visit) {
+          // level 2: a Q sub-ball separated from the key tile's ball is separated from each of
+          // its sub-balls, and a K sub-ball separated from the query tile's ball from each of
+          // the query's; only the pairs left over are tested one by one
+          unsigned ufail = 0u;
+          for (int u = 0; u < 8; ++u)
+            if (!separated(qball + (1 + u) * d, ru[u], Rsb[u >> 1], kcg, krg, d, f2)) ufail |= 1u << u;
+          visit = false;
+          if (ufail) {
+            const int nsb = max(1, bn / SUB);
+            const int64_t kb0 = k0 / SUB;
+            for (int v = 0; v < 2 * nsb && !visit; ++v) {
+              const float* cw = sc + (2 * kb0 + v) * d;
+              const float rw = sr[2 * kb0 + v];
+              if (rw < 0.f || separated(qball, rq, Rq, cw, rw, d, f2)) continue;
+              for (unsigned m = ufail; m; m &= m - 1u) {
+                const int u = __ffs(m) - 1;
+                if (!separated(qball + (1 + u) * d, ru[u], Rsb[u >> 1], cw, rw, d, f2)) {
+                  visit = true;
+                  break;
+                }
+              }
+            }
+          }
+        }
+      }
+      const uint32_t bits = __ballot_sync(FULL, visit);
+      if (lane == 0) {
+        out[base >> 5] = bits;
+        nvis += __popc(bits);
+      }
+    }
+    ntot += nkt - (hi - lo + 1);
+  }
+  if (prof && lane == 0) {
+    atomicAdd(&g_prune_tiles[0], (unsigned long long)nvis);
+    atomicAdd(&g_prune_tiles[1], (unsigned long long)ntot);
+  }
+}
+
+int grid_for(int64_t n) {
+  return int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, PR_T), int64_t(num_sms()) * 8)));
+}
+
+}  // namespace
+
+int prune_mask_words(int64_t max_seg, int bn) {
+  return int(ceil_div(ceil_div(max_seg, bn), 32));
+}
+
+size_t prune_workspace_bytes(int64_t npacked, int nseg, int d, int64_t n_items, int words) {
+  Carver c(nullptr);
+  carve_prune(c, npacked, nseg, d, n_items, words);
+  return c.bytes();
+}
+
+PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words) {
+  PruneWs w{};
+  w.leaf = c.take<int32_t>(npacked);
+  w.leaf2 = c.take<int32_t>(npacked);
+  w.perm2 = c.take<int32_t>(npacked);
+  w.reg = c.take<int32_t>(npacked);
+  w.S = c.take<int64_t>(npacked + 1);
+  w.scan_scratch = c.take<int64_t>(scan_i32_scratch_elems(npacked));
+  w.rpos = c.take<double>(npacked);
+  w.rpos2 = c.take<double>(npacked);
+  w.mean = c.take<double>(nseg);
+  const int64_t nq = npacked / QTILE, nk = npacked / 256, ns = npacked / SUB;
+  w.qc = c.take<float>(size_t(nq) * d);
+  w.qr = c.take<float>(nq);
+  w.kc = c.take<float>(size_t(nk) * d);
+  w.kr = c.take<float>(nk);
+  w.sc = c.take<float>(size_t(2 * ns) * d);
+  w.sr = c.take<float>(2 * ns);
+  w.rsub = c.take<double>(ns);
+  w.mask = c.take<uint32_t>(size_t(n_items) * words);
+  w.seed = c.take<float>(npacked);
+  return w;
+}
+
+int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
+                           int32_t* perm, const float* cand_thr, const QStat* qs,
+                           const KeyMax* km, int prec, int kmma, const PruneWs& w,
+                           cudaStream_t st) {
+  (void)X;
+  const int grid = grid_for(npacked);
+  row_radius_kernel<<<grid, PR_T, 0, st>>>(perm, npacked, cand_thr, qs, km, prec, kmma, d, w.rpos);
+  MSC_LAUNCH_CHECK();
+  sample_mean_kernel<<<nseg, PR_T, 0, st>>>(seg, w.rpos, w.mean);
+  MSC_LAUNCH_CHECK();
+  regular_flag_kernel<<<grid, PR_T, 0, st>>>(perm, npacked, seg, nseg, w.rpos, w.mean, w.reg);
+  MSC_LAUNCH_CHECK();
+  MSC_TRY(scan_excl_i32(w.reg, npacked, w.S, w.scan_scratch, st));
+  partition_kernel<<<grid, PR_T, 0, st>>>(perm, w.leaf, w.rpos, npacked, seg, nseg, w.reg, w.S,
+                                          cand_thr, qs, km, prec, kmma, d, w.perm2, w.leaf2,
+                                          w.rpos2, w.seed);
+  MSC_LAUNCH_CHECK();
+  MSC_CUDA_TRY(cudaMemcpyAsync(perm, w.perm2, sizeof(int32_t) * npacked,
+                               cudaMemcpyDeviceToDevice, st));
+  return MSC_OK;
+}
+
+int prune_counters(unsigned long long* out) {
+  MSC_CUDA_TRY(cudaMemcpyFromSymbol(out, g_prune_tiles, sizeof(unsigned long long) * 2));
+  return MSC_OK;
+}
+int prune_counters_clear() {
+  const unsigned long long z[2] = {0, 0};
+  MSC_CUDA_TRY(cudaMemcpyToSymbol(g_prune_tiles, z, sizeof(z)));
+  return MSC_OK;
+}
+
+int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* perm,
+                      const WorkItem* items, int64_t n_items, int bn, const Ctl* ctl, int prec,
+                      const PruneWs& w, int words, cudaStream_t st) {
+  if (d > 128 || bn > 256 || (npacked % 256) != 0) {
+    set_error("prune plan: unsupported shape (d=%d, bn=%d)", d, bn);
+    return MSC_ERR_INVALID_ARG;
+  }
+  const int64_t nq = npacked / QTILE, nk = npacked / 256, ns = npacked / SUB;
+  const int wgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(nq, 8), num_sms() * 16)));
+  group_ball_kernel<QTILE><<<wgrid, PR_T, 0, st>>>(X, d, perm, nq, w.qc, w.qr);
+  MSC_LAUNCH_CHECK();
+  group_ball_kernel<256><<<wgrid, PR_T, 0, st>>>(X, d, perm, nk, w.kc, w.kr);
+  MSC_LAUNCH_CHECK();
+  const int sgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(ns, 8), num_sms() * 16)));
+  sub_ball_kernel<<<sgrid, PR_T, 0, st>>>(X, d, perm, w.leaf2, w.rpos2, ns, w.sc, w.sr, w.rsub);
+  MSC_LAUNCH_CHECK();
+  const size_t smem = size_t(PLAN_WARPS) * 9 * d * sizeof(float);
+  const int pgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, PLAN_WARPS),
+                                                              int64_t(num_sms()) * 16)));
+  plan_kernel<<<pgrid, PLAN_WARPS * 32, smem, st>>>(items, n_items, bn, d, ctl, prec, w.qc, w.qr,
+                                                    w.kc, w.kr, w.sc, w.sr, w.rsub, words, w.mask,
+                                                    profiling_enabled() ? 1 : 0);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+}  // namespace msc

@@ -107,18 +107,8 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
   const int kk = k - 1;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   // key-side maxima and the scale
-  const double Kh = __uint_as_float(km->hi), Kl = __uint_as_float(km->lo);
-  const double Kr = __uint_as_float(km->res), Kn = __uint_as_float(km->nerr);
-  const double Ks = __uint_as_float(km->sq);
-  double f = 1.0;
-  if (prec == PREC_FP16) {
-    float mx = __uint_as_float(ctl->max_sq_bits);
-    if (mx > 0.f) {
-      int e = int(floor(0.5 * log2(16384.0 / double(mx))));
-      e = max(-60, min(60, e));
-      f = ldexp(1.0, e);
-    }
-  }
+  const KeyMax kmv = *km;
+  const double f = op_scale(prec, ctl);
   const double f2 = f * f;
   const double delta = double(d + 4) * 0x1p-24;
   int64_t n_cert = 0, n_ties = 0;
@@ -166,14 +156,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
       cert = true;                                      // every key is a candidate
     } else {
       const QStat q = qs[p];
-      const double qh = q.hi, ql = q.lo, qr = q.res;
-      const double dot_err = ql * Kl + (qh + ql) * Kr + qr * (Kh + Kl) + qr * Kr;
-      double acc_err;
-      if (prec == PREC_FP32)
-        acc_err = 0x1p-23 * ((2.0 * d + 4.0) * qh * Kh + 2.0 * Ks);
-      else
-        acc_err = double(kmma) * 0x1p-22 * (2.0 * (qh + ql) * (Kh + Kl) + Ks);
-      const double eps = 2.0 * dot_err + Kn + acc_err + 0x1p-40 * (q.sq + Ks);
+      const double eps = cert_eps(q, kmv, prec, kmma, d);
       const double T = double(cand_thr[i]);
       cert = f2 * Dk < q.sq + T - eps;
     }
