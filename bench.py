@@ -248,23 +248,31 @@ def run_ours(args):
     step()
     torch.cuda.synchronize()
     import ctypes
-    buf = (ctypes.c_float * 8)()
-    ns = lib.msc_profile_read(buf, 8)
+    buf = (ctypes.c_float * 12)()
+    ns = lib.msc_profile_read(buf, 12)
     lib.msc_profile_enable(0)
-    stage_names = ["prep", "prune_plan", "candidates", "rerank_fp64", "csr_rho_sigma_membership",
-                   "union"]
+    stage_names = ["prep", "near_pass", "prune_plan", "candidates", "rerank_fp64",
+                   "csr_rho_sigma_membership", "union"]
     stages = {stage_names[i]: round(buf[i], 3) for i in range(min(ns, len(stage_names)))}
-    cnt = (ctypes.c_ulonglong * 16)()
-    lib.msc_profile_counters(cnt, 16)
-    ctas = max(int(cnt[9]), 1)
-    pipeline = {"producer_wait_stage": cnt[0] / ctas, "mma_wait_keys": cnt[1] / ctas,
-                "mma_wait_accumulator": cnt[2] / ctas, "epilogue_wait_accumulator": cnt[3] / ctas / 4,
-                "epilogue_loop": cnt[4] / ctas / 4, "kernel": cnt[5] / ctas,
-                "hot_chunks_per_warp": cnt[6] / ctas / 4, "compactions_per_thread": cnt[7] / ctas / 128,
-                "appends_per_row": cnt[8] / max(n, 1), "ctas": ctas}
+    cnt = (ctypes.c_ulonglong * 64)()
+    lib.msc_profile_counters(cnt, 64)
+
+    def pipe(base):
+        c = [int(cnt[base + i]) for i in range(16)]
+        ctas = max(c[9], 1)
+        nepi = c[10] / ctas if c[10] else 4.0
+        return {"producer_wait_stage": c[0] / ctas, "mma_wait_keys": c[1] / ctas,
+                "mma_wait_accumulator": c[2] / ctas,
+                "epilogue_wait_accumulator": c[3] / ctas / nepi,
+                "epilogue_loop": c[4] / ctas / nepi, "kernel": c[5] / ctas,
+                "hot_chunks_per_warp": c[6] / ctas / nepi,
+                "insertions_per_row": c[8] / max(n, 1), "ctas": c[9], "epilogue_warps": nepi}
+    pipeline = {"near_pass": pipe(16), "main": pipe(32), "refine": pipe(48)}
     # key tiles beyond the near ones: kept by the pruning plan / all of them
     pruning = {"far_tiles_visited": int(cnt[10]), "far_tiles_total": int(cnt[11]),
-               "visited_frac": (cnt[10] / cnt[11]) if cnt[11] else None}
+               "visited_frac": (cnt[10] / cnt[11]) if cnt[11] else None,
+               "level1_failed": int(cnt[12]), "pair_stage_tiles": int(cnt[13]),
+               "pair_tests": int(cnt[14])}
 
     pk, pk_kind = peaks()
     cand_ms = stages.get("candidates")

@@ -69,18 +69,20 @@ const char* msc_last_error(void);
 /* Instrumentation (no counterpart in the reference).
  *   msc_launch_count   kernels this library has launched in this process;
  *   msc_profile_enable process-wide switch: record CUDA events between pipeline stages
- *                      (prep | key-tile pruning plan | candidates | re-rank + FP64 scan |
- *                      CSR + rho/sigma + memberships | fuzzy union) of the following calls — not
- *                      for concurrent callers;
+ *                      (prep | near pass | key-tile pruning plan | candidates | re-rank +
+ *                      FP64 scan | CSR + rho/sigma + memberships | fuzzy union) of the following
+ *                      calls — not for concurrent callers;
  *   msc_profile_read   waits for the last profiled call's events and writes its stage times in ms;
  *                      returns the number of stages written. */
 long long msc_launch_count(void);
 int       msc_profile_enable(int on);
 int       msc_profile_read(float* ms_out, int max_stages);
 /* pipeline counters of the tensor-core candidate kernel summed over CTAs since the last
- * msc_profile_enable(1) (cycles waiting / busy per role, hot chunks, compactions, appends, CTAs),
- * and in slots 10 and 11 the key tiles beyond the near ones that pruning kept / could have kept;
- * synchronizes the device. */
+ * msc_profile_enable(1) (cycles waiting / busy per role, hot chunks, compactions, candidate
+ * insertions, CTAs), and in slots 10 and 11 the key tiles beyond the near ones that pruning
+ * kept / could have kept; with max_counters >= 64, out[16 + 16·j + i] holds counter i of the
+ * near pass (j = 0), the main scan (j = 1) and the refine pass (j = 2) alone; synchronizes the
+ * device. */
 int       msc_profile_counters(unsigned long long* out, int max_counters);
 
 /* Self-test of the bounded device waits that every pipeline wait uses (no counterpart in the

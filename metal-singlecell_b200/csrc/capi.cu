@@ -274,7 +274,7 @@ int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
     if (env && *env) code = int32_t(std::strtol(env, nullptr, 0));
   }
   if (code == 0) return MSC_OK;
-  TcConfig c{code & 0xfff, (code >> 12) & 0xff, P.kprime <= 32 ? 32 : 64, (code >> 20) & 0x7f,
+  TcConfig c{code & 0xfff, (code >> 12) & 0xff, heap_slots(P.kprime), (code >> 20) & 0x7f,
              (code >> 27) & 1 ? 8 : 4, (code >> 28) & 1};
   if (!tc_config_ok(c, P.L.kp, P.kprime)) {
     set_error("tile_config 0x%x (bn=%d stages=%d cb=%d epi=%d pair=%d) is not valid here", code,
@@ -325,6 +325,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                                w.sq32, w.qs, w.km, st));
       stage_mark(st, 1);
       stage_mark(st, 2);
+      stage_mark(st, 3);
       MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
                               P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
     } else {
@@ -342,6 +343,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                               P.L.kmma, w.items, n_items, w.perm, nullptr, nullptr,
                               &w.ctl->tc_counter[2], w.ctl, P.kprime, w.cand_idx, w.cand_thr,
                               P.kprime, st, nullptr, 0, true));
+        stage_mark(st, 2);
         MSC_TRY(launch_prune_partition(Xu, P.d, w.seg, P.nseg, P.npacked, w.perm, w.cand_thr,
                                        w.qs, w.km, P.prec, P.L.kmma, w.pr, st));
         MSC_CUDA_TRY(cudaMemsetAsync(w.km, 0, sizeof(KeyMax), st));
@@ -351,15 +353,17 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
         MSC_TRY(launch_prune_plan(Xu, P.d, P.npacked, w.perm, w.items, n_items, cfg.bn, w.ctl,
                                   P.prec, w.pr, words, st));
         mask = w.pr.mask;
+      } else {
+        stage_mark(st, 2);
       }
-      stage_mark(st, 2);
+      stage_mark(st, 3);
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
                             w.items, n_items, w.perm, nullptr, nullptr, &w.ctl->tc_counter[0],
                             w.ctl, P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask, words,
                             false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr));
     }
   }
-  stage_mark(st, 3);
+  stage_mark(st, 4);
   if (P.refine) MSC_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * P.npacked, st));
   MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                         P.kprime, P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx,
@@ -387,7 +391,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   }
   MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
                            knn_idx, knn_dist, w.ctl, st));
-  stage_mark(st, 4);
+  stage_mark(st, 5);
   return MSC_OK;
 }
 
@@ -470,9 +474,10 @@ int msc_profile_counters(unsigned long long* out, int max_counters) {
   if (!out || max_counters < 1) { set_error("out/max_counters invalid"); return MSC_ERR_INVALID_ARG; }
   MSC_CUDA_TRY(cudaDeviceSynchronize());
   MSC_TRY(tc_counters(out, max_counters));
-  unsigned long long pt[2];
+  unsigned long long pt[5];
   MSC_TRY(prune_counters(pt));
   for (int i = 0; i < 2 && 10 + i < max_counters; ++i) out[10 + i] = pt[i];
+  for (int i = 2; i < 5 && 10 + i < max_counters; ++i) out[10 + i] = pt[i];
   return MSC_OK;
 }
 
@@ -572,18 +577,18 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
   if (method == MSC_METHOD_UMAP) {
     MSC_TRY(launch_smooth_knn(knn_dist_dev, n, k, 1.0f, g.sigma, g.rho, g.gsum, st));
     MSC_TRY(launch_membership(knn_idx_dev, knn_dist_dev, g.sigma, g.rho, n, k, g.w, st));
-    stage_mark(st, 5);
+    stage_mark(st, 6);
     MSC_TRY(launch_union(0, knn_idx_dev, g.w, nullptr, n, k, conn_indptr_dev, conn_indices_dev,
                          conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
   } else {
     MSC_TRY(launch_gauss_sigma(knn_dist_dev, n, k, g.sig2, st));
-    stage_mark(st, 5);
+    stage_mark(st, 6);
     MSC_TRY(launch_union(1, knn_idx_dev, knn_dist_dev, g.sig2, n, k, conn_indptr_dev,
                          conn_indices_dev, conn_data_dev, nullptr, g.uws, g.uws_bytes, st));
   }
   store_nnz_kernel<<<1, 32, 0, st>>>(conn_indptr_dev, n, w.ctl);
   MSC_LAUNCH_CHECK();
-  stage_mark(st, 6);
+  stage_mark(st, 7);
   return copy_stats(w, stats_dev, st);
 }
 

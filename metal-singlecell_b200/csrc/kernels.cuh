@@ -163,12 +163,13 @@ int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const 
 struct TcConfig {
   int bn;        // key tile rows (32, 64, 128, 256)
   int stages;    // smem pipeline depth of the key tiles
-  int kpl;       // selector list length (32 / 64)
-  int cb;        // selector buffer (16 / 32)
+  int kpl;       // slots of the per-row candidate heap (32 / 48 / 64), >= k'
+  int cb;        // 16 or 32; kept in the tile code for compatibility, no longer used
   int epi;       // epilogue warps: 4 (one per TMEM lane quarter) or 8 (two, splitting the columns)
   int pair;      // 1: CTA pairs (cta_group::2, M=256, each CTA stages half of every key tile)
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
+int heap_slots(int kprime);
 int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st);
 int tc_counters(unsigned long long* out, int max);
 int tc_counters_clear();

@@ -307,6 +307,7 @@ struct TcParams {
   int near_only;                // near pass: the near tiles only
   int reverse;                  // claim the work items from the last one down
   const float* seed;            // per packed query row: bound on its final k'-th value, or null
+  int prof_slot;                // counter block of this launch (near / main / refine)
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -344,7 +345,10 @@ struct KeyTileWalk {
     nkt = (item.nkeys + bn - 1) / bn;
     diag = (qref - item.key0) / bn;
     const int lo = max(0, diag - NEAR_SIDE), hi = min(nkt - 1, diag + NEAR_SIDE);
-    np = hi - lo + 1;
+    // the near pass only needs an upper bound on each row's k'-th value: the query tile's own
+    // key tile gives one at a fifth of the cost of all near tiles (its lists fill from +inf, so
+    // nearly every value is inserted)
+    np = near ? 1 : hi - lo + 1;
     j = 0;
     near_only = near;
     mask = m;
@@ -374,20 +378,22 @@ struct KeyTileWalk {
 //   2 MMA waiting for a free accumulator         3 epilogue waiting for an accumulator
 //   4 epilogue cycles in its tile loops          5 kernel cycles (thread 0)
 //   6 hot chunks (any row below its threshold)   7 compactions   8 appends   9 CTAs
-__device__ unsigned long long g_tc_prof[16];
+// one block of 16 counters per launch kind: 0 near pass, 1 main scan, 2 refine pass
+constexpr int PROF_SLOTS = 3;
+__device__ unsigned long long g_tc_prof[PROF_SLOTS][16];
 
 struct SmemPlan {
   size_t a_off, b_off, sel_off, pub_off, bar_off, total;
 };
 // brows = key rows this CTA stages per tile (BN, or BN/2 in a CTA pair);
 // nh = column groups per TMEM lane quarter (1: four epilogue warps, 2: eight)
-template <int KPL, int CB>
+template <int KH>
 __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int na, int nh) {
   SmemPlan p;
   p.a_off = 0;
   p.b_off = p.a_off + size_t(na) * kb * BM * 128;
   p.sel_off = p.b_off + size_t(stages) * brows * 128;
-  p.pub_off = p.sel_off + size_t(nh) * RowSelect<KPL, CB, BM>::smem_bytes();
+  p.pub_off = p.sel_off + size_t(nh) * RowHeap<KH, BM>::smem_bytes();
   p.bar_off = p.pub_off + (nh > 1 ? size_t(2) * BM * sizeof(float) : 0);
   p.total = p.bar_off + 512 + 1024;          // barriers + slack for 1024-byte alignment
   return p;
@@ -397,19 +403,19 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
 // quarter, each filtering half of the columns into its own list; the two lists of a row share
 // their thresholds while filtering and are merged when the query tile is done).
 // PAIR: two-CTA clusters, 256-row work items (see the file comment).
-template <int KPL, int CB, int NEPI, bool PAIR>
+template <int KH, int NEPI, bool PAIR>
 __global__ void __launch_bounds__(128 + 32 * NEPI, 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const TcParams P, const WorkItem* __restrict__ items, Ctl* __restrict__ ctl,
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
   static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
   constexpr int NH = NEPI / 4;
-  using Sel = RowSelect<KPL, CB, BM>;
+  using Sel = RowHeap<KH, BM>;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
   const int brows = PAIR ? P.bn / 2 : P.bn;            // key rows this CTA stages per tile
-  const SmemPlan sp = smem_plan<KPL, CB>(P.kb, brows, P.stages, P.na, NH);
+  const SmemPlan sp = smem_plan<KH>(P.kb, brows, P.stages, P.na, NH);
   unsigned char* Asm = smem + sp.a_off;
   unsigned char* Bsm = smem + sp.b_off;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + sp.bar_off);
@@ -556,7 +562,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         }
         if (!ok) break;
       }
-      if (P.prof) atomicAdd(&g_tc_prof[0], (unsigned long long)c_wait);
+      if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
       // drain: every load this thread armed completes on its own; wait for them (bounded)
       for (int s = 0; s < P.stages; ++s) {
         // stages armed in the current lap have parity sphase for indices < stage
@@ -654,8 +660,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
       }
       if (P.prof) {
-        atomicAdd(&g_tc_prof[1], (unsigned long long)c_b);
-        atomicAdd(&g_tc_prof[2], (unsigned long long)c_acc);
+        atomicAdd(&g_tc_prof[P.prof_slot][1], (unsigned long long)c_b);
+        atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
       }
     }
   } else if (warp >= EPI_WARP0) {
@@ -774,12 +780,12 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
     if (P.prof) {
       if (lane == 0) {
-        atomicAdd(&g_tc_prof[3], (unsigned long long)c_ew);
-        atomicAdd(&g_tc_prof[4], (unsigned long long)c_loop);
-        atomicAdd(&g_tc_prof[6], (unsigned long long)sel.n_hot);
+        atomicAdd(&g_tc_prof[P.prof_slot][3], (unsigned long long)c_ew);
+        atomicAdd(&g_tc_prof[P.prof_slot][4], (unsigned long long)c_loop);
+        atomicAdd(&g_tc_prof[P.prof_slot][6], (unsigned long long)sel.n_hot);
       }
-      atomicAdd(&g_tc_prof[7], (unsigned long long)sel.n_compact);
-      atomicAdd(&g_tc_prof[8], (unsigned long long)sel.n_append);
+      atomicAdd(&g_tc_prof[P.prof_slot][7], (unsigned long long)sel.n_compact);
+      atomicAdd(&g_tc_prof[P.prof_slot][8], (unsigned long long)sel.n_append);
     }
   }
 
@@ -794,8 +800,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   if (PAIR) cluster_sync();
   if (warp == 2) tmem_dealloc_g<PAIR>(tmem_base, tmem_cols);
   if (P.prof && threadIdx.x == 0) {
-    atomicAdd(&g_tc_prof[5], (unsigned long long)(clock64() - t_kernel0));
-    atomicAdd(&g_tc_prof[9], 1ull);
+    atomicAdd(&g_tc_prof[P.prof_slot][5], (unsigned long long)(clock64() - t_kernel0));
+    atomicAdd(&g_tc_prof[P.prof_slot][9], 1ull);
+    atomicAdd(&g_tc_prof[P.prof_slot][10], (unsigned long long)NEPI);
   }
   if (threadIdx.x == 0 && *abort_flag) {
     atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->stats[MSC_STAT_TIMEOUT]), 1ull);
@@ -869,22 +876,21 @@ int make_map(CUtensorMap* m, const void* base, int64_t rows, int kp, int box_row
 size_t config_smem(const TcConfig& c, int kb, int na) {
   const int nh = c.epi / 4;
   const int brows = c.pair ? c.bn / 2 : c.bn;
-  if (c.kpl == 32 && c.cb == 16) return smem_plan<32, 16>(kb, brows, c.stages, na, nh).total;
-  if (c.kpl == 32 && c.cb == 32) return smem_plan<32, 32>(kb, brows, c.stages, na, nh).total;
-  if (c.kpl == 64 && c.cb == 16) return smem_plan<64, 16>(kb, brows, c.stages, na, nh).total;
-  if (c.kpl == 64 && c.cb == 32) return smem_plan<64, 32>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 32) return smem_plan<32>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 48) return smem_plan<48>(kb, brows, c.stages, na, nh).total;
+  if (c.kpl == 64) return smem_plan<64>(kb, brows, c.stages, na, nh).total;
   return SIZE_MAX;
 }
 
 int pick_na(const TcConfig& c, int kb) { return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1; }
 
-template <int KPL, int CB, int NEPI, bool PAIR>
+template <int KH, int NEPI, bool PAIR>
 int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
                 const WorkItem* items, Ctl* ctl, int32_t* cand_idx, float* cand_thr,
                 cudaStream_t st) {
   const int brows = PAIR ? P.bn / 2 : P.bn;
-  const size_t smem = smem_plan<KPL, CB>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
-  auto kern = knn_tc_kernel<KPL, CB, NEPI, PAIR>;
+  const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
+  auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   if (!PAIR) {
     const int grid = std::max(1, std::min(P.n_items, num_sms()));
@@ -915,25 +921,29 @@ template <int NEPI, bool PAIR>
 int launch_tc_epi(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
                   const CUtensorMap& mb, const WorkItem* items, Ctl* ctl, int32_t* cand_idx,
                   float* cand_thr, cudaStream_t st) {
-  if (cfg.kpl == 32 && cfg.cb == 16)
-    return launch_tc_t<32, 16, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  if (cfg.kpl == 32 && cfg.cb == 32)
-    return launch_tc_t<32, 32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  if (cfg.kpl == 64 && cfg.cb == 16)
-    return launch_tc_t<64, 16, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  return launch_tc_t<64, 32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 32)
+    return launch_tc_t<32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  if (cfg.kpl == 48)
+    return launch_tc_t<48, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  return launch_tc_t<64, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
 }
 
 }  // namespace
 
+// out[0..15]: all launches summed; out[16 + 16·slot + i]: launch kind `slot` alone
 int tc_counters(unsigned long long* out, int max) {
-  unsigned long long buf[16];
+  unsigned long long buf[PROF_SLOTS][16];
   MSC_CUDA_TRY(cudaMemcpyFromSymbol(buf, g_tc_prof, sizeof(buf)));
-  for (int i = 0; i < max && i < 16; ++i) out[i] = buf[i];
+  for (int i = 0; i < max && i < 16; ++i) {
+    out[i] = 0;
+    for (int sl = 0; sl < PROF_SLOTS; ++sl) out[i] += buf[sl][i];
+  }
+  for (int sl = 0; sl < PROF_SLOTS; ++sl)
+    for (int i = 0; i < 16 && 16 + 16 * sl + i < max; ++i) out[16 + 16 * sl + i] = buf[sl][i];
   return MSC_OK;
 }
 int tc_counters_clear() {
-  unsigned long long z[16] = {};
+  unsigned long long z[PROF_SLOTS][16] = {};
   MSC_CUDA_TRY(cudaMemcpyToSymbol(g_tc_prof, z, sizeof(z)));
   return MSC_OK;
 }
@@ -947,7 +957,7 @@ int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st) {
 bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;
   if (c.stages < 2 || c.stages > 8) return false;
-  if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 64)) return false;
+  if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 48 && c.kpl != 64)) return false;
   if (c.cb != 16 && c.cb != 32) return false;
   if (c.epi != 4 && c.epi != 8) return false;
   if (c.epi == 8 && c.bn < 64) return false;         // each column group takes >= 32 columns
@@ -956,23 +966,25 @@ bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   return config_smem(c, kp / 64, 1) <= SMEM_LIMIT;
 }
 
+// heap capacity of a k' (32, 48 or 64 slots per row)
+int heap_slots(int kprime) { return kprime <= 32 ? 32 : (kprime <= 48 ? 48 : 64); }
+
 TcConfig tc_default_config(int prec, int d, int kprime) {
   const OpLayout L = op_layout(prec, d);
-  const int kpl = kprime <= 32 ? 32 : 64;
+  const int kpl = heap_slots(kprime);
   // Single CTAs first: CTA pairs halve the key bytes per SM and double the K-atom stages that
   // fit, but measured slower at 1.3M × 50 (1057 vs 819 ms for the candidate stage), so they are
   // taken only when nothing else fits.  N=256 key tiles (one MMA costs the same ~186 cycles at
   // N = 64..256, so only N=256 reaches the tensor peak); eight epilogue warps (a warp's TMEM reads
   // are serialised, so read bandwidth grows with the number of reading warps), else four; then
-  // the deepest K-atom pipeline and the largest selector buffer that fit
+  // the deepest K-atom pipeline that fits
   for (int pair : {0, 1})
     for (int bn : {256, 128, 64, 32})
       for (int epi : {8, 4})
-        for (int stages = 8; stages >= 2; --stages)
-          for (int cb : {32, 16}) {
-            TcConfig c{bn, stages, kpl, cb, epi, pair};
-            if (tc_config_ok(c, L.kp, kprime)) return c;
-          }
+        for (int stages = 8; stages >= 2; --stages) {
+          TcConfig c{bn, stages, kpl, 16, epi, pair};
+          if (tc_config_ok(c, L.kp, kprime)) return c;
+        }
   return TcConfig{64, 2, kpl, 16, 4, 0};
 }
 
@@ -983,6 +995,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask, int mask_words, bool near_only, bool reverse,
                   const float* seed) {
+  const int prof_slot = near_only ? 0 : (qmap ? 2 : 1);
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
               cfg.bn, cfg.stages, cfg.kpl, cfg.cb, cfg.epi, cfg.pair);
@@ -1013,6 +1026,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.near_only = near_only ? 1 : 0;
   P.reverse = reverse ? 1 : 0;
   P.seed = seed;
+  P.prof_slot = prof_slot;
   if (cfg.pair && (mask || near_only)) {
     set_error("pruned scans run on single CTAs only");
     return MSC_ERR_INVALID_ARG;

@@ -246,4 +246,176 @@ struct RowSelect {
   }
 };
 
+
+// --- the row heap (tensor-core epilogue) ------------------------------------------------------------
+//
+// The same three-level filter, but a value that passes goes straight into a max-heap of the row's
+// k' smallest values kept in shared memory (one sift-down of at most log2(k') levels), and the
+// row's threshold is the heap's root at once.  Compared with the buffered list above this costs a
+// few dozen instructions per insertion instead of a sort and a k'-step merge per buffer, and it
+// tightens the threshold after every insertion.  The list's order does not matter to the callers
+// (the re-rank sorts the candidates itself), so the heap is written out as it stands.
+//
+// Shared memory (slot-major, so the 32 rows of a warp hit 32 banks whatever slot each lane is at):
+//   hv/hi[KH][ROWS]   heap per row: max of (value) at slot 0; +inf / -1 while not full
+template <int KH, int ROWS>
+struct RowHeap {
+  static_assert(KH == 32 || KH == 48 || KH == 64, "heap of 32, 48 or 64");
+  __host__ __device__ static constexpr size_t smem_bytes() { return size_t(KH) * ROWS * 8; }
+
+  int2* he;       // heap entries [KH][ROWS]: (float bits of the value, column)
+  int row;        // this thread's row within the ROWS rows
+  int kp;         // k' (<= KH)
+  float thr;      // the heap's root: the k'-th smallest value kept (+inf while not full)
+  float thr_f;    // filter threshold: min(thr, seed, the partner heap's published root)
+  // An upper bound on the row's final k'-th value known before the scan (from an earlier pass
+  // over a subset of its keys), +inf if none.  Values at or above it are never kept; the
+  // threshold reported by finish() is min(root, seed), so every value not kept is at least the
+  // reported threshold even if fewer than k' values passed the filter.
+  float seed = F_INF;
+  // When two heaps split one row's columns, each publishes its root here (shared memory) and
+  // filters against the smaller of the two: the k'-th smallest of the union is at most either
+  // heap's k'-th value, so nothing it drops can belong to the union's k' smallest.
+  float* pub_own = nullptr;
+  const float* pub_other = nullptr;
+  int n_hot = 0, n_compact = 0, n_append = 0;   // counters for the pipeline profile
+
+  __device__ void bind(void* smem, int row_, int kprime) {
+    he = static_cast<int2*>(smem);
+    row = row_;
+    kp = kprime;
+  }
+
+  __device__ void reset() {
+    for (int s = 0; s < KH; ++s) he[s * ROWS + row] = make_int2(__float_as_int(F_INF), -1);
+    thr = F_INF;
+    thr_f = F_INF;
+    seed = F_INF;
+  }
+
+  __device__ __forceinline__ void set_seed(float s) {
+    seed = s;
+    thr_f = fminf(thr_f, s);
+  }
+
+  __device__ __forceinline__ void refresh() {
+    thr_f = fminf(thr, seed);
+    if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
+  }
+
+  // replace the root by (v, col) (v < root) and restore the heap: one 8-byte load per child and
+  // one 8-byte store per level
+  __device__ __forceinline__ void insert(float v, int col) {
+    ++n_append;
+    int2* H = he + row;
+    int i = 0;
+    for (;;) {
+      const int l = 2 * i + 1;
+      if (l >= kp) break;
+      int2 c = H[l * ROWS];
+      int ci = l;
+      if (l + 1 < kp) {
+        const int2 r = H[(l + 1) * ROWS];
+        if (__int_as_float(r.x) > __int_as_float(c.x)) { c = r; ci = l + 1; }
+      }
+      if (!(__int_as_float(c.x) > v)) break;
+      H[i * ROWS] = c;
+      i = ci;
+    }
+    H[i * ROWS] = make_int2(__float_as_int(v), col);
+    thr = __int_as_float(H[0].x);
+    if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
+    refresh();
+  }
+
+  // Merge another heap of the same row (same layout, base `other`) into this one.  Nothing is
+  // published meanwhile: the partner reads this row's published root as +inf until the next tile.
+  __device__ void merge_from(const void* other) {
+    const int2* O = static_cast<const int2*>(other) + row;
+    float* keep = pub_own;
+    pub_own = nullptr;
+    for (int s = 0; s < kp; ++s) {
+      const int2 e = O[s * ROWS];
+      if (__int_as_float(e.x) < thr) insert(__int_as_float(e.x), e.y);
+    }
+    pub_own = keep;
+  }
+
+  // the e-th of 32 register values without indexing the register array (a 5-level select tree)
+  __device__ __forceinline__ static float pick32(const float (&v)[32], int e) {
+    float a[16], b[8], c[4], d[2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = (e & 1) ? v[2 * i + 1] : v[2 * i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) b[i] = (e & 2) ? a[2 * i + 1] : a[2 * i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) c[i] = (e & 4) ? b[2 * i + 1] : b[2 * i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) d[i] = (e & 8) ? c[2 * i + 1] : c[2 * i];
+    return (e & 16) ? d[1] : d[0];
+  }
+
+  // Offer 32 consecutive candidate columns col0..col0+31 of this row (warp-collective).
+  // Columns equal to `self` or >= `limit` are never kept.  Every lane first marks its values
+  // below the threshold; then the lanes insert their next marked value together, so that the
+  // sift-downs of the warp's 32 rows run side by side instead of one lane after another.
+  __device__ __forceinline__ void push32(const float (&v)[32], int col0, int self, int limit) {
+    float g[11];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) g[q] = min3f(v[3 * q], v[3 * q + 1], v[3 * q + 2]);
+    g[10] = fminf(v[30], v[31]);
+    const float n0 = min3f(g[0], g[1], g[2]), n1 = min3f(g[3], g[4], g[5]);
+    const float n2 = min3f(g[6], g[7], g[8]), n3 = fminf(g[9], g[10]);
+    const float mn = fminf(min3f(n0, n1, n2), n3);
+    if (!__any_sync(FULL, mn < thr_f)) return;
+    ++n_hot;
+    unsigned m = 0u;
+    if (mn < thr_f) {
+#pragma unroll
+      for (int e = 0; e < 32; ++e) m |= (v[e] < thr_f ? 1u : 0u) << e;
+      const int ds = self - col0;
+      if (ds >= 0 && ds < 32) m &= ~(1u << ds);
+      const int dl = limit - col0;
+      if (dl < 32) m &= dl <= 0 ? 0u : ((1u << dl) - 1u);
+    }
+    while (__any_sync(FULL, m != 0u)) {
+      if (m) {
+        const int e = __ffs(m) - 1;
+        m &= m - 1u;
+        const float x = pick32(v, e);
+        if (x < thr_f) insert(x, col0 + e);
+      }
+    }
+  }
+
+  __device__ __forceinline__ void push1(float v, int c, int self, int limit) {
+    if (v < thr_f && c != self && c < limit) insert(v, c);
+  }
+
+  __device__ void flush() {}
+
+  // warp-collective: write the k' kept columns (heap order) and the threshold min(root, seed) of
+  // the warp's first `nvalid_rows` rows; columns are packed positions mapped to original rows
+  // through perm (see RowSelect::finish)
+  __device__ void finish(int* out_idx, float* out_thr, int out_stride,
+                         const int32_t* __restrict__ perm, const int32_t* __restrict__ qmap,
+                         int64_t first_row, int nvalid_rows, int kout) {
+    __syncwarp();
+    const int lane = lane_id();
+    const int row0 = row - lane;
+    for (int r = 0; r < nvalid_rows; ++r) {
+      const int rr = row0 + r;
+      const int64_t prow = qmap ? int64_t(qmap[first_row + r]) : first_row + r;
+      const int64_t orow = perm[prow];
+      const float sd = __shfl_sync(FULL, seed, r);
+      for (int s = lane; s < kout; s += 32) {
+        const int c = he[s * ROWS + rr].y;
+        out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
+      }
+      if (lane == 0) out_thr[orow] = fminf(__int_as_float(he[rr].x), sd);
+    }
+    __syncwarp();
+  }
+};
+
 }  // namespace msc

@@ -68,14 +68,36 @@ __global__ void order_init_kernel(const SegDesc* __restrict__ seg, int nseg, int
   }
 }
 
+// atomicMax of key into best[s]; the lanes of a warp that share node s combine first (positions
+// are contiguous, so a warp almost always lies inside one node and issues a single atomic)
+__device__ __forceinline__ void warp_far_max(unsigned long long* best, int s, bool active,
+                                             unsigned long long key) {
+  const int s0 = __shfl_sync(FULL, s, 0);
+  if (__all_sync(FULL, active && s == s0)) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(FULL, key, o);
+      key = other > key ? other : key;
+    }
+    if (lane_id() == 0) atomicMax(&best[s0], key);
+  } else if (active) {
+    atomicMax(&best[s], key);
+  }
+}
+
+// The loops below keep the 32 lanes of a warp on 32 consecutive positions (warp-uniform trip
+// counts) so that warp_far_max can combine them.
 __global__ void far_a_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                              const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                              const int32_t* __restrict__ ne, unsigned long long* __restrict__ best) {
-  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int s = ns[p], e = ne[p];
-    if (e - s <= leaf) continue;
-    atomicMax(&best[s], far_key(row_d2(X, d, perm[p], perm[s]), p));
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+       b += stride) {
+    const int64_t p = b + lane_id();
+    int s = 0, e = 0;
+    if (p < npacked) { s = ns[p]; e = ne[p]; }
+    const bool active = p < npacked && e - s > leaf;
+    const unsigned long long key = active ? far_key(row_d2(X, d, perm[p], perm[s]), p) : 0ull;
+    warp_far_max(best, s, active, key);
   }
 }
 
@@ -83,13 +105,20 @@ __global__ void far_b_kernel(const float* __restrict__ X, int d, int64_t npacked
                              const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                              const int32_t* __restrict__ ne, const unsigned long long* __restrict__ best_a,
                              float* __restrict__ da, unsigned long long* __restrict__ best_b) {
-  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int s = ns[p], e = ne[p];
-    if (e - s <= leaf) continue;
-    const float v = row_d2(X, d, perm[p], perm[far_pos(best_a[s])]);
-    da[p] = v;
-    atomicMax(&best_b[s], far_key(v, p));
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+       b += stride) {
+    const int64_t p = b + lane_id();
+    int s = 0, e = 0;
+    if (p < npacked) { s = ns[p]; e = ne[p]; }
+    const bool active = p < npacked && e - s > leaf;
+    unsigned long long key = 0ull;
+    if (active) {
+      const float v = row_d2(X, d, perm[p], perm[far_pos(best_a[s])]);
+      da[p] = v;
+      key = far_key(v, p);
+    }
+    warp_far_max(best_b, s, active, key);
   }
 }
 

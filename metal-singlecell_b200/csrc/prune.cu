@@ -35,8 +35,9 @@ namespace {
 
 constexpr int PR_T = 256;
 
-// key tiles visited beyond the near tiles, and all such tiles, summed over plans while profiling
-__device__ unsigned long long g_prune_tiles[2];
+// summed over plans while profiling: key tiles visited beyond the near tiles, all such tiles,
+// tiles that failed level 1, tiles that reached the pair tests, pair tests
+__device__ unsigned long long g_prune_tiles[5];
 constexpr int SUB = 32;          // rows per sub-block (two balls each)
 constexpr float NO_BALL = -1.f;  // radius of a ball without rows
 constexpr double OUTLIER_FACTOR = 4.0;
@@ -143,7 +144,7 @@ __global__ void partition_kernel(const int32_t* __restrict__ perm, const int32_t
 // One ball per group of G packed rows (G = 128 or 256): centre = float(mean of the rows), radius =
 // max distance to that centre, rounded up.  One warp per group; lane t sums dimensions t, t+32, ...
 template <int G>
-__global__ void group_ball_kernel(const float* __restrict__ X, int d,
+__global__ void group_ball_kernel(const float* __restrict__ X, int d, int dp,
                                   const int32_t* __restrict__ perm, int64_t ngroups,
                                   float* __restrict__ centre, float* __restrict__ radius) {
   const int lane = lane_id();
@@ -164,8 +165,8 @@ __global__ void group_ball_kernel(const float* __restrict__ X, int d,
     float c[4];
     for (int j = 0; j < 4; ++j) {
       const int t = lane + 32 * j;
-      c[j] = cnt ? float(s[j] / cnt) : 0.f;
-      if (t < d) centre[g * d + t] = c[j];
+      c[j] = (cnt && t < d) ? float(s[j] / cnt) : 0.f;
+      if (t < dp) centre[g * dp + t] = c[j];
     }
     double mx = 0.0;
     for (int r = 0; r < G; ++r) {
@@ -189,7 +190,7 @@ __global__ void group_ball_kernel(const float* __restrict__ X, int d,
 // Two balls per 32-row block, split at the first row whose leaf differs from the block's first
 // row (rows of one leaf are close, rows of two leaves may lie in two clusters), and the block's
 // max R.  Ball 2b covers rows [0, m), ball 2b+1 rows [m, 32).
-__global__ void sub_ball_kernel(const float* __restrict__ X, int d,
+__global__ void sub_ball_kernel(const float* __restrict__ X, int d, int dp,
                                 const int32_t* __restrict__ perm,
                                 const int32_t* __restrict__ leaf,
                                 const double* __restrict__ rpos, int64_t nsub,
@@ -226,11 +227,11 @@ __global__ void sub_ball_kernel(const float* __restrict__ X, int d,
         }
       }
       float c[4];
-      float* cdst = centre + (2 * b + h) * d;
+      float* cdst = centre + (2 * b + h) * dp;
       for (int j = 0; j < 4; ++j) {
         const int t = lane + 32 * j;
-        c[j] = cnt ? float(s[j] / cnt) : 0.f;
-        if (t < d) cdst[t] = c[j];
+        c[j] = (cnt && t < d) ? float(s[j] / cnt) : 0.f;
+        if (t < dp) cdst[t] = c[j];
       }
       double mx = 0.0;
       for (int r = r0; r < r1; ++r) {
@@ -254,96 +255,123 @@ __global__ void sub_ball_kernel(const float* __restrict__ X, int d,
 
 // Are the balls (cu, ru) and (cw, rw) so far apart that no row of u can take a key of w?  R = max
 // R over u's rows (z-space), f2 = square of the operand scale.  An empty ball is separated from
-// everything; an unknown R (inf / NaN) from nothing.  The FP32 distance is lowered by its
-// rounding bound (d+8 units of 2^-23 relative) before the test.
+// everything; an unknown R (inf / NaN) from nothing.  Centres are n4 float4 (zero padded); the
+// FP32 distance is lowered by its rounding bound (d+8 units of 2^-23 relative) before the test.
 __device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru, double R,
-                                          const float* __restrict__ cw, float rw, int d,
+                                          const float* __restrict__ cw, float rw, int n4, int d,
                                           double f2) {
   if (ru < 0.f || rw < 0.f) return true;
   if (!(R < 1e300)) return false;
-  float s = 0.f;
-  for (int t = 0; t < d; ++t) {
-    const float df = cu[t] - cw[t];
-    s = fmaf(df, df, s);
+  const float4* a = reinterpret_cast<const float4*>(cu);
+  const float4* b = reinterpret_cast<const float4*>(cw);
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll 4
+  for (int t = 0; t < n4; ++t) {
+    const float4 x = a[t], y = b[t];
+    const float e0 = x.x - y.x, e1 = x.y - y.y, e2 = x.z - y.z, e3 = x.w - y.w;
+    s0 = fmaf(e0, e0, s0);
+    s1 = fmaf(e1, e1, s1);
+    s2 = fmaf(e2, e2, s2);
+    s3 = fmaf(e3, e3, s3);
   }
+  const float s = (s0 + s1) + (s2 + s3);
   const double lo = double(s) * (1.0 - double(d + 8) * 0x1p-23);
   const double L = sqrt(lo) - double(ru) - double(rw);
   return L > 0.0 && f2 * L * L > R * (1.0 + 1e-9);
 }
 
-// One warp per query tile (work item); lane = key tile.  Level 1: the query tile's ball against
-// the 256-row ball holding the key tile; level 2: every ball pair of the two tiles.
+// One warp per query tile (work item).  Level 1, lane = key tile: the query tile's ball against
+// the 256-row ball holding the key tile.  The key tiles of a 32-tile chunk that fail it go to
+// level 2 together: (a) every query sub-ball against the key tile's ball, (b) every key sub-ball
+// against the query tile's ball — a sub-ball separated there is separated from every sub-ball of
+// the other side — with the (key tile, sub-ball) tests spread over the lanes; then, per key tile
+// left, the remaining sub-ball pairs, one pair per lane.
 constexpr int PLAN_WARPS = 4;
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
-plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, const Ctl* ctl,
-            int prec, const float* __restrict__ qc, const float* __restrict__ qr,
+plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
+            const Ctl* ctl, int prec, const float* __restrict__ qc, const float* __restrict__ qr,
             const float* __restrict__ kc, const float* __restrict__ kr,
             const float* __restrict__ sc, const float* __restrict__ sr,
             const double* __restrict__ rsub, int words, uint32_t* __restrict__ mask, int prof) {
-  extern __shared__ float sm[];
+  extern __shared__ float4 sm4[];
+  __shared__ unsigned ubits_all[PLAN_WARPS][32], wbits_all[PLAN_WARPS][32];
   const int lane = lane_id(), wib = warp_id();
-  float* qball = sm + wib * (9 * d);            // [0]: the tile's ball, [1..8]: its sub-balls
+  float* qball = reinterpret_cast<float*>(sm4) + wib * (9 * dp);   // [0]: tile, [1..8]: sub-balls
+  unsigned* ubits = ubits_all[wib];
+  unsigned* wbits = wbits_all[wib];
+  const int n4 = dp / 4;
   const double f = op_scale(prec, ctl);
   const double f2 = f * f;
   const int64_t warps = int64_t(gridDim.x) * PLAN_WARPS;
-  long long nvis = 0, ntot = 0;
+  const int nv = 2 * max(1, bn / SUB);          // key sub-balls per key tile
+  long long nvis = 0, ntot = 0, nl1 = 0, npt = 0, npr = 0;
   for (int64_t it = int64_t(blockIdx.x) * PLAN_WARPS + wib; it < n_items; it += warps) {
     const WorkItem w = items[it];
     const int64_t qt = w.qrow0 / QTILE;          // 128-row tile of packed rows
     const int64_t sb0 = int64_t(w.qrow0) / SUB;  // its first 32-row block
     __syncwarp();
-    for (int t = lane; t < d; t += 32) qball[t] = qc[qt * d + t];
+    for (int t = lane; t < dp; t += 32) qball[t] = qc[qt * dp + t];
     for (int u = 0; u < 8; ++u)
-      for (int t = lane; t < d; t += 32) qball[(1 + u) * d + t] = sc[(2 * sb0 + u) * d + t];
+      for (int t = lane; t < dp; t += 32) qball[(1 + u) * dp + t] = sc[(2 * sb0 + u) * dp + t];
     __syncwarp();
     const float rq = qr[qt];
-    double Rsb[4], Rq = 0.0;
-    for (int j = 0; j < 4; ++j) {
-      Rsb[j] = rsub[sb0 + j];
-      Rq = fmax(Rq, Rsb[j]);                      // NaN never occurs: rsub is >= 0 or +inf
-    }
-    float ru[8];
-    for (int u = 0; u < 8; ++u) ru[u] = sr[2 * sb0 + u];
+    double Rq = 0.0;
+    for (int j = 0; j < 4; ++j) Rq = fmax(Rq, rsub[sb0 + j]);    // rsub is >= 0 or +inf
     const int nkt = (w.nkeys + bn - 1) / bn;
     const int diag = (w.qrow0 - w.key0) / bn;
     const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
     uint32_t* out = mask + it * int64_t(words);
     for (int base = 0; base < words * 32; base += 32) {
       const int kt = base + lane;
-      bool visit = false;
+      bool l1 = false;                           // not separated at level 1
       if (kt < nkt && (kt < lo || kt > hi)) {
-        const int64_t k0 = int64_t(w.key0) + int64_t(kt) * bn;   // first packed key row
-        const int64_t g = k0 / 256;
-        const float* kcg = kc + g * d;
-        const float krg = kr[g];
-        visit = !separated(qball, rq, Rq, kcg, krg, d, f2);
-        if (visit) {
-          // level 2: a Q sub-ball separated from the key tile's ball is separated from each of
-          // its sub-balls, and a K sub-ball separated from the query tile's ball from each of
-          // the query's; only the pairs left over are tested one by one
-          unsigned ufail = 0u;
-          for (int u = 0; u < 8; ++u)
-            if (!separated(qball + (1 + u) * d, ru[u], Rsb[u >> 1], kcg, krg, d, f2)) ufail |= 1u << u;
-          visit = false;
-          if (ufail) {
-            const int nsb = max(1, bn / SUB);
-            const int64_t kb0 = k0 / SUB;
-            for (int v = 0; v < 2 * nsb && !visit; ++v) {
-              const float* cw = sc + (2 * kb0 + v) * d;
-              const float rw = sr[2 * kb0 + v];
-              if (rw < 0.f || separated(qball, rq, Rq, cw, rw, d, f2)) continue;
-              for (unsigned m = ufail; m; m &= m - 1u) {
-                const int u = __ffs(m) - 1;
-                if (!separated(qball + (1 + u) * d, ru[u], Rsb[u >> 1], cw, rw, d, f2)) {
-                  visit = true;
-                  break;
-                }
-              }
-            }
+        const int64_t g = (int64_t(w.key0) + int64_t(kt) * bn) / 256;
+        l1 = !separated(qball, rq, Rq, kc + g * dp, kr[g], n4, d, f2);
+      }
+      const uint32_t fm = __ballot_sync(FULL, l1);
+      uint32_t bits = 0u;
+      if (fm) {
+        const int nf = __popc(fm);
+        nl1 += nf;
+        ubits[lane] = 0u;
+        wbits[lane] = 0u;
+        __syncwarp();
+        // (a) query sub-ball u of failing tile i
+        for (int x = lane; x < 8 * nf; x += 32) {
+          const int i = x >> 3, u = x & 7;
+          const int kti = base + __fns(fm, 0, i + 1);
+          const int64_t g = (int64_t(w.key0) + int64_t(kti) * bn) / 256;
+          if (!separated(qball + (1 + u) * dp, sr[2 * sb0 + u], rsub[sb0 + (u >> 1)],
+                         kc + g * dp, kr[g], n4, d, f2))
+            atomicOr(&ubits[i], 1u << u);
+        }
+        // (b) key sub-ball v of failing tile i
+        for (int x = lane; x < nv * nf; x += 32) {
+          const int i = x / nv, v = x - i * nv;
+          const int kti = base + __fns(fm, 0, i + 1);
+          const int64_t kb0 = (int64_t(w.key0) + int64_t(kti) * bn) / SUB;
+          const float rw = sr[2 * kb0 + v];
+          if (rw >= 0.f && !separated(qball, rq, Rq, sc + (2 * kb0 + v) * dp, rw, n4, d, f2))
+            atomicOr(&wbits[i], 1u << v);
+        }
+        __syncwarp();
+        for (int i = 0; i < nf; ++i) {
+          const uint32_t ub = ubits[i], wb = wbits[i];
+          if (!ub || !wb) continue;                 // warp-uniform
+          const int kti = base + __fns(fm, 0, i + 1);
+          const int64_t kb0 = (int64_t(w.key0) + int64_t(kti) * bn) / SUB;
+          const int nu = __popc(ub), npair = nu * __popc(wb);
+          ++npt;
+          npr += npair;
+          bool hit = false;
+          for (int pr = lane; pr < npair && !hit; pr += 32) {
+            const int u = __fns(ub, 0, pr % nu + 1), vv = __fns(wb, 0, pr / nu + 1);
+            hit = !separated(qball + (1 + u) * dp, sr[2 * sb0 + u], rsub[sb0 + (u >> 1)],
+                             sc + (2 * kb0 + vv) * dp, sr[2 * kb0 + vv], n4, d, f2);
           }
+          if (__any_sync(FULL, hit)) bits |= 1u << (kti - base);
         }
       }
-      const uint32_t bits = __ballot_sync(FULL, visit);
       if (lane == 0) {
         out[base >> 5] = bits;
         nvis += __popc(bits);
@@ -354,6 +382,9 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
   if (prof && lane == 0) {
     atomicAdd(&g_prune_tiles[0], (unsigned long long)nvis);
     atomicAdd(&g_prune_tiles[1], (unsigned long long)ntot);
+    atomicAdd(&g_prune_tiles[2], (unsigned long long)nl1);
+    atomicAdd(&g_prune_tiles[3], (unsigned long long)npt);
+    atomicAdd(&g_prune_tiles[4], (unsigned long long)npr);
   }
 }
 
@@ -385,11 +416,12 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.rpos2 = c.take<double>(npacked);
   w.mean = c.take<double>(nseg);
   const int64_t nq = npacked / QTILE, nk = npacked / 256, ns = npacked / SUB;
-  w.qc = c.take<float>(size_t(nq) * d);
+  const int dp = int(round_up(d, 4));
+  w.qc = c.take<float>(size_t(nq) * dp);
   w.qr = c.take<float>(nq);
-  w.kc = c.take<float>(size_t(nk) * d);
+  w.kc = c.take<float>(size_t(nk) * dp);
   w.kr = c.take<float>(nk);
-  w.sc = c.take<float>(size_t(2 * ns) * d);
+  w.sc = c.take<float>(size_t(2 * ns) * dp);
   w.sr = c.take<float>(2 * ns);
   w.rsub = c.take<double>(ns);
   w.mask = c.take<uint32_t>(size_t(n_items) * words);
@@ -420,11 +452,11 @@ int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, 
 }
 
 int prune_counters(unsigned long long* out) {
-  MSC_CUDA_TRY(cudaMemcpyFromSymbol(out, g_prune_tiles, sizeof(unsigned long long) * 2));
+  MSC_CUDA_TRY(cudaMemcpyFromSymbol(out, g_prune_tiles, sizeof(unsigned long long) * 5));
   return MSC_OK;
 }
 int prune_counters_clear() {
-  const unsigned long long z[2] = {0, 0};
+  const unsigned long long z[5] = {0, 0, 0, 0, 0};
   MSC_CUDA_TRY(cudaMemcpyToSymbol(g_prune_tiles, z, sizeof(z)));
   return MSC_OK;
 }
@@ -437,20 +469,21 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
     return MSC_ERR_INVALID_ARG;
   }
   const int64_t nq = npacked / QTILE, nk = npacked / 256, ns = npacked / SUB;
+  const int dp = int(round_up(d, 4));
   const int wgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(nq, 8), num_sms() * 16)));
-  group_ball_kernel<QTILE><<<wgrid, PR_T, 0, st>>>(X, d, perm, nq, w.qc, w.qr);
+  group_ball_kernel<QTILE><<<wgrid, PR_T, 0, st>>>(X, d, dp, perm, nq, w.qc, w.qr);
   MSC_LAUNCH_CHECK();
-  group_ball_kernel<256><<<wgrid, PR_T, 0, st>>>(X, d, perm, nk, w.kc, w.kr);
+  group_ball_kernel<256><<<wgrid, PR_T, 0, st>>>(X, d, dp, perm, nk, w.kc, w.kr);
   MSC_LAUNCH_CHECK();
   const int sgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(ns, 8), num_sms() * 16)));
-  sub_ball_kernel<<<sgrid, PR_T, 0, st>>>(X, d, perm, w.leaf2, w.rpos2, ns, w.sc, w.sr, w.rsub);
+  sub_ball_kernel<<<sgrid, PR_T, 0, st>>>(X, d, dp, perm, w.leaf2, w.rpos2, ns, w.sc, w.sr, w.rsub);
   MSC_LAUNCH_CHECK();
-  const size_t smem = size_t(PLAN_WARPS) * 9 * d * sizeof(float);
+  const size_t smem = size_t(PLAN_WARPS) * 9 * dp * sizeof(float);
   const int pgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, PLAN_WARPS),
                                                               int64_t(num_sms()) * 16)));
-  plan_kernel<<<pgrid, PLAN_WARPS * 32, smem, st>>>(items, n_items, bn, d, ctl, prec, w.qc, w.qr,
-                                                    w.kc, w.kr, w.sc, w.sr, w.rsub, words, w.mask,
-                                                    profiling_enabled() ? 1 : 0);
+  plan_kernel<<<pgrid, PLAN_WARPS * 32, smem, st>>>(items, n_items, bn, d, dp, ctl, prec, w.qc,
+                                                    w.qr, w.kc, w.kr, w.sc, w.sr, w.rsub, words,
+                                                    w.mask, profiling_enabled() ? 1 : 0);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }

@@ -171,7 +171,7 @@ def autotune(X, offsets, n_neighbors: int = 15, *, metric: str = "euclidean",
                 pass
     if configs is None:
         configs = [tile_code(bn, st, cb, ep, pr) for pr in (1, 0) for ep in (8, 4)
-                   for bn in (256, 128, 64) for st in (2, 3, 4, 6) for cb in (16, 32)]
+                   for bn in (256, 128, 64) for st in (2, 3, 4, 6) for cb in (16,)]
     table = []
     for code in configs:
         try:
