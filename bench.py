@@ -362,6 +362,7 @@ def run_ours(args):
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
                 "cpu_baseline": cpu, "fp32_form": fp32,
                 "stats": {"certified": int(stats[_lib.STAT_CERTIFIED]),
+                          "refined": int(stats[_lib.STAT_REFINED]),
                           "rescanned": int(stats[_lib.STAT_RESCANNED]),
                           "fp64_boundary_recomputes": int(stats[_lib.STAT_FP64_TIES]),
                           "conn_nnz": int(stats[_lib.STAT_CONN_NNZ])},

@@ -250,7 +250,8 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
     w.qs3 = c.take<QStat>(P.npacked);
     w.km3 = c.take<KeyMax>(1);
   }
-  if (P.prune) w.pr = carve_prune(c, P.npacked, P.nseg, P.d, P.ntiles, P.prune_words);
+  if (P.prune)
+    w.pr = carve_prune(c, P.npacked, P.nseg, P.d, P.ntiles, P.prune_words, P.n, P.kprime);
   return w;
 }
 
@@ -336,16 +337,17 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       stage_mark(st, 1);
       const uint32_t* mask = nullptr;
       int words = 0;
+      const NearInit init{w.pr.cand_val, w.cand_idx, w.pr.iperm, w.pr.excl};
       if (prune) {
         // near pass -> per-row radius -> outliers to the end of each sample -> operands of the
         // new order -> balls and the visit mask of every query tile
         MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp,
                               P.L.kmma, w.items, n_items, w.perm, nullptr, nullptr,
                               &w.ctl->tc_counter[2], w.ctl, P.kprime, w.cand_idx, w.cand_thr,
-                              P.kprime, st, nullptr, 0, true));
+                              P.kprime, st, nullptr, 0, true, false, nullptr, &init));
         stage_mark(st, 2);
         MSC_TRY(launch_prune_partition(Xu, P.d, w.seg, P.nseg, P.npacked, w.perm, w.cand_thr,
-                                       w.qs, w.km, P.prec, P.L.kmma, w.pr, st));
+                                       w.qs, w.km, P.prec, P.L.kmma, cfg.bn, w.pr, st));
         MSC_CUDA_TRY(cudaMemsetAsync(w.km, 0, sizeof(KeyMax), st));
         MSC_TRY(launch_pack_tc(P.prec, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
                                nullptr, nullptr, 0, w.Aop, w.Bop, w.qs, w.km, w.ctl, st));
@@ -360,7 +362,8 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
                             w.items, n_items, w.perm, nullptr, nullptr, &w.ctl->tc_counter[0],
                             w.ctl, P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask, words,
-                            false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr));
+                            false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr,
+                            prune ? &init : nullptr));
     }
   }
   stage_mark(st, 4);
@@ -380,10 +383,19 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                            w.qmap, &w.ctl->n_refine, P.n, w.A3, nullptr, nullptr, nullptr, w.ctl,
                            st));
     const TcConfig cfg3 = tc_default_config(PREC_BF16X3, P.d, P.kprime);
+    const uint32_t* mask3 = nullptr;
+    int words3 = 0;
+    if (prune && !cfg3.pair && cfg3.bn == PRUNE_BN) {
+      words3 = prune_mask_words(P.max_seg, cfg3.bn);
+      MSC_TRY(launch_refine_mask(w.items3, &w.ctl->n_items_refine, w.qmap, P.ntiles, w.seg,
+                                 P.nseg, cfg3.bn, words3, w.qs, w.km, w.qs3, w.km3, w.ctl,
+                                 P.prec, P.L.kmma, P.L3.kmma, P.d, w.pr, st));
+      mask3 = w.pr.mask3;
+    }
     MSC_TRY(launch_knn_tc(PREC_BF16X3, cfg3, w.A3, w.B3, P.n, P.npacked, P.L3.kp, P.L3.kmma,
                           w.items3, P.ntiles, w.perm, w.qmap, &w.ctl->n_items_refine,
                           &w.ctl->tc_counter[1], w.ctl,
-                          P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
+                          P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask3, words3));
     MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                           P.kprime, P.kprime, w.qs3, w.km3, PREC_BF16X3, P.L3.kmma, P.k, cosine,
                           knn_idx, knn_dist, w.fail_rows, w.ctl, w.qmap, &w.ctl->n_refine, P.n,

@@ -133,20 +133,31 @@ struct PruneWs {
   float *sc, *sr;     // two balls per 32-row block
   double* rsub;       // max R per 32-row block
   uint32_t* mask;     // visit bits per work item
+  uint32_t* mask3;    // visit bits per work item of the refine pass
   float* seed;        // per packed row (final layout): bound on its final k'-th value
+  float* cand_val;    // n × k' near-pass candidate values
+  int32_t* iperm;     // original row -> packed position (final layout)
+  int4* excl;         // per packed row (final layout): the key ranges the near pass scored
 };
 int prune_mask_words(int64_t max_seg, int bn);
-PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words);
-size_t prune_workspace_bytes(int64_t npacked, int nseg, int d, int64_t n_items, int words);
-// after the near pass: R per row, outliers to the end of each sample (perm is rewritten)
+PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words,
+                    int64_t n, int kprime);
+// after the near pass (key tiles of bn rows): R per row, outliers to the end of each sample
+// (perm is rewritten), the inverse permutation and every row's near-pass key ranges
 int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
                            int32_t* perm, const float* cand_thr, const QStat* qs,
-                           const KeyMax* km, int prec, int kmma, const PruneWs& w,
+                           const KeyMax* km, int prec, int kmma, int bn, const PruneWs& w,
                            cudaStream_t st);
 // balls of the final layout and the visit mask of every work item
 int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* perm,
                       const WorkItem* items, int64_t n_items, int bn, const Ctl* ctl, int prec,
                       const PruneWs& w, int words, cudaStream_t st);
+// visit masks of the refine pass's work items (from the main pass's masks)
+int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const int32_t* qmap,
+                       int64_t max_items, const SegDesc* seg, int nseg, int bn, int words,
+                       const QStat* qs, const KeyMax* km, const QStat* qs3, const KeyMax* km3,
+                       const Ctl* ctl, int prec, int kmma, int kmma3, int d, const PruneWs& w,
+                       cudaStream_t st);
 int prune_counters(unsigned long long* out);
 int prune_counters_clear();
 
@@ -154,6 +165,16 @@ int prune_counters_clear();
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
                     int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
                     int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
+
+// The near pass's candidates handed to the main pass: the near pass writes val (and the usual
+// candidate rows); the main pass loads them as every row's starting heap and never offers the
+// keys the near pass scored again (excl: two packed-position ranges per row).
+struct NearInit {
+  float* val;              // n × k' values
+  const int32_t* idx;      // n × k' original rows (the near pass's candidate rows)
+  const int32_t* iperm;    // original row -> packed position of the main pass
+  const int4* excl;        // per packed row of the main pass: [x, y) and [z, w)
+};
 
 // ---- knn_tc.cu ----
 // Work items are claimed dynamically by the persistent CTAs, in index order or (reverse) from the
@@ -181,7 +202,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask = nullptr, int mask_words = 0, bool near_only = false,
-                  bool reverse = false, const float* seed = nullptr);
+                  bool reverse = false, const float* seed = nullptr,
+                  const NearInit* init = nullptr);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

@@ -308,6 +308,13 @@ struct TcParams {
   int reverse;                  // claim the work items from the last one down
   const float* seed;            // per packed query row: bound on its final k'-th value, or null
   int prof_slot;                // counter block of this launch (near / main / refine)
+  float* cand_val;              // near pass: also write the values of the kept candidates
+  // main pass after a near pass: load every row's heap from the near pass's candidates (values,
+  // original rows -> packed positions through iperm) and never offer its keys again (excl)
+  const float* init_val;
+  const int32_t* init_idx;
+  const int32_t* iperm;
+  const int4* excl;
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -701,6 +708,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       const int qrow = w.qrow0 + int(rank) * BM;
       const int self = P.qmap ? (row < nq ? P.qmap[qrow + row] : -1) : qrow + row;
       sel.set_seed((P.seed && row < nq) ? P.seed[qrow + row] : F_INF);
+      if (P.init_val && row < nq) {
+        if (h == 0) sel.load(P.init_val, P.init_idx, P.iperm, P.perm[qrow + row], P.cand_stride);
+        const int4 ex = P.excl[qrow + row];
+        sel.ex_r0 = ex.x; sel.ex_r1 = ex.y; sel.ex_o0 = ex.z; sel.ex_o1 = ex.w;
+      }
       const int limit = w.key0 + w.nkeys;
       KeyTileWalk walk;
       walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
@@ -755,7 +767,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       if (NH == 1) {
         if (nvalid > 0)
           sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
-                     nvalid, P.kprime);
+                     nvalid, P.kprime, P.cand_val);
         else
           sel.flush();
       } else {
@@ -769,7 +781,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           sel.merge_from(smem + sp.sel_off + Sel::smem_bytes());
           if (nvalid > 0)
             sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
-                       nvalid, P.kprime);
+                       nvalid, P.kprime, P.cand_val);
         }
         ok = quarter_sync();                       // the partner's list is read; reuse it
         if (!ok) break;
@@ -994,7 +1006,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask, int mask_words, bool near_only, bool reverse,
-                  const float* seed) {
+                  const float* seed, const NearInit* init) {
   const int prof_slot = near_only ? 0 : (qmap ? 2 : 1);
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
@@ -1027,6 +1039,12 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.reverse = reverse ? 1 : 0;
   P.seed = seed;
   P.prof_slot = prof_slot;
+  P.cand_val = init && near_only ? init->val : nullptr;
+  const bool load = init && !near_only;
+  P.init_val = load ? init->val : nullptr;
+  P.init_idx = load ? init->idx : nullptr;
+  P.iperm = load ? init->iperm : nullptr;
+  P.excl = load ? init->excl : nullptr;
   if (cfg.pair && (mask || near_only)) {
     set_error("pruned scans run on single CTAs only");
     return MSC_ERR_INVALID_ARG;

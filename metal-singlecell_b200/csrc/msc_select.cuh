@@ -278,6 +278,9 @@ struct RowHeap {
   // heap's k'-th value, so nothing it drops can belong to the union's k' smallest.
   float* pub_own = nullptr;
   const float* pub_other = nullptr;
+  // columns never offered again: [ex_r0, ex_r1) and [ex_o0, ex_o1) (keys whose values an earlier
+  // pass already put into the heap it was loaded from)
+  int ex_r0 = 0, ex_r1 = 0, ex_o0 = 0, ex_o1 = 0;
   int n_hot = 0, n_compact = 0, n_append = 0;   // counters for the pipeline profile
 
   __device__ void bind(void* smem, int row_, int kprime) {
@@ -301,6 +304,27 @@ struct RowHeap {
   __device__ __forceinline__ void refresh() {
     thr_f = fminf(thr, seed);
     if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
+  }
+
+  // Load a heap written by finish() of an earlier pass (slot order is heap order): k' values and
+  // original rows per row, the rows mapped to packed positions through iperm.
+  __device__ void load(const float* __restrict__ vals, const int32_t* __restrict__ idx,
+                       const int32_t* __restrict__ iperm, int64_t orow, int stride) {
+    for (int s = 0; s < kp; ++s) {
+      const float v = vals[orow * stride + s];
+      const int32_t c = idx[orow * stride + s];
+      he[s * ROWS + row] = make_int2(__float_as_int(v), c >= 0 ? iperm[c] : -1);
+    }
+    thr = __int_as_float(he[row].x);
+    if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
+    refresh();
+  }
+
+  __device__ __forceinline__ static unsigned span_bits(int col0, int a, int b) {
+    const int lo = max(a - col0, 0), hi = min(b - col0, 32);
+    if (hi <= lo) return 0u;
+    const unsigned upto = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+    return upto & ~((1u << lo) - 1u);
   }
 
   // replace the root by (v, col) (v < root) and restore the heap: one 8-byte load per child and
@@ -377,6 +401,7 @@ struct RowHeap {
       if (ds >= 0 && ds < 32) m &= ~(1u << ds);
       const int dl = limit - col0;
       if (dl < 32) m &= dl <= 0 ? 0u : ((1u << dl) - 1u);
+      m &= ~(span_bits(col0, ex_r0, ex_r1) | span_bits(col0, ex_o0, ex_o1));
     }
     while (__any_sync(FULL, m != 0u)) {
       if (m) {
@@ -399,7 +424,7 @@ struct RowHeap {
   // through perm (see RowSelect::finish)
   __device__ void finish(int* out_idx, float* out_thr, int out_stride,
                          const int32_t* __restrict__ perm, const int32_t* __restrict__ qmap,
-                         int64_t first_row, int nvalid_rows, int kout) {
+                         int64_t first_row, int nvalid_rows, int kout, float* out_val = nullptr) {
     __syncwarp();
     const int lane = lane_id();
     const int row0 = row - lane;
@@ -409,8 +434,9 @@ struct RowHeap {
       const int64_t orow = perm[prow];
       const float sd = __shfl_sync(FULL, seed, r);
       for (int s = lane; s < kout; s += 32) {
-        const int c = he[s * ROWS + rr].y;
-        out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
+        const int2 e = he[s * ROWS + rr];
+        out_idx[orow * out_stride + s] = e.y >= 0 ? perm[e.y] : -1;
+        if (out_val) out_val[orow * out_stride + s] = __int_as_float(e.x);
       }
       if (lane == 0) out_thr[orow] = fminf(__int_as_float(he[rr].x), sd);
     }

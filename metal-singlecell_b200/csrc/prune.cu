@@ -110,9 +110,10 @@ __global__ void partition_kernel(const int32_t* __restrict__ perm, const int32_t
                                  const SegDesc* __restrict__ seg, int nseg,
                                  const int32_t* __restrict__ reg, const int64_t* __restrict__ S,
                                  const float* __restrict__ cand_thr, const QStat* __restrict__ qs,
-                                 const KeyMax* __restrict__ km, int prec, int kmma, int d,
+                                 const KeyMax* __restrict__ km, int prec, int kmma, int d, int bn,
                                  int32_t* __restrict__ perm2, int32_t* __restrict__ leaf2,
-                                 double* __restrict__ rpos2, float* __restrict__ seed2) {
+                                 double* __restrict__ rpos2, float* __restrict__ seed2,
+                                 int32_t* __restrict__ iperm, int4* __restrict__ excl) {
   for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
        p += int64_t(gridDim.x) * blockDim.x) {
     const SegDesc s = seg[find_seg(seg, nseg, p)];
@@ -138,6 +139,19 @@ __global__ void partition_kernel(const int32_t* __restrict__ perm, const int32_t
     leaf2[pos] = lf;
     rpos2[pos] = rpos[p];
     seed2[pos] = sd;
+    int4 ex = make_int4(0, 0, 0, 0);
+    if (i >= 0) {
+      iperm[i] = int32_t(pos);
+      // the near pass scored row i against key tile diag of its query tile (bn rows); those keys
+      // are a run of regular rows and a run of outliers in the new order
+      const int64_t qt = (p - s.poff) / QTILE;
+      const int64_t a = s.poff + (qt * QTILE / bn) * bn, b = min64(a + bn, s.poff + s.n);
+      const int64_t ra = S[a] - S[s.poff], rb = S[b] - S[s.poff];
+      const int64_t nreg = S[s.poff + s.n] - S[s.poff];
+      ex = make_int4(int(s.poff + ra), int(s.poff + rb), int(s.poff + nreg + (a - s.poff) - ra),
+                     int(s.poff + nreg + (b - s.poff) - rb));
+    }
+    excl[pos] = ex;
   }
 }
 
@@ -287,6 +301,7 @@ __device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru
 // the other side — with the (key tile, sub-ball) tests spread over the lanes; then, per key tile
 // left, the remaining sub-ball pairs, one pair per lane.
 constexpr int PLAN_WARPS = 4;
+constexpr int PLAN_WORDS = 8;     // mask words (256 key tiles) per warp task
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
 plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
             const Ctl* ctl, int prec, const float* __restrict__ qc, const float* __restrict__ qr,
@@ -305,7 +320,13 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
   const int64_t warps = int64_t(gridDim.x) * PLAN_WARPS;
   const int nv = 2 * max(1, bn / SUB);          // key sub-balls per key tile
   long long nvis = 0, ntot = 0, nl1 = 0, npt = 0, npr = 0;
-  for (int64_t it = int64_t(blockIdx.x) * PLAN_WARPS + wib; it < n_items; it += warps) {
+  // tasks = (query tile, block of PLAN_WORDS mask words): the level-2 work of a query tile varies
+  // widely, so whole tiles per warp would leave most SMs idle behind the slowest few
+  const int nblk = (words + PLAN_WORDS - 1) / PLAN_WORDS;
+  const int64_t ntasks = n_items * nblk;
+  for (int64_t task = int64_t(blockIdx.x) * PLAN_WARPS + wib; task < ntasks; task += warps) {
+    const int64_t it = task / nblk;
+    const int wblk = int(task - it * nblk);
     const WorkItem w = items[it];
     const int64_t qt = w.qrow0 / QTILE;          // 128-row tile of packed rows
     const int64_t sb0 = int64_t(w.qrow0) / SUB;  // its first 32-row block
@@ -321,7 +342,8 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
     const int diag = (w.qrow0 - w.key0) / bn;
     const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
     uint32_t* out = mask + it * int64_t(words);
-    for (int base = 0; base < words * 32; base += 32) {
+    const int wend = min(words, (wblk + 1) * PLAN_WORDS);
+    for (int base = wblk * PLAN_WORDS * 32; base < wend * 32; base += 32) {
       const int kt = base + lane;
       bool l1 = false;                           // not separated at level 1
       if (kt < nkt && (kt < lo || kt > hi)) {
@@ -377,7 +399,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
         nvis += __popc(bits);
       }
     }
-    ntot += nkt - (hi - lo + 1);
+    if (wblk == 0) ntot += nkt - (hi - lo + 1);
   }
   if (prof && lane == 0) {
     atomicAdd(&g_prune_tiles[0], (unsigned long long)nvis);
@@ -385,6 +407,66 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
     atomicAdd(&g_prune_tiles[2], (unsigned long long)nl1);
     atomicAdd(&g_prune_tiles[3], (unsigned long long)npt);
     atomicAdd(&g_prune_tiles[4], (unsigned long long)npr);
+  }
+}
+
+
+// Visit mask of every work item of the refine pass (the rows whose one-term certificate failed,
+// re-scanned with the three-term split).  A refine item holds up to 128 such rows from anywhere in
+// their sample; its mask is the union of its rows' query-tile masks and near tiles, minus the near
+// tiles its own walk visits first.  This stays exact for the refine values v3 if each row's
+// one-term error bound, in the unscaled space, covers the three-term one (eps1 >= f²·eps3): the
+// skipped keys have v > (thr + 3·eps1)/f², the near-pass keys (never skipped) v <= (thr + eps1)/f²,
+// so every skipped key's v3 lies above the refine threshold.  An item with a row where that fails
+// scans every key tile.
+__global__ void refine_mask_kernel(const WorkItem* __restrict__ items3,
+                                   const int32_t* __restrict__ n_items3,
+                                   const int32_t* __restrict__ qmap,
+                                   const SegDesc* __restrict__ seg, int nseg,
+                                   const uint32_t* __restrict__ mask, int words, int bn,
+                                   const QStat* __restrict__ qs, const KeyMax* __restrict__ km,
+                                   const QStat* __restrict__ qs3, const KeyMax* __restrict__ km3,
+                                   const Ctl* __restrict__ ctl, int prec, int kmma, int kmma3,
+                                   int d, uint32_t* __restrict__ mask3) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int nitems = *n_items3;
+  const double f = op_scale(prec, ctl);
+  const KeyMax K1 = *km, K3 = *km3;
+  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < nitems; r += warps) {
+    const WorkItem w = items3[r];
+    const int nkt = (w.nkeys + bn - 1) / bn;
+    const int diag = (qmap[w.qrow0] - w.key0) / bn;
+    const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
+    bool ok = true;
+    for (int j = lane; j < w.nq; j += 32) {
+      const int32_t p = qmap[w.qrow0 + j];
+      ok = ok && cert_eps(qs[p], K1, prec, kmma, d) >= f * f * cert_eps(qs3[p], K3, PREC_BF16X3, kmma3, d);
+    }
+    ok = __all_sync(FULL, ok);
+    uint32_t* out = mask3 + r * int64_t(words);
+    for (int wi = lane; wi < words; wi += 32) {
+      uint32_t acc = 0u;
+      if (!ok) {
+        acc = 0xffffffffu;
+      } else {
+        for (int j = 0; j < w.nq; ++j) {
+          const int32_t p = qmap[w.qrow0 + j];
+          const SegDesc sg = seg[find_seg(seg, nseg, p)];
+          const int64_t mi = sg.tile0 + (p - sg.poff) / QTILE;       // its query tile's item
+          acc |= mask[mi * words + wi];
+          const int dj = int(((p - sg.poff) / QTILE * QTILE) / bn);    // that tile's near range
+          const int l0 = max(0, dj - 2) - wi * 32, h0 = min(nkt - 1, dj + 2) - wi * 32;
+          for (int b = max(0, l0); b <= min(31, h0); ++b) acc |= 1u << b;
+        }
+      }
+      // never beyond the sample, never the item's own near tiles (its walk visits them first)
+      for (int b = 0; b < 32; ++b) {
+        const int kt = wi * 32 + b;
+        if (kt >= nkt || (kt >= lo && kt <= hi)) acc &= ~(1u << b);
+      }
+      out[wi] = acc;
+    }
   }
 }
 
@@ -398,13 +480,8 @@ int prune_mask_words(int64_t max_seg, int bn) {
   return int(ceil_div(ceil_div(max_seg, bn), 32));
 }
 
-size_t prune_workspace_bytes(int64_t npacked, int nseg, int d, int64_t n_items, int words) {
-  Carver c(nullptr);
-  carve_prune(c, npacked, nseg, d, n_items, words);
-  return c.bytes();
-}
-
-PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words) {
+PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words,
+                    int64_t n, int kprime) {
   PruneWs w{};
   w.leaf = c.take<int32_t>(npacked);
   w.leaf2 = c.take<int32_t>(npacked);
@@ -425,13 +502,17 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.sr = c.take<float>(2 * ns);
   w.rsub = c.take<double>(ns);
   w.mask = c.take<uint32_t>(size_t(n_items) * words);
+  w.mask3 = c.take<uint32_t>(size_t(n_items) * words);
+  w.cand_val = c.take<float>(size_t(n) * kprime);
+  w.iperm = c.take<int32_t>(n);
+  w.excl = c.take<int4>(npacked);
   w.seed = c.take<float>(npacked);
   return w;
 }
 
 int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked,
                            int32_t* perm, const float* cand_thr, const QStat* qs,
-                           const KeyMax* km, int prec, int kmma, const PruneWs& w,
+                           const KeyMax* km, int prec, int kmma, int bn, const PruneWs& w,
                            cudaStream_t st) {
   (void)X;
   const int grid = grid_for(npacked);
@@ -443,8 +524,8 @@ int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, 
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl_i32(w.reg, npacked, w.S, w.scan_scratch, st));
   partition_kernel<<<grid, PR_T, 0, st>>>(perm, w.leaf, w.rpos, npacked, seg, nseg, w.reg, w.S,
-                                          cand_thr, qs, km, prec, kmma, d, w.perm2, w.leaf2,
-                                          w.rpos2, w.seed);
+                                          cand_thr, qs, km, prec, kmma, d, bn, w.perm2,
+                                          w.leaf2, w.rpos2, w.seed, w.iperm, w.excl);
   MSC_LAUNCH_CHECK();
   MSC_CUDA_TRY(cudaMemcpyAsync(perm, w.perm2, sizeof(int32_t) * npacked,
                                cudaMemcpyDeviceToDevice, st));
@@ -479,11 +560,25 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
   sub_ball_kernel<<<sgrid, PR_T, 0, st>>>(X, d, dp, perm, w.leaf2, w.rpos2, ns, w.sc, w.sr, w.rsub);
   MSC_LAUNCH_CHECK();
   const size_t smem = size_t(PLAN_WARPS) * 9 * dp * sizeof(float);
-  const int pgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, PLAN_WARPS),
-                                                              int64_t(num_sms()) * 16)));
+  const int64_t ntasks = n_items * ceil_div(words, PLAN_WORDS);
+  const int pgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(ntasks, PLAN_WARPS),
+                                                              int64_t(num_sms()) * 32)));
   plan_kernel<<<pgrid, PLAN_WARPS * 32, smem, st>>>(items, n_items, bn, d, dp, ctl, prec, w.qc,
                                                     w.qr, w.kc, w.kr, w.sc, w.sr, w.rsub, words,
                                                     w.mask, profiling_enabled() ? 1 : 0);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const int32_t* qmap,
+                       int64_t max_items, const SegDesc* seg, int nseg, int bn, int words,
+                       const QStat* qs, const KeyMax* km, const QStat* qs3, const KeyMax* km3,
+                       const Ctl* ctl, int prec, int kmma, int kmma3, int d, const PruneWs& w,
+                       cudaStream_t st) {
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_items, 8),
+                                                             int64_t(num_sms()) * 8)));
+  refine_mask_kernel<<<grid, PR_T, 0, st>>>(items3, n_items3, qmap, seg, nseg, w.mask, words, bn,
+                                            qs, km, qs3, km3, ctl, prec, kmma, kmma3, d, w.mask3);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
