@@ -276,7 +276,21 @@ def run_ours(args):
 
     pk, pk_kind = peaks()
     cand_ms = stages.get("candidates")
-    alg_flop = 2.0 * d * float(n) * float(n)
+    # Work of the main candidate launch: the (128-row query tile, 256-key tile) pairs it computes
+    # -- every query tile's near tiles (its own key tile and two either side) plus the far tiles
+    # the pruning plan kept -- each 2·d·128·256 FLOP (d unpadded).  Without pruning every pair of
+    # the n×n matrix is computed.
+    dense_flop = 2.0 * d * float(n) * float(n)
+    if cnt[11]:
+        nkt = -(-n // 256)
+        q = np.arange(-(-n // 128))
+        diag = (128 * q) // 256
+        near_tiles = int((np.minimum(nkt - 1, diag + 2) - np.maximum(0, diag - 2) + 1).sum())
+        tile_pairs = near_tiles + int(cnt[10])
+        alg_flop = min(dense_flop, 2.0 * d * 128.0 * 256.0 * tile_pairs)
+    else:
+        tile_pairs = None
+        alg_flop = dense_flop
     achieved = alg_flop / (cand_ms / 1000.0) / 1e12 if cand_ms else None
     peak = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops")
     traffic = None
@@ -290,6 +304,9 @@ def run_ours(args):
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "kernel": "knn_tc_kernel" if args.precision != "fp32" else "knn_fp32_kernel",
                 "algorithmic_flop_per_launch": alg_flop, "kernel_ms": cand_ms,
+                "tile_pairs_computed": tile_pairs,
+                "dense_equivalent_tflops": (dense_flop / (cand_ms / 1000.0) / 1e12)
+                                           if cand_ms else None,
                 "peak_kind": f"{pk_kind} bf16 sustained (kernel timed inside a full step)",
                 "stage_ms": stages, "pipeline_cycles_per_cta": pipeline, "pruning": pruning}
 

@@ -374,8 +374,11 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                         P.refine ? w.flags : nullptr, st));
   if (P.refine) {
     // the rows the one-term candidates could not certify, again with the three-term split
+    // with pruning, a small refine set is split over key ranges (prune.cu)
+    const bool split = prune;
     MSC_TRY(launch_refine_plan(w.flags, P.npacked, w.seg, P.nseg, w.qmap, w.items3, w.S,
-                               w.scan_scratch, w.ctl, st));
+                               w.scan_scratch, w.ctl, split ? REFINE_SPLIT : 1,
+                               split ? w.pr.max_split_items : 0, st));
     MSC_CUDA_TRY(cudaMemsetAsync(w.km3, 0, sizeof(KeyMax), st));
     MSC_TRY(launch_pack_tc(PREC_BF16X3, Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.npacked,
                            nullptr, nullptr, 0, nullptr, w.B3, w.qs3, w.km3, w.ctl, st));
@@ -392,10 +395,19 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                                  P.prec, P.L.kmma, P.L3.kmma, P.d, w.pr, st));
       mask3 = w.pr.mask3;
     }
+    const RefineSplit rs{&w.ctl->refine_split, split ? w.pr.part : nullptr,
+                         split ? w.pr.part_thr : nullptr};
+    const int64_t max_work = split ? std::max<int64_t>(P.ntiles,
+                                                       int64_t(w.pr.max_split_items) * REFINE_SPLIT)
+                                   : P.ntiles;
     MSC_TRY(launch_knn_tc(PREC_BF16X3, cfg3, w.A3, w.B3, P.n, P.npacked, P.L3.kp, P.L3.kmma,
-                          w.items3, P.ntiles, w.perm, w.qmap, &w.ctl->n_items_refine,
-                          &w.ctl->tc_counter[1], w.ctl,
-                          P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask3, words3));
+                          w.items3, max_work, w.perm, w.qmap, &w.ctl->n_items_refine_eff,
+                          &w.ctl->tc_counter[1], w.ctl, P.kprime, w.cand_idx, w.cand_thr,
+                          P.kprime, st, mask3, words3, false, false, nullptr, nullptr,
+                          split ? &rs : nullptr));
+    if (split)
+      MSC_TRY(launch_refine_merge(w.items3, &w.ctl->n_items_refine, w.ctl, w.qmap, w.perm, P.n,
+                                  w.pr, P.kprime, w.cand_idx, w.cand_thr, st));
     MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                           P.kprime, P.kprime, w.qs3, w.km3, PREC_BF16X3, P.L3.kmma, P.k, cosine,
                           knn_idx, knn_dist, w.fail_rows, w.ctl, w.qmap, &w.ctl->n_refine, P.n,

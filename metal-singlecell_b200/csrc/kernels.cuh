@@ -138,6 +138,9 @@ struct PruneWs {
   float* cand_val;    // n × k' near-pass candidate values
   int32_t* iperm;     // original row -> packed position (final layout)
   int4* excl;         // per packed row (final layout): the key ranges the near pass scored
+  int2* part;         // refine split: k' (value, row) per row per work item
+  float* part_thr;
+  int max_split_items;
 };
 int prune_mask_words(int64_t max_seg, int bn);
 PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words,
@@ -158,6 +161,12 @@ int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const in
                        const QStat* qs, const KeyMax* km, const QStat* qs3, const KeyMax* km3,
                        const Ctl* ctl, int prec, int kmma, int kmma3, int d, const PruneWs& w,
                        cudaStream_t st);
+// after a split refine pass: every refine row's k' smallest of its work items' heaps
+int launch_refine_merge(const WorkItem* items3, const int32_t* n_items3, const Ctl* ctl,
+                        const int32_t* qmap, const int32_t* perm, int64_t max_rows,
+                        const PruneWs& w, int kprime, int32_t* cand_idx, float* cand_thr,
+                        cudaStream_t st);
+constexpr int REFINE_SPLIT = 8;
 int prune_counters(unsigned long long* out);
 int prune_counters_clear();
 
@@ -174,6 +183,14 @@ struct NearInit {
   const int32_t* idx;      // n × k' original rows (the near pass's candidate rows)
   const int32_t* iperm;    // original row -> packed position of the main pass
   const int4* excl;        // per packed row of the main pass: [x, y) and [z, w)
+};
+
+// The refine pass split over key ranges (prune.cu): split_dev (device int) work items per refine
+// item; each writes its rows' heaps to part (k' entries per row) and part_thr, merged afterwards.
+struct RefineSplit {
+  const int32_t* split_dev;
+  int2* part;
+  float* part_thr;
 };
 
 // ---- knn_tc.cu ----
@@ -203,7 +220,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask = nullptr, int mask_words = 0, bool near_only = false,
                   bool reverse = false, const float* seed = nullptr,
-                  const NearInit* init = nullptr);
+                  const NearInit* init = nullptr, const RefineSplit* split = nullptr);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
@@ -215,9 +232,11 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   int32_t* fail_flags, cudaStream_t st);
 // refine plan: compact the flagged packed rows (sorted) into qmap, count them (ctl->n_refine)
 // and cut them into per-sample query tiles (items, ctl->n_items_refine); S: npacked+1 int64
+// split > 1: when there are at most max_split_items refine items, each becomes `split` work
+// items over key ranges (ctl->refine_split, ctl->n_items_refine_eff)
 int launch_refine_plan(const int32_t* flags, int64_t npacked, const SegDesc* seg, int nseg,
                        int32_t* qmap, WorkItem* items, int64_t* S, int64_t* scan_scratch,
-                       Ctl* ctl, cudaStream_t st);
+                       Ctl* ctl, int split, int max_split_items, cudaStream_t st);
 int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
                          cudaStream_t st);
 int launch_fp64_scan(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

@@ -308,6 +308,11 @@ struct TcParams {
   int reverse;                  // claim the work items from the last one down
   const float* seed;            // per packed query row: bound on its final k'-th value, or null
   int prof_slot;                // counter block of this launch (near / main / refine)
+  // refine pass split over key ranges: *split_dev work items per refine item (1: no split), each
+  // writing its rows' heaps to part / part_thr for refine_merge
+  const int32_t* split_dev;
+  int2* part;
+  float* part_thr;
   float* cand_val;              // near pass: also write the values of the kept candidates
   // main pass after a near pass: load every row's heap from the near pass's candidates (values,
   // original rows -> packed positions through iperm) and never offer its keys again (excl)
@@ -347,6 +352,8 @@ struct KeyTileWalk {
   int w, nw;
   uint32_t cur, nxt;
   bool near_only;
+  int khi = 1 << 30;     // range walks stop before this tile
+  bool range = false;
   __device__ __forceinline__ void init(const WorkItem& item, int qref, int bn,
                                        const uint32_t* m, int words, bool near) {
     nkt = (item.nkeys + bn - 1) / bn;
@@ -364,11 +371,27 @@ struct KeyTileWalk {
     cur = m ? m[0] : 0u;
     nxt = (m && words > 1) ? m[1] : 0u;     // one word ahead: its load overlaps the near tiles
   }
+  // A range walk (the refine pass): no near phase, only the tiles [lo, hi), in plain order or
+  // as the mask's bits.
+  __device__ __forceinline__ void set_range(int lo, int hi) {
+    range = true;
+    np = 0;
+    j = lo;
+    khi = hi;
+    if (mask) {
+      w = lo >> 5;
+      cur = w < nw ? (mask[w] & (~0u << (lo & 31))) : 0u;
+      nxt = w + 1 < nw ? mask[w + 1] : 0u;
+    }
+  }
   // the next key tile, or -1
   __device__ __forceinline__ int next() {
     if (j < np) return key_tile_at(j++, diag, nkt);
     if (near_only) return -1;
-    if (!mask) return j < nkt ? key_tile_at(j++, diag, nkt) : -1;
+    if (!mask) {
+      if (range) return j < khi ? j++ : -1;
+      return j < nkt ? key_tile_at(j++, diag, nkt) : -1;
+    }
     while (cur == 0u) {
       if (++w >= nw) return -1;
       cur = nxt;
@@ -376,7 +399,8 @@ struct KeyTileWalk {
     }
     const int b = __ffs(cur) - 1;
     cur &= cur - 1u;
-    return w * 32 + b;
+    const int kt = w * 32 + b;
+    return kt < khi ? kt : -1;
   }
 };
 
@@ -514,6 +538,20 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     it = v;
     return true;
   };
+  // Refine items split over key ranges: work item it = (refine item it / S, range it % S).
+  const int S = P.split_dev ? max(1, *P.split_dev) : 1;
+  auto item_of = [&](int it) { return S > 1 ? it / S : it; };
+  auto walk_init = [&](KeyTileWalk& walk, const WorkItem& w, int it) {
+    const int r = item_of(it);
+    walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
+              P.mask ? P.mask + int64_t(r) * P.mask_words : nullptr, P.mask_words,
+              P.near_only != 0);
+    if (P.qmap) {
+      const int sidx = S > 1 ? it % S : 0;
+      const int chunk = (walk.nkt + S - 1) / S;
+      walk.set_range(sidx * chunk, min(walk.nkt, (sidx + 1) * chunk));
+    }
+  };
   // consumers: the next published item, by one thread or by a whole warp (warp_wide)
   auto receive = [&](int& it, bool warp_wide) -> bool {
     if (PAIR) {
@@ -543,7 +581,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         int it;
         if (!claim(it)) { ok = false; break; }
         if (it < 0) break;
-        const WorkItem w = items[it];
+        const WorkItem w = items[item_of(it)];
         ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
         if (!ok) break;
         mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
@@ -552,9 +590,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                       w.qrow0 + int(rank) * BM);
         if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
         KeyTileWalk walk;
-        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
-                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
-                  P.near_only != 0);
+        walk_init(walk, w, it);
         for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
             const long long tw = P.prof ? clock64() : 0;
@@ -588,15 +624,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       uint32_t sphase = 0, aphase = 0;
       bool ok = true;
       for (int it = unit; it < n_items && ok; it += nunits) {
-        const WorkItem w = items[it];
+        const WorkItem w = items[item_of(it)];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (!ok) break;
         mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
         if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
         KeyTileWalk walk;
-        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
-                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
-                  P.near_only != 0);
+        walk_init(walk, w, it);
         for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           for (int kb = 0; kb < P.kb; ++kb) {
             ok = mbar_wait(&b_full[stage], sphase, abort_flag);
@@ -618,15 +652,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         int it;
         if (!receive(it, false)) { ok = false; break; }
         if (it < 0) break;
-        const WorkItem w = items[it];
+        const WorkItem w = items[item_of(it)];
         ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
         if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
         if (!ok) break;
         const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
         KeyTileWalk walk;
-        walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
-                  P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
-                  P.near_only != 0);
+        walk_init(walk, w, it);
         for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
           const long long t2 = P.prof ? clock64() : 0;
           ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
@@ -701,7 +733,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       int it;
       if (!receive(it, true)) { ok = false; break; }
       if (it < 0) break;
-      const WorkItem w = items[it];
+      const WorkItem w = items[item_of(it)];
       const long long tl = P.prof ? clock64() : 0;
       // neighbour ids are packed positions here; finish() maps them to original rows
       const int nq = min(BM, w.nq - int(rank) * BM);   // this CTA's valid query rows (may be <= 0)
@@ -715,9 +747,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       }
       const int limit = w.key0 + w.nkeys;
       KeyTileWalk walk;
-      walk.init(w, P.qmap ? P.qmap[w.qrow0] : w.qrow0, P.bn,
-                P.mask ? P.mask + int64_t(it) * P.mask_words : nullptr, P.mask_words,
-                P.near_only != 0);
+      walk_init(walk, w, it);
       for (int kt = walk.next(); kt >= 0; kt = walk.next()) {
         const long long te = P.prof ? clock64() : 0;
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
@@ -764,10 +794,17 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       if (!ok) break;
       const int wrow0 = q * 32;
       const int nvalid = min(32, nq - wrow0);
-      if (NH == 1) {
-        if (nvalid > 0)
+      auto write_out = [&]() {
+        if (S > 1)
+          sel.finish_partial(P.part, P.part_thr, int64_t(it) * BM + wrow0, P.perm, nvalid,
+                             P.kprime);
+        else
           sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
                      nvalid, P.kprime, P.cand_val);
+      };
+      if (NH == 1) {
+        if (nvalid > 0)
+          write_out();
         else
           sel.flush();
       } else {
@@ -779,9 +816,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         if (!ok) break;
         if (h == 0) {
           sel.merge_from(smem + sp.sel_off + Sel::smem_bytes());
-          if (nvalid > 0)
-            sel.finish(cand_idx, cand_thr, P.cand_stride, P.perm, P.qmap, int64_t(qrow) + wrow0,
-                       nvalid, P.kprime, P.cand_val);
+          if (nvalid > 0) write_out();
         }
         ok = quarter_sync();                       // the partner's list is read; reuse it
         if (!ok) break;
@@ -1006,7 +1041,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask, int mask_words, bool near_only, bool reverse,
-                  const float* seed, const NearInit* init) {
+                  const float* seed, const NearInit* init, const RefineSplit* split) {
   const int prof_slot = near_only ? 0 : (qmap ? 2 : 1);
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
@@ -1039,6 +1074,9 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.reverse = reverse ? 1 : 0;
   P.seed = seed;
   P.prof_slot = prof_slot;
+  P.split_dev = split ? split->split_dev : nullptr;
+  P.part = split ? split->part : nullptr;
+  P.part_thr = split ? split->part_thr : nullptr;
   P.cand_val = init && near_only ? init->val : nullptr;
   const bool load = init && !near_only;
   P.init_val = load ? init->val : nullptr;

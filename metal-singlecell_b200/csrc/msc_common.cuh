@@ -118,6 +118,9 @@ struct Ctl {
   int32_t n_refine;         // rows compacted for the BF16x3 refine pass
   int32_t n_items_refine;   // query tiles of the refine pass
   int32_t tc_counter[3];    // item counters of the tensor-core launches (main, refine, near)
+  int32_t refine_split;     // work items per refine item (key ranges), 1 = not split
+  int32_t n_items_refine_eff;   // n_items_refine × refine_split
+  int32_t pad2[3];
 };
 
 // ------------------------------------------------------------------------------------------------

@@ -257,7 +257,8 @@ struct RowSelect {
 // (the re-rank sorts the candidates itself), so the heap is written out as it stands.
 //
 // Shared memory (slot-major, so the 32 rows of a warp hit 32 banks whatever slot each lane is at):
-//   hv/hi[KH][ROWS]   heap per row: max of (value) at slot 0; +inf / -1 while not full
+//   he[KH][ROWS]   binary max-heap per row of (value, column): root at slot 0; +inf / -1 while
+//                  not full
 template <int KH, int ROWS>
 struct RowHeap {
   static_assert(KH == 32 || KH == 48 || KH == 64, "heap of 32, 48 or 64");
@@ -328,7 +329,7 @@ struct RowHeap {
   }
 
   // replace the root by (v, col) (v < root) and restore the heap: one 8-byte load per child and
-  // one 8-byte store per level
+  // one 8-byte store per level (a new value just below the root usually stops within two levels)
   __device__ __forceinline__ void insert(float v, int col) {
     ++n_append;
     int2* H = he + row;
@@ -418,6 +419,26 @@ struct RowHeap {
   }
 
   __device__ void flush() {}
+
+  // warp-collective: the first nvalid_rows rows of the warp into part (k' (value, original row)
+  // per row, rows at part_row0 + r) and part_thr (min(root, seed)), for a later merge
+  __device__ void finish_partial(int2* part, float* part_thr, int64_t part_row0,
+                                 const int32_t* __restrict__ perm, int nvalid_rows, int kout) {
+    __syncwarp();
+    const int lane = lane_id();
+    const int row0 = row - lane;
+    for (int r = 0; r < nvalid_rows; ++r) {
+      const int rr = row0 + r;
+      const float sd = __shfl_sync(FULL, seed, r);
+      int2* out = part + (part_row0 + r) * kout;
+      for (int s = lane; s < kout; s += 32) {
+        const int2 e = he[s * ROWS + rr];
+        out[s] = make_int2(e.x, e.y >= 0 ? perm[e.y] : -1);
+      }
+      if (lane == 0) part_thr[part_row0 + r] = fminf(__int_as_float(he[rr].x), sd);
+    }
+    __syncwarp();
+  }
 
   // warp-collective: write the k' kept columns (heap order) and the threshold min(root, seed) of
   // the warp's first `nvalid_rows` rows; columns are packed positions mapped to original rows

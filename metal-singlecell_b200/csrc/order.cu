@@ -214,13 +214,31 @@ __global__ void side_sum_kernel(const float* __restrict__ X, int d, int64_t npac
       }
       c0 = 0; c1 = 0;
     };
-    for (int64_t p = p0; p < p1; ++p) {
-      const int st = ns[p];
-      if (ne[p] - st <= leaf) continue;      // warp-uniform
-      const int64_t id = S[st];
+    // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
+    // only loads row data (independent from position to position)
+    int32_t idh[2], rowh[2], sdh[2];
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+      const int64_t p = p0 + 32 * hh + lane;
+      idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
+      if (p < p1) {
+        const int st = ns[p];
+        if (ne[p] - st > leaf) {
+          idh[hh] = int32_t(S[st]);
+          rowh[hh] = perm[p];
+          sdh[hh] = side[p];
+        }
+      }
+    }
+#pragma unroll 4
+    for (int jj = 0; jj < SUM_RUN; ++jj) {
+      const int hh = jj >> 5;
+      const int32_t id = __shfl_sync(FULL, hh ? idh[1] : idh[0], jj & 31);
+      if (id < 0) continue;                  // warp-uniform
+      const int32_t rw = __shfl_sync(FULL, hh ? rowh[1] : rowh[0], jj & 31);
+      const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
       if (id != cur) { flush(); cur = id; }
-      const float* x = X + int64_t(perm[p]) * d;
-      const bool one = side[p] != 0;
+      const float* x = X + int64_t(rw) * d;
       for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
         if (t < d) {

@@ -413,8 +413,8 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
 
 // Visit mask of every work item of the refine pass (the rows whose one-term certificate failed,
 // re-scanned with the three-term split).  A refine item holds up to 128 such rows from anywhere in
-// their sample; its mask is the union of its rows' query-tile masks and near tiles, minus the near
-// tiles its own walk visits first.  This stays exact for the refine values v3 if each row's
+// their sample; its mask is the union of its rows' query-tile masks and near tiles.  This stays
+// exact for the refine values v3 if each row's
 // one-term error bound, in the unscaled space, covers the three-term one (eps1 >= f²·eps3): the
 // skipped keys have v > (thr + 3·eps1)/f², the near-pass keys (never skipped) v <= (thr + eps1)/f²,
 // so every skipped key's v3 lies above the refine threshold.  An item with a row where that fails
@@ -436,8 +436,6 @@ __global__ void refine_mask_kernel(const WorkItem* __restrict__ items3,
   for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < nitems; r += warps) {
     const WorkItem w = items3[r];
     const int nkt = (w.nkeys + bn - 1) / bn;
-    const int diag = (qmap[w.qrow0] - w.key0) / bn;
-    const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
     bool ok = true;
     for (int j = lane; j < w.nq; j += 32) {
       const int32_t p = qmap[w.qrow0 + j];
@@ -460,13 +458,79 @@ __global__ void refine_mask_kernel(const WorkItem* __restrict__ items3,
           for (int b = max(0, l0); b <= min(31, h0); ++b) acc |= 1u << b;
         }
       }
-      // never beyond the sample, never the item's own near tiles (its walk visits them first)
+      // never beyond the sample (refine walks have no near phase: the item's own near tiles
+      // stay in the mask)
       for (int b = 0; b < 32; ++b) {
         const int kt = wi * 32 + b;
-        if (kt >= nkt || (kt >= lo && kt <= hi)) acc &= ~(1u << b);
+        if (kt >= nkt) acc &= ~(1u << b);
       }
       out[wi] = acc;
     }
+  }
+}
+
+// Merge of a split refine pass: warp per refine row; the S·k' entries of its S work items, the k'
+// smallest kept (ties: lower lane, then lower slot).  The threshold is the k'-th smallest: each
+// work item's heap holds k' values at or below its own root, so the merged k'-th value is at most
+// every root, and every key a work item dropped is at least its root.
+__global__ void refine_merge_kernel(const WorkItem* __restrict__ items3,
+                                    const int32_t* __restrict__ n_items3,
+                                    const Ctl* __restrict__ ctl, const int32_t* __restrict__ qmap,
+                                    const int32_t* __restrict__ perm,
+                                    const int2* __restrict__ part,
+                                    const float* __restrict__ part_thr, int kprime,
+                                    int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
+  const int S = ctl->refine_split;
+  if (S <= 1) return;
+  const int lane = lane_id();
+  const int nitems = *n_items3;
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int per = (S * kprime + 31) / 32;              // entries per lane (<= 16)
+  for (int64_t x = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+       x < int64_t(nitems) * QTILE; x += warps) {
+    const int r = int(x / QTILE), j = int(x % QTILE);
+    const WorkItem w = items3[r];
+    if (j >= w.nq) continue;                          // warp-uniform
+    float v[16];
+    int id[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      v[t] = F_INF;
+      id[t] = -1;
+      const int e = lane + 32 * t;
+      if (t < per && e < S * kprime) {
+        const int s = e / kprime, slot = e - s * kprime;
+        const int2 pe = part[((int64_t(r) * S + s) * QTILE + j) * kprime + slot];
+        if (pe.y >= 0) { v[t] = __int_as_float(pe.x); id[t] = pe.y; }
+      }
+    }
+    const int64_t orow = perm[qmap[w.qrow0 + j]];
+    float kth = F_INF;
+    for (int o = 0; o < kprime; ++o) {
+      float bv = F_INF;
+      int bt = 16;
+#pragma unroll
+      for (int t = 0; t < 16; ++t)
+        if (v[t] < bv) { bv = v[t]; bt = t; }
+      // warp argmin of (value, lane)
+      float mv = bv;
+      int ml = lane;
+      for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(FULL, mv, off);
+        const int ol = __shfl_xor_sync(FULL, ml, off);
+        if (ov < mv || (ov == mv && ol < ml)) { mv = ov; ml = ol; }
+      }
+      int out = -1;
+      if (lane == ml && bt < 16) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+          if (t == bt) { out = id[t]; v[t] = F_INF; }
+      }
+      out = __shfl_sync(FULL, out, ml);
+      if (lane == 0) cand_idx[orow * kprime + o] = mv < F_INF ? out : -1;
+      kth = mv;
+    }
+    if (lane == 0) cand_thr[orow] = kth;
   }
 }
 
@@ -506,6 +570,10 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.cand_val = c.take<float>(size_t(n) * kprime);
   w.iperm = c.take<int32_t>(n);
   w.excl = c.take<int4>(npacked);
+  w.max_split_items = int(std::min<int64_t>(256, n_items));
+  const int64_t prow = int64_t(w.max_split_items) * REFINE_SPLIT * QTILE;
+  w.part = c.take<int2>(size_t(prow) * kprime);
+  w.part_thr = c.take<float>(prow);
   w.seed = c.take<float>(npacked);
   return w;
 }
@@ -579,6 +647,19 @@ int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const in
                                                              int64_t(num_sms()) * 8)));
   refine_mask_kernel<<<grid, PR_T, 0, st>>>(items3, n_items3, qmap, seg, nseg, w.mask, words, bn,
                                             qs, km, qs3, km3, ctl, prec, kmma, kmma3, d, w.mask3);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_refine_merge(const WorkItem* items3, const int32_t* n_items3, const Ctl* ctl,
+                        const int32_t* qmap, const int32_t* perm, int64_t max_rows,
+                        const PruneWs& w, int kprime, int32_t* cand_idx, float* cand_thr,
+                        cudaStream_t st) {
+  const int64_t rows = std::min<int64_t>(max_rows, int64_t(w.max_split_items) * QTILE);
+  const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(rows, 8),
+                                                             int64_t(num_sms()) * 8)));
+  refine_merge_kernel<<<grid, PR_T, 0, st>>>(items3, n_items3, ctl, qmap, perm, w.part,
+                                             w.part_thr, kprime, cand_idx, cand_thr);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }

@@ -302,7 +302,7 @@ __global__ void compact_flags_kernel(const int32_t* __restrict__ flags,
 // short and the tile count is written once)
 __global__ void refine_items_kernel(const SegDesc* __restrict__ seg, int nseg,
                                     const int64_t* __restrict__ S, WorkItem* __restrict__ items,
-                                    Ctl* __restrict__ ctl) {
+                                    Ctl* __restrict__ ctl, int split, int max_split_items) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int32_t n = 0;
   for (int s = 0; s < nseg; ++s) {
@@ -320,6 +320,10 @@ __global__ void refine_items_kernel(const SegDesc* __restrict__ seg, int nseg,
     }
   }
   ctl->n_items_refine = n;
+  // few refine items (the usual case) would leave most SMs idle: split each over key ranges
+  const int sp = (split > 1 && n <= max_split_items) ? split : 1;
+  ctl->refine_split = sp;
+  ctl->n_items_refine_eff = n * sp;
 }
 
 }  // namespace
@@ -354,12 +358,12 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
 
 int launch_refine_plan(const int32_t* flags, int64_t npacked, const SegDesc* seg, int nseg,
                        int32_t* qmap, WorkItem* items, int64_t* S, int64_t* scan_scratch,
-                       Ctl* ctl, cudaStream_t st) {
+                       Ctl* ctl, int split, int max_split_items, cudaStream_t st) {
   MSC_TRY(scan_excl_i32(flags, npacked, S, scan_scratch, st));
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
   compact_flags_kernel<<<std::max(blocks, 1), 256, 0, st>>>(flags, S, npacked, qmap, ctl);
   MSC_LAUNCH_CHECK();
-  refine_items_kernel<<<1, 32, 0, st>>>(seg, nseg, S, items, ctl);
+  refine_items_kernel<<<1, 32, 0, st>>>(seg, nseg, S, items, ctl, split, max_split_items);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
