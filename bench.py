@@ -266,7 +266,9 @@ def run_ours(args):
                 "epilogue_wait_accumulator": c[3] / ctas / nepi,
                 "epilogue_loop": c[4] / ctas / nepi, "kernel": c[5] / ctas,
                 "hot_chunks_per_warp": c[6] / ctas / nepi,
-                "insertions_per_row": c[8] / max(n, 1), "ctas": c[9], "epilogue_warps": nepi}
+                "insertions_per_row": c[8] / max(n, 1), "ctas": c[9], "epilogue_warps": nepi,
+                "insert_rounds_per_warp": c[11] / ctas / nepi,
+                "hot_path_cycles_per_warp": c[12] / ctas / nepi}
     pipeline = {"near_pass": pipe(16), "main": pipe(32), "refine": pipe(48)}
     # key tiles beyond the near ones: kept by the pruning plan / all of them
     pruning = {"far_tiles_visited": int(cnt[10]), "far_tiles_total": int(cnt[11]),

@@ -360,8 +360,8 @@ struct KeyTileWalk {
     diag = (qref - item.key0) / bn;
     const int lo = max(0, diag - NEAR_SIDE), hi = min(nkt - 1, diag + NEAR_SIDE);
     // the near pass only needs an upper bound on each row's k'-th value: the query tile's own
-    // key tile gives one at a fifth of the cost of all near tiles (its lists fill from +inf, so
-    // nearly every value is inserted)
+    // key tile gives one (measured: all five near tiles cost more in the near pass than they
+    // save in the main scan)
     np = near ? 1 : hi - lo + 1;
     j = 0;
     near_only = near;
@@ -424,7 +424,7 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
   p.a_off = 0;
   p.b_off = p.a_off + size_t(na) * kb * BM * 128;
   p.sel_off = p.b_off + size_t(stages) * brows * 128;
-  p.pub_off = p.sel_off + size_t(nh) * RowHeap<KH, BM>::smem_bytes();
+  p.pub_off = p.sel_off + size_t(nh) * RowTopK<KH, BM>::smem_bytes();
   p.bar_off = p.pub_off + (nh > 1 ? size_t(2) * BM * sizeof(float) : 0);
   p.total = p.bar_off + 512 + 1024;          // barriers + slack for 1024-byte alignment
   return p;
@@ -441,7 +441,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
   static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
   constexpr int NH = NEPI / 4;
-  using Sel = RowHeap<KH, BM>;
+  using Sel = RowTopK<KH, BM>;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));
@@ -715,6 +715,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       sel.pub_other = pub + (1 - h) * BM + row;
     }
     sel.reset();
+    sel.prof = P.prof != 0;
     const int gcols = P.bn / NH;                   // accumulator columns of this group
     const int nch = gcols / 32;
     int acc = 0;
@@ -741,7 +742,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       const int self = P.qmap ? (row < nq ? P.qmap[qrow + row] : -1) : qrow + row;
       sel.set_seed((P.seed && row < nq) ? P.seed[qrow + row] : F_INF);
       if (P.init_val && row < nq) {
-        if (h == 0) sel.load(P.init_val, P.init_idx, P.iperm, P.perm[qrow + row], P.cand_stride);
+        // both column halves start from the near pass's heap (merge_from skips the copies)
+        sel.load(P.init_val, P.init_idx, P.iperm, P.perm[qrow + row], P.cand_stride);
         const int4 ex = P.excl[qrow + row];
         sel.ex_r0 = ex.x; sel.ex_r1 = ex.y; sel.ex_o0 = ex.z; sel.ex_o1 = ex.w;
       }
@@ -830,6 +832,8 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         atomicAdd(&g_tc_prof[P.prof_slot][3], (unsigned long long)c_ew);
         atomicAdd(&g_tc_prof[P.prof_slot][4], (unsigned long long)c_loop);
         atomicAdd(&g_tc_prof[P.prof_slot][6], (unsigned long long)sel.n_hot);
+        atomicAdd(&g_tc_prof[P.prof_slot][11], (unsigned long long)sel.n_rounds);
+        atomicAdd(&g_tc_prof[P.prof_slot][12], (unsigned long long)sel.c_hot);
       }
       atomicAdd(&g_tc_prof[P.prof_slot][7], (unsigned long long)sel.n_compact);
       atomicAdd(&g_tc_prof[P.prof_slot][8], (unsigned long long)sel.n_append);

@@ -247,52 +247,94 @@ struct RowSelect {
 };
 
 
-// --- the row heap (tensor-core epilogue) ------------------------------------------------------------
+// --- the row top-k' of the tensor-core epilogue ---------------------------------------------------
 //
-// The same three-level filter, but a value that passes goes straight into a max-heap of the row's
-// k' smallest values kept in shared memory (one sift-down of at most log2(k') levels), and the
-// row's threshold is the heap's root at once.  Compared with the buffered list above this costs a
-// few dozen instructions per insertion instead of a sort and a k'-step merge per buffer, and it
-// tightens the threshold after every insertion.  The list's order does not matter to the callers
-// (the re-rank sorts the candidates itself), so the heap is written out as it stands.
+// The same three-level filter as above, but a value that passes replaces the row's current
+// k'-th value at once.  The k' (value, column) pairs of a row sit unsorted in shared memory in 8
+// groups of KH/8 slots; each thread keeps, in registers, every group's largest value and its slot,
+// and which group holds the overall largest (the row's threshold).  An insertion overwrites that
+// slot, re-reads that one group (KH/8 independent loads) and re-takes two small maxima — a short
+// dependency chain, where a binary heap's sift-down is a chain of up to log2(k') dependent
+// shared-memory round trips.  The candidates' order does not matter to the callers (the re-rank
+// sorts them).
 //
 // Shared memory (slot-major, so the 32 rows of a warp hit 32 banks whatever slot each lane is at):
-//   he[KH][ROWS]   binary max-heap per row of (value, column): root at slot 0; +inf / -1 while
-//                  not full
+//   he[KH][ROWS]   (value bits, column); +inf / -1 while free, -inf in slots >= k'
 template <int KH, int ROWS>
-struct RowHeap {
-  static_assert(KH == 32 || KH == 48 || KH == 64, "heap of 32, 48 or 64");
+struct RowTopK {
+  static_assert(KH == 32 || KH == 48 || KH == 64, "32, 48 or 64 slots");
+  static constexpr int G = 8;           // groups
+  static constexpr int GS = KH / G;     // slots per group
   __host__ __device__ static constexpr size_t smem_bytes() { return size_t(KH) * ROWS * 8; }
 
-  int2* he;       // heap entries [KH][ROWS]: (float bits of the value, column)
+  int2* he;
   int row;        // this thread's row within the ROWS rows
   int kp;         // k' (<= KH)
-  float thr;      // the heap's root: the k'-th smallest value kept (+inf while not full)
-  float thr_f;    // filter threshold: min(thr, seed, the partner heap's published root)
+  float gmax[G];  // largest value of each group
+  int gslot[G];   // its slot
+  int gstar;      // group of the overall largest
+  float thr;      // the k'-th smallest value kept (+inf while fewer than k' are kept)
+  float thr_f;    // filter threshold: min(thr, seed, the partner's published threshold)
   // An upper bound on the row's final k'-th value known before the scan (from an earlier pass
   // over a subset of its keys), +inf if none.  Values at or above it are never kept; the
-  // threshold reported by finish() is min(root, seed), so every value not kept is at least the
+  // threshold reported by finish() is min(thr, seed), so every value not kept is at least the
   // reported threshold even if fewer than k' values passed the filter.
   float seed = F_INF;
-  // When two heaps split one row's columns, each publishes its root here (shared memory) and
-  // filters against the smaller of the two: the k'-th smallest of the union is at most either
-  // heap's k'-th value, so nothing it drops can belong to the union's k' smallest.
+  // When two selectors split one row's columns, each publishes its threshold here (shared
+  // memory) and filters against the smaller of the two: the k'-th smallest of the union is at
+  // most either one's k'-th value, so nothing it drops can belong to the union's k' smallest.
   float* pub_own = nullptr;
   const float* pub_other = nullptr;
   // columns never offered again: [ex_r0, ex_r1) and [ex_o0, ex_o1) (keys whose values an earlier
-  // pass already put into the heap it was loaded from)
+  // pass already put into the list this one was loaded from)
   int ex_r0 = 0, ex_r1 = 0, ex_o0 = 0, ex_o1 = 0;
   int n_hot = 0, n_compact = 0, n_append = 0;   // counters for the pipeline profile
+  bool prof = false;                            // also time the hot path (clock64)
+  long long c_hot = 0, n_rounds = 0;
 
-  __device__ void bind(void* smem, int row_, int kprime) {
+  __device__ __forceinline__ void bind(void* smem, int row_, int kprime) {
     he = static_cast<int2*>(smem);
     row = row_;
     kp = kprime;
   }
 
-  __device__ void reset() {
-    for (int s = 0; s < KH; ++s) he[s * ROWS + row] = make_int2(__float_as_int(F_INF), -1);
+  // the group maxima and the overall largest, from shared memory
+  __device__ __forceinline__ void rescan_all() {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      float m = __int_as_float(he[(g * GS) * ROWS + row].x);
+      int ms = g * GS;
+#pragma unroll
+      for (int t = 1; t < GS; ++t) {
+        const float x = __int_as_float(he[(g * GS + t) * ROWS + row].x);
+        if (x > m) { m = x; ms = g * GS + t; }
+      }
+      gmax[g] = m;
+      gslot[g] = ms;
+    }
+    take_max();
+  }
+
+  __device__ __forceinline__ void take_max() {
+    float m = gmax[0];
+    int gs = 0;
+#pragma unroll
+    for (int g = 1; g < G; ++g)
+      if (gmax[g] > m) { m = gmax[g]; gs = g; }
+    thr = m;
+    gstar = gs;
+  }
+
+  __device__ __forceinline__ void reset() {
+    for (int s = 0; s < KH; ++s)
+      he[s * ROWS + row] = make_int2(__float_as_int(s < kp ? F_INF : -F_INF), -1);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      gmax[g] = g * GS < kp ? F_INF : -F_INF;
+      gslot[g] = g * GS;
+    }
     thr = F_INF;
+    gstar = 0;
     thr_f = F_INF;
     seed = F_INF;
   }
@@ -307,16 +349,16 @@ struct RowHeap {
     if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
   }
 
-  // Load a heap written by finish() of an earlier pass (slot order is heap order): k' values and
-  // original rows per row, the rows mapped to packed positions through iperm.
-  __device__ void load(const float* __restrict__ vals, const int32_t* __restrict__ idx,
+  // Load a list written by finish() of an earlier pass: k' values and original rows per row, the
+  // rows mapped to packed positions through iperm.
+  __device__ __forceinline__ void load(const float* __restrict__ vals, const int32_t* __restrict__ idx,
                        const int32_t* __restrict__ iperm, int64_t orow, int stride) {
     for (int s = 0; s < kp; ++s) {
       const float v = vals[orow * stride + s];
       const int32_t c = idx[orow * stride + s];
       he[s * ROWS + row] = make_int2(__float_as_int(v), c >= 0 ? iperm[c] : -1);
     }
-    thr = __int_as_float(he[row].x);
+    rescan_all();
     if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
     refresh();
   }
@@ -328,40 +370,43 @@ struct RowHeap {
     return upto & ~((1u << lo) - 1u);
   }
 
-  // replace the root by (v, col) (v < root) and restore the heap: one 8-byte load per child and
-  // one 8-byte store per level (a new value just below the root usually stops within two levels)
+  // (v, col) replaces the largest kept value (v < thr)
   __device__ __forceinline__ void insert(float v, int col) {
     ++n_append;
-    int2* H = he + row;
-    int i = 0;
-    for (;;) {
-      const int l = 2 * i + 1;
-      if (l >= kp) break;
-      int2 c = H[l * ROWS];
-      int ci = l;
-      if (l + 1 < kp) {
-        const int2 r = H[(l + 1) * ROWS];
-        if (__int_as_float(r.x) > __int_as_float(c.x)) { c = r; ci = l + 1; }
-      }
-      if (!(__int_as_float(c.x) > v)) break;
-      H[i * ROWS] = c;
-      i = ci;
+    int s0 = 0;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (g == gstar) s0 = gslot[g];
+    he[s0 * ROWS + row] = make_int2(__float_as_int(v), col);
+    // re-take the maximum of that group
+    const int base = gstar * GS;
+    float m = __int_as_float(he[base * ROWS + row].x);
+    int ms = base;
+#pragma unroll
+    for (int t = 1; t < GS; ++t) {
+      const float x = __int_as_float(he[(base + t) * ROWS + row].x);
+      if (x > m) { m = x; ms = base + t; }
     }
-    H[i * ROWS] = make_int2(__float_as_int(v), col);
-    thr = __int_as_float(H[0].x);
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (g == gstar) { gmax[g] = m; gslot[g] = ms; }
+    take_max();
     if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
     refresh();
   }
 
-  // Merge another heap of the same row (same layout, base `other`) into this one.  Nothing is
-  // published meanwhile: the partner reads this row's published root as +inf until the next tile.
-  __device__ void merge_from(const void* other) {
+  // Merge another selector of the same row (same layout, base `other`) into this one.  Nothing is
+  // published meanwhile: the partner reads this row's published threshold as +inf until the next
+  // tile.  Entries in the excluded ranges are skipped: both were loaded with the same earlier
+  // candidates, so this one holds its own copy or has dropped the key for k' better ones.
+  __device__ __forceinline__ void merge_from(const void* other) {
     const int2* O = static_cast<const int2*>(other) + row;
     float* keep = pub_own;
     pub_own = nullptr;
     for (int s = 0; s < kp; ++s) {
       const int2 e = O[s * ROWS];
-      if (__int_as_float(e.x) < thr) insert(__int_as_float(e.x), e.y);
+      const bool loaded = (e.y >= ex_r0 && e.y < ex_r1) || (e.y >= ex_o0 && e.y < ex_o1);
+      if (__int_as_float(e.x) < thr && !loaded) insert(__int_as_float(e.x), e.y);
     }
     pub_own = keep;
   }
@@ -394,6 +439,7 @@ struct RowHeap {
     const float mn = fminf(min3f(n0, n1, n2), n3);
     if (!__any_sync(FULL, mn < thr_f)) return;
     ++n_hot;
+    const long long t_hot = prof ? clock64() : 0;
     unsigned m = 0u;
     if (mn < thr_f) {
 #pragma unroll
@@ -405,6 +451,7 @@ struct RowHeap {
       m &= ~(span_bits(col0, ex_r0, ex_r1) | span_bits(col0, ex_o0, ex_o1));
     }
     while (__any_sync(FULL, m != 0u)) {
+      ++n_rounds;
       if (m) {
         const int e = __ffs(m) - 1;
         m &= m - 1u;
@@ -412,17 +459,18 @@ struct RowHeap {
         if (x < thr_f) insert(x, col0 + e);
       }
     }
+    if (prof) c_hot += clock64() - t_hot;
   }
 
   __device__ __forceinline__ void push1(float v, int c, int self, int limit) {
     if (v < thr_f && c != self && c < limit) insert(v, c);
   }
 
-  __device__ void flush() {}
+  __device__ __forceinline__ void flush() {}
 
   // warp-collective: the first nvalid_rows rows of the warp into part (k' (value, original row)
-  // per row, rows at part_row0 + r) and part_thr (min(root, seed)), for a later merge
-  __device__ void finish_partial(int2* part, float* part_thr, int64_t part_row0,
+  // per row, rows at part_row0 + r) and part_thr (min(thr, seed)), for a later merge
+  __device__ __forceinline__ void finish_partial(int2* part, float* part_thr, int64_t part_row0,
                                  const int32_t* __restrict__ perm, int nvalid_rows, int kout) {
     __syncwarp();
     const int lane = lane_id();
@@ -435,15 +483,16 @@ struct RowHeap {
         const int2 e = he[s * ROWS + rr];
         out[s] = make_int2(e.x, e.y >= 0 ? perm[e.y] : -1);
       }
-      if (lane == 0) part_thr[part_row0 + r] = fminf(__int_as_float(he[rr].x), sd);
+      const float th = __shfl_sync(FULL, thr, r);
+      if (lane == 0) part_thr[part_row0 + r] = fminf(th, sd);
     }
     __syncwarp();
   }
 
-  // warp-collective: write the k' kept columns (heap order) and the threshold min(root, seed) of
+  // warp-collective: write the k' kept columns (slot order) and the threshold min(thr, seed) of
   // the warp's first `nvalid_rows` rows; columns are packed positions mapped to original rows
   // through perm (see RowSelect::finish)
-  __device__ void finish(int* out_idx, float* out_thr, int out_stride,
+  __device__ __forceinline__ void finish(int* out_idx, float* out_thr, int out_stride,
                          const int32_t* __restrict__ perm, const int32_t* __restrict__ qmap,
                          int64_t first_row, int nvalid_rows, int kout, float* out_val = nullptr) {
     __syncwarp();
@@ -459,7 +508,8 @@ struct RowHeap {
         out_idx[orow * out_stride + s] = e.y >= 0 ? perm[e.y] : -1;
         if (out_val) out_val[orow * out_stride + s] = __int_as_float(e.x);
       }
-      if (lane == 0) out_thr[orow] = fminf(__int_as_float(he[rr].x), sd);
+      const float th = __shfl_sync(FULL, thr, r);
+      if (lane == 0) out_thr[orow] = fminf(th, sd);
     }
     __syncwarp();
   }

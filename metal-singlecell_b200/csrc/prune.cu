@@ -6,8 +6,8 @@
 // above x's running k'-th value can never enter x's candidate list.  This file proves it per tile
 // pair with bounding balls:
 //
-//   1. near pass: the candidate kernel visits only the few key tiles around each query tile's own
-//      keys (the cells are in locality order) and returns every row's k'-th smallest value thr_x.
+//   1. near pass: the candidate kernel visits only each query tile's own key tile (the cells are
+//      in locality order) and returns every row's k'-th smallest value thr_x.
 //      R_x = thr_x + |z_x|² + 3·eps_x bounds, in the scaled space z of the operands, the squared
 //      distance below which x can still take a key (eps_x = the certificate's bound on the
 //      operand and accumulation error, see rerank.cu);
