@@ -741,11 +741,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       const int qrow = w.qrow0 + int(rank) * BM;
       const int self = P.qmap ? (row < nq ? P.qmap[qrow + row] : -1) : qrow + row;
       sel.set_seed((P.seed && row < nq) ? P.seed[qrow + row] : F_INF);
-      if (P.init_val && row < nq) {
-        // both column halves start from the near pass's heap (merge_from skips the copies)
-        sel.load(P.init_val, P.init_idx, P.iperm, P.perm[qrow + row], P.cand_stride);
-        const int4 ex = P.excl[qrow + row];
-        sel.ex_r0 = ex.x; sel.ex_r1 = ex.y; sel.ex_o0 = ex.z; sel.ex_o1 = ex.w;
+      if (P.init_val) {
+        // both column halves start from the near pass's lists (merge_from skips the copies)
+        const int nv = min(32, nq - q * 32);
+        if (nv > 0)
+          sel.load_warp(P.init_val, P.init_idx, P.iperm, P.perm, int64_t(qrow) + q * 32, nv,
+                        P.cand_stride);
+        if (row < nq) {
+          const int4 ex = P.excl[qrow + row];
+          sel.ex_r0 = ex.x; sel.ex_r1 = ex.y; sel.ex_o0 = ex.z; sel.ex_o1 = ex.w;
+        }
       }
       const int limit = w.key0 + w.nkeys;
       KeyTileWalk walk;

@@ -271,7 +271,6 @@ struct RowTopK {
   int row;        // this thread's row within the ROWS rows
   int kp;         // k' (<= KH)
   float gmax[G];  // largest value of each group
-  int gslot[G];   // its slot
   int gstar;      // group of the overall largest
   float thr;      // the k'-th smallest value kept (+inf while fewer than k' are kept)
   float thr_f;    // filter threshold: min(thr, seed, the partner's published threshold)
@@ -303,14 +302,9 @@ struct RowTopK {
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       float m = __int_as_float(he[(g * GS) * ROWS + row].x);
-      int ms = g * GS;
 #pragma unroll
-      for (int t = 1; t < GS; ++t) {
-        const float x = __int_as_float(he[(g * GS + t) * ROWS + row].x);
-        if (x > m) { m = x; ms = g * GS + t; }
-      }
+      for (int t = 1; t < GS; ++t) m = fmaxf(m, __int_as_float(he[(g * GS + t) * ROWS + row].x));
       gmax[g] = m;
-      gslot[g] = ms;
     }
     take_max();
   }
@@ -329,10 +323,7 @@ struct RowTopK {
     for (int s = 0; s < KH; ++s)
       he[s * ROWS + row] = make_int2(__float_as_int(s < kp ? F_INF : -F_INF), -1);
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-      gmax[g] = g * GS < kp ? F_INF : -F_INF;
-      gslot[g] = g * GS;
-    }
+    for (int g = 0; g < G; ++g) gmax[g] = g * GS < kp ? F_INF : -F_INF;
     thr = F_INF;
     gstar = 0;
     thr_f = F_INF;
@@ -349,18 +340,33 @@ struct RowTopK {
     if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
   }
 
-  // Load a list written by finish() of an earlier pass: k' values and original rows per row, the
-  // rows mapped to packed positions through iperm.
-  __device__ __forceinline__ void load(const float* __restrict__ vals, const int32_t* __restrict__ idx,
-                       const int32_t* __restrict__ iperm, int64_t orow, int stride) {
-    for (int s = 0; s < kp; ++s) {
-      const float v = vals[orow * stride + s];
-      const int32_t c = idx[orow * stride + s];
-      he[s * ROWS + row] = make_int2(__float_as_int(v), c >= 0 ? iperm[c] : -1);
+  // warp-collective: load the lists an earlier pass wrote with finish() for the warp's first
+  // nvalid_rows rows (packed rows first_row + r): k' values and original rows per row, the rows
+  // mapped to packed positions through iperm.  The lanes read one row's list at a time (coalesced),
+  // several rows in flight; then every lane takes its own row's group maxima.
+  __device__ __forceinline__ void load_warp(const float* __restrict__ vals,
+                                            const int32_t* __restrict__ idx,
+                                            const int32_t* __restrict__ iperm,
+                                            const int32_t* __restrict__ perm, int64_t first_row,
+                                            int nvalid_rows, int stride) {
+    const int lane = lane_id();
+    const int row0 = row - lane;
+    const int64_t my_orow = lane < nvalid_rows ? int64_t(perm[first_row + lane]) : 0;
+#pragma unroll 4
+    for (int r = 0; r < nvalid_rows; ++r) {
+      const int64_t orow = __shfl_sync(FULL, my_orow, r);
+      for (int s = lane; s < kp; s += 32) {
+        const float v = vals[orow * stride + s];
+        const int32_t c = idx[orow * stride + s];
+        he[s * ROWS + row0 + r] = make_int2(__float_as_int(v), c >= 0 ? iperm[c] : -1);
+      }
     }
-    rescan_all();
-    if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
-    refresh();
+    __syncwarp();
+    if (lane < nvalid_rows) {
+      rescan_all();
+      if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
+      refresh();
+    }
   }
 
   __device__ __forceinline__ static unsigned span_bits(int col0, int a, int b) {
@@ -370,26 +376,28 @@ struct RowTopK {
     return upto & ~((1u << lo) - 1u);
   }
 
-  // (v, col) replaces the largest kept value (v < thr)
+  // (v, col) replaces the largest kept value (v < thr): the group holding it is read (its
+  // largest is the slot equal to the group's maximum), the slot overwritten, the group's and the
+  // overall maxima re-taken
   __device__ __forceinline__ void insert(float v, int col) {
     ++n_append;
-    int s0 = 0;
-#pragma unroll
-    for (int g = 0; g < G; ++g)
-      if (g == gstar) s0 = gslot[g];
-    he[s0 * ROWS + row] = make_int2(__float_as_int(v), col);
-    // re-take the maximum of that group
     const int base = gstar * GS;
-    float m = __int_as_float(he[base * ROWS + row].x);
-    int ms = base;
+    const float* hv = reinterpret_cast<const float*>(he);      // .x of the entries, stride 2
+    float x[GS];
 #pragma unroll
-    for (int t = 1; t < GS; ++t) {
-      const float x = __int_as_float(he[(base + t) * ROWS + row].x);
-      if (x > m) { m = x; ms = base + t; }
-    }
+    for (int t = 0; t < GS; ++t) x[t] = hv[2 * ((base + t) * ROWS + row)];
+    int ts = GS - 1;
+#pragma unroll
+    for (int t = GS - 2; t >= 0; --t)
+      if (x[t] == thr) ts = t;                  // the first slot holding the maximum
+    he[(base + ts) * ROWS + row] = make_int2(__float_as_int(v), col);
+    float m = v;
+#pragma unroll
+    for (int t = 0; t < GS; ++t)
+      if (t != ts) m = fmaxf(m, x[t]);
 #pragma unroll
     for (int g = 0; g < G; ++g)
-      if (g == gstar) { gmax[g] = m; gslot[g] = ms; }
+      if (g == gstar) gmax[g] = m;
     take_max();
     if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
     refresh();
@@ -475,6 +483,7 @@ struct RowTopK {
     __syncwarp();
     const int lane = lane_id();
     const int row0 = row - lane;
+#pragma unroll 4
     for (int r = 0; r < nvalid_rows; ++r) {
       const int rr = row0 + r;
       const float sd = __shfl_sync(FULL, seed, r);
@@ -498,10 +507,13 @@ struct RowTopK {
     __syncwarp();
     const int lane = lane_id();
     const int row0 = row - lane;
+    int64_t my_orow = 0;
+    if (lane < nvalid_rows)
+      my_orow = perm[qmap ? int64_t(qmap[first_row + lane]) : first_row + lane];
+#pragma unroll 4
     for (int r = 0; r < nvalid_rows; ++r) {
       const int rr = row0 + r;
-      const int64_t prow = qmap ? int64_t(qmap[first_row + r]) : first_row + r;
-      const int64_t orow = perm[prow];
+      const int64_t orow = __shfl_sync(FULL, my_orow, r);
       const float sd = __shfl_sync(FULL, seed, r);
       for (int s = lane; s < kout; s += 32) {
         const int2 e = he[s * ROWS + rr];
