@@ -324,9 +324,11 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
   // widely, so whole tiles per warp would leave most SMs idle behind the slowest few
   const int nblk = (words + PLAN_WORDS - 1) / PLAN_WORDS;
   const int64_t ntasks = n_items * nblk;
+  // consecutive warps take consecutive query tiles of the same key-tile block, so the key-side
+  // centres they read are shared through L1
   for (int64_t task = int64_t(blockIdx.x) * PLAN_WARPS + wib; task < ntasks; task += warps) {
-    const int64_t it = task / nblk;
-    const int wblk = int(task - it * nblk);
+    const int wblk = int(task / n_items);
+    const int64_t it = task - int64_t(wblk) * n_items;
     const WorkItem w = items[it];
     const int64_t qt = w.qrow0 / QTILE;          // 128-row tile of packed rows
     const int64_t sb0 = int64_t(w.qrow0) / SUB;  // its first 32-row block

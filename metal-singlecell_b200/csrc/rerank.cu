@@ -78,13 +78,32 @@ __device__ __forceinline__ double d2_f64(const float* xs, const float* __restric
   return acc;
 }
 
+// FP32 squared distance of a shared-memory row xs and a gathered row y.  Four partial sums over
+// 8-byte loads (when y is 8-byte aligned) keep several loads of the gathered row in flight; the
+// sum of d positive terms in any order stays within the (d+4)·2^-24 relative bound the re-rank
+// window assumes.
 __device__ __forceinline__ float d2_f32(const float* xs, const float* __restrict__ y, int d) {
-  float acc = 0.f;
-  for (int t = 0; t < d; ++t) {
-    float df = xs[t] - y[t];
-    acc = fmaf(df, df, acc);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  int t = 0;
+  if ((reinterpret_cast<uintptr_t>(y) & 7) == 0) {
+    const float2* y2 = reinterpret_cast<const float2*>(y);
+    const float2* x2 = reinterpret_cast<const float2*>(xs);
+#pragma unroll 4
+    for (; t + 4 <= d; t += 4) {
+      const float2 u = y2[t >> 1], w = y2[(t >> 1) + 1];
+      const float2 p = x2[t >> 1], q = x2[(t >> 1) + 1];
+      const float e0 = p.x - u.x, e1 = p.y - u.y, e2 = q.x - w.x, e3 = q.y - w.y;
+      a0 = fmaf(e0, e0, a0);
+      a1 = fmaf(e1, e1, a1);
+      a2 = fmaf(e2, e2, a2);
+      a3 = fmaf(e3, e3, a3);
+    }
   }
-  return acc;
+  for (; t < d; ++t) {
+    const float df = xs[t] - y[t];
+    a0 = fmaf(df, df, a0);
+  }
+  return (a0 + a1) + (a2 + a3);
 }
 
 __device__ __forceinline__ float out_dist(double d2, int cosine) {
@@ -101,7 +120,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
               float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows,
               const int32_t* __restrict__ rows, const int32_t* __restrict__ nrows,
               int32_t* __restrict__ fail_flags) {
-  __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
+  __shared__ __align__(16) float xs_all[RR_WARPS][MSC_MAX_D];
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
   const int kk = k - 1;
@@ -206,7 +225,7 @@ fp64_scan_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__
                  const SegDesc* __restrict__ seg, int nseg,
                  const int32_t* __restrict__ fail_rows, Ctl* __restrict__ ctl, int k, int cosine,
                  int32_t* __restrict__ knn_idx, float* __restrict__ knn_dist) {
-  __shared__ float xs_all[RR_WARPS][MSC_MAX_D];
+  __shared__ __align__(16) float xs_all[RR_WARPS][MSC_MAX_D];
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
   const int kk = k - 1;
