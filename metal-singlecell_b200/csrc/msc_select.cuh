@@ -259,7 +259,8 @@ struct RowSelect {
 // sorts them).
 //
 // Shared memory (slot-major, so the 32 rows of a warp hit 32 banks whatever slot each lane is at):
-//   he[KH][ROWS]   (value bits, column); +inf / -1 while free, -inf in slots >= k'
+//   hv[KH][ROWS]   values: +inf while free, -inf in slots >= k'
+//   hc[KH][ROWS]   columns (-1 while free); kept apart so that reading values is conflict-free
 template <int KH, int ROWS>
 struct RowTopK {
   static_assert(KH == 32 || KH == 48 || KH == 64, "32, 48 or 64 slots");
@@ -267,7 +268,8 @@ struct RowTopK {
   static constexpr int GS = KH / G;     // slots per group
   __host__ __device__ static constexpr size_t smem_bytes() { return size_t(KH) * ROWS * 8; }
 
-  int2* he;
+  float* hv;
+  int* hc;
   int row;        // this thread's row within the ROWS rows
   int kp;         // k' (<= KH)
   float gmax[G];  // largest value of each group
@@ -292,7 +294,8 @@ struct RowTopK {
   long long c_hot = 0, n_rounds = 0;
 
   __device__ __forceinline__ void bind(void* smem, int row_, int kprime) {
-    he = static_cast<int2*>(smem);
+    hv = static_cast<float*>(smem);
+    hc = reinterpret_cast<int*>(hv + KH * ROWS);
     row = row_;
     kp = kprime;
   }
@@ -301,9 +304,9 @@ struct RowTopK {
   __device__ __forceinline__ void rescan_all() {
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-      float m = __int_as_float(he[(g * GS) * ROWS + row].x);
+      float m = hv[(g * GS) * ROWS + row];
 #pragma unroll
-      for (int t = 1; t < GS; ++t) m = fmaxf(m, __int_as_float(he[(g * GS + t) * ROWS + row].x));
+      for (int t = 1; t < GS; ++t) m = fmaxf(m, hv[(g * GS + t) * ROWS + row]);
       gmax[g] = m;
     }
     take_max();
@@ -320,8 +323,10 @@ struct RowTopK {
   }
 
   __device__ __forceinline__ void reset() {
-    for (int s = 0; s < KH; ++s)
-      he[s * ROWS + row] = make_int2(__float_as_int(s < kp ? F_INF : -F_INF), -1);
+    for (int s = 0; s < KH; ++s) {
+      hv[s * ROWS + row] = s < kp ? F_INF : -F_INF;
+      hc[s * ROWS + row] = -1;
+    }
 #pragma unroll
     for (int g = 0; g < G; ++g) gmax[g] = g * GS < kp ? F_INF : -F_INF;
     thr = F_INF;
@@ -358,7 +363,8 @@ struct RowTopK {
       for (int s = lane; s < kp; s += 32) {
         const float v = vals[orow * stride + s];
         const int32_t c = idx[orow * stride + s];
-        he[s * ROWS + row0 + r] = make_int2(__float_as_int(v), c >= 0 ? iperm[c] : -1);
+        hv[s * ROWS + row0 + r] = v;
+        hc[s * ROWS + row0 + r] = c >= 0 ? iperm[c] : -1;
       }
     }
     __syncwarp();
@@ -382,15 +388,15 @@ struct RowTopK {
   __device__ __forceinline__ void insert(float v, int col) {
     ++n_append;
     const int base = gstar * GS;
-    const float* hv = reinterpret_cast<const float*>(he);      // .x of the entries, stride 2
     float x[GS];
 #pragma unroll
-    for (int t = 0; t < GS; ++t) x[t] = hv[2 * ((base + t) * ROWS + row)];
+    for (int t = 0; t < GS; ++t) x[t] = hv[(base + t) * ROWS + row];
     int ts = GS - 1;
 #pragma unroll
     for (int t = GS - 2; t >= 0; --t)
       if (x[t] == thr) ts = t;                  // the first slot holding the maximum
-    he[(base + ts) * ROWS + row] = make_int2(__float_as_int(v), col);
+    hv[(base + ts) * ROWS + row] = v;
+    hc[(base + ts) * ROWS + row] = col;
     float m = v;
 #pragma unroll
     for (int t = 0; t < GS; ++t)
@@ -408,13 +414,15 @@ struct RowTopK {
   // tile.  Entries in the excluded ranges are skipped: both were loaded with the same earlier
   // candidates, so this one holds its own copy or has dropped the key for k' better ones.
   __device__ __forceinline__ void merge_from(const void* other) {
-    const int2* O = static_cast<const int2*>(other) + row;
+    const float* OV = static_cast<const float*>(other) + row;
+    const int* OC = reinterpret_cast<const int*>(static_cast<const float*>(other) + KH * ROWS) + row;
     float* keep = pub_own;
     pub_own = nullptr;
     for (int s = 0; s < kp; ++s) {
-      const int2 e = O[s * ROWS];
-      const bool loaded = (e.y >= ex_r0 && e.y < ex_r1) || (e.y >= ex_o0 && e.y < ex_o1);
-      if (__int_as_float(e.x) < thr && !loaded) insert(__int_as_float(e.x), e.y);
+      const float v = OV[s * ROWS];
+      const int c = OC[s * ROWS];
+      const bool loaded = (c >= ex_r0 && c < ex_r1) || (c >= ex_o0 && c < ex_o1);
+      if (v < thr && !loaded) insert(v, c);
     }
     pub_own = keep;
   }
@@ -489,8 +497,8 @@ struct RowTopK {
       const float sd = __shfl_sync(FULL, seed, r);
       int2* out = part + (part_row0 + r) * kout;
       for (int s = lane; s < kout; s += 32) {
-        const int2 e = he[s * ROWS + rr];
-        out[s] = make_int2(e.x, e.y >= 0 ? perm[e.y] : -1);
+        const int c = hc[s * ROWS + rr];
+        out[s] = make_int2(__float_as_int(hv[s * ROWS + rr]), c >= 0 ? perm[c] : -1);
       }
       const float th = __shfl_sync(FULL, thr, r);
       if (lane == 0) part_thr[part_row0 + r] = fminf(th, sd);
@@ -516,9 +524,9 @@ struct RowTopK {
       const int64_t orow = __shfl_sync(FULL, my_orow, r);
       const float sd = __shfl_sync(FULL, seed, r);
       for (int s = lane; s < kout; s += 32) {
-        const int2 e = he[s * ROWS + rr];
-        out_idx[orow * out_stride + s] = e.y >= 0 ? perm[e.y] : -1;
-        if (out_val) out_val[orow * out_stride + s] = __int_as_float(e.x);
+        const int c = hc[s * ROWS + rr];
+        out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
+        if (out_val) out_val[orow * out_stride + s] = hv[s * ROWS + rr];
       }
       const float th = __shfl_sync(FULL, thr, r);
       if (lane == 0) out_thr[orow] = fminf(th, sd);

@@ -302,6 +302,7 @@ __device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru
 // left, the remaining sub-ball pairs, one pair per lane.
 constexpr int PLAN_WARPS = 4;
 constexpr int PLAN_WORDS = 8;     // mask words (256 key tiles) per warp task
+constexpr int PLAN_MAX_PAIRS = 32;  // sub-ball pairs tested per key tile (one per lane)
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
 plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
             const Ctl* ctl, int prec, const float* __restrict__ qc, const float* __restrict__ qr,
@@ -385,6 +386,12 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
           const int kti = base + __fns(fm, 0, i + 1);
           const int64_t kb0 = (int64_t(w.key0) + int64_t(kti) * bn) / SUB;
           const int nu = __popc(ub), npair = nu * __popc(wb);
+          // many overlapping sub-ball pairs: the tiles share a cluster, and testing every pair
+          // would almost always end in a visit anyway
+          if (npair > PLAN_MAX_PAIRS) {
+            bits |= 1u << (kti - base);
+            continue;
+          }
           ++npt;
           npr += npair;
           bool hit = false;
