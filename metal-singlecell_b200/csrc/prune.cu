@@ -27,6 +27,8 @@
 //
 // Each query tile gets a bit mask over its sample's key tiles (set = visit, near tiles excluded);
 // the candidate kernel walks its near tiles first and then the set bits in ascending order.
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace msc {
@@ -40,7 +42,7 @@ constexpr int PR_T = 256;
 __device__ unsigned long long g_prune_tiles[5];
 constexpr int SUB = 32;          // rows per sub-block (two balls each)
 constexpr float NO_BALL = -1.f;  // radius of a ball without rows
-constexpr double OUTLIER_FACTOR = 4.0;
+constexpr double OUTLIER_FACTOR = 4.0;   // default; MSC_B200_OUTLIER_FACTOR overrides (tuning)
 
 __device__ __forceinline__ double warp_sum_d(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
@@ -92,12 +94,13 @@ __global__ void sample_mean_kernel(const SegDesc* __restrict__ seg, const double
 __global__ void regular_flag_kernel(const int32_t* __restrict__ perm, int64_t npacked,
                                     const SegDesc* __restrict__ seg, int nseg,
                                     const double* __restrict__ rpos,
-                                    const double* __restrict__ mean, int32_t* __restrict__ reg) {
+                                    const double* __restrict__ mean, double factor,
+                                    int32_t* __restrict__ reg) {
   for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
        p += int64_t(gridDim.x) * blockDim.x) {
     if (perm[p] < 0) { reg[p] = 0; continue; }
     const double m = mean[find_seg(seg, nseg, p)];
-    reg[p] = rpos[p] > OUTLIER_FACTOR * m ? 0 : 1;        // NaN / inf mean: regular
+    reg[p] = rpos[p] > factor * m ? 0 : 1;                // NaN / inf mean: regular
   }
 }
 
@@ -302,13 +305,15 @@ __device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru
 // left, the remaining sub-ball pairs, one pair per lane.
 constexpr int PLAN_WARPS = 4;
 constexpr int PLAN_WORDS = 8;     // mask words (256 key tiles) per warp task
-constexpr int PLAN_MAX_PAIRS = 32;  // sub-ball pairs tested per key tile (one per lane)
+constexpr int PLAN_MAX_PAIRS = 32;  // sub-ball pairs tested per key tile (one per lane);
+                                    // MSC_B200_PLAN_PAIRS overrides (tuning)
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
 plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
             const Ctl* ctl, int prec, const float* __restrict__ qc, const float* __restrict__ qr,
             const float* __restrict__ kc, const float* __restrict__ kr,
             const float* __restrict__ sc, const float* __restrict__ sr,
-            const double* __restrict__ rsub, int words, uint32_t* __restrict__ mask, int prof) {
+            const double* __restrict__ rsub, int words, uint32_t* __restrict__ mask, int prof,
+            int max_pairs) {
   extern __shared__ float4 sm4[];
   __shared__ unsigned ubits_all[PLAN_WARPS][32], wbits_all[PLAN_WARPS][32];
   const int lane = lane_id(), wib = warp_id();
@@ -388,7 +393,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
           const int nu = __popc(ub), npair = nu * __popc(wb);
           // many overlapping sub-ball pairs: the tiles share a cluster, and testing every pair
           // would almost always end in a visit anyway
-          if (npair > PLAN_MAX_PAIRS) {
+          if (npair > max_pairs) {
             bits |= 1u << (kti - base);
             continue;
           }
@@ -597,7 +602,13 @@ int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, 
   MSC_LAUNCH_CHECK();
   sample_mean_kernel<<<nseg, PR_T, 0, st>>>(seg, w.rpos, w.mean);
   MSC_LAUNCH_CHECK();
-  regular_flag_kernel<<<grid, PR_T, 0, st>>>(perm, npacked, seg, nseg, w.rpos, w.mean, w.reg);
+  double factor = OUTLIER_FACTOR;
+  if (const char* env = std::getenv("MSC_B200_OUTLIER_FACTOR")) {
+    const double v = std::atof(env);
+    if (v > 1.0) factor = v;
+  }
+  regular_flag_kernel<<<grid, PR_T, 0, st>>>(perm, npacked, seg, nseg, w.rpos, w.mean, factor,
+                                             w.reg);
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl_i32(w.reg, npacked, w.S, w.scan_scratch, st));
   partition_kernel<<<grid, PR_T, 0, st>>>(perm, w.leaf, w.rpos, npacked, seg, nseg, w.reg, w.S,
@@ -637,12 +648,15 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
   sub_ball_kernel<<<sgrid, PR_T, 0, st>>>(X, d, dp, perm, w.leaf2, w.rpos2, ns, w.sc, w.sr, w.rsub);
   MSC_LAUNCH_CHECK();
   const size_t smem = size_t(PLAN_WARPS) * 9 * dp * sizeof(float);
+  int max_pairs = PLAN_MAX_PAIRS;
+  if (const char* env = std::getenv("MSC_B200_PLAN_PAIRS")) max_pairs = std::max(0, std::atoi(env));
   const int64_t ntasks = n_items * ceil_div(words, PLAN_WORDS);
   const int pgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(ntasks, PLAN_WARPS),
                                                               int64_t(num_sms()) * 32)));
   plan_kernel<<<pgrid, PLAN_WARPS * 32, smem, st>>>(items, n_items, bn, d, dp, ctl, prec, w.qc,
                                                     w.qr, w.kc, w.kr, w.sc, w.sr, w.rsub, words,
-                                                    w.mask, profiling_enabled() ? 1 : 0);
+                                                    w.mask, profiling_enabled() ? 1 : 0,
+                                                    max_pairs);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
