@@ -275,7 +275,7 @@ int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
     if (env && *env) code = int32_t(std::strtol(env, nullptr, 0));
   }
   if (code == 0) return MSC_OK;
-  TcConfig c{code & 0xfff, (code >> 12) & 0xff, heap_slots(P.kprime), (code >> 20) & 0x7f,
+  TcConfig c{code & 0xfff, (code >> 12) & 0xff, list_slots(P.kprime), (code >> 20) & 0x7f,
              (code >> 27) & 1 ? 8 : 4, (code >> 28) & 1};
   if (!tc_config_ok(c, P.L.kp, P.kprime)) {
     set_error("tile_config 0x%x (bn=%d stages=%d cb=%d epi=%d pair=%d) is not valid here", code,

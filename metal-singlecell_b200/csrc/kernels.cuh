@@ -161,7 +161,7 @@ int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const in
                        const QStat* qs, const KeyMax* km, const QStat* qs3, const KeyMax* km3,
                        const Ctl* ctl, int prec, int kmma, int kmma3, int d, const PruneWs& w,
                        cudaStream_t st);
-// after a split refine pass: every refine row's k' smallest of its work items' heaps
+// after a split refine pass: every refine row's k' smallest of its work items' lists
 int launch_refine_merge(const WorkItem* items3, const int32_t* n_items3, const Ctl* ctl,
                         const int32_t* qmap, const int32_t* perm, int64_t max_rows,
                         const PruneWs& w, int kprime, int32_t* cand_idx, float* cand_thr,
@@ -176,7 +176,7 @@ int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const 
                     int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
 
 // The near pass's candidates handed to the main pass: the near pass writes val (and the usual
-// candidate rows); the main pass loads them as every row's starting heap and never offers the
+// candidate rows); the main pass loads them as every row's starting list and never offers the
 // keys the near pass scored again (excl: two packed-position ranges per row).
 struct NearInit {
   float* val;              // n × k' values
@@ -186,7 +186,7 @@ struct NearInit {
 };
 
 // The refine pass split over key ranges (prune.cu): split_dev (device int) work items per refine
-// item; each writes its rows' heaps to part (k' entries per row) and part_thr, merged afterwards.
+// item; each writes its rows' lists to part (k' entries per row) and part_thr, merged afterwards.
 struct RefineSplit {
   const int32_t* split_dev;
   int2* part;
@@ -201,13 +201,13 @@ struct RefineSplit {
 struct TcConfig {
   int bn;        // key tile rows (32, 64, 128, 256)
   int stages;    // smem pipeline depth of the key tiles
-  int kpl;       // slots of the per-row candidate heap (32 / 48 / 64), >= k'
+  int kpl;       // slots of the per-row candidate list (32 / 48 / 64), >= k'
   int cb;        // 16 or 32; kept in the tile code for compatibility, no longer used
   int epi;       // epilogue warps: 4 (one per TMEM lane quarter) or 8 (two, splitting the columns)
   int pair;      // 1: CTA pairs (cta_group::2, M=256, each CTA stages half of every key tile)
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
-int heap_slots(int kprime);
+int list_slots(int kprime);
 int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st);
 int tc_counters(unsigned long long* out, int max);
 int tc_counters_clear();

@@ -309,12 +309,12 @@ struct TcParams {
   const float* seed;            // per packed query row: bound on its final k'-th value, or null
   int prof_slot;                // counter block of this launch (near / main / refine)
   // refine pass split over key ranges: *split_dev work items per refine item (1: no split), each
-  // writing its rows' heaps to part / part_thr for refine_merge
+  // writing its rows' candidate lists to part / part_thr for refine_merge
   const int32_t* split_dev;
   int2* part;
   float* part_thr;
   float* cand_val;              // near pass: also write the values of the kept candidates
-  // main pass after a near pass: load every row's heap from the near pass's candidates (values,
+  // main pass after a near pass: load every row's list from the near pass's candidates (values,
   // original rows -> packed positions through iperm) and never offer its keys again (excl)
   const float* init_val;
   const int32_t* init_idx;
@@ -1022,12 +1022,12 @@ bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   return config_smem(c, kp / 64, 1) <= SMEM_LIMIT;
 }
 
-// heap capacity of a k' (32, 48 or 64 slots per row)
-int heap_slots(int kprime) { return kprime <= 32 ? 32 : (kprime <= 48 ? 48 : 64); }
+// capacity of the per-row candidate list for a k' (32, 48 or 64 slots)
+int list_slots(int kprime) { return kprime <= 32 ? 32 : (kprime <= 48 ? 48 : 64); }
 
 TcConfig tc_default_config(int prec, int d, int kprime) {
   const OpLayout L = op_layout(prec, d);
-  const int kpl = heap_slots(kprime);
+  const int kpl = list_slots(kprime);
   // Single CTAs first: CTA pairs halve the key bytes per SM and double the K-atom stages that
   // fit, but measured slower at 1.3M × 50 (1057 vs 819 ms for the candidate stage), so they are
   // taken only when nothing else fits.  N=256 key tiles (one MMA costs the same ~186 cycles at

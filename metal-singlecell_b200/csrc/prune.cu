@@ -485,8 +485,8 @@ __global__ void refine_mask_kernel(const WorkItem* __restrict__ items3,
 
 // Merge of a split refine pass: warp per refine row; the S·k' entries of its S work items, the k'
 // smallest kept (ties: lower lane, then lower slot).  The threshold is the k'-th smallest: each
-// work item's heap holds k' values at or below its own root, so the merged k'-th value is at most
-// every root, and every key a work item dropped is at least its root.
+// work item's list holds k' values at or below its own k'-th value, so the merged k'-th value is
+// at most every work item's, and every key a work item dropped is at least that item's.
 __global__ void refine_merge_kernel(const WorkItem* __restrict__ items3,
                                     const int32_t* __restrict__ n_items3,
                                     const Ctl* __restrict__ ctl, const int32_t* __restrict__ qmap,
