@@ -6,15 +6,17 @@
 
 A step = one full graph (exact kNN → distances CSR → UMAP connectivities) of the workload's
 synthetic embedding.  Default workload: 1,300,000 cells × 50 PCs, 200-cluster Gaussian mixture with
-lognormal sizes and 1% noise cells, euclidean, k=15, method='umap', BF16 tensor-core candidates
-(three-term split) + exact re-rank.
+lognormal sizes and 1% noise cells, euclidean, k=15, method='umap'; default path: FP16
+tensor-core candidates with key-tile pruning, exact re-rank (BF16x3 refine, FP64 at the boundary).
 
 value   cells/s with the embedding resident in HBM (whole job: N replicas × cells / max time);
 e2e     the same through the public call with host buffers: pinned host → device copy of the
         embedding and device → host copy of both CSR matrices inside the timed region;
-roofline: the tensor-core candidate kernel, algorithmic 2·d·n² FLOP over its event-timed
-        duration, against the measured dense BF16 peak (MEASURED_PEAKS.json);
-cpu_baseline: the CPU oracle port on this host's cores, on a bounded sample of query rows.
+roofline: the main tensor-core candidate launch, 2·d·128·256 FLOP per (query tile, key tile) pair
+        it computes (near + kept far tiles) over its event-timed duration, against the measured
+        sustained dense BF16 peak (MEASURED_PEAKS.json); dense_equivalent_tflops divides 2·d·n²;
+cpu_baseline: the CPU oracle port on this host's cores, on a bounded sample of query rows;
+fp32_form: the plain FP32 SIMT form of the same exact graph (full scan).
 
 With --impl reference the CPU implementation alone runs (rank 0), on bounded samples.
 Multi-GPU (torchrun): every rank builds its own full graph (replicas; the path runs on one GPU).
