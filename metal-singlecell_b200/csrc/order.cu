@@ -184,21 +184,31 @@ __global__ void split_start_kernel(int64_t npacked, int leaf, const int32_t* __r
 // dimensions t, t+32, ...; partial sums go out with one atomic per (node, side, dimension) each
 // time the node changes along the walk.  acc layout per node: [2][d] sums, then [2] counts.
 constexpr int SUM_RUN = 64;
-__global__ void side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
-                                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
-                                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                                const int32_t* __restrict__ side, double* __restrict__ acc) {
-  const int lane = lane_id();
-  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+constexpr int SUM_WARPS = OR_T / 32;
+constexpr int SUM_SLOT = 2 * 128 + 2;       // sums and counts of one node (d <= 128)
+__global__ void __launch_bounds__(OR_T)
+side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
+                const int32_t* __restrict__ side, double* __restrict__ acc) {
+  // Runs that lie inside one node (almost all of them) are first combined across the warps of the
+  // block in shared memory, so that at the top levels, where every run belongs to the same one or
+  // two nodes, a block issues one set of atomics instead of one per warp.
+  __shared__ double part[SUM_WARPS][SUM_SLOT];
+  __shared__ int64_t part_node[SUM_WARPS];
+  const int lane = lane_id(), wib = warp_id();
   const int64_t nruns = (npacked + SUM_RUN - 1) / SUM_RUN;
   const int per = (d + 31) / 32;            // dimensions per lane (d <= 128)
-  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < nruns; r += warps) {
-    const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
+  for (int64_t rb = int64_t(blockIdx.x) * SUM_WARPS; rb < nruns;
+       rb += int64_t(gridDim.x) * SUM_WARPS) {          // block-uniform
+    const int64_t r = rb + wib;
     double s0[4] = {0, 0, 0, 0}, s1[4] = {0, 0, 0, 0};
     double c0 = 0, c1 = 0;
     int64_t cur = -1;                        // node id being accumulated
+    bool flushed = false;
     auto flush = [&]() {
       if (cur < 0) return;
+      flushed = true;
       double* a = acc + cur * (2 * d + 2);
       for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
@@ -214,40 +224,75 @@ __global__ void side_sum_kernel(const float* __restrict__ X, int d, int64_t npac
       }
       c0 = 0; c1 = 0;
     };
-    // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
-    // only loads row data (independent from position to position)
-    int32_t idh[2], rowh[2], sdh[2];
+    if (r < nruns) {                         // warp-uniform
+      const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
+      // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
+      // only loads row data (independent from position to position)
+      int32_t idh[2], rowh[2], sdh[2];
 #pragma unroll
-    for (int hh = 0; hh < 2; ++hh) {
-      const int64_t p = p0 + 32 * hh + lane;
-      idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
-      if (p < p1) {
-        const int st = ns[p];
-        if (ne[p] - st > leaf) {
-          idh[hh] = int32_t(S[st]);
-          rowh[hh] = perm[p];
-          sdh[hh] = side[p];
+      for (int hh = 0; hh < 2; ++hh) {
+        const int64_t p = p0 + 32 * hh + lane;
+        idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
+        if (p < p1) {
+          const int st = ns[p];
+          if (ne[p] - st > leaf) {
+            idh[hh] = int32_t(S[st]);
+            rowh[hh] = perm[p];
+            sdh[hh] = side[p];
+          }
         }
       }
-    }
 #pragma unroll 4
-    for (int jj = 0; jj < SUM_RUN; ++jj) {
-      const int hh = jj >> 5;
-      const int32_t id = __shfl_sync(FULL, hh ? idh[1] : idh[0], jj & 31);
-      if (id < 0) continue;                  // warp-uniform
-      const int32_t rw = __shfl_sync(FULL, hh ? rowh[1] : rowh[0], jj & 31);
-      const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
-      if (id != cur) { flush(); cur = id; }
-      const float* x = X + int64_t(rw) * d;
+      for (int jj = 0; jj < SUM_RUN; ++jj) {
+        const int hh = jj >> 5;
+        const int32_t id = __shfl_sync(FULL, hh ? idh[1] : idh[0], jj & 31);
+        if (id < 0) continue;                // warp-uniform
+        const int32_t rw = __shfl_sync(FULL, hh ? rowh[1] : rowh[0], jj & 31);
+        const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
+        if (id != cur) { flush(); cur = id; }
+        const float* x = X + int64_t(rw) * d;
+        for (int j = 0; j < per; ++j) {
+          const int t = lane + 32 * j;
+          if (t < d) {
+            if (one) s1[j] += x[t]; else s0[j] += x[t];
+          }
+        }
+        if (one) c1 += 1.0; else c0 += 1.0;
+      }
+    }
+    // a run that met one node only hands its sums to the block; any other flushes its last node
+    int64_t slot_node = -1;
+    if (cur >= 0 && !flushed) {
+      slot_node = cur;
       for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
-        if (t < d) {
-          if (one) s1[j] += x[t]; else s0[j] += x[t];
-        }
+        if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
       }
-      if (one) c1 += 1.0; else c0 += 1.0;
+      if (lane == 0) { part[wib][2 * d] = c0; part[wib][2 * d + 1] = c1; }
+    } else {
+      flush();
     }
-    flush();
+    if (lane == 0) part_node[wib] = slot_node;
+    __syncthreads();
+    if (wib == 0) {
+      // consecutive warps with the same node: one atomic per value per node
+      int w0 = 0;
+      while (w0 < SUM_WARPS) {
+        const int64_t nd = part_node[w0];
+        int w1 = w0 + 1;
+        while (w1 < SUM_WARPS && part_node[w1] == nd) ++w1;
+        if (nd >= 0) {
+          double* a = acc + nd * (2 * d + 2);
+          for (int t = lane; t < 2 * d + 2; t += 32) {
+            double v = 0.0;
+            for (int w = w0; w < w1; ++w) v += part[w][t];
+            if (v != 0.0) atomicAdd(&a[t], v);
+          }
+        }
+        w0 = w1;
+      }
+    }
+    __syncthreads();
   }
 }
 
