@@ -27,14 +27,51 @@ namespace msc {
 namespace {
 
 constexpr int OR_T = 256;
+constexpr int OR_W = OR_T / 32;
 
-__device__ __forceinline__ float row_d2(const float* __restrict__ X, int d, int64_t a, int64_t b) {
-  const float* x = X + a * d;
-  const float* y = X + b * d;
+// One warp's 32 rows, 32 dimensions at a time: row r's dimensions c..c+31 in tile[r][0..31].
+// Lanes load a row together (one coalesced line per row and chunk), then each lane reads its own
+// row back from the tile (stride 33 floats: no bank conflicts).  A thread reading its row alone,
+// one float per load, keeps 32 rows' lines live per warp and thrashes L1.
+using RowTile = float[32][33];
+
+// stage dimensions c..c+31 of the lanes' rows (row < 0: not staged); sixteen loads are issued
+// before their stores so that a warp keeps sixteen lines in flight
+__device__ __forceinline__ void stage_rows(const float* __restrict__ X, int d, int c, int32_t row,
+                                           RowTile& tile) {
+  const int t = c + lane_id();
+#pragma unroll
+  for (int r0 = 0; r0 < 32; r0 += 16) {
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int32_t rr = __shfl_sync(FULL, row, r0 + u);
+      v[u] = (rr >= 0 && t < d) ? X[int64_t(rr) * d + t] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) tile[r0 + u][lane_id()] = v[u];
+  }
+  __syncwarp();
+}
+
+// squared distance between the lane's row and row `other`, summed over t = 0..d-1 in order
+// (the same sum as a plain loop over the two rows); lanes with row < 0 return 0
+__device__ __forceinline__ float warp_row_d2(const float* __restrict__ X, int d, int32_t row,
+                                             int64_t other, RowTile& tile) {
+  const unsigned act = __ballot_sync(FULL, row >= 0);
   float acc = 0.f;
-  for (int t = 0; t < d; ++t) {
-    const float df = x[t] - y[t];
-    acc = fmaf(df, df, acc);
+  if (act == 0) return acc;
+  for (int c = 0; c < d; c += 32) {
+    stage_rows(X, d, c, row, tile);
+    if (row >= 0) {
+      const float* y = X + other * d + c;
+      const int tn = min(32, d - c);
+      for (int j = 0; j < tn; ++j) {
+        const float df = tile[lane_id()][j] - y[j];
+        acc = fmaf(df, df, acc);
+      }
+    }
+    __syncwarp();
   }
   return acc;
 }
@@ -85,10 +122,13 @@ __device__ __forceinline__ void warp_far_max(unsigned long long* best, int s, bo
 }
 
 // The loops below keep the 32 lanes of a warp on 32 consecutive positions (warp-uniform trip
-// counts) so that warp_far_max can combine them.
-__global__ void far_a_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
-                             const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
-                             const int32_t* __restrict__ ne, unsigned long long* __restrict__ best) {
+// counts) so that warp_far_max can combine them and warp_row_d2 can stage their rows.
+__global__ void __launch_bounds__(OR_T)
+far_a_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+             const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+             const int32_t* __restrict__ ne, unsigned long long* __restrict__ best) {
+  __shared__ RowTile tiles[OR_W];
+  RowTile& tile = tiles[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
@@ -96,15 +136,19 @@ __global__ void far_a_kernel(const float* __restrict__ X, int d, int64_t npacked
     int s = 0, e = 0;
     if (p < npacked) { s = ns[p]; e = ne[p]; }
     const bool active = p < npacked && e - s > leaf;
-    const unsigned long long key = active ? far_key(row_d2(X, d, perm[p], perm[s]), p) : 0ull;
-    warp_far_max(best, s, active, key);
+    const int32_t row = active ? perm[p] : -1;
+    const float v = warp_row_d2(X, d, row, active ? perm[s] : 0, tile);
+    warp_far_max(best, s, active, active ? far_key(v, p) : 0ull);
   }
 }
 
-__global__ void far_b_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
-                             const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
-                             const int32_t* __restrict__ ne, const unsigned long long* __restrict__ best_a,
-                             float* __restrict__ da, unsigned long long* __restrict__ best_b) {
+__global__ void __launch_bounds__(OR_T)
+far_b_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+             const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+             const int32_t* __restrict__ ne, const unsigned long long* __restrict__ best_a,
+             float* __restrict__ da, unsigned long long* __restrict__ best_b) {
+  __shared__ RowTile tiles[OR_W];
+  RowTile& tile = tiles[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
@@ -112,30 +156,30 @@ __global__ void far_b_kernel(const float* __restrict__ X, int d, int64_t npacked
     int s = 0, e = 0;
     if (p < npacked) { s = ns[p]; e = ne[p]; }
     const bool active = p < npacked && e - s > leaf;
-    unsigned long long key = 0ull;
-    if (active) {
-      const float v = row_d2(X, d, perm[p], perm[far_pos(best_a[s])]);
-      da[p] = v;
-      key = far_key(v, p);
-    }
-    warp_far_max(best_b, s, active, key);
+    const int32_t row = active ? perm[p] : -1;
+    const float v = warp_row_d2(X, d, row, active ? perm[far_pos(best_a[s])] : 0, tile);
+    if (active) da[p] = v;
+    warp_far_max(best_b, s, active, active ? far_key(v, p) : 0ull);
   }
 }
 
-__global__ void side_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
-                            const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
-                            const int32_t* __restrict__ ne, const float* __restrict__ da,
-                            const unsigned long long* __restrict__ best_b,
-                            int32_t* __restrict__ side) {
-  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int s = ns[p], e = ne[p];
-    int v = 0;
-    if (e - s > leaf) {
-      const float db = row_d2(X, d, perm[p], perm[far_pos(best_b[s])]);
-      v = da[p] > db ? 1 : 0;                    // nearer to b: second half
-    }
-    side[p] = v;
+__global__ void __launch_bounds__(OR_T)
+side_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+            const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+            const int32_t* __restrict__ ne, const float* __restrict__ da,
+            const unsigned long long* __restrict__ best_b, int32_t* __restrict__ side) {
+  __shared__ RowTile tiles[OR_W];
+  RowTile& tile = tiles[warp_id()];
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+       b += stride) {
+    const int64_t p = b + lane_id();
+    int s = 0, e = 0;
+    if (p < npacked) { s = ns[p]; e = ne[p]; }
+    const bool active = p < npacked && e - s > leaf;
+    const int32_t row = active ? perm[p] : -1;
+    const float db = warp_row_d2(X, d, row, active ? perm[far_pos(best_b[s])] : 0, tile);
+    if (p < npacked) side[p] = active && da[p] > db ? 1 : 0;   // nearer to b: second half
   }
 }
 
@@ -298,27 +342,49 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
 
 // second assignment: the nearer of the two side means (ties to side 0); a side left empty by the
 // first assignment keeps it
-__global__ void reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
-                                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
-                                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                                const double* __restrict__ acc, int32_t* __restrict__ side) {
-  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int st = ns[p];
-    if (ne[p] - st <= leaf) continue;
-    const double* a = acc + S[st] * (2 * d + 2);
-    const double n0 = a[2 * d], n1 = a[2 * d + 1];
-    if (n0 == 0.0 || n1 == 0.0) continue;
-    const double i0 = 1.0 / n0, i1 = 1.0 / n1;
-    const float* x = X + int64_t(perm[p]) * d;
-    double d0 = 0.0, d1 = 0.0;
-    for (int t = 0; t < d; ++t) {
-      const double v = x[t];
-      const double u0 = v - a[t] * i0, u1 = v - a[d + t] * i1;
-      d0 += u0 * u0;
-      d1 += u1 * u1;
+__global__ void __launch_bounds__(OR_T)
+reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+                const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+                const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
+                const double* __restrict__ acc, int32_t* __restrict__ side) {
+  __shared__ RowTile tiles[OR_W];
+  RowTile& tile = tiles[warp_id()];
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+       b += stride) {
+    const int64_t p = b + lane_id();
+    const double* a = nullptr;
+    double i0 = 0.0, i1 = 0.0;
+    int32_t row = -1;
+    if (p < npacked) {
+      const int st = ns[p];
+      if (ne[p] - st > leaf) {
+        a = acc + S[st] * (2 * d + 2);
+        const double n0 = a[2 * d], n1 = a[2 * d + 1];
+        if (n0 != 0.0 && n1 != 0.0) {
+          i0 = 1.0 / n0;
+          i1 = 1.0 / n1;
+          row = perm[p];
+        }
+      }
     }
-    side[p] = d0 > d1 ? 1 : 0;
+    const unsigned act = __ballot_sync(FULL, row >= 0);
+    if (act == 0) continue;                  // warp-uniform
+    double d0 = 0.0, d1 = 0.0;
+    for (int c = 0; c < d; c += 32) {
+      stage_rows(X, d, c, row, tile);
+      if (row >= 0) {
+        const int tn = min(32, d - c);
+        for (int j = 0; j < tn; ++j) {
+          const double v = tile[lane_id()][j];
+          const double u0 = v - a[c + j] * i0, u1 = v - a[d + c + j] * i1;
+          d0 += u0 * u0;
+          d1 += u1 * u1;
+        }
+      }
+      __syncwarp();
+    }
+    if (row >= 0) side[p] = d0 > d1 ? 1 : 0;
   }
 }
 
