@@ -32,7 +32,7 @@ extern "C" {
 #define MSC_ERR_WORKSPACE       2   /* workspace smaller than *_workspace_bytes() (MemoryError) */
 #define MSC_ERR_TIMEOUT         3   /* a device-side wait hit its bound (RuntimeError)          */
 #define MSC_ERR_CUDA            4   /* a CUDA runtime call failed (RuntimeError)                */
-#define MSC_ERR_UNSUPPORTED     5   /* valid request this build does not handle (NotImplemented)*/
+#define MSC_ERR_UNSUPPORTED     5   /* valid request the library does not handle (NotImplemented)*/
 
 /* metric (the reference accepts only euclidean, pp.py:768-769) */
 #define MSC_METRIC_EUCLIDEAN    0

@@ -13,11 +13,15 @@ This package restates, in NumPy/SciPy on the host, what the reference computes f
 * ``graph.distances_csr`` — the distances graph exactly as ``neighbors.py:755-759`` builds it.
 * ``graph.gauss_connectivities`` — the locally scaled Gaussian kernel (Haghverdi et al. 2016)
   for ``method='gauss'``, which the reference does not implement.
+* ``bbknn.bbknn`` / ``bbknn.trim_graph`` — the batch-balanced graph of ``pp.bbknn``
+  (``pp.py:809-833`` → ``neighbors.py:491-559``, trimming ``neighbors.py:465-488``), the next
+  caller of the same kNN and fuzzy-set steps.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import this
 package, and only as the checker.  The product (``metal-singlecell_b200/``) never imports it.
 
-Pinning: the kNN restatement is pinned by the reference's own known-answer tests
+Pinning: ``bbknn.trim_graph`` equals the reference's own ``_trim_graph`` bit for bit on the
+fixtures of ``tests/golden/make_golden.py``.  The kNN restatement is pinned by the reference's own known-answer tests
 (``tests/test_postfix_fixes.py:108-121``, 500×20 recall vs NumPy brute force;
 ``tests/test_postfix_fixes.py:197-207``, coincident points stay finite) and by fixtures generated
 from the reference's NumPy-expressible code (``tests/golden/make_golden.py``).  Connectivity

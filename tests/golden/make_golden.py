@@ -12,8 +12,12 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
 * the vendored mlx-vis ``UMAP._fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271) on an
   exact kNN graph: the per-row ρ and the bisection σ are captured from its ``mx.eval`` calls.
 
+* ``neighbors._trim_graph`` (neighbors.py:465-488), pure SciPy, run as is on batch-balanced
+  connectivities built by the oracle (the reference test's tiny-batch input,
+  tests/test_postfix_fixes.py:186-193, and a 3-batch mixture), at several trims.
+
 Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
-Writes tests/golden/reference_knn_500x20.npz and tests/golden/reference_rho_sigma.npz.
+Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz and reference_trim.npz.
 """
 import sys
 import types
@@ -99,6 +103,30 @@ def main():
     sigma = np.asarray([c[0] for c in mx.captured if c[0].shape == rho.shape][-1], np.float32)
     np.savez_compressed(OUT / "reference_rho_sigma.npz", X=Xg, knn_idx=idx, knn_dist=dist,
                         rho=rho, sigma=sigma, k=k)
+
+    # the reference's _trim_graph on batch-balanced connectivities: the reference test's own
+    # tiny-batch input (tests/test_postfix_fixes.py:186-193) and a 3-batch mixture, several trims
+    from oracle import bbknn as obb
+    r0 = np.random.default_rng(0)
+    cases = [(r0.standard_normal((60, 10)).astype(np.float32),
+              np.array(["a"] * 40 + ["b"] * 2 + ["c"] * 18), 3, (0, 4, 6, 30)),
+             (synth.gaussian_mixture(500, 16, 5, seed=23),
+              np.random.default_rng(29).choice(np.array(["p", "q", "r"]), 500), 5, (8, 12, 20, 150))]
+    trim_out = {}
+    for c, (Xc, bc, kwb, trims) in enumerate(cases):
+        _, _, K, inter = obb.bbknn(Xc, bc, neighbors_within_batch=kwb)
+        conn = inter["untrimmed"].tocsr()
+        trim_out[f"c{c}_indptr"] = conn.indptr.astype(np.int64)
+        trim_out[f"c{c}_indices"] = conn.indices.astype(np.int64)
+        trim_out[f"c{c}_data"] = conn.data.astype(np.float32)
+        trim_out[f"c{c}_trims"] = np.asarray(trims, np.int64)
+        for t in trims:
+            R = ref_nb._trim_graph(conn, t).tocsr()
+            R.sort_indices()
+            trim_out[f"c{c}_t{t}_indptr"] = R.indptr.astype(np.int64)
+            trim_out[f"c{c}_t{t}_indices"] = R.indices.astype(np.int64)
+            trim_out[f"c{c}_t{t}_data"] = R.data.astype(np.float32)
+    np.savez_compressed(OUT / "reference_trim.npz", n_cases=len(cases), **trim_out)
     print("wrote", sorted(p.name for p in OUT.glob("reference_*.npz")))
 
 

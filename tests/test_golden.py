@@ -8,13 +8,18 @@
 * mlx-vis ``_fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271): ρ must be identical and σ
   within the bisection tolerance (1e-5 relative on the sum ⇒ ~1e-5 on σ), wherever that function
   and umap-learn share semantics (ρ > 1e-8, no mean-distance floor).
+* ``_trim_graph`` (neighbors.py:465-488) on batch-balanced connectivities at several trims:
+  the oracle's ``trim_graph`` must give the same CSR bit for bit.
 """
 from pathlib import Path
 
 import numpy as np
 import pytest
 
+import scipy.sparse as sp
+
 import oracle
+from oracle import bbknn as obb
 
 G = Path(__file__).resolve().parent / "golden"
 
@@ -43,3 +48,21 @@ def test_oracle_vs_reference_rho_sigma():
     assert np.array_equal(rho, g["rho"])
     rel = np.abs(sigma - g["sigma"]) / g["sigma"]
     assert rel.max() < 1e-5
+
+
+def test_oracle_trim_vs_reference():
+    g = np.load(G / "reference_trim.npz")
+    checked = 0
+    for c in range(int(g["n_cases"])):
+        ip = g[f"c{c}_indptr"]
+        n = ip.size - 1
+        A = sp.csr_matrix((g[f"c{c}_data"], g[f"c{c}_indices"], ip), shape=(n, n))
+        for t in g[f"c{c}_trims"]:
+            R = obb.trim_graph(A, int(t))
+            assert R.data.dtype == np.float32
+            np.testing.assert_array_equal(R.indptr, g[f"c{c}_t{t}_indptr"])
+            np.testing.assert_array_equal(R.indices, g[f"c{c}_t{t}_indices"])
+            np.testing.assert_array_equal(R.data, g[f"c{c}_t{t}_data"])
+            checked += 1
+    # the cases trim hard, lightly and not at all
+    assert checked == 8

@@ -4,8 +4,8 @@ The bar is bit-exact: neighbour indices and their order, float32 distances, the 
 the connectivities CSR (structure and float32 values) must equal the oracle's.  The design makes
 that possible: candidates are certified or re-scanned, the boundary is resolved in FP64 with the
 oracle's (distance, index) order, and the fuzzy-set arithmetic is fixed to the same float32
-operations (see oracle/graph.py).  The north-star tolerance (1e-5 relative on distances and
-connectivities) is therefore checked in its strongest form, equality.
+operations (see oracle/graph.py).  The stated tolerance of the path (1e-5 relative on distances
+and connectivities) is therefore checked in its strongest form, equality.
 """
 import numpy as np
 import pytest

@@ -1,6 +1,6 @@
 """The CPU oracle against the reference's own known answers and against independent restatements.
 
-Pins (the reference's tests for this path):
+Pins (the reference's own tests and code for this path):
 * tests/test_postfix_fixes.py:108-121 — 500×20 N(0,1), default_rng(0), k ∈ {15, 33, 50}: recall
   ≥ 0.99 against NumPy brute force (`np.argsort(D)[:, :k]`); the oracle must be exact (1.0);
 * tests/test_postfix_fixes.py:197-207 — 60×10 + 5 exact duplicates, k=10: finite connectivities;
