@@ -65,12 +65,13 @@ def knn_cross(Q: np.ndarray, B: np.ndarray, kk: int, chunk_elems: int = 1 << 24)
 
 
 def trim_graph(conn: sp.spmatrix, trim: int | None) -> sp.csr_matrix:
-    """Keep the edges (i, j) with value ≥ θ_i and ≥ θ_j; θ_i = the trim-th largest value of
-    row i if it holds more than ``trim`` entries, else 0.  ``trim`` None or ≤ 0: unchanged."""
+    """Keep the non-zero entries (i, j) with value ≥ θ_i and ≥ θ_j; θ_i = the trim-th largest
+    value of row i (its stored entries, explicit zeros included) if it stores more than ``trim``
+    entries, else 0.  ``trim`` None or ≤ 0: unchanged.  (The reference zeroes the entries below
+    the thresholds and eliminates zeros, which also drops stored zeros.)"""
     A = sp.csr_matrix(conn, copy=True)
     if trim is None or trim <= 0:
         return A
-    A.sum_duplicates()
     n = A.shape[0]
     cnt = np.diff(A.indptr)
     theta = np.zeros(n, np.float64)
@@ -78,7 +79,7 @@ def trim_graph(conn: sp.spmatrix, trim: int | None) -> sp.csr_matrix:
         row = A.data[A.indptr[i]:A.indptr[i + 1]]
         theta[i] = np.partition(row, row.size - trim)[row.size - trim]
     rows = np.repeat(np.arange(n), cnt)
-    keep = (A.data >= theta[rows]) & (A.data >= theta[A.indices])
+    keep = (A.data >= theta[rows]) & (A.data >= theta[A.indices]) & (A.data != 0)
     out = sp.csr_matrix((A.data[keep], (rows[keep], A.indices[keep])), shape=A.shape,
                         dtype=A.dtype)
     out.sort_indices()

@@ -14,7 +14,8 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
 
 * ``neighbors._trim_graph`` (neighbors.py:465-488), pure SciPy, run as is on batch-balanced
   connectivities built by the oracle (the reference test's tiny-batch input,
-  tests/test_postfix_fixes.py:186-193, and a 3-batch mixture), at several trims.
+  tests/test_postfix_fixes.py:186-193, and a 3-batch mixture) and on a random symmetric graph
+  that stores explicit zeros, at several trims.
 
 Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
 Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz and reference_trim.npz.
@@ -126,7 +127,23 @@ def main():
             trim_out[f"c{c}_t{t}_indptr"] = R.indptr.astype(np.int64)
             trim_out[f"c{c}_t{t}_indices"] = R.indices.astype(np.int64)
             trim_out[f"c{c}_t{t}_data"] = R.data.astype(np.float32)
-    np.savez_compressed(OUT / "reference_trim.npz", n_cases=len(cases), **trim_out)
+    # and a symmetric random graph that stores explicit zeros (the reference drops them)
+    import scipy.sparse as sp
+    Z = sp.random(300, 300, density=0.08, random_state=2, format="csr", dtype=np.float32)
+    Z = (Z + Z.T).tocsr()
+    Z.data[np.random.default_rng(1).random(Z.nnz) < 0.1] = 0.0
+    c = len(cases)
+    trim_out[f"c{c}_indptr"] = Z.indptr.astype(np.int64)
+    trim_out[f"c{c}_indices"] = Z.indices.astype(np.int64)
+    trim_out[f"c{c}_data"] = Z.data.astype(np.float32)
+    trim_out[f"c{c}_trims"] = np.asarray((3, 5, 8, 12), np.int64)
+    for t in (3, 5, 8, 12):
+        R = ref_nb._trim_graph(Z, t).tocsr()
+        R.sort_indices()
+        trim_out[f"c{c}_t{t}_indptr"] = R.indptr.astype(np.int64)
+        trim_out[f"c{c}_t{t}_indices"] = R.indices.astype(np.int64)
+        trim_out[f"c{c}_t{t}_data"] = R.data.astype(np.float32)
+    np.savez_compressed(OUT / "reference_trim.npz", n_cases=len(cases) + 1, **trim_out)
     print("wrote", sorted(p.name for p in OUT.glob("reference_*.npz")))
 
 

@@ -64,5 +64,5 @@ def test_oracle_trim_vs_reference():
             np.testing.assert_array_equal(R.indices, g[f"c{c}_t{t}_indices"])
             np.testing.assert_array_equal(R.data, g[f"c{c}_t{t}_data"])
             checked += 1
-    # the cases trim hard, lightly and not at all
-    assert checked == 8
+    # the cases trim hard, lightly and not at all, and drop stored zeros
+    assert checked == 12
