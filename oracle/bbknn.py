@@ -43,24 +43,65 @@ from .graph import smooth_knn_dist, membership_strengths, fuzzy_union
 from .knn import sq_dist_f64
 
 
-def knn_cross(Q: np.ndarray, B: np.ndarray, kk: int, chunk_elems: int = 1 << 24):
+def _cross_full(Q32, B32, rows, kk):
+    """Full FP64 scan of B for a few query rows, ordered by (d², B index)."""
+    cols = np.arange(B32.shape[0])
+    oi = np.empty((rows.size, kk), np.int64)
+    od = np.empty((rows.size, kk), np.float64)
+    for r, i in enumerate(rows):
+        D = sq_dist_f64(Q32[i:i + 1], B32)[0]
+        o = np.lexsort((cols, D))[:kk]
+        oi[r] = o
+        od[r] = D[o]
+    return oi, od
+
+
+def knn_cross(Q: np.ndarray, B: np.ndarray, kk: int, chunk_elems: int = 1 << 25):
     """Exact kk nearest rows of ``B`` for every row of ``Q``: ``(idx int64 (m,kk) into B,
-    d2 float64 (m,kk), dist float32 (m,kk))``, ordered by (FP64 squared distance, B index)."""
+    d2 float64 (m,kk), dist float32 (m,kk))``, ordered by (FP64 squared distance, B index).
+
+    An FP64 Gram form |q|² + |b|² − 2q·b pre-selects kk+8 candidates per row; their distances are
+    recomputed as FP64 sums of squared differences in dimension order, and a row whose kk-th
+    recomputed value does not clear the pre-selection threshold by the Gram form's error bound
+    is scanned in full."""
     Q32 = np.ascontiguousarray(Q, np.float32)
     B32 = np.ascontiguousarray(B, np.float32)
     m, nb = Q32.shape[0], B32.shape[0]
+    d = Q32.shape[1]
     if not 0 <= kk <= nb:
         raise ValueError(f"kk={kk} must be in [0, {nb}]")
     idx = np.empty((m, kk), np.int64)
     d2 = np.empty((m, kk), np.float64)
-    chunk = int(max(1, min(1024, chunk_elems // max(nb * Q32.shape[1], 1))))
-    cols = np.arange(nb)
+    if kk == 0 or m == 0:
+        return idx, d2, np.sqrt(d2).astype(np.float32)
+    Q64, B64 = Q32.astype(np.float64), B32.astype(np.float64)
+    sq_q = np.einsum("ij,ij->i", Q64, Q64)
+    sq_b = np.einsum("ij,ij->i", B64, B64)
+    sbmax = float(sq_b.max())
+    eps64 = 64.0 * (d + 8) * 2.0 ** -53
+    m_extra = min(nb, kk + 8)
+    chunk = int(max(8, min(2048, chunk_elems // max(nb, 1))))
     for s in range(0, m, chunk):
         e = min(s + chunk, m)
-        D = sq_dist_f64(Q32[s:e], B32)
-        o = np.lexsort((np.broadcast_to(cols, D.shape), D), axis=1)[:, :kk]
-        idx[s:e] = o
-        d2[s:e] = np.take_along_axis(D, o, axis=1)
+        V = sq_q[s:e, None] + sq_b[None, :] - 2.0 * (Q64[s:e] @ B64.T)
+        if m_extra < nb:
+            cand = np.argpartition(V, m_extra - 1, axis=1)[:, :m_extra]
+            thr = np.take_along_axis(V, cand, axis=1).max(axis=1)
+        else:
+            cand = np.broadcast_to(np.arange(nb), (e - s, nb))
+            thr = np.full(e - s, np.inf)
+        D = sq_dist_f64(Q32[s:e], B32[cand])
+        o = np.lexsort((cand, D), axis=1)
+        ci = np.take_along_axis(cand, o, axis=1)[:, :kk]
+        cd = np.take_along_axis(D, o, axis=1)[:, :kk]
+        err = eps64 * (sq_q[s:e] + sbmax)
+        bad = np.flatnonzero(~(cd[:, kk - 1] < thr - 2.0 * err))
+        if bad.size:
+            bi, bd = _cross_full(Q32, B32, s + bad, kk)
+            ci[bad] = bi
+            cd[bad] = bd
+        idx[s:e] = ci
+        d2[s:e] = cd
     return idx, d2, np.sqrt(d2).astype(np.float32)
 
 
