@@ -125,6 +125,47 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class Replicas:
+    """One process per GPU, each building its own full graph (the path runs on one GPU, so the
+    ranks are independent replicas with no collective on the data path): a barrier on both sides
+    of the timed region, per-rank times combined as their max, and the whole-job rate
+    world × cells / time.  RANK / WORLD_SIZE / MASTER_* come from the environment (torchrun)."""
+
+    def __init__(self, backend: str = "nccl", device=None, timeout_s: float = 600.0):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.backend = backend
+        self.device = device
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            kw = {"device_id": device} if backend == "nccl" and device is not None else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        dev = self.device if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rate(self, cells_per_rank: int, seconds: float) -> float:
+        return self.world * cells_per_rank / seconds
+
+    def close(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
 def cpu_baseline(X, k, metric, budget_s: float = 15.0):
     """Oracle port on the host: exact kNN of a seeded sample of query rows against the whole
     embedding, plus the per-row ρ/σ and membership stages; cells/s = rows / time."""
@@ -179,17 +220,13 @@ def run_reference(args):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     from msc_b200 import neighbors as nbm, _lib
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    reps = Replicas("nccl", dev)
+    world, rank = reps.world, reps.rank
     lib = _lib.load()
 
     X, p, desc = workload(args.workload, args.n)
@@ -205,16 +242,7 @@ def run_ours(args):
         return nbm.neighbors_device(Xd, k, metric=metric, method=method, precision=precision,
                                     kprime=kprime, workspace=ws, out=out)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     for _ in range(args.warmup):
         step()
@@ -243,7 +271,7 @@ def run_ours(args):
         barrier()
     launches = lib.msc_launch_count() - launches0
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = world * n / (ms / 1000.0)
+    value = reps.rate(n, ms / 1000.0)
 
     # per-stage times of one profiled step (events on the launching stream)
     lib.msc_profile_enable(1)
@@ -349,7 +377,7 @@ def run_ours(args):
     barrier()
     h2d = X.nbytes
     d2h = 8 + 2 * (n + 1) * 8 + n * m * 8 + nnzs[-1] * 8
-    e2e = {"value": world * n / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
+    e2e = {"value": reps.rate(n, e2e_s), "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_s}
 
     # the plain FP32 GPU form of the same graph (the comparison the metric names)
@@ -363,7 +391,7 @@ def run_ours(args):
         f1.record(st)
         torch.cuda.synchronize()
         fms = max_over_ranks(f0.elapsed_time(f1))
-        fp32 = {"value": world * n / (fms / 1000.0), "unit": "cells/s", "ms_per_step": fms,
+        fp32 = {"value": reps.rate(n, fms / 1000.0), "unit": "cells/s", "ms_per_step": fms,
                 "speedup_of_headline": fms / ms}
 
     cpu = None
@@ -389,8 +417,7 @@ def run_ours(args):
                           "conn_nnz": int(stats[_lib.STAT_CONN_NNZ])},
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    reps.close()
 
 
 def run_batch(args):
