@@ -8,7 +8,6 @@ Lanes (mirroring the reference's CPU / GPU split, tests/conftest.py:19-43 there)
 import sys
 from pathlib import Path
 
-import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
