@@ -14,6 +14,8 @@
 
 #include <cstdlib>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kernels.cuh"
 
 namespace msc {
@@ -49,7 +51,40 @@ StageTimer& timer() {
 
 bool profiling_enabled() { return timer().on; }
 
+// NVTX ranges over the same stages, on the host timeline (the enqueue of each stage), for users
+// of Nsight tools; with no tool attached the calls return at once.  A mark ends the previous
+// stage's range and opens the next one's; the entry points close what is left open.
+namespace {
+const char* const kStageNames[] = {"msc: prep",
+                                   "msc: near pass",
+                                   "msc: pruning plan",
+                                   "msc: candidates",
+                                   "msc: re-rank + FP64 scan",
+                                   "msc: CSR + rho/sigma + memberships",
+                                   "msc: fuzzy union"};
+constexpr int N_STAGE_NAMES = int(sizeof(kStageNames) / sizeof(kStageNames[0]));
+thread_local nvtxRangeId_t g_range = 0;
+thread_local bool g_range_open = false;
+
+void stage_range_close() {
+  if (g_range_open) {
+    nvtxRangeEnd(g_range);
+    g_range_open = false;
+  }
+}
+
+// closes the open stage range when an entry point returns, on every path
+struct StageRangeGuard {
+  ~StageRangeGuard() { stage_range_close(); }
+};
+}  // namespace
+
 void stage_mark(cudaStream_t st, int stage) {
+  stage_range_close();
+  if (stage >= 0 && stage < N_STAGE_NAMES) {
+    g_range = nvtxRangeStartA(kStageNames[stage]);
+    g_range_open = true;
+  }
   StageTimer& t = timer();
   if (!t.on || stage < 0 || stage >= MAX_MARKS) return;
   if (!t.ev[stage] && cudaEventCreate(&t.ev[stage]) != cudaSuccess) return;
@@ -540,6 +575,7 @@ size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, 
 int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
             int32_t precision, int32_t kprime, int32_t* knn_idx_dev, float* knn_dist_dev,
             int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  StageRangeGuard range_guard;
   Problem P;
   MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
   if (bad_ptr(X_dev, "X") || bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
@@ -574,6 +610,7 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
                   float* dist_data_dev, int64_t* conn_indptr_dev, int32_t* conn_indices_dev,
                   float* conn_data_dev, int64_t* stats_dev, void* workspace,
                   size_t workspace_bytes, void* stream) {
+  StageRangeGuard range_guard;
   Problem P;
   MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
   if (method != MSC_METHOD_UMAP && method != MSC_METHOD_GAUSS) {
@@ -677,6 +714,7 @@ int msc_batched_knn(const float* X_dev, const int64_t* offsets_host, int32_t n_s
                     int32_t k, int32_t metric, int32_t precision, int32_t kprime,
                     int32_t tile_config, int32_t* knn_idx_dev, float* knn_dist_dev,
                     int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  StageRangeGuard range_guard;
   if (!offsets_host || n_samples < 1) { set_error("offsets/n_samples invalid"); return MSC_ERR_INVALID_ARG; }
   Problem P;
   MSC_TRY(make_problem(P, offsets_host[n_samples], d, k, metric, precision, kprime, offsets_host,
