@@ -19,6 +19,7 @@ from __future__ import annotations
 import collections
 import threading
 import time
+from concurrent.futures import CancelledError
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -27,7 +28,7 @@ from . import _lib
 from .neighbors import _torch, _ids, DEFAULT_PRECISION
 
 
-@dataclass
+@dataclass(eq=False)                   # requests compare by identity
 class Request:
     X: object                      # host numpy (n, d) float32, or a CUDA tensor
     n_neighbors: int = 15
@@ -100,6 +101,22 @@ class GraphServer:
             self.pending.append(req)
         return req
 
+    def cancel(self, req: Request) -> bool:
+        """Withdraw a request that has not been admitted yet: it completes at once with a
+        ``CancelledError`` and never reaches the GPU.  False if it was already admitted or done."""
+        with self.lock:
+            for i, r in enumerate(self.pending):
+                if r is req:
+                    del self.pending[i]
+                    break
+            else:
+                return False
+            req.error = CancelledError(f"request {req.rid} cancelled before admission")
+            req.done = self.now()
+            self.completed.append(req)
+        req.event.set()
+        return True
+
     def close(self):
         self._stop = True
         self._thread.join()
@@ -160,15 +177,20 @@ class GraphServer:
                                      req.metric, req.method, req.precision)
                 if need < 0 or need > self.budget:
                     with self.lock:
+                        if not self.pending or self.pending[0] is not req:
+                            continue           # cancelled meanwhile
                         self.pending.popleft()
-                    req.error = ValueError(f"request needs {need} bytes > budget {self.budget}")
-                    req.done = self.now()
-                    self.completed.append(req)
+                        req.error = ValueError(f"request needs {need} bytes > budget "
+                                               f"{self.budget}")
+                        req.done = self.now()
+                        self.completed.append(req)
                     req.event.set()
                     continue
                 if self.in_use + need > self.budget:
                     break                      # wait for memory to free up (FIFO admission)
                 with self.lock:
+                    if not self.pending or self.pending[0] is not req:
+                        continue               # cancelled meanwhile
                     self.pending.popleft()
                 slot = self.free_slots.popleft()
                 self.in_use += need
