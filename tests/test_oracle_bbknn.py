@@ -103,3 +103,27 @@ def test_trim_keeps_symmetry_and_respects_thresholds():
     for t in (None, 0, 10 * K):
         T = obb.trim_graph(A, t)
         assert (T != A).nnz == 0
+
+
+def test_edge_batches():
+    rng = np.random.default_rng(21)
+    X = rng.standard_normal((200, 5)).astype(np.float32)
+    # a one-cell batch: every row holds that cell; its own row holds only itself from its batch
+    batch = np.array([0] * 199 + [1])
+    _, conn, K, inter = obb.bbknn(X, batch, neighbors_within_batch=4)
+    assert K == 4 + 1 and inter["kk"].tolist() == [4, 1]
+    assert all(199 in inter["idx"][i].tolist() for i in range(200))
+    assert conn.nnz > 0 and np.isfinite(conn.data).all()
+    # neighbors_within_batch = 1: a cell of batch b gets itself from b
+    batch = rng.integers(0, 3, 200)
+    _, _, K, inter = obb.bbknn(X, batch, neighbors_within_batch=1)
+    assert K == 3 and (inter["idx"][:, 0] == np.arange(200)).all()
+    # 40 batches of 5 cells, 3 each: K = 120 (within the 128-entry limit of the GPU path)
+    batch = np.repeat(np.arange(40), 5)
+    _, conn, K, inter = obb.bbknn(X, batch, neighbors_within_batch=3)
+    assert K == 120 and inter["idx"].shape == (200, 120)
+    assert (np.diff(inter["dist"], axis=1) >= 0).all()
+    # labels of any sortable type give the same graph as their codes
+    labels = np.array([f"s{b:02d}" for b in batch])
+    _, conn2, _, _ = obb.bbknn(X, labels, neighbors_within_batch=3)
+    assert (conn != conn2).nnz == 0
