@@ -162,6 +162,48 @@ def graph_to_host(res: dict, n: int, k: int):
     return dist, conn
 
 
+def csr_device(res: dict, n: int, which: str = "connectivities"):
+    """``(indptr int64 (n+1,), indices int32 (nnz,), data float32 (nnz,))`` of a device result of
+    ``neighbors_device`` (``which`` = "connectivities" or "distances"), as views of its buffers
+    trimmed to the valid length.  Reading that length is one 8-byte device-to-host copy."""
+    if which not in ("connectivities", "distances"):
+        raise ValueError(f"which={which!r} must be 'connectivities' or 'distances'")
+    pre = "conn_" if which == "connectivities" else "dist_"
+    indptr = res[pre + "indptr"]
+    nnz = int(indptr[n].item())
+    return indptr, res[pre + "indices"][:nnz], res[pre + "data"][:nnz]
+
+
+def to_torch_csr(res: dict, n: int, which: str = "connectivities"):
+    """The graph as a ``torch.sparse_csr_tensor`` on the result's device, sharing its buffers:
+    GPU consumers take it without a host round trip."""
+    import torch
+    indptr, indices, data = csr_device(res, n, which)
+    if indices.numel() < 2 ** 31:          # 32-bit row pointers: the column indices stay shared
+        indptr = indptr.to(torch.int32)
+    else:
+        indices = indices.to(torch.int64)
+    import warnings
+    with warnings.catch_warnings():                # torch's notes on sparse CSR support
+        warnings.filterwarnings("ignore", message="Sparse invariant checks are implicitly")
+        warnings.filterwarnings("ignore", message="Sparse CSR tensor support is in beta")
+        return torch.sparse_csr_tensor(indptr, indices, data, size=(n, n),
+                                       check_invariants=False)
+
+
+def graph_arrays(res: dict, n: int, which: str = "connectivities") -> dict:
+    """The layout of the reference's graph container (``Graph.from_scipy``,
+    graph/csr_graph.py:15-40: ``indptr``, ``indices``, ``weights``, ``edge_src`` = the source row of
+    every edge, ``n``) built on the device from a ``neighbors_device`` result, for the graph
+    consumers (Leiden, UMAP epochs) that the reference feeds through a host CSR."""
+    import torch
+    indptr, indices, data = csr_device(res, n, which)
+    deg = indptr[1:] - indptr[:-1]
+    src = torch.repeat_interleave(torch.arange(n, device=indptr.device, dtype=torch.int32), deg)
+    return {"indptr": indptr.to(torch.int32), "indices": indices, "weights": data,
+            "edge_src": src, "n": n}
+
+
 def neighbors(X_pca: np.ndarray, n_neighbors: int = 15, random_state: int = 0,
               approx: bool | None = None, *, metric: str = "euclidean", method: str = "umap",
               precision: str = DEFAULT_PRECISION, kprime: int = 0, device=None):
