@@ -12,13 +12,17 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
 * the vendored mlx-vis ``UMAP._fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271) on an
   exact kNN graph: the per-row ρ and the bisection σ are captured from its ``mx.eval`` calls.
 
+* ``neighbors.neighbors`` (neighbors.py:727-760) with the exact oracle's kNN lists in place of its
+  Metal kNN and the oracle's fuzzy set in place of umap-learn: the distances CSR its own code
+  builds (neighbors.py:755-759), on an input with duplicate cells (stored zero distances);
 * ``neighbors._trim_graph`` (neighbors.py:465-488), pure SciPy, run as is on batch-balanced
   connectivities built by the oracle (the reference test's tiny-batch input,
   tests/test_postfix_fixes.py:186-193, and a 3-batch mixture) and on a random symmetric graph
   that stores explicit zeros, at several trims.
 
 Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
-Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz and reference_trim.npz.
+Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz, reference_distances_csr.npz
+and reference_trim.npz.
 """
 import sys
 import types
@@ -104,6 +108,41 @@ def main():
     sigma = np.asarray([c[0] for c in mx.captured if c[0].shape == rho.shape][-1], np.float32)
     np.savez_compressed(OUT / "reference_rho_sigma.npz", X=Xg, knn_idx=idx, knn_dist=dist,
                         rho=rho, sigma=sigma, k=k)
+
+    # the reference's own neighbors() (neighbors.py:727-760) builds the distances graph from the
+    # kNN lists: its kNN engine (Metal) and umap-learn are absent, so the lists come from the
+    # exact oracle and the fuzzy set from the oracle's restatement (its output is not stored:
+    # that would pin the oracle against itself); the distances CSR is the reference's code.
+    # Input with exact duplicates, so that zero distances are stored explicitly.
+    Xd = np.random.default_rng(5).standard_normal((300, 12)).astype(np.float32)
+    Xd[250:260] = Xd[0:10]
+    kd = 10
+
+    def _knn_exact(X, k, random_state=0, approx=None):
+        i, _, dd = oracle.knn_exact(X, k)
+        return i, dd
+
+    def _fss(X, n_neighbors, random_state, metric, knn_indices, knn_dists, **kw):
+        sg, rh = oracle.smooth_knn_dist(knn_dists, float(n_neighbors))
+        w = oracle.membership_strengths(knn_indices, knn_dists, sg, rh)
+        return oracle.fuzzy_union(knn_indices, w, knn_indices.shape[0]), sg, rh
+
+    umap_pkg, umap_mod = types.ModuleType("umap"), types.ModuleType("umap.umap_")
+    umap_mod.fuzzy_simplicial_set = _fss
+    umap_pkg.umap_ = umap_mod
+    sys.modules.setdefault("umap", umap_pkg)
+    sys.modules.setdefault("umap.umap_", umap_mod)
+    saved_knn = ref_nb._knn
+    ref_nb._knn = _knn_exact
+    try:
+        Dref, _ = ref_nb.neighbors(Xd, kd)
+    finally:
+        ref_nb._knn = saved_knn
+    Dref = Dref.tocsr()
+    ki, _, kdist = oracle.knn_exact(Xd, kd)
+    np.savez_compressed(OUT / "reference_distances_csr.npz", X=Xd, k=kd, knn_idx=ki,
+                        knn_dist=kdist, indptr=Dref.indptr.astype(np.int64),
+                        indices=Dref.indices.astype(np.int64), data=Dref.data)
 
     # the reference's _trim_graph on batch-balanced connectivities: the reference test's own
     # tiny-batch input (tests/test_postfix_fixes.py:186-193) and a 3-batch mixture, several trims

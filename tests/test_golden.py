@@ -8,6 +8,9 @@
 * mlx-vis ``_fuzzy_simplicial_set`` (_vendor/mlx_vis/umap.py:199-271): ρ must be identical and σ
   within the bisection tolerance (1e-5 relative on the sum ⇒ ~1e-5 on σ), wherever that function
   and umap-learn share semantics (ρ > 1e-8, no mean-distance floor).
+* ``neighbors`` (neighbors.py:727-760) with the exact oracle's lists standing in for its Metal
+  kNN: the distances CSR its own lines build (neighbors.py:755-759) must equal the oracle's
+  ``distances_csr`` bit for bit, stored zero distances of duplicate cells included.
 * ``_trim_graph`` (neighbors.py:465-488) on batch-balanced connectivities at several trims:
   the oracle's ``trim_graph`` must give the same CSR bit for bit.
 """
@@ -66,3 +69,18 @@ def test_oracle_trim_vs_reference():
             checked += 1
     # the cases trim hard, lightly and not at all, and drop stored zeros
     assert checked == 12
+
+
+def test_oracle_distances_csr_vs_reference():
+    g = np.load(G / "reference_distances_csr.npz")
+    X, k = g["X"], int(g["k"])
+    n = X.shape[0]
+    idx, _, dist = oracle.knn_exact(X, k)
+    np.testing.assert_array_equal(idx, g["knn_idx"])
+    np.testing.assert_array_equal(dist, g["knn_dist"])
+    D = oracle.distances_csr(idx, dist, n)
+    assert D.data.dtype == np.float32
+    np.testing.assert_array_equal(D.indptr, g["indptr"])
+    np.testing.assert_array_equal(D.indices, g["indices"])
+    np.testing.assert_array_equal(D.data, g["data"])
+    assert D.nnz == n * (k - 1) and (D.data == 0).sum() == 20     # 10 duplicate pairs, both ways

@@ -92,6 +92,22 @@ def test_coincident_points(precision):
     assert np.isfinite(conn.data).all()
 
 
+@pytest.mark.parametrize("precision", ["fp16", "bf16x3"])
+def test_distances_csr_equals_reference_golden(precision):
+    """The distances CSR that the reference's own ``neighbors`` builds (neighbors.py:755-759) on
+    an input with 10 duplicated cells (tests/golden/reference_distances_csr.npz): stored zero
+    distances included, bit for bit."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "reference_distances_csr.npz")
+    X, k = g["X"], int(g["k"])
+    gi, gd, gdist, _, _ = run_graph(X, k, precision=precision)
+    np.testing.assert_array_equal(gi, g["knn_idx"].astype(np.int32))
+    np.testing.assert_array_equal(gd, g["knn_dist"])
+    np.testing.assert_array_equal(np.asarray(gdist.indptr, np.int64), g["indptr"])
+    np.testing.assert_array_equal(np.asarray(gdist.indices, np.int64), g["indices"])
+    np.testing.assert_array_equal(gdist.data, g["data"])
+
+
 def test_many_duplicates_hub():
     """A large group of identical cells: ties at distance 0 resolved by index, hub rows with
     in-degree above the warp tier of the fuzzy union."""
