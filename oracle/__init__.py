@@ -16,6 +16,9 @@ This package restates, in NumPy/SciPy on the host, what the reference computes f
 * ``bbknn.bbknn`` / ``bbknn.trim_graph`` — the batch-balanced graph of ``pp.bbknn``
   (``pp.py:809-833`` → ``neighbors.py:491-559``, trimming ``neighbors.py:465-488``), the next
   caller of the same kNN and fuzzy-set steps.
+* ``spatial.grid_knn`` / ``spatial.grid_radius`` / ``spatial.knn_edges`` — the uniform-grid
+  spatial kNN and radius search of 2-D/3-D coordinates (``neighbors.py:143-417``, used by
+  ``gr.py:186-255``), pinned against sklearn by the reference's own known-answer criteria.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import this
 package, and only as the checker.  The product (``metal-singlecell_b200/``) never imports it.

@@ -18,11 +18,16 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
 * ``neighbors._trim_graph`` (neighbors.py:465-488), pure SciPy, run as is on batch-balanced
   connectivities built by the oracle (the reference test's tiny-batch input,
   tests/test_postfix_fixes.py:186-193, and a 3-batch mixture) and on a random symmetric graph
-  that stores explicit zeros, at several trims.
+  that stores explicit zeros, at several trims;
+* ``gr.spatial_neighbors_knn`` / ``gr.spatial_neighbors_radius`` (gr.py:198-255) with the oracle's
+  grid kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
+  selection, FP64 edge lengths, the percentile / set_diag / transform tail and the per-library
+  blocks are the reference's code, on a jittered hex lattice, a 3-D point cloud and two
+  interleaved sections.
 
 Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
-Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz, reference_distances_csr.npz
-and reference_trim.npz.
+Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz, reference_distances_csr.npz,
+reference_trim.npz and reference_spatial.npz.
 """
 import sys
 import types
@@ -183,7 +188,81 @@ def main():
         trim_out[f"c{c}_t{t}_indices"] = R.indices.astype(np.int64)
         trim_out[f"c{c}_t{t}_data"] = R.data.astype(np.float32)
     np.savez_compressed(OUT / "reference_trim.npz", n_cases=len(cases) + 1, **trim_out)
+
+    # the reference's spatial graph builders (gr.py:198-255: edge selection, FP64 edge lengths,
+    # the percentile / set_diag / transform tail gr.py:81-104, per-library blocks gr.py:107-147)
+    # with the oracle's grid kNN and radius search standing in for the Metal grid kernels
+    from metalsinglecell import gr as ref_gr
+    from oracle import spatial as osp
+    spatial_golden(ref_nb, ref_gr, osp)
     print("wrote", sorted(p.name for p in OUT.glob("reference_*.npz")))
+
+
+def spatial_inputs():
+    """Seeded coordinate sets of the spatial cases (float64, as ``adata.obsm['spatial']``)."""
+    def lattice(side, jitter, seed):
+        r, c = np.divmod(np.arange(side * side), side)
+        xy = np.c_[c * 100.0 + (r % 2) * 50.0, r * 86.6]
+        return xy + np.random.default_rng(seed).normal(0, jitter, xy.shape)
+    lat = lattice(25, 1.0, 0)
+    vol = np.random.default_rng(3).uniform(0, 50, (800, 3))
+    two = np.vstack([lattice(16, 1.0, 1), lattice(16, 1.0, 2)])
+    perm = np.random.default_rng(4).permutation(two.shape[0])
+    lib = np.repeat([0, 2], 256)[perm]                   # category 1 unused; interleaved order
+    return {"lat": (lat, None), "vol": (vol, None), "two": (two[perm], lib)}
+
+
+SPATIAL_CASES = [
+    ("knn", "lat", {"n_neighs": 6}),
+    ("knn", "lat", {"n_neighs": 6, "set_diag": True}),
+    ("knn", "lat", {"n_neighs": 6, "transform": "spectral"}),
+    ("knn", "lat", {"n_neighs": 6, "transform": "cosine"}),
+    ("knn", "lat", {"n_neighs": 10, "percentile": 80.0}),
+    ("knn", "two", {"n_neighs": 6}),
+    ("knn", "vol", {"n_neighs": 8}),
+    ("radius", "lat", {"radius": 150.0}),
+    ("radius", "lat", {"radius": (90.0, 150.0)}),
+    ("radius", "lat", {"radius": 150.0, "percentile": 50.0}),
+    ("radius", "lat", {"radius": 150.0, "set_diag": True, "transform": "spectral"}),
+    ("radius", "two", {"radius": 120.0}),
+    ("radius", "vol", {"radius": 7.0}),
+]
+
+
+def spatial_golden(ref_nb, ref_gr, osp):
+    import json
+    import pandas as pd
+    out = {}
+    inputs = spatial_inputs()
+    for name, (xy, lib) in inputs.items():
+        out[f"{name}_coords"] = xy
+        if lib is not None:
+            out[f"{name}_library"] = lib
+    saved = ref_nb._knn_grid, ref_nb._radius_grid
+    ref_nb._knn_grid = lambda coords, k, min_n=4_000: osp.grid_knn(coords, k)
+    ref_nb._radius_grid = lambda coords, radius, min_radius=0.0: osp.grid_radius(
+        coords, radius, min_radius)
+    try:
+        for c, (kind, name, kw) in enumerate(SPATIAL_CASES):
+            xy, lib = inputs[name]
+            obs = pd.DataFrame(index=[str(i) for i in range(xy.shape[0])])
+            extra = {}
+            if lib is not None:
+                obs["library"] = pd.Categorical.from_codes(lib, ["s0", "s1", "s2"])
+                extra["library_key"] = "library"
+            adata = types.SimpleNamespace(obsm={"spatial": xy}, obs=obs, obsp={}, uns={})
+            fn = ref_gr.spatial_neighbors_knn if kind == "knn" else ref_gr.spatial_neighbors_radius
+            adj, dst = fn(adata, copy=True, **kw, **extra)
+            out[f"c{c}_case"] = np.array(json.dumps([kind, name, kw]))
+            for tag, M in (("adj", adj), ("dst", dst)):
+                M = M.tocsr()
+                M.sort_indices()
+                out[f"c{c}_{tag}_indptr"] = M.indptr.astype(np.int64)
+                out[f"c{c}_{tag}_indices"] = M.indices.astype(np.int64)
+                out[f"c{c}_{tag}_data"] = M.data
+    finally:
+        ref_nb._knn_grid, ref_nb._radius_grid = saved
+    np.savez_compressed(OUT / "reference_spatial.npz", n_cases=len(SPATIAL_CASES), **out)
 
 
 if __name__ == "__main__":

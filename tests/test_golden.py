@@ -13,6 +13,10 @@
   ``distances_csr`` bit for bit, stored zero distances of duplicate cells included.
 * ``_trim_graph`` (neighbors.py:465-488) on batch-balanced connectivities at several trims:
   the oracle's ``trim_graph`` must give the same CSR bit for bit.
+* ``gr.spatial_neighbors_knn`` / ``gr.spatial_neighbors_radius`` (gr.py:198-255) with the
+  oracle's grid search in place of the Metal grid kernels: the oracle's restatement of the
+  builders (edge selection, FP64 edge lengths, percentile / set_diag / transform, per-library
+  blocks) must give the same two CSR matrices bit for bit, 13 cases.
 """
 from pathlib import Path
 
@@ -84,3 +88,35 @@ def test_oracle_distances_csr_vs_reference():
     np.testing.assert_array_equal(D.indices, g["indices"])
     np.testing.assert_array_equal(D.data, g["data"])
     assert D.nnz == n * (k - 1) and (D.data == 0).sum() == 20     # 10 duplicate pairs, both ways
+
+
+def _spatial_cases():
+    import json
+    g = np.load(G / "reference_spatial.npz")
+    for c in range(int(g["n_cases"])):
+        kind, name, kw = json.loads(str(g[f"c{c}_case"]))
+        if "radius" in kw and isinstance(kw["radius"], list):
+            kw["radius"] = tuple(kw["radius"])
+        lib = g[f"{name}_library"] if f"{name}_library" in g else None
+        yield c, kind, g[f"{name}_coords"], lib, kw, g
+
+
+def test_oracle_spatial_graphs_vs_reference():
+    """The reference's own gr.spatial_neighbors_knn / _radius (run with the oracle's search in
+    place of its Metal grid kernels) against the oracle's restatement of the whole builder:
+    adjacency and distances bit for bit, dtypes included."""
+    from oracle import spatial as osp
+    checked = 0
+    for c, kind, xy, lib, kw, g in _spatial_cases():
+        fn = osp.spatial_neighbors_knn if kind == "knn" else osp.spatial_neighbors_radius
+        adj, dst = fn(xy, library=lib, **kw)
+        for tag, M in (("adj", adj), ("dst", dst)):
+            M = sp.csr_matrix(M)
+            M.sort_indices()
+            np.testing.assert_array_equal(M.indptr, g[f"c{c}_{tag}_indptr"], err_msg=f"{c} {tag}")
+            np.testing.assert_array_equal(M.indices, g[f"c{c}_{tag}_indices"], err_msg=f"{c} {tag}")
+            ref = g[f"c{c}_{tag}_data"]
+            assert M.data.dtype == ref.dtype, (c, tag, M.data.dtype, ref.dtype)
+            np.testing.assert_array_equal(M.data, ref, err_msg=f"{c} {tag}")
+        checked += 1
+    assert checked == 13
