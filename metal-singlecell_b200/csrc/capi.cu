@@ -176,7 +176,12 @@ int default_kprime(int prec, int k) {
 int check_common(int64_t n, int d, int k, int metric, int prec, int kprime) {
   if (n < 1 || n >= (int64_t(1) << 30)) { set_error("n=%lld out of range", (long long)n); return MSC_ERR_INVALID_ARG; }
   if (d < 1 || d > MSC_MAX_D) { set_error("d=%d must be in [1, %d]", d, MSC_MAX_D); return MSC_ERR_INVALID_ARG; }
-  if (k < 1 || k > MSC_MAX_K) { set_error("n_neighbors=%d must be in [1, %d]", k, MSC_MAX_K); return MSC_ERR_INVALID_ARG; }
+  if (k < 1) { set_error("n_neighbors=%d must be at least 1", k); return MSC_ERR_INVALID_ARG; }
+  if (k > MSC_MAX_K) {
+    // a valid request (any k <= n is), above the widest list the kernels keep
+    set_error("n_neighbors=%d is above the supported %d", k, MSC_MAX_K);
+    return MSC_ERR_UNSUPPORTED;
+  }
   if (metric != MSC_METRIC_EUCLIDEAN && metric != MSC_METRIC_COSINE) { set_error("unknown metric %d", metric); return MSC_ERR_INVALID_ARG; }
   if (prec < 0 || prec > 3) { set_error("unknown precision %d", prec); return MSC_ERR_INVALID_ARG; }
   if (kprime != 0 && (kprime < k - 1 || kprime > 64)) {

@@ -40,6 +40,7 @@ def test_version_and_constants():
     (10, 0, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # d = 0
     (10, 129, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),     # d > MSC_MAX_D
     (10, 5, 0, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # k = 0
+    (1000, 30, 130, 0, 1, 0, _lib.MSC_ERR_UNSUPPORTED),  # k above MSC_MAX_K: valid, unsupported
     (10, 5, 3, 7, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # metric
     (10, 5, 3, 0, 9, 0, _lib.MSC_ERR_INVALID_ARG),       # precision
     (100, 5, 30, 0, 1, 20, _lib.MSC_ERR_INVALID_ARG),    # kprime < k-1
