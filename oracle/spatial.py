@@ -50,20 +50,22 @@ def _row_blocks(n: int, m: int, budget: int = 32_000_000):
         yield s, min(n, s + step)
 
 
-def grid_knn(coords: np.ndarray, k: int):
-    """(idx int64 (n, k), dist float32 (n, k)): self first, then (float32 distance, index)."""
+def grid_knn(coords: np.ndarray, k: int, rows=None):
+    """(idx int64 (m, k), dist float32 (m, k)) for the query ``rows`` (all points by default):
+    self first, then (float32 distance, index)."""
     X = np.ascontiguousarray(coords, np.float32)
     n = X.shape[0]
     if not 1 <= k <= n:
         raise ValueError(f"k={k} must be in [1, n={n}]")
-    idx = np.empty((n, k), np.int64)
-    dist = np.empty((n, k), np.float32)
+    q = np.arange(n) if rows is None else np.asarray(rows, np.int64)
+    m = q.size
+    idx = np.empty((m, k), np.int64)
+    dist = np.empty((m, k), np.float32)
     cols = np.arange(n)
-    for s, e in _row_blocks(n, n):
-        d2 = sq_dist_f32(X[s:e], X)
+    for s, e in _row_blocks(m, n):
+        d2 = sq_dist_f32(X[q[s:e]], X)
         sd = np.sqrt(d2)
-        rows = np.arange(s, e)
-        sd[rows - s, rows] = -1.0                      # self ranks first
+        sd[np.arange(e - s), q[s:e]] = -1.0            # self ranks first
         if k < n:
             part = np.argpartition(sd, k - 1, axis=1)[:, :k]
             kth = np.take_along_axis(sd, part, axis=1).max(1)

@@ -127,3 +127,12 @@ def test_edge_cases():
         osp.grid_knn(X, 6)
     with pytest.raises(ValueError):
         osp.knn_edges(X, 5)
+
+
+def test_knn_rows_subset_equals_full():
+    X = np.random.default_rng(9).uniform(0, 100, (2000, 2)).astype(np.float32)
+    full_i, full_d = osp.grid_knn(X, 9)
+    rows = np.array([0, 5, 1999, 777, 5])
+    i, d = osp.grid_knn(X, 9, rows=rows)
+    np.testing.assert_array_equal(i, full_i[rows])
+    np.testing.assert_array_equal(d, full_d[rows])
