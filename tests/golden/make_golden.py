@@ -19,11 +19,11 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
   connectivities built by the oracle (the reference test's tiny-batch input,
   tests/test_postfix_fixes.py:186-193, and a 3-batch mixture) and on a random symmetric graph
   that stores explicit zeros, at several trims;
-* ``gr.spatial_neighbors_knn`` / ``gr.spatial_neighbors_radius`` (gr.py:198-255) with the oracle's
-  grid kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
-  selection, FP64 edge lengths, the percentile / set_diag / transform tail and the per-library
-  blocks are the reference's code, on a jittered hex lattice, a 3-D point cloud and two
-  interleaved sections.
+* ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid`` (gr.py:198-315) with the oracle's grid
+  kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
+  selection, FP64 edge lengths, the lattice median correction and ring expansion, the
+  percentile / set_diag / transform tail and the per-library blocks are the reference's code,
+  on jittered and exact hex lattices, a 3-D point cloud and interleaved sections.
 
 Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
 Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz, reference_distances_csr.npz,
@@ -209,7 +209,13 @@ def spatial_inputs():
     two = np.vstack([lattice(16, 1.0, 1), lattice(16, 1.0, 2)])
     perm = np.random.default_rng(4).permutation(two.shape[0])
     lib = np.repeat([0, 2], 256)[perm]                   # category 1 unused; interleaved order
-    return {"lat": (lat, None), "vol": (vol, None), "two": (two[perm], lib)}
+    hexl = lattice(30, 0.0, 0)                            # an exact Visium-like lattice
+    fine = lattice(16, 0.0, 0) * 0.5 + np.array([5000.0, 0.0])   # a section at half the spacing
+    both = np.vstack([lattice(16, 0.0, 0), fine])
+    perm2 = np.random.default_rng(5).permutation(both.shape[0])
+    lib2 = np.repeat([0, 1], 256)[perm2]
+    return {"lat": (lat, None), "vol": (vol, None), "two": (two[perm], lib),
+            "hex": (hexl, None), "hexlib": (both[perm2], lib2)}
 
 
 SPATIAL_CASES = [
@@ -226,6 +232,13 @@ SPATIAL_CASES = [
     ("radius", "lat", {"radius": 150.0, "set_diag": True, "transform": "spectral"}),
     ("radius", "two", {"radius": 120.0}),
     ("radius", "vol", {"radius": 7.0}),
+    ("grid", "hex", {"n_neighs": 6}),
+    ("grid", "hex", {"n_neighs": 6, "n_rings": 2}),
+    ("grid", "hex", {"n_neighs": 6, "n_rings": 3, "set_diag": True}),
+    ("grid", "hex", {"n_neighs": 6, "transform": "spectral"}),
+    ("grid", "hexlib", {"n_neighs": 6, "n_rings": 2}),
+    ("grid", "hex", {"delaunay": True}),
+    ("grid", "hex", {"delaunay": True, "n_rings": 2, "set_diag": True}),
 ]
 
 
@@ -251,7 +264,8 @@ def spatial_golden(ref_nb, ref_gr, osp):
                 obs["library"] = pd.Categorical.from_codes(lib, ["s0", "s1", "s2"])
                 extra["library_key"] = "library"
             adata = types.SimpleNamespace(obsm={"spatial": xy}, obs=obs, obsp={}, uns={})
-            fn = ref_gr.spatial_neighbors_knn if kind == "knn" else ref_gr.spatial_neighbors_radius
+            fn = {"knn": ref_gr.spatial_neighbors_knn, "radius": ref_gr.spatial_neighbors_radius,
+                  "grid": ref_gr.spatial_neighbors_grid}[kind]
             adj, dst = fn(adata, copy=True, **kw, **extra)
             out[f"c{c}_case"] = np.array(json.dumps([kind, name, kw]))
             for tag, M in (("adj", adj), ("dst", dst)):
