@@ -19,8 +19,8 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
   connectivities built by the oracle (the reference test's tiny-batch input,
   tests/test_postfix_fixes.py:186-193, and a 3-batch mixture) and on a random symmetric graph
   that stores explicit zeros, at several trims;
-* ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid`` (gr.py:198-315) with the oracle's grid
-  kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
+* ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid`` / ``_delaunay`` (gr.py:198-368) with the
+  oracle's grid kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
   selection, FP64 edge lengths, the lattice median correction and ring expansion, the
   percentile / set_diag / transform tail and the per-library blocks are the reference's code,
   on jittered and exact hex lattices, a 3-D point cloud and interleaved sections.
@@ -239,6 +239,8 @@ SPATIAL_CASES = [
     ("grid", "hexlib", {"n_neighs": 6, "n_rings": 2}),
     ("grid", "hex", {"delaunay": True}),
     ("grid", "hex", {"delaunay": True, "n_rings": 2, "set_diag": True}),
+    ("delaunay", "lat", {}),
+    ("delaunay", "two", {"radius": (20.0, 150.0), "percentile": 90.0, "transform": "spectral"}),
 ]
 
 
@@ -265,7 +267,8 @@ def spatial_golden(ref_nb, ref_gr, osp):
                 extra["library_key"] = "library"
             adata = types.SimpleNamespace(obsm={"spatial": xy}, obs=obs, obsp={}, uns={})
             fn = {"knn": ref_gr.spatial_neighbors_knn, "radius": ref_gr.spatial_neighbors_radius,
-                  "grid": ref_gr.spatial_neighbors_grid}[kind]
+                  "grid": ref_gr.spatial_neighbors_grid,
+                  "delaunay": ref_gr.spatial_neighbors_delaunay}[kind]
             adj, dst = fn(adata, copy=True, **kw, **extra)
             out[f"c{c}_case"] = np.array(json.dumps([kind, name, kw]))
             for tag, M in (("adj", adj), ("dst", dst)):
