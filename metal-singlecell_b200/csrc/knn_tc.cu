@@ -342,18 +342,34 @@ __device__ __forceinline__ int key_tile_at(int j, int diag, int nkt) {
   return right > left ? diag + (j - m) : diag - (j - m);
 }
 
+// Mask word of a pruned walk at position k: the word holding the query tile's own key tile
+// first, then outward, alternating right and left (dw, dw+1, dw-1, dw+2, ...), clipped to the
+// sample.  In the locality order, key tiles near in packed position are mostly near in space, so
+// the rows' thresholds fall early and fewer candidates are inserted.
+__device__ __forceinline__ int mask_word_at(int k, int dw, int nw) {
+  const int left = dw, right = nw - 1 - dw;
+  const int m = min(left, right);
+  if (k == 0) return dw;
+  if (k <= 2 * m) return (k & 1) ? dw + ((k + 1) >> 1) : dw - (k >> 1);
+  return right > left ? dw + (k - m) : dw - (k - m);
+}
+
 // The key tiles of one work item in the order every role walks them: the near tiles
 // (key_tile_at), then all other tiles in plain order, or only those whose bit is set in the
-// item's visit mask (the pruned scan), or none (the near pass).  Every role of the CTA walks the
-// same sequence, so the tiles need no hand-off between them.
+// item's visit mask (the pruned scan; its words from the query tile's own word outward), or none
+// (the near pass).  Every role of the CTA walks the same sequence, so the tiles need no hand-off
+// between them.
 struct KeyTileWalk {
   int nkt, diag, np, j;
   const uint32_t* mask;
-  int w, nw;
+  int w, nw;             // position in the word sequence, words in the mask
+  int dw;                // first word of the outward order
   uint32_t cur, nxt;
   bool near_only;
   int khi = 1 << 30;     // range walks stop before this tile
   bool range = false;
+  // the mask word at position k: outward from dw, or in plain order for range walks
+  __device__ __forceinline__ int word(int k) const { return range ? k : mask_word_at(k, dw, nw); }
   __device__ __forceinline__ void init(const WorkItem& item, int qref, int bn,
                                        const uint32_t* m, int words, bool near) {
     nkt = (item.nkeys + bn - 1) / bn;
@@ -368,8 +384,9 @@ struct KeyTileWalk {
     mask = m;
     w = 0;
     nw = words;
-    cur = m ? m[0] : 0u;
-    nxt = (m && words > 1) ? m[1] : 0u;     // one word ahead: its load overlaps the near tiles
+    dw = min(max(diag >> 5, 0), max(words - 1, 0));
+    cur = m ? m[word(0)] : 0u;
+    nxt = (m && words > 1) ? m[word(1)] : 0u;   // one word ahead: its load overlaps the near tiles
   }
   // A range walk (the refine pass): no near phase, only the tiles [lo, hi), in plain order or
   // as the mask's bits.
@@ -395,11 +412,11 @@ struct KeyTileWalk {
     while (cur == 0u) {
       if (++w >= nw) return -1;
       cur = nxt;
-      nxt = w + 1 < nw ? mask[w + 1] : 0u;
+      nxt = w + 1 < nw ? mask[word(w + 1)] : 0u;
     }
     const int b = __ffs(cur) - 1;
     cur &= cur - 1u;
-    const int kt = w * 32 + b;
+    const int kt = word(w) * 32 + b;
     return kt < khi ? kt : -1;
   }
 };
