@@ -78,39 +78,43 @@ __device__ __forceinline__ double d2_f64(const float* xs, const float* __restric
   return acc;
 }
 
-// FP32 squared distance of a shared-memory row xs and a gathered row y.  Four partial sums over
-// 8-byte loads (when y is 8-byte aligned) keep several loads of the gathered row in flight; the
-// sum of d positive terms in any order stays within the (d+4)·2^-24 relative bound the re-rank
-// window assumes.
-__device__ __forceinline__ float d2_f32(const float* xs, const float* __restrict__ y, int d) {
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-  int t = 0;
+// One lane's share of the FP32 squared distance of a shared-memory row xs and row y when the 4
+// lanes of a group split the row (part = lane & 3 takes every 4th 8-byte pair, or every 4th
+// element of a row that is not 8-byte aligned); the group then sums the four shares.  The warp
+// reads 8 candidate rows per instruction in 32-byte pieces instead of an 8-byte piece of each of
+// 32 rows.  Any summation order of the d positive terms stays within the (d+4)·2^-24 relative
+// bound the re-rank window assumes.
+__device__ __forceinline__ float group_part_d2_f32(const float* xs, const float* __restrict__ y,
+                                                   int d, int part) {
+  float a0 = 0.f, a1 = 0.f;
   if ((reinterpret_cast<uintptr_t>(y) & 7) == 0) {
     const float2* y2 = reinterpret_cast<const float2*>(y);
     const float2* x2 = reinterpret_cast<const float2*>(xs);
-#pragma unroll 4
-    for (; t + 4 <= d; t += 4) {
-      const float2 u = y2[t >> 1], w = y2[(t >> 1) + 1];
-      const float2 p = x2[t >> 1], q = x2[(t >> 1) + 1];
-      const float e0 = p.x - u.x, e1 = p.y - u.y, e2 = q.x - w.x, e3 = q.y - w.y;
+    const int h = d >> 1;
+    for (int t = part; t < h; t += 4) {
+      const float2 u = y2[t], p = x2[t];
+      const float e0 = p.x - u.x, e1 = p.y - u.y;
       a0 = fmaf(e0, e0, a0);
       a1 = fmaf(e1, e1, a1);
-      a2 = fmaf(e2, e2, a2);
-      a3 = fmaf(e3, e3, a3);
+    }
+    if ((d & 1) && part == 0) {
+      const float e = xs[d - 1] - y[d - 1];
+      a0 = fmaf(e, e, a0);
+    }
+  } else {
+    for (int t = part; t < d; t += 4) {
+      const float e = xs[t] - y[t];
+      a0 = fmaf(e, e, a0);
     }
   }
-  for (; t < d; ++t) {
-    const float df = xs[t] - y[t];
-    a0 = fmaf(df, df, a0);
-  }
-  return (a0 + a1) + (a2 + a3);
+  return a0 + a1;
 }
 
 __device__ __forceinline__ float out_dist(double d2, int cosine) {
   return cosine ? __double2float_rn(d2 * 0.5) : __double2float_rn(sqrt(d2));
 }
 
-__global__ void __launch_bounds__(RR_WARPS * 32)
+__global__ void __launch_bounds__(RR_WARPS * 32, 3)
 rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
               const SegDesc* __restrict__ seg, int nseg,
               int64_t npacked, const int32_t* __restrict__ cand_idx,
@@ -145,11 +149,29 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
       if (lane == 0) { knn_idx[i * k] = int32_t(i); knn_dist[i * k] = 0.f; ++n_cert; }
       continue;
     }
-    // 1. FP32 distances of the candidates (lane: slots lane and lane+32)
+    // 1. FP32 distances of the candidates (lane: slots lane and lane+32), eight candidates at a
+    //    time, four lanes each; candidate c's value goes to lane c & 31, slot c >> 5
     int c0 = lane < kprime ? cand_idx[i * cand_stride + lane] : -1;
     int c1 = lane + 32 < kprime ? cand_idx[i * cand_stride + lane + 32] : -1;
-    float e0 = c0 >= 0 ? d2_f32(xs, X + int64_t(c0) * d, d) : __int_as_float(0x7f800000);
-    float e1 = c1 >= 0 ? d2_f32(xs, X + int64_t(c1) * d, d) : __int_as_float(0x7f800000);
+    float e0 = __int_as_float(0x7f800000), e1 = __int_as_float(0x7f800000);
+    {
+      const int part = lane & 3, grp = lane >> 2;
+      for (int r = 0; r < kprime; r += 8) {              // warp-uniform
+        const int c = r + grp;
+        // the candidate ids sit in lanes c & 31 of c0 (c < 32) or c1
+        const int id0 = __shfl_sync(FULL, c0, c & 31), id1 = __shfl_sync(FULL, c1, c & 31);
+        const int cid = c < kprime ? (c < 32 ? id0 : id1) : -1;
+        float v = cid >= 0 ? group_part_d2_f32(xs, X + int64_t(cid) * d, d, part) : 0.f;
+        v += __shfl_xor_sync(FULL, v, 1);                // the group's four shares
+        v += __shfl_xor_sync(FULL, v, 2);
+        if (cid < 0) v = __int_as_float(0x7f800000);
+        const int rb = r & 31;                            // lanes rb .. rb+7 receive this round
+        const float got = __shfl_sync(FULL, v, ((lane - rb) & 7) * 4);
+        if (lane >= rb && lane < rb + 8) {
+          if (r < 32) e0 = got; else e1 = got;
+        }
+      }
+    }
     // 2. sort by (FP32 distance, index)
     {
       double v0 = e0, v1 = e1;
