@@ -40,6 +40,16 @@ namespace msc {
 namespace {
 
 constexpr int EPI_WARP0 = 4;
+// register split of the eight-epilogue-warp kernels (see knn_tc_kernel)
+constexpr int REG_LOW = 56, REG_HIGH = 224;
+constexpr int REG_LAUNCH = (REG_LOW * 128 + REG_HIGH * 256) / 384;     // 168
+static_assert(REG_LOW * 128 + REG_HIGH * 256 == REG_LAUNCH * 384, "split must fill the pool");
+__device__ __forceinline__ void reg_dec() {
+  asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_LOW));
+}
+__device__ __forceinline__ void reg_inc() {
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_HIGH));
+}
 constexpr int BM = 128;
 constexpr int ITEM_RING = 4;                        // claimed work items in flight per CTA
 constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
@@ -79,7 +89,7 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of `parity` to complete.  false = gave up (abort raised).
-__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
+__device__ __forceinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
                                             volatile int* abort_flag,
                                             uint64_t limit_ns = WAIT_LIMIT_NS) {
   const uint64_t t0 = globaltimer();
@@ -99,7 +109,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
 }
 // Teardown wait for work this thread itself started (copies, MMAs): ignores the abort flag
 // because such work completes on its own, but is still bounded in time.
-__device__ __noinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 0;; ++it) {
     if (mbar_test(bar, parity)) return true;
@@ -204,7 +214,7 @@ __device__ __forceinline__ bool mbar_test_cl(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __noinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
+__device__ __forceinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
                                                volatile int* abort_flag) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
@@ -515,6 +525,10 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const long long t_kernel0 = clock64();
+  // Register split (eight epilogue warps): each role of warpgroup 0 (producer, MMA, TMEM,
+  // relay) starts by giving up registers, each epilogue warp by taking them.
+  // REG_LOW·128 + REG_HIGH·256 equals the block's pool at the launch allocation REG_LAUNCH; the
+  // launcher checks that allocation first, since an increase beyond the pool would wait forever.
 
   // Work distribution.  A single CTA claims work items dynamically: its producer thread takes the
   // next item from a global counter and hands it to the MMA thread and the epilogue warps through
@@ -572,6 +586,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
 
   if (warp == 0) {
     // ------------------------------------------------------------------ TMA producer (each CTA)
+    if constexpr (NEPI == 8) reg_dec();
     if (lane == 0) {
       int stage = 0, abuf = 0;
       uint32_t sphase = 0, aphase = 0;
@@ -619,6 +634,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
   } else if (warp == 3) {
     // ------------------------------------------------------------------ relay (odd CTA of a pair)
+    if constexpr (NEPI == 8) reg_dec();
     if (PAIR && !leader && lane == 0) {
       int stage = 0, abuf = 0;
       uint32_t sphase = 0, aphase = 0;
@@ -643,6 +659,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
   } else if (warp == 1) {
     // ------------------------------------------------------------------ MMA issuer (even CTA)
+    if constexpr (NEPI == 8) reg_dec();
     if (leader && lane == 0) {
       int stage = 0, abuf = 0, acc = 0;
       uint32_t sphase = 0, aphase = 0, accphase = 0;
@@ -703,8 +720,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
       }
     }
+  } else if (warp == 2) {
+    if constexpr (NEPI == 8) reg_dec();              // TMEM owner: no role until the teardown
   } else if (warp >= EPI_WARP0) {
     // ------------------------------------------------------------------ epilogue (each CTA)
+    if constexpr (NEPI == 8) reg_inc();
     const int q = warp & 3;                        // TMEM lane quarter this warp may access
     const int h = (warp - EPI_WARP0) >> 2;         // column group
     const int row = q * 32 + lane;
@@ -776,23 +796,62 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             else mbar_arrive(&acc_empty[acc]);
           }
         };
-        tmem_ld32_async(t0, ra);
-        tmem_wait(ra);
-        if (nch == 1) release();
-        for (int c = 0; c < nch; c += 2) {
-          const bool more = c + 1 < nch;
-          if (more) tmem_ld32_async(t0 + uint32_t((c + 1) * 32), rb);
-          sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
-          if (more) {
-            tmem_wait(rb);
-            if (c + 1 == nch - 1) release();
-            const bool more2 = c + 2 < nch;
-            if (more2) tmem_ld32_async(t0 + uint32_t((c + 2) * 32), ra);
-            sel.push32(reinterpret_cast<const float(&)[32]>(rb), col_base + (c + 1) * 32, self,
-                       limit);
-            if (more2) {
-              tmem_wait(ra);
-              if (c + 2 == nch - 1) release();
+        if constexpr (NEPI == 8) {
+          // With the register split: three chunk buffers.  tcgen05.wait::ld waits for all of a
+          // thread's loads, so chunks go two per wait: a cycle starts with chunks c, c+1 loaded
+          // and a free third buffer, loads c+2 (free buffer) and c+3 (c's buffer, once c is
+          // filtered) while it filters c and c+1, then waits.  Rotating the buffers over three
+          // cycles keeps them in registers.  The accumulator is released once, right after the
+          // wait that covers its last chunk.
+          uint32_t rc[32];
+          auto ld = [&](int c, uint32_t(&x)[32]) { tmem_ld32_async(t0 + uint32_t(c * 32), x); };
+          auto push = [&](int c, uint32_t(&x)[32]) {
+            sel.push32(reinterpret_cast<const float(&)[32]>(x), col_base + c * 32, self, limit);
+          };
+          auto cycle = [&](int c, uint32_t(&x)[32], uint32_t(&y)[32], uint32_t(&z)[32]) {
+            const bool l2 = c + 2 < nch, l3 = c + 3 < nch;
+            if (l2) ld(c + 2, z);
+            push(c, x);
+            if (c + 1 < nch) {
+              if (l3) ld(c + 3, x);
+              push(c + 1, y);
+            }
+            if (l2) {
+              tmem_wait(z);
+              if (l3) tmem_wait(x);
+              if (c + 4 >= nch) release();
+            }
+            return l2;                             // chunk c+2 exists: another cycle follows
+          };
+          ld(0, ra);
+          if (nch > 1) ld(1, rb);
+          tmem_wait(ra);
+          if (nch > 1) tmem_wait(rb);
+          if (nch <= 2) release();
+          for (int c = 0;; c += 6) {
+            if (!cycle(c, ra, rb, rc)) break;
+            if (!cycle(c + 2, rc, ra, rb)) break;
+            if (!cycle(c + 4, rb, rc, ra)) break;
+          }
+        } else {
+          tmem_ld32_async(t0, ra);
+          tmem_wait(ra);
+          if (nch == 1) release();
+          for (int c = 0; c < nch; c += 2) {
+            const bool more = c + 1 < nch;
+            if (more) tmem_ld32_async(t0 + uint32_t((c + 1) * 32), rb);
+            sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
+            if (more) {
+              tmem_wait(rb);
+              if (c + 1 == nch - 1) release();
+              const bool more2 = c + 2 < nch;
+              if (more2) tmem_ld32_async(t0 + uint32_t((c + 2) * 32), ra);
+              sel.push32(reinterpret_cast<const float(&)[32]>(rb), col_base + (c + 1) * 32,
+                         self, limit);
+              if (more2) {
+                tmem_wait(ra);
+                if (c + 2 == nch - 1) release();
+              }
             }
           }
         }
@@ -948,6 +1007,16 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
   auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (NEPI == 8) {
+    // the register split needs the block's pool at REG_LAUNCH registers per thread
+    cudaFuncAttributes fa{};
+    MSC_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (((fa.numRegs + 7) / 8) * 8 < REG_LAUNCH) {
+      set_error("candidate kernel compiled to %d registers; its register split needs %d",
+                fa.numRegs, REG_LAUNCH);
+      return MSC_ERR_UNSUPPORTED;
+    }
+  }
   if (!PAIR) {
     const int grid = std::max(1, std::min(P.n_items, num_sms()));
     kern<<<grid, 128 + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
