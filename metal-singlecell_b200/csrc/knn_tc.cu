@@ -525,10 +525,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const long long t_kernel0 = clock64();
-  // Register split (eight epilogue warps): each role of warpgroup 0 (producer, MMA, TMEM,
-  // relay) starts by giving up registers, each epilogue warp by taking them.
-  // REG_LOW·128 + REG_HIGH·256 equals the block's pool at the launch allocation REG_LAUNCH; the
-  // launcher checks that allocation first, since an increase beyond the pool would wait forever.
+  // Register split (eight epilogue warps): warpgroup 0 (producer, MMA, TMEM owner, relay) gives
+  // up registers and the two epilogue warpgroups take them, one setmaxnreg per warpgroup at the
+  // head of its branch.  REG_LOW·128 + REG_HIGH·256 equals the block's pool at the launch
+  // allocation REG_LAUNCH; the launcher checks that allocation first, since an increase beyond
+  // the pool would wait forever.
 
   // Work distribution.  A single CTA claims work items dynamically: its producer thread takes the
   // next item from a global counter and hands it to the MMA thread and the epilogue warps through
@@ -584,145 +585,145 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     return true;
   };
 
-  if (warp == 0) {
-    // ------------------------------------------------------------------ TMA producer (each CTA)
+  if (warp < EPI_WARP0) {
+    // warpgroup 0: one register decrease for the whole warpgroup (the split needs one
+    // setmaxnreg per warpgroup), then the roles; warp 2 (TMEM owner) waits for the teardown
     if constexpr (NEPI == 8) reg_dec();
-    if (lane == 0) {
-      int stage = 0, abuf = 0;
-      uint32_t sphase = 0, aphase = 0;
-      bool ok = true;
-      long long c_wait = 0;
-      for (;;) {
-        int it;
-        if (!claim(it)) { ok = false; break; }
-        if (it < 0) break;
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
-        if (!ok) break;
-        mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
-        for (int kb = 0; kb < P.kb; ++kb)
-          tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
-                      w.qrow0 + int(rank) * BM);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
-            const long long tw = P.prof ? clock64() : 0;
-            ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
-            if (P.prof) c_wait += clock64() - tw;
-            if (!ok) break;
-            mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
-            tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
-                        w.key0 + kt * P.bn + int(rank) * brows);
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
-          }
-        }
-        if (!ok) break;
-      }
-      if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
-      // drain: every load this thread armed completes on its own; wait for them (bounded)
-      for (int s = 0; s < P.stages; ++s) {
-        // stages armed in the current lap have parity sphase for indices < stage
-        const uint32_t par = s < stage ? sphase : (sphase ^ 1);
-        (void)mbar_drain(&b_full[s], par);
-      }
-      for (int a = 0; a < P.na; ++a) {
-        const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
-        (void)mbar_drain(&a_full[a], par);
-      }
-    }
-  } else if (warp == 3) {
-    // ------------------------------------------------------------------ relay (odd CTA of a pair)
-    if constexpr (NEPI == 8) reg_dec();
-    if (PAIR && !leader && lane == 0) {
-      int stage = 0, abuf = 0;
-      uint32_t sphase = 0, aphase = 0;
-      bool ok = true;
-      for (int it = unit; it < n_items && ok; it += nunits) {
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
-        if (!ok) break;
-        mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          for (int kb = 0; kb < P.kb; ++kb) {
-            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-            if (!ok) break;
-            mbar_arrive_remote(mapa_shared(smem_u32(&b_peer[stage]), 0));
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
-          }
-        }
-      }
-    }
-  } else if (warp == 1) {
-    // ------------------------------------------------------------------ MMA issuer (even CTA)
-    if constexpr (NEPI == 8) reg_dec();
-    if (leader && lane == 0) {
-      int stage = 0, abuf = 0, acc = 0;
-      uint32_t sphase = 0, aphase = 0, accphase = 0;
-      bool ok = true, issued = false;
-      long long c_b = 0, c_acc = 0;
-      for (;;) {
-        int it;
-        if (!receive(it, false)) { ok = false; break; }
-        if (it < 0) break;
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
-        if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
-        if (!ok) break;
-        const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          const long long t2 = P.prof ? clock64() : 0;
-          ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
-                    : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
-          if (P.prof) c_acc += clock64() - t2;
+    if (warp == 0) {
+      // ------------------------------------------------------------------ TMA producer (each CTA)
+      if (lane == 0) {
+        int stage = 0, abuf = 0;
+        uint32_t sphase = 0, aphase = 0;
+        bool ok = true;
+        long long c_wait = 0;
+        for (;;) {
+          int it;
+          if (!claim(it)) { ok = false; break; }
+          if (it < 0) break;
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
           if (!ok) break;
-          tc_fence_after();
-          const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
-          for (int kb = 0; kb < P.kb; ++kb) {
-            const long long t1 = P.prof ? clock64() : 0;
-            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-            if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
-            if (P.prof) c_b += clock64() - t1;
-            if (!ok) break;
-            const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
-            const int ks1 = min(P.ksteps, 4 * kb + 4);
-            for (int ks = 4 * kb; ks < ks1; ++ks) {
-              const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
-              umma_f16_g<PAIR>(d_tmem, sdesc(a_base + ao), sdesc(b_base + uint32_t((ks & 3) * 32)),
-                               P.idesc, ks > 0 ? 1u : 0u);
+          mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
+          for (int kb = 0; kb < P.kb; ++kb)
+            tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
+                        w.qrow0 + int(rank) * BM);
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
+              const long long tw = P.prof ? clock64() : 0;
+              ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+              if (P.prof) c_wait += clock64() - tw;
+              if (!ok) break;
+              mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
+              tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
+                          w.key0 + kt * P.bn + int(rank) * brows);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
             }
-            umma_commit_g<PAIR>(&b_empty[stage]);
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
           if (!ok) break;
-          issued = true;
-          umma_commit_g<PAIR>(&acc_full[acc]);
-          if (++acc == 2) { acc = 0; accphase ^= 1; }
         }
-        if (!ok) break;
-        umma_commit_g<PAIR>(&a_empty[abuf]);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
+        // drain: every load this thread armed completes on its own; wait for them (bounded)
+        for (int s = 0; s < P.stages; ++s) {
+          // stages armed in the current lap have parity sphase for indices < stage
+          const uint32_t par = s < stage ? sphase : (sphase ^ 1);
+          (void)mbar_drain(&b_full[s], par);
+        }
+        for (int a = 0; a < P.na; ++a) {
+          const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
+          (void)mbar_drain(&a_full[a], par);
+        }
       }
-      if (issued) {
-        umma_commit_g<PAIR>(done_bar);
-      } else {
-        mbar_arrive(done_bar);
-        if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
+    } else if (warp == 3) {
+      // ------------------------------------------------------------------ relay (odd CTA of a pair)
+      if (PAIR && !leader && lane == 0) {
+        int stage = 0, abuf = 0;
+        uint32_t sphase = 0, aphase = 0;
+        bool ok = true;
+        for (int it = unit; it < n_items && ok; it += nunits) {
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+          if (!ok) break;
+          mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            for (int kb = 0; kb < P.kb; ++kb) {
+              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+              if (!ok) break;
+              mbar_arrive_remote(mapa_shared(smem_u32(&b_peer[stage]), 0));
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            }
+          }
+        }
       }
-      if (P.prof) {
-        atomicAdd(&g_tc_prof[P.prof_slot][1], (unsigned long long)c_b);
-        atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
+    } else if (warp == 1) {
+      // ------------------------------------------------------------------ MMA issuer (even CTA)
+      if (leader && lane == 0) {
+        int stage = 0, abuf = 0, acc = 0;
+        uint32_t sphase = 0, aphase = 0, accphase = 0;
+        bool ok = true, issued = false;
+        long long c_b = 0, c_acc = 0;
+        for (;;) {
+          int it;
+          if (!receive(it, false)) { ok = false; break; }
+          if (it < 0) break;
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+          if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
+          if (!ok) break;
+          const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            const long long t2 = P.prof ? clock64() : 0;
+            ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
+                      : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+            if (P.prof) c_acc += clock64() - t2;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
+            for (int kb = 0; kb < P.kb; ++kb) {
+              const long long t1 = P.prof ? clock64() : 0;
+              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+              if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
+              if (P.prof) c_b += clock64() - t1;
+              if (!ok) break;
+              const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
+              const int ks1 = min(P.ksteps, 4 * kb + 4);
+              for (int ks = 4 * kb; ks < ks1; ++ks) {
+                const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
+                umma_f16_g<PAIR>(d_tmem, sdesc(a_base + ao), sdesc(b_base + uint32_t((ks & 3) * 32)),
+                                 P.idesc, ks > 0 ? 1u : 0u);
+              }
+              umma_commit_g<PAIR>(&b_empty[stage]);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            }
+            if (!ok) break;
+            issued = true;
+            umma_commit_g<PAIR>(&acc_full[acc]);
+            if (++acc == 2) { acc = 0; accphase ^= 1; }
+          }
+          if (!ok) break;
+          umma_commit_g<PAIR>(&a_empty[abuf]);
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        }
+        if (issued) {
+          umma_commit_g<PAIR>(done_bar);
+        } else {
+          mbar_arrive(done_bar);
+          if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
+        }
+        if (P.prof) {
+          atomicAdd(&g_tc_prof[P.prof_slot][1], (unsigned long long)c_b);
+          atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
+        }
       }
     }
-  } else if (warp == 2) {
-    if constexpr (NEPI == 8) reg_dec();              // TMEM owner: no role until the teardown
-  } else if (warp >= EPI_WARP0) {
+  } else {
     // ------------------------------------------------------------------ epilogue (each CTA)
     if constexpr (NEPI == 8) reg_inc();
     const int q = warp & 3;                        // TMEM lane quarter this warp may access
