@@ -40,6 +40,16 @@ namespace msc {
 namespace {
 
 constexpr int EPI_WARP0 = 4;
+// register split of the eight-epilogue-warp kernels (see knn_tc_kernel)
+constexpr int REG_LOW = 56, REG_HIGH = 224;
+constexpr int REG_LAUNCH = (REG_LOW * 128 + REG_HIGH * 256) / 384;     // 168
+static_assert(REG_LOW * 128 + REG_HIGH * 256 == REG_LAUNCH * 384, "split must fill the pool");
+__device__ __forceinline__ void reg_dec() {
+  asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_LOW));
+}
+__device__ __forceinline__ void reg_inc() {
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_HIGH));
+}
 constexpr int BM = 128;
 constexpr int ITEM_RING = 4;                        // claimed work items in flight per CTA
 constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
@@ -79,7 +89,7 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of `parity` to complete.  false = gave up (abort raised).
-__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
+__device__ __forceinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
                                             volatile int* abort_flag,
                                             uint64_t limit_ns = WAIT_LIMIT_NS) {
   const uint64_t t0 = globaltimer();
@@ -99,7 +109,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
 }
 // Teardown wait for work this thread itself started (copies, MMAs): ignores the abort flag
 // because such work completes on its own, but is still bounded in time.
-__device__ __noinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 0;; ++it) {
     if (mbar_test(bar, parity)) return true;
@@ -204,7 +214,7 @@ __device__ __forceinline__ bool mbar_test_cl(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __noinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
+__device__ __forceinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
                                                volatile int* abort_flag) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
@@ -532,6 +542,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   const long long t_kernel0 = clock64();
+  // Register split (eight epilogue warps): warpgroup 0 (producer, MMA, TMEM owner, relay) gives
+  // up registers and the two epilogue warpgroups take them, one setmaxnreg per warpgroup at the
+  // head of its branch.  REG_LOW·128 + REG_HIGH·256 equals the block's pool at the launch
+  // allocation REG_LAUNCH; the launcher checks that allocation first, since an increase beyond
+  // the pool would wait forever.
 
   // Work distribution.  A single CTA claims work items dynamically: its producer thread takes the
   // next item from a global counter and hands it to the MMA thread and the epilogue warps through
@@ -587,141 +602,147 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     return true;
   };
 
-  if (warp == 0) {
-    // ------------------------------------------------------------------ TMA producer (each CTA)
-    if (lane == 0) {
-      int stage = 0, abuf = 0;
-      uint32_t sphase = 0, aphase = 0;
-      bool ok = true;
-      long long c_wait = 0;
-      for (;;) {
-        int it;
-        if (!claim(it)) { ok = false; break; }
-        if (it < 0) break;
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
-        if (!ok) break;
-        mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
-        for (int kb = 0; kb < P.kb; ++kb)
-          tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
-                      w.qrow0 + int(rank) * BM);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
-            const long long tw = P.prof ? clock64() : 0;
-            ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
-            if (P.prof) c_wait += clock64() - tw;
-            if (!ok) break;
-            mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
-            tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
-                        w.key0 + kt * P.bn + int(rank) * brows);
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
-          }
-        }
-        if (!ok) break;
-      }
-      if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
-      // drain: every load this thread armed completes on its own; wait for them (bounded)
-      for (int s = 0; s < P.stages; ++s) {
-        // stages armed in the current lap have parity sphase for indices < stage
-        const uint32_t par = s < stage ? sphase : (sphase ^ 1);
-        (void)mbar_drain(&b_full[s], par);
-      }
-      for (int a = 0; a < P.na; ++a) {
-        const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
-        (void)mbar_drain(&a_full[a], par);
-      }
-    }
-  } else if (warp == 3) {
-    // ------------------------------------------------------------------ relay (odd CTA of a pair)
-    if (PAIR && !leader && lane == 0) {
-      int stage = 0, abuf = 0;
-      uint32_t sphase = 0, aphase = 0;
-      bool ok = true;
-      for (int it = unit; it < n_items && ok; it += nunits) {
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
-        if (!ok) break;
-        mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          for (int kb = 0; kb < P.kb; ++kb) {
-            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-            if (!ok) break;
-            mbar_arrive_remote(mapa_shared(smem_u32(&b_peer[stage]), 0));
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
-          }
-        }
-      }
-    }
-  } else if (warp == 1) {
-    // ------------------------------------------------------------------ MMA issuer (even CTA)
-    if (leader && lane == 0) {
-      int stage = 0, abuf = 0, acc = 0;
-      uint32_t sphase = 0, aphase = 0, accphase = 0;
-      bool ok = true, issued = false;
-      long long c_b = 0, c_acc = 0;
-      for (;;) {
-        int it;
-        if (!receive(it, false)) { ok = false; break; }
-        if (it < 0) break;
-        const WorkItem w = items[item_of(it)];
-        ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
-        if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
-        if (!ok) break;
-        const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
-        KeyTileWalk walk;
-        walk_init(walk, w, it);
-        for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
-          const long long t2 = P.prof ? clock64() : 0;
-          ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
-                    : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
-          if (P.prof) c_acc += clock64() - t2;
+  if (warp < EPI_WARP0) {
+    // warpgroup 0: one register decrease for the whole warpgroup (the split needs one
+    // setmaxnreg per warpgroup), then the roles; warp 2 (TMEM owner) waits for the teardown
+    if constexpr (NEPI == 8) reg_dec();
+    if (warp == 0) {
+      // ------------------------------------------------------------------ TMA producer (each CTA)
+      if (lane == 0) {
+        int stage = 0, abuf = 0;
+        uint32_t sphase = 0, aphase = 0;
+        bool ok = true;
+        long long c_wait = 0;
+        for (;;) {
+          int it;
+          if (!claim(it)) { ok = false; break; }
+          if (it < 0) break;
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_empty[abuf], aphase ^ 1, abort_flag);
           if (!ok) break;
-          tc_fence_after();
-          const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
-          for (int kb = 0; kb < P.kb; ++kb) {
-            const long long t1 = P.prof ? clock64() : 0;
-            ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-            if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
-            if (P.prof) c_b += clock64() - t1;
-            if (!ok) break;
-            const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
-            const int ks1 = min(P.ksteps, 4 * kb + 4);
-            for (int ks = 4 * kb; ks < ks1; ++ks) {
-              const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
-              umma_f16_g<PAIR>(d_tmem, sdesc(a_base + ao), sdesc(b_base + uint32_t((ks & 3) * 32)),
-                               P.idesc, ks > 0 ? 1u : 0u);
+          mbar_expect_tx(&a_full[abuf], uint32_t(a_bytes));
+          for (int kb = 0; kb < P.kb; ++kb)
+            tma_load_2d(Asm + abuf * a_bytes + size_t(kb) * BM * 128, &tmA, &a_full[abuf], kb * 64,
+                        w.qrow0 + int(rank) * BM);
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
+              const long long tw = P.prof ? clock64() : 0;
+              ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+              if (P.prof) c_wait += clock64() - tw;
+              if (!ok) break;
+              mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
+              tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
+                          w.key0 + kt * P.bn + int(rank) * brows);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
             }
-            umma_commit_g<PAIR>(&b_empty[stage]);
-            if (++stage == P.stages) { stage = 0; sphase ^= 1; }
           }
           if (!ok) break;
-          issued = true;
-          umma_commit_g<PAIR>(&acc_full[acc]);
-          if (++acc == 2) { acc = 0; accphase ^= 1; }
         }
-        if (!ok) break;
-        umma_commit_g<PAIR>(&a_empty[abuf]);
-        if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
+        // drain: every load this thread armed completes on its own; wait for them (bounded)
+        for (int s = 0; s < P.stages; ++s) {
+          // stages armed in the current lap have parity sphase for indices < stage
+          const uint32_t par = s < stage ? sphase : (sphase ^ 1);
+          (void)mbar_drain(&b_full[s], par);
+        }
+        for (int a = 0; a < P.na; ++a) {
+          const uint32_t par = a < abuf ? aphase : (aphase ^ 1);
+          (void)mbar_drain(&a_full[a], par);
+        }
       }
-      if (issued) {
-        umma_commit_g<PAIR>(done_bar);
-      } else {
-        mbar_arrive(done_bar);
-        if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
+    } else if (warp == 3) {
+      // ------------------------------------------------------------------ relay (odd CTA of a pair)
+      if (PAIR && !leader && lane == 0) {
+        int stage = 0, abuf = 0;
+        uint32_t sphase = 0, aphase = 0;
+        bool ok = true;
+        for (int it = unit; it < n_items && ok; it += nunits) {
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+          if (!ok) break;
+          mbar_arrive_remote(mapa_shared(smem_u32(&a_peer[abuf]), 0));
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            for (int kb = 0; kb < P.kb; ++kb) {
+              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+              if (!ok) break;
+              mbar_arrive_remote(mapa_shared(smem_u32(&b_peer[stage]), 0));
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            }
+          }
+        }
       }
-      if (P.prof) {
-        atomicAdd(&g_tc_prof[P.prof_slot][1], (unsigned long long)c_b);
-        atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
+    } else if (warp == 1) {
+      // ------------------------------------------------------------------ MMA issuer (even CTA)
+      if (leader && lane == 0) {
+        int stage = 0, abuf = 0, acc = 0;
+        uint32_t sphase = 0, aphase = 0, accphase = 0;
+        bool ok = true, issued = false;
+        long long c_b = 0, c_acc = 0;
+        for (;;) {
+          int it;
+          if (!receive(it, false)) { ok = false; break; }
+          if (it < 0) break;
+          const WorkItem w = items[item_of(it)];
+          ok = mbar_wait(&a_full[abuf], aphase, abort_flag);
+          if (ok && PAIR) ok = mbar_wait_cl(&a_peer[abuf], aphase, abort_flag);
+          if (!ok) break;
+          const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
+          KeyTileWalk walk;
+          walk_init(walk, w, it);
+          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+            const long long t2 = P.prof ? clock64() : 0;
+            ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
+                      : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+            if (P.prof) c_acc += clock64() - t2;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
+            for (int kb = 0; kb < P.kb; ++kb) {
+              const long long t1 = P.prof ? clock64() : 0;
+              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+              if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
+              if (P.prof) c_b += clock64() - t1;
+              if (!ok) break;
+              const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
+              const int ks1 = min(P.ksteps, 4 * kb + 4);
+              for (int ks = 4 * kb; ks < ks1; ++ks) {
+                const uint32_t ao = uint32_t((ks >> 2) * BM * 128 + (ks & 3) * 32);
+                umma_f16_g<PAIR>(d_tmem, sdesc(a_base + ao), sdesc(b_base + uint32_t((ks & 3) * 32)),
+                                 P.idesc, ks > 0 ? 1u : 0u);
+              }
+              umma_commit_g<PAIR>(&b_empty[stage]);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            }
+            if (!ok) break;
+            issued = true;
+            umma_commit_g<PAIR>(&acc_full[acc]);
+            if (++acc == 2) { acc = 0; accphase ^= 1; }
+          }
+          if (!ok) break;
+          umma_commit_g<PAIR>(&a_empty[abuf]);
+          if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
+        }
+        if (issued) {
+          umma_commit_g<PAIR>(done_bar);
+        } else {
+          mbar_arrive(done_bar);
+          if (PAIR) mbar_arrive_remote(mapa_shared(smem_u32(done_bar), 1));
+        }
+        if (P.prof) {
+          atomicAdd(&g_tc_prof[P.prof_slot][1], (unsigned long long)c_b);
+          atomicAdd(&g_tc_prof[P.prof_slot][2], (unsigned long long)c_acc);
+        }
       }
     }
-  } else if (warp >= EPI_WARP0) {
+  } else {
     // ------------------------------------------------------------------ epilogue (each CTA)
+    if constexpr (NEPI == 8) reg_inc();
     const int q = warp & 3;                        // TMEM lane quarter this warp may access
     const int h = (warp - EPI_WARP0) >> 2;         // column group
     const int row = q * 32 + lane;
@@ -793,23 +814,62 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             else mbar_arrive(&acc_empty[acc]);
           }
         };
-        tmem_ld32_async(t0, ra);
-        tmem_wait(ra);
-        if (nch == 1) release();
-        for (int c = 0; c < nch; c += 2) {
-          const bool more = c + 1 < nch;
-          if (more) tmem_ld32_async(t0 + uint32_t((c + 1) * 32), rb);
-          sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
-          if (more) {
-            tmem_wait(rb);
-            if (c + 1 == nch - 1) release();
-            const bool more2 = c + 2 < nch;
-            if (more2) tmem_ld32_async(t0 + uint32_t((c + 2) * 32), ra);
-            sel.push32(reinterpret_cast<const float(&)[32]>(rb), col_base + (c + 1) * 32, self,
-                       limit);
-            if (more2) {
-              tmem_wait(ra);
-              if (c + 2 == nch - 1) release();
+        if constexpr (NEPI == 8) {
+          // With the register split: three chunk buffers.  tcgen05.wait::ld waits for all of a
+          // thread's loads, so chunks go two per wait: a cycle starts with chunks c, c+1 loaded
+          // and a free third buffer, loads c+2 (free buffer) and c+3 (c's buffer, once c is
+          // filtered) while it filters c and c+1, then waits.  Rotating the buffers over three
+          // cycles keeps them in registers.  The accumulator is released once, right after the
+          // wait that covers its last chunk.
+          uint32_t rc[32];
+          auto ld = [&](int c, uint32_t(&x)[32]) { tmem_ld32_async(t0 + uint32_t(c * 32), x); };
+          auto push = [&](int c, uint32_t(&x)[32]) {
+            sel.push32(reinterpret_cast<const float(&)[32]>(x), col_base + c * 32, self, limit);
+          };
+          auto cycle = [&](int c, uint32_t(&x)[32], uint32_t(&y)[32], uint32_t(&z)[32]) {
+            const bool l2 = c + 2 < nch, l3 = c + 3 < nch;
+            if (l2) ld(c + 2, z);
+            push(c, x);
+            if (c + 1 < nch) {
+              if (l3) ld(c + 3, x);
+              push(c + 1, y);
+            }
+            if (l2) {
+              tmem_wait(z);
+              if (l3) tmem_wait(x);
+              if (c + 4 >= nch) release();
+            }
+            return l2;                             // chunk c+2 exists: another cycle follows
+          };
+          ld(0, ra);
+          if (nch > 1) ld(1, rb);
+          tmem_wait(ra);
+          if (nch > 1) tmem_wait(rb);
+          if (nch <= 2) release();
+          for (int c = 0;; c += 6) {
+            if (!cycle(c, ra, rb, rc)) break;
+            if (!cycle(c + 2, rc, ra, rb)) break;
+            if (!cycle(c + 4, rb, rc, ra)) break;
+          }
+        } else {
+          tmem_ld32_async(t0, ra);
+          tmem_wait(ra);
+          if (nch == 1) release();
+          for (int c = 0; c < nch; c += 2) {
+            const bool more = c + 1 < nch;
+            if (more) tmem_ld32_async(t0 + uint32_t((c + 1) * 32), rb);
+            sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
+            if (more) {
+              tmem_wait(rb);
+              if (c + 1 == nch - 1) release();
+              const bool more2 = c + 2 < nch;
+              if (more2) tmem_ld32_async(t0 + uint32_t((c + 2) * 32), ra);
+              sel.push32(reinterpret_cast<const float(&)[32]>(rb), col_base + (c + 1) * 32,
+                         self, limit);
+              if (more2) {
+                tmem_wait(ra);
+                if (c + 2 == nch - 1) release();
+              }
             }
           }
         }
@@ -965,6 +1025,16 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
   auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  if (NEPI == 8) {
+    // the register split needs the block's pool at REG_LAUNCH registers per thread
+    cudaFuncAttributes fa{};
+    MSC_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (((fa.numRegs + 7) / 8) * 8 < REG_LAUNCH) {
+      set_error("candidate kernel compiled to %d registers; its register split needs %d",
+                fa.numRegs, REG_LAUNCH);
+      return MSC_ERR_UNSUPPORTED;
+    }
+  }
   if (!PAIR) {
     const int grid = std::max(1, std::min(P.n_items, num_sms()));
     kern<<<grid, 128 + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
