@@ -108,6 +108,18 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
                   int64_t* conn_indptr_dev, int32_t* conn_indices_dev, float* conn_data_dev,
                   int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream);
 
+/* msc_neighbors with one more argument: distances_ready_event (a cudaEvent_t, or NULL) is recorded
+ * on the stream as soon as the kNN lists and the distances CSR are final, before the
+ * connectivities are computed, so a caller can copy them to the host on another stream meanwhile.
+ * No counterpart in the reference. */
+int msc_neighbors_ex(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+                     int32_t method, int32_t precision, int32_t kprime,
+                     int32_t* knn_idx_dev, float* knn_dist_dev,
+                     int64_t* dist_indptr_dev, int32_t* dist_indices_dev, float* dist_data_dev,
+                     int64_t* conn_indptr_dev, int32_t* conn_indices_dev, float* conn_data_dev,
+                     int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream,
+                     void* distances_ready_event);
+
 /* ---------------------------------------------------------------------------------------------
  * Exact kNN — replaces `_knn` / `_knn_gpu` (neighbors.py:698-724, 82-132): the fp16 Gram
  * distance (neighbors.py:117-118), the register top-k kernel `topk_rows` (neighbors.py:25-79),

@@ -615,6 +615,18 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
                   float* dist_data_dev, int64_t* conn_indptr_dev, int32_t* conn_indices_dev,
                   float* conn_data_dev, int64_t* stats_dev, void* workspace,
                   size_t workspace_bytes, void* stream) {
+  return msc_neighbors_ex(X_dev, n, d, k, metric, method, precision, kprime, knn_idx_dev,
+                          knn_dist_dev, dist_indptr_dev, dist_indices_dev, dist_data_dev,
+                          conn_indptr_dev, conn_indices_dev, conn_data_dev, stats_dev, workspace,
+                          workspace_bytes, stream, nullptr);
+}
+
+int msc_neighbors_ex(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
+                     int32_t method, int32_t precision, int32_t kprime, int32_t* knn_idx_dev,
+                     float* knn_dist_dev, int64_t* dist_indptr_dev, int32_t* dist_indices_dev,
+                     float* dist_data_dev, int64_t* conn_indptr_dev, int32_t* conn_indices_dev,
+                     float* conn_data_dev, int64_t* stats_dev, void* workspace,
+                     size_t workspace_bytes, void* stream, void* distances_ready_event) {
   StageRangeGuard range_guard;
   Problem P;
   MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
@@ -640,6 +652,10 @@ int msc_neighbors(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t m
   MSC_TRY(run_knn(P, w, X_dev, knn_idx_dev, knn_dist_dev, 0, st));
   MSC_TRY(launch_distances_csr(knn_idx_dev, knn_dist_dev, n, k, dist_indptr_dev, dist_indices_dev,
                                dist_data_dev, st));
+  // the distances CSR (and the kNN lists) are final here: a caller can copy them out on another
+  // stream while the connectivities are computed
+  if (distances_ready_event)
+    MSC_CUDA_TRY(cudaEventRecord(static_cast<cudaEvent_t>(distances_ready_event), st));
   if (method == MSC_METHOD_UMAP) {
     MSC_TRY(launch_smooth_knn(knn_dist_dev, n, k, 1.0f, g.sigma, g.rho, g.gsum, st));
     MSC_TRY(launch_membership(knn_idx_dev, knn_dist_dev, g.sigma, g.rho, n, k, g.w, st));

@@ -43,6 +43,8 @@ SIGNATURES = {
     "msc_neighbors_workspace_bytes": (SZ, [I64, I32, I32, I32, I32, I32, I32]),
     "msc_neighbors": (I32, [P, I64, I32, I32, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P, P,
                             SZ, P]),
+    "msc_neighbors_ex": (I32, [P, I64, I32, I32, I32, I32, I32, I32, P, P, P, P, P, P, P, P, P,
+                               P, SZ, P, P]),
     "msc_knn_workspace_bytes": (SZ, [I64, I32, I32, I32, I32, I32]),
     "msc_knn": (I32, [P, I64, I32, I32, I32, I32, I32, P, P, P, P, SZ, P]),
     "msc_batched_workspace_bytes": (SZ, [P, I32, I32, I32, I32, I32, I32]),

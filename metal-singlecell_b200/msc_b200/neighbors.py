@@ -140,6 +140,104 @@ def knn_device(X, n_neighbors: int = 15, *, metric: str = "euclidean",
     return idx, dist, stats
 
 
+class HostGraphState:
+    """Buffers reused by ``neighbors_host`` across calls of one shape: device input and outputs,
+    the workspace, pinned host outputs, a copy stream and the distances-ready event."""
+
+    def __init__(self, n: int, d: int, k: int, device=None):
+        torch = _torch()
+        self.shape = (int(n), int(d), int(k))
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        self.dev_out: dict = {}
+        self.workspace = Workspace(self.device)
+        self.copy_stream = torch.cuda.Stream(device=self.device)
+        # torch creates an event's CUDA handle at its first record: record once now, so that the
+        # handle passed to msc_neighbors_ex exists (a wait on a never-recorded event would not
+        # wait at all)
+        self.ready = torch.cuda.Event()
+        self.ready.record(torch.cuda.current_stream(self.device))
+        m = max(int(k) - 1, 0)
+        pin = lambda numel, dt: torch.empty(max(numel, 1), dtype=dt).pin_memory()
+        self.host = {"dist_indptr": pin(n + 1, torch.int64),
+                     "dist_indices": pin(n * m, torch.int32),
+                     "dist_data": pin(n * m, torch.float32),
+                     "conn_indptr": pin(n + 1, torch.int64),
+                     "conn_indices": pin(2 * n * m, torch.int32),
+                     "conn_data": pin(2 * n * m, torch.float32),
+                     "stats": pin(_lib.STATS_LEN, torch.int64)}
+        self.X = torch.empty((int(n), int(d)), dtype=torch.float32, device=self.device)
+
+
+def neighbors_host(Xh, n_neighbors: int = 15, *, metric: str = "euclidean",
+                   method: str = "umap", precision: str = DEFAULT_PRECISION, kprime: int = 0,
+                   state: HostGraphState | None = None) -> dict:
+    """The whole graph from a host embedding to host CSR matrices, with the copies overlapped.
+
+    ``Xh`` is a float32 (n, d) CPU tensor (pinned for an asynchronous upload).  The graph runs
+    through ``msc_neighbors_ex``; as soon as the kNN lists and the distances CSR are final its
+    event fires, and a second stream copies the distances CSR to the host while the
+    connectivities are computed; the connectivities follow once their size is known.  Returns the
+    pinned host tensors of ``state.host`` with ``conn_nnz``: the distances CSR is
+    ``dist_indptr`` / ``dist_indices`` / ``dist_data``, the connectivities the first ``conn_nnz``
+    entries of ``conn_indices`` / ``conn_data`` with ``conn_indptr``."""
+    torch = _torch()
+    lib = _lib.load()
+    n, d = int(Xh.shape[0]), int(Xh.shape[1])
+    k = int(n_neighbors)
+    st = state if state is not None else HostGraphState(n, d, k)
+    if st.shape != (n, d, k):
+        raise ValueError(f"state was made for {st.shape}, not {(n, d, k)}")
+    mid, meth, pid = _ids(metric, method, precision)
+    nbytes = lib.msc_neighbors_workspace_bytes(n, d, k, mid, meth, pid, int(kprime))
+    if nbytes == 0:
+        _lib.check(lib.msc_neighbors(0, n, d, k, mid, meth, pid, int(kprime), *([0] * 10), 0, 0),
+                   "msc_neighbors")
+        raise ValueError("msc_neighbors: invalid arguments")
+    ws = st.workspace.get(nbytes)
+    if not st.ready.cuda_event:
+        raise RuntimeError("neighbors_host: the distances-ready event has no CUDA handle")
+    main = torch.cuda.current_stream(st.device)
+    st.X.copy_(Xh, non_blocking=True)
+    o = st.dev_out
+    def buf(name, shape, dtype):
+        t = o.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=st.device)
+            o[name] = t
+        return t
+    m = max(k - 1, 0)
+    knn_idx, knn_dist = buf("knn_idx", (n, k), torch.int32), buf("knn_dist", (n, k), torch.float32)
+    d_ptr, d_ind = buf("dist_indptr", (n + 1,), torch.int64), buf("dist_indices", (max(n * m, 1),), torch.int32)
+    d_dat = buf("dist_data", (max(n * m, 1),), torch.float32)
+    c_ptr = buf("conn_indptr", (n + 1,), torch.int64)
+    c_ind = buf("conn_indices", (max(2 * n * m, 1),), torch.int32)
+    c_dat = buf("conn_data", (max(2 * n * m, 1),), torch.float32)
+    stats = buf("stats", (_lib.STATS_LEN,), torch.int64)
+    rc = lib.msc_neighbors_ex(st.X.data_ptr(), n, d, k, mid, meth, pid, int(kprime),
+                              knn_idx.data_ptr(), knn_dist.data_ptr(), d_ptr.data_ptr(),
+                              d_ind.data_ptr(), d_dat.data_ptr(), c_ptr.data_ptr(),
+                              c_ind.data_ptr(), c_dat.data_ptr(), stats.data_ptr(), ws.data_ptr(),
+                              ws.numel(), main.cuda_stream, st.ready.cuda_event)
+    _lib.check(rc, "msc_neighbors_ex")
+    h = st.host
+    with torch.cuda.stream(st.copy_stream):
+        st.copy_stream.wait_event(st.ready)
+        h["dist_indptr"].copy_(d_ptr, non_blocking=True)
+        h["dist_indices"][: n * m].copy_(d_ind[: n * m], non_blocking=True)
+        h["dist_data"][: n * m].copy_(d_dat[: n * m], non_blocking=True)
+    h["stats"].copy_(stats, non_blocking=True)
+    h["conn_indptr"].copy_(c_ptr, non_blocking=True)
+    main.synchronize()
+    _lib.check_stats(h["stats"].numpy())
+    nnz = int(h["conn_indptr"][n])
+    h["conn_indices"][:nnz].copy_(c_ind[:nnz], non_blocking=True)
+    h["conn_data"][:nnz].copy_(c_dat[:nnz], non_blocking=True)
+    main.synchronize()
+    st.copy_stream.synchronize()
+    return dict(h, conn_nnz=nnz)
+
+
 def graph_to_host(res: dict, n: int, k: int):
     """Device result of ``neighbors_device`` → (distances CSR, connectivities CSR) on the host,
     in SciPy's canonical layout with int32 index arrays (what SciPy itself produces for
