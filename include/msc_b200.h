@@ -61,6 +61,7 @@ extern "C" {
 #define MSC_STATS_LEN           8
 
 #define MSC_MAX_K               129 /* largest n_neighbors (above 65 every row takes the FP64 scan) */
+#define MSC_MAX_K_KNN           513 /* largest n_neighbors of msc_knn alone (FP64 scan above 65)  */
 #define MSC_MAX_D               128 /* largest representation width                             */
 
 int         msc_version(void);
@@ -124,7 +125,9 @@ int msc_neighbors_ex(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_
  * Exact kNN — replaces `_knn` / `_knn_gpu` (neighbors.py:698-724, 82-132): the fp16 Gram
  * distance (neighbors.py:117-118), the register top-k kernel `topk_rows` (neighbors.py:25-79),
  * the fp32 recompute (neighbors.py:122-123) and the host sort (neighbors.py:129-131), as one fused
- * candidate kernel + exact re-rank.  Self first; ties by index.
+ * candidate kernel + exact re-rank.  Self first; ties by index.  n_neighbors up to MSC_MAX_K_KNN
+ * (scrublet's k_adj + 1 over observed and simulated cells reaches several hundred); above 65
+ * every row takes the exact FP64 scan.
  * ------------------------------------------------------------------------------------------- */
 size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, int32_t precision,
                                int32_t kprime);

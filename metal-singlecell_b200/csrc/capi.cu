@@ -173,13 +173,14 @@ int default_kprime(int prec, int k) {
   return std::min(64, std::max(48, k + 15));
 }
 
-int check_common(int64_t n, int d, int k, int metric, int prec, int kprime) {
+int check_common(int64_t n, int d, int k, int metric, int prec, int kprime,
+                 int max_k = MSC_MAX_K) {
   if (n < 1 || n >= (int64_t(1) << 30)) { set_error("n=%lld out of range", (long long)n); return MSC_ERR_INVALID_ARG; }
   if (d < 1 || d > MSC_MAX_D) { set_error("d=%d must be in [1, %d]", d, MSC_MAX_D); return MSC_ERR_INVALID_ARG; }
   if (k < 1) { set_error("n_neighbors=%d must be at least 1", k); return MSC_ERR_INVALID_ARG; }
-  if (k > MSC_MAX_K) {
+  if (k > max_k) {
     // a valid request (any k <= n is), above the widest list the kernels keep
-    set_error("n_neighbors=%d is above the supported %d", k, MSC_MAX_K);
+    set_error("n_neighbors=%d is above the supported %d", k, max_k);
     return MSC_ERR_UNSUPPORTED;
   }
   if (metric != MSC_METRIC_EUCLIDEAN && metric != MSC_METRIC_COSINE) { set_error("unknown metric %d", metric); return MSC_ERR_INVALID_ARG; }
@@ -197,8 +198,8 @@ constexpr int PRUNE_BN = 256;
 constexpr int64_t PRUNE_MASK_MAX = int64_t(2) << 30;
 
 int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int kprime,
-                 const int64_t* offsets, int nseg) {
-  MSC_TRY(check_common(n, d, k, metric, prec, kprime));
+                 const int64_t* offsets, int nseg, int max_k = MSC_MAX_K) {
+  MSC_TRY(check_common(n, d, k, metric, prec, kprime, max_k));
   P.n = n; P.d = d; P.k = k; P.metric = metric; P.prec = prec;
   P.kprime = kprime ? kprime : default_kprime(prec, k);
   P.candidates = (k - 1) <= 64;
@@ -571,7 +572,8 @@ int msc_selftest_wait_timeout(int64_t limit_ns, int32_t* out_dev, void* stream) 
 size_t msc_knn_workspace_bytes(int64_t n, int32_t d, int32_t k, int32_t metric, int32_t precision,
                                int32_t kprime) {
   Problem P;
-  if (make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1) != MSC_OK) return 0;
+  if (make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1, MSC_MAX_K_KNN) != MSC_OK)
+    return 0;
   Carver c(nullptr);
   carve_knn(c, P);
   return c.bytes();
@@ -582,7 +584,7 @@ int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
             int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream) {
   StageRangeGuard range_guard;
   Problem P;
-  MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1));
+  MSC_TRY(make_problem(P, n, d, k, metric, precision, kprime, nullptr, 1, MSC_MAX_K_KNN));
   if (bad_ptr(X_dev, "X") || bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
       bad_ptr(workspace, "workspace"))
     return MSC_ERR_INVALID_ARG;

@@ -26,6 +26,7 @@ STAT_NONFINITE, STAT_TIMEOUT, STAT_CERTIFIED, STAT_REFINED, STAT_RESCANNED, STAT
     STAT_CONN_NNZ, STAT_PRECISION = range(8)
 STATS_LEN = 8
 MAX_K = 129
+MAX_K_KNN = 513
 MAX_D = 128
 
 P = c_void_p

@@ -40,7 +40,7 @@ def test_version_and_constants():
     (10, 0, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # d = 0
     (10, 129, 3, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),     # d > MSC_MAX_D
     (10, 5, 0, 0, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # k = 0
-    (1000, 30, 130, 0, 1, 0, _lib.MSC_ERR_UNSUPPORTED),  # k above MSC_MAX_K: valid, unsupported
+    (1000, 30, 514, 0, 1, 0, _lib.MSC_ERR_UNSUPPORTED),  # k above MSC_MAX_K_KNN: unsupported
     (10, 5, 3, 7, 1, 0, _lib.MSC_ERR_INVALID_ARG),       # metric
     (10, 5, 3, 0, 9, 0, _lib.MSC_ERR_INVALID_ARG),       # precision
     (100, 5, 30, 0, 1, 20, _lib.MSC_ERR_INVALID_ARG),    # kprime < k-1
@@ -85,3 +85,13 @@ def test_status_mapping():
         _lib.check_stats([0, 1, 0, 0, 0, 0, 0, 0])
     with pytest.raises(ValueError):
         _lib.check_stats([3, 0, 0, 0, 0, 0, 0, 0])
+
+
+def test_knn_alone_reaches_large_k():
+    lib = _lib.load()
+    assert lib.msc_knn_workspace_bytes(3000, 20, _lib.MAX_K_KNN, 0, 2, 0) > 0
+    assert lib.msc_knn_workspace_bytes(3000, 20, _lib.MAX_K_KNN + 1, 0, 2, 0) == 0
+    assert lib.msc_knn_workspace_bytes(100, 20, 101, 0, 2, 0) == 0          # k > n
+    # the whole graph keeps its own limit
+    assert lib.msc_neighbors_workspace_bytes(3000, 20, _lib.MAX_K + 1, 0, 0, 2, 0) == 0
+    assert re.search(rf"#define MSC_MAX_K_KNN\s+{_lib.MAX_K_KNN}\b", HEADER.read_text())

@@ -6,8 +6,9 @@ simulated cells among its neighbours (:300-305).
 
 Here: the same call through ``msc_b200.neighbors._knn`` on a synthetic 30-PC embedding whose
 simulated doublets are midpoints of random observed pairs, bit-identical to the oracle (indices
-and distances), so the doublet scores are identical too; at the largest n the kernels serve
-(k_adj + 1 = 127 at n = 7,225, r = 2) and one above it, which is refused as unsupported.
+and distances), so the doublet scores are identical too; up to k_adj + 1 = 214 (n = 20,000,
+r = 2; ``msc_knn`` serves k ≤ 513, n ≤ ~116k at r = 2), and one request above that width, which
+is refused as unsupported.
 """
 import numpy as np
 import pytest
@@ -38,11 +39,11 @@ def scores(knn_idx, n, k_adj, rho=0.05, r=2.0):
     return (q * rho / r) / (q * rho / r + (1 - q) * (1 - rho) + 1e-12)
 
 
-@pytest.mark.parametrize("n", [3000, 7225])
+@pytest.mark.parametrize("n", [3000, 7225, 7226, 20000])
 def test_scrublet_knn_call_equals_oracle(n):
     X, n_sim = scrublet_embedding(n)
     k_adj = k_adj_of(n, n_sim)
-    assert k_adj + 1 == {3000: 82, 7225: 127}[n]
+    assert k_adj + 1 == {3000: 82, 7225: 127, 7226: 130, 20000: 214}[n]
     idx, dist = nbm._knn(X, k_adj + 1, random_state=0)
     ridx, _, rdist = oracle.knn_exact(X, k_adj + 1)
     np.testing.assert_array_equal(idx, ridx.astype(np.int32))
@@ -51,9 +52,9 @@ def test_scrublet_knn_call_equals_oracle(n):
 
 
 def test_scrublet_above_the_supported_width_is_refused():
-    n = 7226
+    n = 116_282                       # round(0.5·√n) = 171: k_adj + 1 = 514
     X, n_sim = scrublet_embedding(n)
     k_adj = k_adj_of(n, n_sim)
-    assert k_adj + 1 == 130
+    assert k_adj + 1 == 514
     with pytest.raises(NotImplementedError):
         nbm._knn(X, k_adj + 1)
