@@ -515,8 +515,10 @@ int run_bbknn(const BbPlan& P, const BbWs& w, const float* X, const int32_t* cod
       if (P.candidates) {
         bb_items_kernel<<<grid_for(P.ntiles, BB_T), BB_T, 0, st>>>(P.n, poff, nbk, w.items);
         MSC_LAUNCH_CHECK();
-        MSC_TRY(launch_knn_tc(P.prec, P.cfg, w.Aop, w.Bop, P.n, P.p1, P.L.kp, P.L.kmma,
-                              w.items, P.ntiles, w.perm, w.qmap, nullptr, &w.counters[b], w.ctl,
+        // the query operand's map spans its zero-filled tail rows too (no box beyond the rows)
+        MSC_TRY(launch_knn_tc(P.prec, P.cfg, w.Aop, w.Bop, round_up(P.n, QTILE), P.p1, P.L.kp,
+                              P.L.kmma, w.items, P.ntiles, w.perm, w.qmap, nullptr,
+                              &w.counters[b], w.ctl,
                               P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
         MSC_CUDA_TRY(cudaMemsetAsync(w.nfail, 0, sizeof(int32_t), st));
         bb_rerank_kernel<<<gw, BB_T, 0, st>>>(X, P.d, P.n, P.p1, w.cand_idx, w.cand_thr,
