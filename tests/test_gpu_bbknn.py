@@ -40,6 +40,15 @@ def _case(name):
     if name == "fp64_only":
         X = synth.gaussian_mixture(2_000, 12, 4, seed=37)
         return X, np.random.default_rng(38).integers(0, 2, X.shape[0]), 64
+    if name == "one_cell_batch":
+        X = np.random.default_rng(44).standard_normal((2_000, 8)).astype(np.float32)
+        return X, np.array([0] * 1_999 + [1]), 4
+    if name == "one_per_batch":
+        X = synth.gaussian_mixture(5_000, 12, 5, seed=45)
+        return X, np.random.default_rng(46).integers(0, 3, X.shape[0]), 1
+    if name == "forty_batches":
+        X = synth.gaussian_mixture(4_000, 10, 8, seed=47)
+        return X, np.random.default_rng(48).integers(0, 40, X.shape[0]), 3
     if name == "coincident":
         X = np.random.default_rng(39).standard_normal((3_000, 20)).astype(np.float32)
         X[2000:2300] = X[0:300]                        # copies of batch-0 cells in batch 2
@@ -69,6 +78,7 @@ def _device_graph(X, batch, kwb, precision, trim=None):
 @pytest.mark.parametrize("name,precision", [
     ("tiny_batch", "fp16"), ("uneven", "fp16"), ("uneven", "bf16x3"), ("wide", "fp16"),
     ("widest_candidates", "fp16"), ("fp64_only", "fp16"), ("coincident", "fp16"),
+    ("one_cell_batch", "fp16"), ("one_per_batch", "fp16"), ("forty_batches", "fp16"),
 ])
 def test_bbknn_equals_oracle(name, precision):
     X, batch, kwb = _case(name)
