@@ -420,8 +420,11 @@ BbPlan bb_plan(int64_t n, int d, const int64_t* counts, int nb, int kwb, int pre
   P.candidates = P.kk_max + 1 <= 64 && prec != PREC_FP32 && d <= MSC_MAX_D;
   P.kprime = 0;
   if (P.candidates) {
+    // over-fetch: the certificate compares the kk-th neighbour with the k'-th candidate, a wide
+    // margin already at k' = 32 for the usual kk = 3 (the self path's k' = 48 is sized for the
+    // 15th neighbour); wider lists for larger kk
     P.kprime = prec == PREC_BF16X3 ? std::min(64, std::max(32, P.kk_max + 9))
-                                   : std::min(64, std::max(48, P.kk_max + 16));
+                                   : std::min(64, std::max(32, P.kk_max + 16));
     P.L = op_layout(prec, d);
     P.cfg = tc_default_config(prec, d, P.kprime);
     if (P.cfg.pair || !tc_config_ok(P.cfg, P.L.kp, P.kprime)) P.candidates = false;
