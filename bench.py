@@ -2,7 +2,8 @@
 """Benchmark of the neighbour-graph path (``pp.neighbors``) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload scale|plain|precision] [--precision fp16|bf16x3|bf16|fp32]
+                    [--workload scale|plain|precision|batch|serve|bbknn]
+                    [--precision fp16|bf16x3|bf16|fp32]
 
 A step = one full graph (exact kNN → distances CSR → UMAP connectivities) of the workload's
 synthetic embedding.  Default workload: 1,300,000 cells × 50 PCs, 200-cluster Gaussian mixture with
@@ -520,6 +521,134 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def bbknn_workload(n: int | None, batches: int, seed: int = 41):
+    """The scale embedding with uneven batch labels (Dirichlet(2) batch weights, cells drawn at
+    random, so every batch spans every cluster, as batches of one tissue do)."""
+    X, _, desc = workload("scale", n)
+    rng = np.random.default_rng(seed)
+    w = rng.dirichlet(np.full(batches, 2.0))
+    batch = rng.choice(batches, X.shape[0], p=w)
+    return X, batch, f"{desc}, {batches} batches (Dirichlet(2) sizes)"
+
+
+def bbknn_cpu_baseline(X, batch, kwb, budget_s: float = 15.0):
+    """Oracle port on the host: the exact per-batch lists of a seeded sample of query cells
+    against every batch, merged by (distance, index); cells/s = query cells / time."""
+    from oracle import bbknn as obb
+    cores = len(os.sched_getaffinity(0))
+    cats, codes = obb.batch_codes(batch)
+    members = [np.flatnonzero(codes == b) for b in range(cats.size)]
+    rng = np.random.default_rng(4321)
+    n = X.shape[0]
+    m, rows, t_total = 64, 0, 0.0
+    while t_total < budget_s * 0.5 and rows < n:
+        q = np.sort(rng.choice(n, m, replace=False))
+        t0 = time.perf_counter()
+        parts_i, parts_d = [], []
+        for mem in members:
+            loc, _, dd = obb.knn_cross(X[q], X[mem], min(kwb, mem.size))
+            parts_i.append(mem[loc])
+            parts_d.append(dd)
+        idx, dist = np.concatenate(parts_i, 1), np.concatenate(parts_d, 1)
+        np.lexsort((idx, dist), axis=1)
+        t_total += time.perf_counter() - t0
+        rows += m
+        m = int(min(n, m * 2))
+    return {"value": rows / t_total, "unit": "cells/s", "cores": cores, "kind": "port",
+            "sample": f"{rows} seeded query cells of the {n}-cell embedding against all "
+                      f"{len(members)} batches (exact per-batch lists + merge), "
+                      f"{t_total:.1f} s on {cores} threads"}
+
+
+def run_bbknn(args):
+    """Batch-balanced graph (pp.bbknn): every cell's neighbours_within_batch nearest cells of each
+    batch, fuzzy set, distances graph and trimming; cells/s with the embedding resident, the kNN
+    stage alone, and end to end through the host call."""
+    import torch
+    from msc_b200 import bbknn as bbm, neighbors as nbm, _lib
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    X, batch, desc = bbknn_workload(args.n, args.batches)
+    n, d = X.shape
+    kwb = args.neighbors_within_batch
+    _, codes, counts = bbm.batch_codes(batch)
+    Xd = torch.from_numpy(X).cuda()
+    cd = torch.from_numpy(codes).cuda()
+    ws = nbm.Workspace(Xd.device)
+
+    def graph():
+        return bbm.bbknn_device(Xd, cd, counts, kwb, precision=args.precision, workspace=ws)
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    for _ in range(max(args.warmup, 3)):
+        res = graph()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(0).uuid)
+    except Exception:
+        uuid = None
+    with ClockSampler(uuid) as cs:
+        ms, res = timed(graph, args.steps)
+    stats = res["stats"].cpu().numpy()
+    _lib.check_stats(stats)
+    K = res["K"]
+    # the kNN stage alone (candidate launches, re-rank, FP64 scans, merge)
+    cptr = np.ascontiguousarray(counts).ctypes.data
+    idx = torch.empty((n, K), dtype=torch.int32, device=Xd.device)
+    dist = torch.empty((n, K), dtype=torch.float32, device=Xd.device)
+    st = torch.cuda.current_stream().cuda_stream
+    kbytes = lib.msc_bbknn_workspace_bytes(n, d, cptr, counts.size, kwb,
+                                           _lib.PRECISION[args.precision])
+    kws = ws.get(kbytes)
+    knn = lambda: _lib.check(lib.msc_bbknn_knn(Xd.data_ptr(), n, d, cd.data_ptr(), cptr,
+                                               counts.size, kwb, _lib.PRECISION[args.precision],
+                                               idx.data_ptr(), dist.data_ptr(), 0, kws.data_ptr(),
+                                               kws.numel(), st), "msc_bbknn_knn")
+    knn()
+    knn_ms, _ = timed(knn, args.steps)
+    # end to end through the host call (host embedding in, host CSR matrices out)
+    bbm.bbknn(X, batch, kwb, n_pcs=None, precision=args.precision)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dm, cm, _ = bbm.bbknn(X, batch, kwb, n_pcs=None, precision=args.precision)
+    e2e_ms = 1000.0 * (time.perf_counter() - t0) / args.steps
+    flop = 2.0 * d * float(n) * float(n)                  # Σ_b 2·d·n·n_b
+    pk, pk_kind = peaks()
+    peak = pk.get("bf16_tflops_sustained", 1400.0)
+    line = {"metric": "bbknn: batch-balanced graph cells/s", "value": n / (ms / 1000),
+            "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "data": "synthetic",
+            "dtype": args.precision,
+            "config": {"workload": desc, "neighbors_within_batch": kwb, "K": K,
+                       "batch_sizes": [int(c) for c in counts], "trim": res["trim"]},
+            "e2e": {"value": n / (e2e_ms / 1000), "unit": "cells/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(X.nbytes + codes.nbytes),
+                    "d2h_bytes_per_step": int(dm.data.nbytes + dm.indices.nbytes
+                                              + dm.indptr.nbytes + cm.data.nbytes
+                                              + cm.indices.nbytes + cm.indptr.nbytes)},
+            "knn_stage": {"ms": knn_ms, "algorithmic_tflops": flop / (knn_ms / 1000) / 1e12,
+                          "frac_of_peak": flop / (knn_ms / 1000) / 1e12 / peak,
+                          "peak": peak, "peak_kind": f"{pk_kind} bf16 sustained",
+                          "flop": "2·d·n·Σ n_b = 2·d·n² (every cell against every batch)"},
+            "stats": {"certified": int(stats[_lib.STAT_CERTIFIED]),
+                      "rescanned": int(stats[_lib.STAT_RESCANNED]),
+                      "precision": int(stats[_lib.STAT_PRECISION])},
+            "clocks": cs.summary()}
+    if not args.skip_cpu:
+        line["cpu_baseline"] = bbknn_cpu_baseline(X, batch, kwb, args.ref_budget)
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -527,7 +656,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="scale",
-                    choices=["scale", "plain", "precision", "batch", "serve"])
+                    choices=["scale", "plain", "precision", "batch", "serve", "bbknn"])
     ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16x3", "bf16", "fp32"])
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
@@ -539,11 +668,15 @@ def main(argv=None):
     ap.add_argument("--hbm-budget-gb", type=float, default=64.0)
     ap.add_argument("--kprime", type=int, default=0, help="over-fetch k' (0: the library default)")
     ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.5, 0.7, 0.9])
+    ap.add_argument("--batches", type=int, default=8, help="bbknn workload: batches")
+    ap.add_argument("--neighbors-within-batch", type=int, default=3, help="bbknn workload")
     args = ap.parse_args(argv)
     if args.workload == "batch":
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "bbknn":
+        return run_bbknn(args)
     if args.impl == "reference":
         run_reference(args)
     else:

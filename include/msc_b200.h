@@ -202,6 +202,43 @@ int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int
                       int32_t k, int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
                       void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batch-balanced kNN — replaces metalsinglecell `neighbors.bbknn` (neighbors.py:491-559), called
+ * by `pp.bbknn` (pp.py:809-833).  Every cell gets its kk_b = min(neighbors_within_batch, n_b)
+ * nearest cells of every batch b (exact; a cell of b finds itself at distance 0), K = Σ kk_b
+ * entries per cell sorted by (distance, index).  The connectivities are the fuzzy set of these
+ * lists (msc_smooth_knn_dist / msc_membership / msc_fuzzy_union with k = K).
+ *   batch_dev   : batch code of every cell, 0 .. n_batches-1
+ *   counts_host : cells per batch (n_batches entries, each >= 1, adding up to n); they must be
+ *                 the histogram of batch_dev
+ *   knn_*_dev   : n x K, K = msc_bbknn_width(counts_host, n_batches, neighbors_within_batch)
+ * ------------------------------------------------------------------------------------------- */
+#define MSC_BBKNN_MAX_WIDTH     128 /* largest K = Σ_b min(neighbors_within_batch, n_b)          */
+int32_t msc_bbknn_width(const int64_t* counts_host, int32_t n_batches,
+                        int32_t neighbors_within_batch);
+size_t msc_bbknn_workspace_bytes(int64_t n, int32_t d, const int64_t* counts_host,
+                                 int32_t n_batches, int32_t neighbors_within_batch,
+                                 int32_t precision);
+int msc_bbknn_knn(const float* X_dev, int64_t n, int32_t d, const int32_t* batch_dev,
+                  const int64_t* counts_host, int32_t n_batches, int32_t neighbors_within_batch,
+                  int32_t precision, int32_t* knn_idx_dev, float* knn_dist_dev,
+                  int64_t* stats_dev, void* workspace, size_t workspace_bytes, void* stream);
+/* the distances graph of the lists (neighbors.py:554-557): diagonal and zero distances dropped,
+ * columns ascending; capacity n*K entries, nnz = indptr[n] */
+size_t msc_bbknn_distances_workspace_bytes(int64_t n);
+int msc_bbknn_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                            int32_t K, int64_t* indptr_dev, int32_t* indices_dev,
+                            float* data_dev, void* workspace, size_t workspace_bytes,
+                            void* stream);
+/* `_trim_graph` (neighbors.py:465-488): keep the stored entry (i, j, v) when v != 0, v >= θ_i and
+ * v >= θ_j, θ_i = the trim-th largest stored value of row i when the row stores more than `trim`
+ * entries, else 0.  Input: CSR without duplicate entries; output capacity = input nnz, in the
+ * input's order within each row; nnz = out_indptr[n] */
+size_t msc_trim_graph_workspace_bytes(int64_t n);
+int msc_trim_graph(const int64_t* indptr_dev, const int32_t* indices_dev, const float* data_dev,
+                   int64_t n, int32_t trim, int64_t* out_indptr_dev, int32_t* out_indices_dev,
+                   float* out_data_dev, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,8 @@
 //   msc_batched_*  = kNN of many samples in one persistent launch
 //   msc_smooth_knn_dist / msc_membership / msc_fuzzy_union / msc_gauss_connectivities /
 //   msc_distances_csr = the individual graph stages
+//   msc_bbknn_*    = batch-balanced kNN lists, their distances graph, and the trimming of the
+//                    connectivities                     (neighbors.py:491-559, 465-488)
 //
 // Nothing here allocates device memory: every buffer is carved out of the caller's workspace.
 #include <mutex>
@@ -838,6 +840,126 @@ int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int
     return MSC_ERR_INVALID_ARG;
   return launch_distances_csr(knn_idx_dev, knn_dist_dev, n, k, indptr_dev, indices_dev, data_dev,
                               as_stream(stream));
+}
+
+// ---- batch-balanced kNN (neighbors.py:491-559, 465-488) ----
+
+static int bb_check(int64_t n, int32_t d, const int64_t* counts_host, int32_t n_batches,
+                    int32_t kwb, int32_t precision) {
+  if (n < 1 || d < 1 || d > MSC_MAX_D) {
+    set_error("n=%lld must be >= 1 and d=%d in [1, %d]", (long long)n, d, MSC_MAX_D);
+    return MSC_ERR_INVALID_ARG;
+  }
+  if (n_batches < 1 || !counts_host) {
+    set_error("n_batches=%d must be >= 1 with a counts array", n_batches);
+    return MSC_ERR_INVALID_ARG;
+  }
+  if (kwb < 1) { set_error("neighbors_within_batch=%d must be >= 1", kwb); return MSC_ERR_INVALID_ARG; }
+  if (precision != MSC_PREC_FP32 && precision != MSC_PREC_BF16X3 && precision != MSC_PREC_FP16 &&
+      precision != MSC_PREC_BF16) {
+    set_error("unknown precision %d", precision);
+    return MSC_ERR_INVALID_ARG;
+  }
+  int64_t tot = 0, keys = 0, width = 0;
+  for (int32_t b = 0; b < n_batches; ++b) {
+    if (counts_host[b] < 1) {
+      set_error("batch %d has %lld cells (every batch needs one)", b, (long long)counts_host[b]);
+      return MSC_ERR_INVALID_ARG;
+    }
+    tot += counts_host[b];
+    keys += round_up(counts_host[b], SEG_PAD);
+    width += std::min<int64_t>(kwb, counts_host[b]);
+  }
+  if (tot != n) {
+    set_error("batch counts add up to %lld, not n=%lld", (long long)tot, (long long)n);
+    return MSC_ERR_INVALID_ARG;
+  }
+  if (width > MSC_BBKNN_MAX_WIDTH) {
+    set_error("neighbors_within_batch x batches = %lld entries per cell > %d", (long long)width,
+              MSC_BBKNN_MAX_WIDTH);
+    return MSC_ERR_INVALID_ARG;
+  }
+  if (keys + round_up(n, QTILE) >= (int64_t(1) << 31)) {
+    set_error("n=%lld is too large for 32-bit packed rows", (long long)n);
+    return MSC_ERR_INVALID_ARG;
+  }
+  return MSC_OK;
+}
+
+int32_t msc_bbknn_width(const int64_t* counts_host, int32_t n_batches, int32_t kwb) {
+  if (!counts_host || n_batches < 1 || kwb < 1) return 0;
+  int64_t width = 0;
+  for (int32_t b = 0; b < n_batches; ++b) width += std::min<int64_t>(kwb, std::max<int64_t>(counts_host[b], 0));
+  return int32_t(std::min<int64_t>(width, INT32_MAX));
+}
+
+size_t msc_bbknn_workspace_bytes(int64_t n, int32_t d, const int64_t* counts_host,
+                                 int32_t n_batches, int32_t kwb, int32_t precision) {
+  if (bb_check(n, d, counts_host, n_batches, kwb, precision) != MSC_OK) return 0;
+  return bb_workspace_bytes(bb_plan(n, d, counts_host, n_batches, kwb, precision));
+}
+
+int msc_bbknn_knn(const float* X_dev, int64_t n, int32_t d, const int32_t* batch_dev,
+                  const int64_t* counts_host, int32_t n_batches, int32_t kwb, int32_t precision,
+                  int32_t* knn_idx_dev, float* knn_dist_dev, int64_t* stats_dev,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+  MSC_TRY(bb_check(n, d, counts_host, n_batches, kwb, precision));
+  if (bad_ptr(X_dev, "X") || bad_ptr(batch_dev, "batch") || bad_ptr(knn_idx_dev, "knn_idx") ||
+      bad_ptr(knn_dist_dev, "knn_dist") || bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  const BbPlan P = bb_plan(n, d, counts_host, n_batches, kwb, precision);
+  BbWs w;
+  const size_t need = bb_carve(P, workspace, w);
+  if (need > workspace_bytes) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, need);
+    return MSC_ERR_WORKSPACE;
+  }
+  cudaStream_t st = as_stream(stream);
+  MSC_TRY(run_bbknn(P, w, X_dev, batch_dev, counts_host, knn_idx_dev, knn_dist_dev, st));
+  MSC_TRY(launch_set_stat(w.ctl, MSC_STAT_PRECISION, P.candidates ? P.prec : -1, st));
+  if (stats_dev)
+    MSC_CUDA_TRY(cudaMemcpyAsync(stats_dev, w.ctl->stats, sizeof(int64_t) * MSC_STATS_LEN,
+                                 cudaMemcpyDeviceToDevice, st));
+  return MSC_OK;
+}
+
+size_t msc_bbknn_distances_workspace_bytes(int64_t n) {
+  return n < 1 ? 0 : bb_distances_workspace_bytes(n);
+}
+
+int msc_bbknn_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
+                            int32_t K, int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || K < 1 || K > MSC_BBKNN_MAX_WIDTH) { set_error("bad n/K"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist") ||
+      bad_ptr(indptr_dev, "indptr") || bad_ptr(indices_dev, "indices") ||
+      bad_ptr(data_dev, "data") || bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (workspace_bytes < bb_distances_workspace_bytes(n)) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, bb_distances_workspace_bytes(n));
+    return MSC_ERR_WORKSPACE;
+  }
+  return launch_bb_distances(knn_idx_dev, knn_dist_dev, n, K, indptr_dev, indices_dev, data_dev,
+                             workspace, as_stream(stream));
+}
+
+size_t msc_trim_graph_workspace_bytes(int64_t n) { return n < 1 ? 0 : trim_workspace_bytes(n); }
+
+int msc_trim_graph(const int64_t* indptr_dev, const int32_t* indices_dev, const float* data_dev,
+                   int64_t n, int32_t trim, int64_t* out_indptr_dev, int32_t* out_indices_dev,
+                   float* out_data_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || trim < 1) { set_error("n=%lld and trim=%d must be >= 1", (long long)n, trim); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(indptr_dev, "indptr") || bad_ptr(indices_dev, "indices") ||
+      bad_ptr(data_dev, "data") || bad_ptr(out_indptr_dev, "out_indptr") ||
+      bad_ptr(out_indices_dev, "out_indices") || bad_ptr(out_data_dev, "out_data") ||
+      bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (workspace_bytes < trim_workspace_bytes(n)) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, trim_workspace_bytes(n));
+    return MSC_ERR_WORKSPACE;
+  }
+  return launch_trim(indptr_dev, indices_dev, data_dev, n, trim, out_indptr_dev, out_indices_dev,
+                     out_data_dev, workspace, as_stream(stream));
 }
 
 }  // extern "C"

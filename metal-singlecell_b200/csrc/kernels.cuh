@@ -259,4 +259,55 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
                  int64_t n, int k, int64_t* indptr, int32_t* indices, float* data,
                  int64_t* nnz_dev, void* ws, size_t ws_bytes, cudaStream_t st);
 
+
+// ---- bbknn.cu ----
+// batch-balanced kNN (neighbors.py:491-559): plan from the per-batch cell counts
+struct BbPlan {
+  int64_t n;
+  int d, nb, kwb, prec;
+  int K;              // Σ_b min(kwb, n_b): entries per cell
+  int kk_max;
+  int64_t p1;         // key rows (batches, each padded to SEG_PAD)
+  int64_t npk;        // p1 + the query region
+  int64_t max_nb;
+  int64_t ntiles;     // 128-cell query tiles
+  bool candidates;    // tensor-core candidates + certificate, else the FP64 scan for every cell
+  int kprime;
+  OpLayout L;
+  TcConfig cfg;
+};
+struct BbWs {
+  Ctl* ctl;
+  KeyMax* km;
+  SegDesc* seg;
+  int32_t* nfail;
+  int32_t* counters;
+  int32_t* perm;
+  int32_t* qmap;
+  int32_t* flag;
+  int64_t* S;
+  int64_t* scan;
+  int32_t* fail_rows;
+  double* mean;
+  double* partial;
+  void* Aop;
+  void* Bop;
+  QStat* qs;
+  WorkItem* items;
+  int32_t* cand_idx;
+  float* cand_thr;
+};
+BbPlan bb_plan(int64_t n, int d, const int64_t* counts, int nb, int kwb, int prec);
+size_t bb_carve(const BbPlan& P, void* base, BbWs& w);
+size_t bb_workspace_bytes(const BbPlan& P);
+int run_bbknn(const BbPlan& P, const BbWs& w, const float* X, const int32_t* codes,
+              const int64_t* counts, int32_t* knn_idx, float* knn_dist, cudaStream_t st);
+size_t bb_distances_workspace_bytes(int64_t n);
+int launch_bb_distances(const int32_t* idx, const float* dist, int64_t n, int K, int64_t* indptr,
+                        int32_t* indices, float* data, void* ws, cudaStream_t st);
+size_t trim_workspace_bytes(int64_t n);
+int launch_trim(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n,
+                int trim, int64_t* out_ptr, int32_t* out_idx, float* out_data, void* ws,
+                cudaStream_t st);
+
 }  // namespace msc

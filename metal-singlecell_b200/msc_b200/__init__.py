@@ -6,11 +6,12 @@ GPU through the C ABI in ``include/msc_b200.h``.
 
     import msc_b200 as msc
     msc.pp.neighbors(adata, n_neighbors=15)
+    msc.pp.bbknn(adata, batch_key="batch")      # batch-balanced graph
 """
 
-from . import pp, neighbors, synth, _lib
+from . import pp, neighbors, bbknn, synth, _lib
 from .anndata_lite import AnnDataLite
 
 __version__ = "0.1.0"
 
-__all__ = ["pp", "neighbors", "synth", "AnnDataLite", "__version__"]
+__all__ = ["pp", "neighbors", "bbknn", "synth", "AnnDataLite", "__version__"]

@@ -28,6 +28,7 @@ STATS_LEN = 8
 MAX_K = 129
 MAX_K_KNN = 513
 MAX_D = 128
+BBKNN_MAX_WIDTH = 128
 
 P = c_void_p
 I32, I64, SZ, F32 = c_int32, c_int64, c_size_t, c_float
@@ -59,6 +60,13 @@ SIGNATURES = {
     "msc_gauss_workspace_bytes": (SZ, [I64, I32]),
     "msc_gauss_connectivities": (I32, [P, P, I64, I32, P, P, P, P, P, SZ, P]),
     "msc_distances_csr": (I32, [P, P, I64, I32, P, P, P, P]),
+    "msc_bbknn_width": (I32, [P, I32, I32]),
+    "msc_bbknn_workspace_bytes": (SZ, [I64, I32, P, I32, I32, I32]),
+    "msc_bbknn_knn": (I32, [P, I64, I32, P, P, I32, I32, I32, P, P, P, P, SZ, P]),
+    "msc_bbknn_distances_workspace_bytes": (SZ, [I64]),
+    "msc_bbknn_distances_csr": (I32, [P, P, I64, I32, P, P, P, P, SZ, P]),
+    "msc_trim_graph_workspace_bytes": (SZ, [I64]),
+    "msc_trim_graph": (I32, [P, P, P, I64, I32, P, P, P, P, SZ, P]),
 }
 
 _lib = None

@@ -1,8 +1,8 @@
-"""A minimal AnnData stand-in: the slots ``pp.neighbors`` reads and writes.
+"""A minimal AnnData stand-in: the slots ``pp.neighbors`` and ``pp.bbknn`` read and write.
 
-``pp.neighbors`` works on any object exposing ``X``, ``n_obs``, ``n_vars``, ``obsm``, ``obsp``,
-``uns`` and ``copy()`` — a real ``anndata.AnnData`` included.  This class provides exactly that
-for environments without anndata.
+They work on any object exposing ``X``, ``n_obs``, ``n_vars``, ``obs`` (per-cell columns),
+``obsm``, ``obsp``, ``uns`` and ``copy()`` — a real ``anndata.AnnData`` included.  This class
+provides exactly that for environments without anndata; ``obs`` is a dict of per-cell arrays.
 """
 
 from __future__ import annotations
@@ -11,8 +11,10 @@ import copy as _copy
 
 
 class AnnDataLite:
-    def __init__(self, X=None, *, obsm=None, obsp=None, uns=None, n_obs=None, n_vars=None):
+    def __init__(self, X=None, *, obs=None, obsm=None, obsp=None, uns=None, n_obs=None,
+                 n_vars=None):
         self.X = X
+        self.obs = dict(obs or {})
         self.obsm = dict(obsm or {})
         self.obsp = dict(obsp or {})
         self.uns = dict(uns or {})
@@ -34,5 +36,5 @@ class AnnDataLite:
         return _copy.deepcopy(self)
 
     def __repr__(self):
-        return (f"AnnDataLite(n_obs={self.n_obs}, n_vars={self.n_vars}, obsm={list(self.obsm)}, "
-                f"obsp={list(self.obsp)}, uns={list(self.uns)})")
+        return (f"AnnDataLite(n_obs={self.n_obs}, n_vars={self.n_vars}, obs={list(self.obs)}, "
+                f"obsm={list(self.obsm)}, obsp={list(self.obsp)}, uns={list(self.uns)})")

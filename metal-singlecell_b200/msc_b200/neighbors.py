@@ -5,7 +5,9 @@ Mirrors metalsinglecell ``neighbors.py``:
 * ``neighbors(X_pca, n_neighbors, random_state, approx)`` → ``(distances, connectivities)`` SciPy
   CSR matrices (neighbors.py:727-760);
 * ``_knn(X_pca, n_neighbors, random_state, approx)`` → ``(indices, dists)`` of shape (n, k), self
-  first, ascending (neighbors.py:698-724).
+  first, ascending (neighbors.py:698-724);
+* ``bbknn(X_pca, batch, neighbors_within_batch, n_pcs, trim, random_state)`` and
+  ``_trim_graph(conn, trim)`` (neighbors.py:491-559, 465-488), implemented in ``msc_b200.bbknn``.
 
 Everything runs on one GPU through the C ABI of ``libmsc_b200.so``; PyTorch only provides the
 device buffers and the current stream.  Unlike the reference, the kNN is exact at every size (no
@@ -344,3 +346,17 @@ def _knn(X_pca: np.ndarray, n_neighbors: int, random_state: int = 0,
     torch.cuda.current_stream(dev).synchronize()
     _lib.check_stats(stats.cpu().numpy())
     return idx.cpu().numpy(), dist.cpu().numpy()
+
+
+def bbknn(X_pca: np.ndarray, batch, neighbors_within_batch: int = 3, n_pcs: int | None = 50,
+          trim: int | None = None, random_state: int = 0, **kw):
+    """Batch-balanced kNN graph (neighbors.py:491-559); see ``msc_b200.bbknn.bbknn``."""
+    from .bbknn import bbknn as _impl
+    return _impl(X_pca, batch, neighbors_within_batch, n_pcs, trim, random_state, **kw)
+
+
+def _trim_graph(conn, trim):
+    """Each cell's ``trim`` strongest connectivities (neighbors.py:465-488), on the GPU; see
+    ``msc_b200.bbknn.trim_graph``."""
+    from .bbknn import trim_graph as _impl
+    return _impl(conn, trim)

@@ -1,4 +1,5 @@
-"""AnnData-facing drop-in for ``msc.pp.neighbors`` (metalsinglecell pp.py:722-788).
+"""AnnData-facing drop-ins for ``msc.pp.neighbors`` (metalsinglecell pp.py:722-788) and
+``msc.pp.bbknn`` (pp.py:809-833).
 
 ``neighbors(adata, n_neighbors=15, n_pcs=None, *, use_rep=None, metric='euclidean',
 method='umap', key_added=None, random_state=0, copy=False)`` writes the same slots as the
@@ -14,6 +15,7 @@ from __future__ import annotations
 import numpy as np
 
 from .neighbors import neighbors as _nb, DEFAULT_PRECISION
+from .bbknn import bbknn as _bbknn
 
 _N_PCS_DEFAULT = 50            # scanpy's settings.N_PCS
 
@@ -73,6 +75,36 @@ def neighbors(adata, n_neighbors: int = 15, n_pcs: int | None = None, *,
         params["n_pcs"] = n_pcs
     adata.uns["neighbors" if key_added is None else key_added] = {
         "connectivities_key": ck, "distances_key": dk, "params": params}
+    return adata if copy else None
+
+
+def _obs_column(adata, key):
+    col = adata.obs[key]
+    return col.to_numpy() if hasattr(col, "to_numpy") else np.asarray(col)
+
+
+def bbknn(adata, batch_key: str = "batch", *, use_rep: str = "X_pca",
+          neighbors_within_batch: int = 3, n_pcs: int | None = 50, trim: int | None = None,
+          random_state: int = 0, copy: bool = False, precision: str = DEFAULT_PRECISION):
+    """Batch-balanced kNN (``sc.external.pp.bbknn``); writes ``obsp['distances']`` /
+    ``['connectivities']`` and ``uns['neighbors']`` with ``n_neighbors`` = the width of the
+    combined lists, ``neighbors_within_batch`` × the batch count for batches of at least that
+    size (pp.py:809-833).  Returns ``None``, or the modified copy if ``copy``."""
+    adata = adata.copy() if copy else adata
+    if use_rep not in adata.obsm:
+        raise ValueError(f"Did not find {use_rep} in .obsm.keys(). You need to compute it first.")
+    dist, conn, n_neighbors = _bbknn(np.asarray(adata.obsm[use_rep], dtype=np.float32),
+                                     _obs_column(adata, batch_key),
+                                     neighbors_within_batch=neighbors_within_batch, n_pcs=n_pcs,
+                                     trim=trim, random_state=random_state, precision=precision)
+    adata.obsp["distances"] = dist
+    adata.obsp["connectivities"] = conn
+    adata.uns["neighbors"] = {
+        "connectivities_key": "connectivities", "distances_key": "distances",
+        "params": {"n_neighbors": n_neighbors, "method": "umap", "metric": "euclidean",
+                   "random_state": random_state, "use_rep": use_rep, "n_pcs": n_pcs,
+                   "bbknn": {"trim": 10 * n_neighbors if trim is None else trim,
+                             "computation": "cuda"}}}
     return adata if copy else None
 
 

@@ -95,3 +95,28 @@ def test_knn_alone_reaches_large_k():
     # the whole graph keeps its own limit
     assert lib.msc_neighbors_workspace_bytes(3000, 20, _lib.MAX_K + 1, 0, 0, 2, 0) == 0
     assert re.search(rf"#define MSC_MAX_K_KNN\s+{_lib.MAX_K_KNN}\b", HEADER.read_text())
+
+
+def test_bbknn_argument_checks():
+    lib = _lib.load()
+    C = lambda *v: (ctypes.c_int64 * len(v))(*v)
+    inv = _lib.MSC_ERR_INVALID_ARG
+    assert lib.msc_bbknn_width(C(40, 2, 18), 3, 3) == 3 + 2 + 3
+    assert lib.msc_bbknn_workspace_bytes(60, 10, C(40, 2, 18), 3, 3, 2) > 0
+    assert lib.msc_bbknn_workspace_bytes(60, 10, C(40, 2, 17), 3, 3, 2) == 0   # counts != n
+    assert lib.msc_bbknn_workspace_bytes(60, 10, C(40, 0, 20), 3, 3, 2) == 0   # an empty batch
+    assert lib.msc_bbknn_workspace_bytes(600, 10, C(300, 300), 2, 65, 2) == 0  # K = 130 > 128
+    assert lib.msc_bbknn_workspace_bytes(600, 10, C(300, 300), 2, 64, 2) > 0   # K = 128
+    assert lib.msc_bbknn_workspace_bytes(60, 129, C(60), 1, 3, 2) == 0         # d > MSC_MAX_D
+    assert lib.msc_bbknn_workspace_bytes(60, 10, C(60), 1, 0, 2) == 0          # k = 0
+    assert lib.msc_bbknn_workspace_bytes(60, 10, C(60), 1, 3, 9) == 0          # precision
+    assert lib.msc_bbknn_knn(None, 60, 10, None, C(40, 2, 18), 3, 3, 2, None, None, None, None,
+                             0, None) == inv
+    assert "X" in _lib.last_error()
+    assert lib.msc_bbknn_distances_csr(None, None, 10, 129, None, None, None, None, 0,
+                                       None) == inv
+    assert lib.msc_trim_graph(None, None, None, 10, 0, None, None, None, None, 0, None) == inv
+    assert lib.msc_bbknn_distances_workspace_bytes(1000) > 0
+    assert lib.msc_trim_graph_workspace_bytes(1000) > 0
+    text = HEADER.read_text()
+    assert re.search(rf"#define MSC_BBKNN_MAX_WIDTH\s+{_lib.BBKNN_MAX_WIDTH}\b", text)

@@ -94,3 +94,53 @@ def test_metric_and_method(fake_compute):
         pp.neighbors(a, 5, metric="manhattan")
     with pytest.raises(ValueError):
         pp.neighbors(a, 5, method="rapids")
+
+
+@pytest.fixture
+def fake_bbknn(monkeypatch):
+    from oracle import bbknn as obb
+    calls = []
+
+    def _bb(X, batch, neighbors_within_batch=3, n_pcs=50, trim=None, random_state=0,
+            precision="fp16"):
+        calls.append((X.shape, neighbors_within_batch, n_pcs, trim))
+        dist, conn, K, _ = obb.bbknn(X, batch, neighbors_within_batch, n_pcs, trim)
+        return dist, conn, K
+
+    monkeypatch.setattr(pp, "_bbknn", _bb)
+    return calls
+
+
+def bb_adata(n=150, d=20):
+    rng = np.random.default_rng(3)
+    return AnnDataLite(X=rng.standard_normal((n, 30)).astype(np.float32),
+                       obs={"batch": np.array(["x", "y", "z"])[rng.integers(0, 3, n)],
+                            "donor": np.array(["d1", "d2"])[rng.integers(0, 2, n)]},
+                       obsm={"X_pca": rng.standard_normal((n, d)).astype(np.float32)})
+
+
+def test_bbknn_slots_and_params(fake_bbknn):
+    a = bb_adata()
+    assert pp.bbknn(a) is None
+    assert set(a.obsp) == {"distances", "connectivities"}
+    u = a.uns["neighbors"]
+    assert u["connectivities_key"] == "connectivities" and u["distances_key"] == "distances"
+    p = u["params"]
+    # n_neighbors = neighbors_within_batch x batches (the combined width)
+    assert p["n_neighbors"] == 9 and p["method"] == "umap" and p["metric"] == "euclidean"
+    assert p["use_rep"] == "X_pca" and p["n_pcs"] == 50
+    assert p["bbknn"]["trim"] == 90
+    assert fake_bbknn[-1] == ((150, 20), 3, 50, None)
+    assert pp.connectivities(a) is a.obsp["connectivities"]
+
+
+def test_bbknn_options_and_copy(fake_bbknn):
+    a = bb_adata()
+    b = pp.bbknn(a, batch_key="donor", neighbors_within_batch=4, n_pcs=10, trim=5, copy=True)
+    assert not a.obsp and b.uns["neighbors"]["params"]["n_neighbors"] == 8
+    assert b.uns["neighbors"]["params"]["bbknn"]["trim"] == 5
+    assert fake_bbknn[-1] == ((150, 20), 4, 10, 5)
+    with pytest.raises(ValueError):
+        pp.bbknn(a, use_rep="X_umap")
+    with pytest.raises(KeyError):
+        pp.bbknn(a, batch_key="sample")
