@@ -259,4 +259,19 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
                  int64_t n, int k, int64_t* indptr, int32_t* indices, float* data,
                  int64_t* nnz_dev, void* ws, size_t ws_bytes, cudaStream_t st);
 
+
+// ---- spatial.cu ----
+size_t spatial_knn_workspace_bytes(int64_t n);
+int launch_spatial_knn(const float* X, int64_t n, int d, int k, int32_t* idx, float* dist,
+                       int64_t* stats, void* ws, cudaStream_t st);
+size_t spatial_radius_workspace_bytes(int64_t n);
+int launch_spatial_radius_count(const float* X, int64_t n, int d, double radius, double min_radius,
+                                int64_t* indptr, int64_t* stats, void* ws, cudaStream_t st);
+size_t spatial_radius_fill_scratch_bytes(int64_t nnz);
+int launch_spatial_radius_fill(int64_t n, int d, double radius, double min_radius,
+                               const int64_t* indptr, int64_t nnz, int32_t* cols, float* dist,
+                               void* ws, void* scratch, cudaStream_t st);
+int launch_spatial_edge_lengths(const double* X, int64_t n, int d, const int64_t* indptr,
+                                const int32_t* cols, double* out, cudaStream_t st);
+
 }  // namespace msc

@@ -1,7 +1,8 @@
 """A minimal AnnData stand-in: the slots ``pp.neighbors`` reads and writes.
 
 ``pp.neighbors`` works on any object exposing ``X``, ``n_obs``, ``n_vars``, ``obsm``, ``obsp``,
-``uns`` and ``copy()`` — a real ``anndata.AnnData`` included.  This class provides exactly that
+``uns`` and ``copy()`` — a real ``anndata.AnnData`` included; the spatial builders also read
+``obs`` (a mapping or DataFrame of per-observation columns).  This class provides exactly that
 for environments without anndata.
 """
 
@@ -11,8 +12,10 @@ import copy as _copy
 
 
 class AnnDataLite:
-    def __init__(self, X=None, *, obsm=None, obsp=None, uns=None, n_obs=None, n_vars=None):
+    def __init__(self, X=None, *, obs=None, obsm=None, obsp=None, uns=None, n_obs=None,
+                 n_vars=None):
         self.X = X
+        self.obs = obs if obs is not None else {}
         self.obsm = dict(obsm or {})
         self.obsp = dict(obsp or {})
         self.uns = dict(uns or {})
