@@ -134,6 +134,11 @@ __global__ void sp_plan_kernel(const unsigned* __restrict__ mm,
     cells = 1;
     for (int a = 0; a < 3; ++a) cells *= ext[a] > 0 ? ceil(ext[a] / cs) + 1.0 : 1.0;
     if (cells <= cap) { ok = true; break; }
+    if (!isfinite(cells) || !(cs > 0)) {
+      // a cell side so small that the cell count overflows: restart from two cells per axis
+      cs = fmax(fmax(ext[0], ext[1]), ext[2]) * 0.5;
+      continue;
+    }
     cs *= pow(cells / cap, 1.0 / (eff > 0 ? eff : 1)) * (1.0 + 1e-9);
   }
   if (!ok || !(cs > 0) || !isfinite(cs)) { g.status = 2; *G = g; return; }
