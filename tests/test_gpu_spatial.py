@@ -201,3 +201,28 @@ def test_errors_and_nonfinite():
         msp.radius_grid_device(torch.from_numpy(X).cuda(), 10.0)
     with pytest.raises(ValueError):
         msp.knn_grid_device(torch.from_numpy(case("jitter")).cuda(), 0)
+
+
+def test_full_size_slide():
+    """1,000,000 spots of the bench's synthetic slide, k = 7 and a 30 µm radius: properties that
+    hold at any size, and bit-exact rows against the oracle on 128 seeded spots (each scanned
+    against all 1M)."""
+    import torch
+    import bench
+    xy = bench.spatial_slide(1_000_000).astype(np.float32)
+    n = xy.shape[0]
+    gi, gd, st = knn_device(xy, 7)
+    assert (gi[:, 0] == np.arange(n)).all() and (gd[:, 0] == 0).all()
+    assert gi.min() >= 0 and gi.max() < n
+    assert (np.diff(gd, axis=1) >= 0).all()
+    s = np.sort(gi, axis=1)
+    assert (np.diff(s, axis=1) > 0).all()
+    rows = np.sort(np.random.default_rng(20261204).choice(n, 128, replace=False))
+    oi, od = osp.grid_knn(xy, 7, rows=rows)
+    np.testing.assert_array_equal(gi[rows], oi.astype(np.int32))
+    np.testing.assert_array_equal(gd[rows], od)
+    ip, c, d = radius_device(xy, 30.0)
+    A = sp.csr_matrix((d, c, ip), shape=(n, n))
+    assert A.has_sorted_indices and A.diagonal().sum() == 0
+    assert (abs(A - A.T) > 0).nnz == 0                    # symmetric, distances bit-equal
+    assert d.max() <= 30.0
