@@ -1,5 +1,5 @@
-"""Spatial graph builders (squidpy's ``gr.spatial_neighbors_knn`` / ``_radius`` contract), as
-metalsinglecell's ``gr`` provides them (gr.py:19-255), on the GPU grid search of
+"""Spatial graph builders (squidpy's ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid``
+contract), as metalsinglecell's ``gr`` provides them (gr.py:19-300), on the GPU grid search of
 ``msc_b200.spatial``.
 
 The search and the FP64 edge lengths run on the device; the tail the reference runs on the host
@@ -149,6 +149,106 @@ def radius_edges(x64: np.ndarray, lo: float, hi: float, device=None):
     indptr, cols, _, _ = _sp.radius_grid_device(x64d.float(), hi, lo)
     length = _sp.edge_lengths_device(x64d, indptr, cols)
     return indptr.cpu().numpy(), cols.cpu().numpy(), length.cpu().numpy()
+
+
+def knn_edges_f32(x64: np.ndarray, n_neighs: int, device=None):
+    """``(cols int32 (n·n_neighs,), dist float32)``: each point's n_neighs nearest other points
+    and their float32 grid distances (the lists the lattice builder corrects by the median)."""
+    torch = _torch()
+    dev = _sp._device(torch, device)
+    n = x64.shape[0]
+    if not 0 < n_neighs < n:
+        raise ValueError(f"n_neighs={n_neighs} must be in [1, n - 1 = {n - 1}]")
+    x32 = torch.from_numpy(np.ascontiguousarray(x64, np.float64)).to(dev).float()
+    idx, dist = _sp.knn_lists_device(x32, n_neighs + 1)
+    return (idx[:, 1:].contiguous().view(-1).cpu().numpy(),
+            dist[:, 1:].contiguous().view(-1).cpu().numpy())
+
+
+def _with_diag(M):
+    """1.0 on the diagonal of a 0/1 (or ring-valued, diagonal ≤ 1) CSR."""
+    import scipy.sparse as sp
+    return M.maximum(sp.identity(M.shape[0], format="csr", dtype=M.dtype)).tocsr()
+
+
+def _without_diag(M):
+    rows = np.repeat(np.arange(M.shape[0]), np.diff(M.indptr))
+    return _keep(M, M.indices != rows)
+
+
+def _rings(adj, n_rings: int):
+    """Breadth-first ring index of every point reachable within ``n_rings`` steps of the
+    graph (the point itself at 1 with its direct neighbours, then 2, 3, ...): squidpy's grid
+    convention, where the distances hold the ring, not a length."""
+    import scipy.sparse as sp
+    step = _with_diag(adj).astype(bool).astype(np.float32)
+    reached = step.copy()
+    level = step.copy()
+    frontier = step
+    for r in range(2, n_rings + 1):
+        nxt = (frontier @ step).astype(bool).tocsr()
+        fresh = (nxt.astype(np.int8) - nxt.multiply(reached.astype(bool)).astype(np.int8)).tocsr()
+        fresh.eliminate_zeros()
+        if fresh.nnz == 0:
+            break
+        fresh = fresh.astype(np.float32)
+        frontier = fresh
+        reached = (reached + fresh).tocsr()
+        fresh.data[:] = float(r)
+        level = (level + fresh).tocsr()
+    return sp.csr_matrix(level)
+
+
+def _delaunay(x32: np.ndarray):
+    """Symmetric 0/1 adjacency of the Delaunay triangulation (SciPy's Qhull, as gr.py:303-310
+    builds it from the float32 working coordinates)."""
+    import scipy.sparse as sp
+    from scipy.spatial import Delaunay
+    tri = Delaunay(np.asarray(x32, dtype=np.float64))
+    indptr, indices = tri.vertex_neighbor_vertices
+    n = x32.shape[0]
+    return sp.csr_matrix((np.ones(indices.size, np.float32), indices, indptr), shape=(n, n))
+
+
+def spatial_neighbors_grid(adata, *, n_neighs: int = 6, n_rings: int = 1, delaunay: bool = False,
+                           spatial_key: str = "spatial", library_key: str | None = None,
+                           transform: str | None = None, set_diag: bool = False,
+                           key_added: str = "spatial", copy: bool = False, device=None):
+    """Lattice spatial graph (gr.py:257-300), the Visium / Stereo-seq mode: the n_neighs-NN
+    graph without the edges longer than 1.3 × the median kNN distance (squidpy's lattice
+    correction; or the Delaunay triangulation), expanded to ``n_rings`` rings; binary
+    connectivities, distances holding the ring index."""
+    import scipy.sparse as sp
+
+    def build(x64):
+        n = x64.shape[0]
+        x32 = x64.astype(np.float32)
+        if delaunay:
+            adj = _delaunay(x32)
+        else:
+            cols, dist = knn_edges_f32(x64, n_neighs, device)
+            rows = np.repeat(np.arange(n), n_neighs)
+            keep = dist < np.median(dist) * 1.3
+            adj = sp.csr_matrix((np.ones(int(keep.sum()), np.float32), (rows[keep], cols[keep])),
+                                shape=(n, n))
+        if n_rings > 1:
+            lv = _rings(adj, n_rings)
+            lv = _with_diag(lv) if set_diag else _without_diag(lv)
+            lv.eliminate_zeros()
+            dst = lv.copy()
+            adj = lv.copy()
+            adj.data[:] = 1.0
+        else:
+            if set_diag:
+                adj = _with_diag(adj)
+            dst = adj.copy()
+        return adj, dst
+
+    adj, dst = _assemble(_coords(adata, spatial_key), _library_groups(adata, library_key), build,
+                         transform, set_diag, None)
+    return _write(adata, adj, dst, {"coord_type": "grid", "n_neighbors": n_neighs,
+                                    "n_rings": n_rings, "delaunay": delaunay},
+                  key_added, transform, copy)
 
 
 def _pair(n, indptr, cols, length):

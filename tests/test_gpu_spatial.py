@@ -178,7 +178,8 @@ def test_builders_equal_reference_gr():
             obs["library"] = pd.Categorical.from_codes(g[f"{name}_library"], ["s0", "s1", "s2"])
             extra["library_key"] = "library"
         a = AnnDataLite(obs=obs, obsm={"spatial": xy}, n_obs=xy.shape[0])
-        fn = gr.spatial_neighbors_knn if kind == "knn" else gr.spatial_neighbors_radius
+        fn = {"knn": gr.spatial_neighbors_knn, "radius": gr.spatial_neighbors_radius,
+              "grid": gr.spatial_neighbors_grid}[kind]
         res = fn(a, copy=True, **kw, **extra)
         for tag, M in (("adj", res.connectivities), ("dst", res.distances)):
             M = sp.csr_matrix(M)

@@ -33,9 +33,15 @@ def _oracle_radius_edges(x64, lo, hi, device=None):
     return indptr, cols, osp.edge_lengths_f64(x64, rows, cols)
 
 
+def _oracle_knn_edges_f32(x64, n_neighs, device=None):
+    _, cols, dist = osp.knn_edges(x64.astype(np.float32), n_neighs)
+    return cols.astype(np.int32), dist
+
+
 @pytest.fixture
 def oracle_search(monkeypatch):
     monkeypatch.setattr(gr, "knn_edges", _oracle_knn_edges)
+    monkeypatch.setattr(gr, "knn_edges_f32", _oracle_knn_edges_f32)
     monkeypatch.setattr(gr, "radius_edges", _oracle_radius_edges)
 
 
@@ -52,7 +58,7 @@ def golden_cases():
 def adata_for(xy, lib):
     obs = {}
     if lib is not None:
-        obs["library"] = pd.Categorical.from_codes(lib, ["s0", "s1", "s2"])
+        obs["library"] = pd.Categorical.from_codes(lib, ["s0", "s1", "s2"][:max(3, lib.max() + 1)])
     return AnnDataLite(obs=obs, obsm={"spatial": xy}, n_obs=xy.shape[0])
 
 
@@ -69,14 +75,15 @@ def assert_same(M, g, c, tag):
 def test_builders_equal_reference_gr(oracle_search):
     n = 0
     for c, kind, xy, lib, kw, g in golden_cases():
-        fn = gr.spatial_neighbors_knn if kind == "knn" else gr.spatial_neighbors_radius
+        fn = {"knn": gr.spatial_neighbors_knn, "radius": gr.spatial_neighbors_radius,
+              "grid": gr.spatial_neighbors_grid}[kind]
         extra = {"library_key": "library"} if lib is not None else {}
         res = fn(adata_for(xy, lib), copy=True, **kw, **extra)
         assert isinstance(res, gr.SpatialNeighborsResult)
         assert_same(res.connectivities, g, c, "adj")
         assert_same(res.distances, g, c, "dst")
         n += 1
-    assert n == 13
+    assert n == 20
 
 
 def test_slots_and_params(oracle_search):
