@@ -1,6 +1,7 @@
-"""Spatial graph builders (squidpy's ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid``
-contract), as metalsinglecell's ``gr`` provides them (gr.py:19-300), on the GPU grid search of
-``msc_b200.spatial``.
+"""Spatial graph builders (squidpy's ``gr.spatial_neighbors_knn`` / ``_radius`` / ``_grid`` /
+``_delaunay`` contract), as metalsinglecell's ``gr`` provides them (gr.py:19-368): the first three
+on the GPU grid search of ``msc_b200.spatial``, the Delaunay triangulation on SciPy's Qhull (as
+the reference has it) with the edge lengths on the GPU.
 
 The search and the FP64 edge lengths run on the device; the tail the reference runs on the host
 with SciPy — percentile pruning on the distances, ``set_diag``, the adjacency transform, the
@@ -248,6 +249,54 @@ def spatial_neighbors_grid(adata, *, n_neighs: int = 6, n_rings: int = 1, delaun
                          transform, set_diag, None)
     return _write(adata, adj, dst, {"coord_type": "grid", "n_neighbors": n_neighs,
                                     "n_rings": n_rings, "delaunay": delaunay},
+                  key_added, transform, copy)
+
+
+def delaunay_edges(x64: np.ndarray, device=None):
+    """``(rows, cols, lengths float64)`` of the Delaunay triangulation of the float64
+    coordinates (SciPy's Qhull, gr.py:313-320, 355-357), lengths on the device."""
+    import scipy.sparse as sp
+    from scipy.spatial import Delaunay
+    torch = _torch()
+    dev = _sp._device(torch, device)
+    n = x64.shape[0]
+    indptr, indices = Delaunay(np.asarray(x64, dtype=np.float64)).vertex_neighbor_vertices
+    A = sp.csr_matrix((np.ones(indices.size, np.float32), indices, indptr), shape=(n, n)).tocoo()
+    # COO of the CSR: rows ascending, columns in stored order within a row
+    ip = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(A.row, minlength=n), out=ip[1:])
+    length = _sp.edge_lengths_device(torch.from_numpy(np.ascontiguousarray(x64, np.float64)).to(dev),
+                                     torch.from_numpy(ip).to(dev),
+                                     torch.from_numpy(A.col.astype(np.int32)).to(dev))
+    return A.row, A.col, length.cpu().numpy()
+
+
+def spatial_neighbors_delaunay(adata, *, radius=None, spatial_key: str = "spatial",
+                               library_key: str | None = None, percentile: float | None = None,
+                               transform: str | None = None, set_diag: bool = False,
+                               key_added: str = "spatial", copy: bool = False, device=None):
+    """Delaunay spatial graph (gr.py:323-368): the triangulation (SciPy's Qhull, as the
+    reference and squidpy use), optionally pruned to edges of length within ``radius`` (a
+    maximum or a (min, max) interval); binary connectivities, FP64 edge lengths."""
+    import scipy.sparse as sp
+    stored = radius
+    if radius is not None:
+        lo, hi = ((0.0, float(radius)) if np.isscalar(radius)
+                  else (float(min(radius)), float(max(radius))))
+        stored = (lo, hi)
+
+    def build(x64):
+        n = x64.shape[0]
+        rows, cols, dist = delaunay_edges(x64, device)
+        if radius is not None:
+            keep = (dist >= lo) & (dist <= hi)
+            rows, cols, dist = rows[keep], cols[keep], dist[keep]
+        return (sp.csr_matrix((np.ones(dist.size, np.float32), (rows, cols)), shape=(n, n)),
+                sp.csr_matrix((dist, (rows, cols)), shape=(n, n)))
+
+    adj, dst = _assemble(_coords(adata, spatial_key), _library_groups(adata, library_key), build,
+                         transform, set_diag, percentile)
+    return _write(adata, adj, dst, {"coord_type": "generic", "radius": stored},
                   key_added, transform, copy)
 
 

@@ -179,7 +179,7 @@ def test_builders_equal_reference_gr():
             extra["library_key"] = "library"
         a = AnnDataLite(obs=obs, obsm={"spatial": xy}, n_obs=xy.shape[0])
         fn = {"knn": gr.spatial_neighbors_knn, "radius": gr.spatial_neighbors_radius,
-              "grid": gr.spatial_neighbors_grid}[kind]
+              "grid": gr.spatial_neighbors_grid, "delaunay": gr.spatial_neighbors_delaunay}[kind]
         res = fn(a, copy=True, **kw, **extra)
         for tag, M in (("adj", res.connectivities), ("dst", res.distances)):
             M = sp.csr_matrix(M)

@@ -38,8 +38,18 @@ def _oracle_knn_edges_f32(x64, n_neighs, device=None):
     return cols.astype(np.int32), dist
 
 
+def _host_delaunay_edges(x64, device=None):
+    import scipy.sparse as sp
+    from scipy.spatial import Delaunay
+    n = x64.shape[0]
+    ip, ind = Delaunay(np.asarray(x64, dtype=np.float64)).vertex_neighbor_vertices
+    A = sp.csr_matrix((np.ones(ind.size, np.float32), ind, ip), shape=(n, n)).tocoo()
+    return A.row, A.col, osp.edge_lengths_f64(x64, A.row, A.col)
+
+
 @pytest.fixture
 def oracle_search(monkeypatch):
+    monkeypatch.setattr(gr, "delaunay_edges", _host_delaunay_edges)
     monkeypatch.setattr(gr, "knn_edges", _oracle_knn_edges)
     monkeypatch.setattr(gr, "knn_edges_f32", _oracle_knn_edges_f32)
     monkeypatch.setattr(gr, "radius_edges", _oracle_radius_edges)
@@ -76,14 +86,14 @@ def test_builders_equal_reference_gr(oracle_search):
     n = 0
     for c, kind, xy, lib, kw, g in golden_cases():
         fn = {"knn": gr.spatial_neighbors_knn, "radius": gr.spatial_neighbors_radius,
-              "grid": gr.spatial_neighbors_grid}[kind]
+              "grid": gr.spatial_neighbors_grid, "delaunay": gr.spatial_neighbors_delaunay}[kind]
         extra = {"library_key": "library"} if lib is not None else {}
         res = fn(adata_for(xy, lib), copy=True, **kw, **extra)
         assert isinstance(res, gr.SpatialNeighborsResult)
         assert_same(res.connectivities, g, c, "adj")
         assert_same(res.distances, g, c, "dst")
         n += 1
-    assert n == 20
+    assert n == 22
 
 
 def test_slots_and_params(oracle_search):
