@@ -340,3 +340,36 @@ def spatial_neighbors_radius(adata, *, radius, spatial_key: str = "spatial",
                          transform, set_diag, percentile)
     return _write(adata, adj, dst, {"coord_type": "generic", "radius": radius},
                   key_added, transform, copy)
+
+
+def spatial_neighbors(adata, n_neighs: int = 6, coord_type: str | None = None, n_rings: int = 1,
+                      delaunay: bool = False, radius=None, spatial_key: str = "spatial",
+                      library_key: str | None = None, transform: str | None = None,
+                      set_diag: bool = False, percentile: float | None = None,
+                      key_added: str = "spatial", copy: bool = False, device=None):
+    """The deprecated single entry point (gr.py:371-411, squidpy's ``gr.spatial_neighbors``):
+    warns, then dispatches to the mode builders.  ``coord_type`` None means 'grid' when
+    ``uns['spatial']`` exists, else 'generic'; 'grid' rejects ``percentile``; with
+    ``delaunay=True`` a scalar ``radius`` is ignored and a (min, max) tuple applied — the legacy
+    behaviour code written against this entry point expects."""
+    import warnings
+    warnings.warn("gr.spatial_neighbors is deprecated (squidpy removes it in 1.9). Use "
+                  "spatial_neighbors_knn / spatial_neighbors_radius / spatial_neighbors_delaunay"
+                  " / spatial_neighbors_grid.", FutureWarning, stacklevel=2)
+    if coord_type is None:
+        coord_type = "grid" if "spatial" in adata.uns else "generic"
+    common = dict(spatial_key=spatial_key, library_key=library_key, transform=transform,
+                  set_diag=set_diag, key_added=key_added, copy=copy, device=device)
+    if coord_type == "grid":
+        if percentile is not None:
+            raise ValueError("'percentile' is not supported for grid coordinates")
+        return spatial_neighbors_grid(adata, n_neighs=n_neighs, n_rings=n_rings,
+                                      delaunay=delaunay, **common)
+    if coord_type != "generic":
+        raise ValueError(f"coord_type must be 'grid', 'generic' or None, got {coord_type!r}")
+    if delaunay:
+        return spatial_neighbors_delaunay(adata, radius=radius if isinstance(radius, tuple)
+                                          else None, percentile=percentile, **common)
+    if radius is not None:
+        return spatial_neighbors_radius(adata, radius=radius, percentile=percentile, **common)
+    return spatial_neighbors_knn(adata, n_neighs=n_neighs, percentile=percentile, **common)

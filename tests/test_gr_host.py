@@ -124,3 +124,37 @@ def test_errors(oracle_search):
         gr.spatial_neighbors_knn(adata_for(xy, None), transform="laplacian")
     with pytest.raises(ValueError):
         gr.spatial_neighbors_knn(adata_for(xy, None), n_neighs=50)
+
+
+def test_deprecated_entry_point_dispatches(oracle_search):
+    xy = np.random.default_rng(4).uniform(0, 1000, (400, 2))
+
+    def same(a, b):
+        for x, y in zip(a, b):
+            x, y = sp.csr_matrix(x), sp.csr_matrix(y)
+            x.sort_indices()
+            y.sort_indices()
+            assert (x != y).nnz == 0 and x.data.dtype == y.data.dtype
+
+    a = adata_for(xy, None)
+    with pytest.warns(FutureWarning):
+        r = gr.spatial_neighbors(a, n_neighs=5, copy=True)
+    same(r, gr.spatial_neighbors_knn(a, n_neighs=5, copy=True))
+    with pytest.warns(FutureWarning):
+        r = gr.spatial_neighbors(a, radius=80.0, copy=True)
+    same(r, gr.spatial_neighbors_radius(a, radius=80.0, copy=True))
+    with pytest.warns(FutureWarning):                  # a scalar radius is ignored with delaunay
+        r = gr.spatial_neighbors(a, delaunay=True, radius=10.0, copy=True)
+    same(r, gr.spatial_neighbors_delaunay(a, copy=True))
+    with pytest.warns(FutureWarning):                  # a tuple radius is applied
+        r = gr.spatial_neighbors(a, delaunay=True, radius=(0.0, 60.0), copy=True)
+    same(r, gr.spatial_neighbors_delaunay(a, radius=(0.0, 60.0), copy=True))
+    g = adata_for(xy, None)
+    g.uns["spatial"] = {}                              # Visium-style: grid inferred
+    with pytest.warns(FutureWarning):
+        r = gr.spatial_neighbors(g, n_neighs=6, n_rings=2, copy=True)
+    same(r, gr.spatial_neighbors_grid(g, n_neighs=6, n_rings=2, copy=True))
+    with pytest.warns(FutureWarning), pytest.raises(ValueError):
+        gr.spatial_neighbors(g, percentile=90.0)
+    with pytest.warns(FutureWarning), pytest.raises(ValueError):
+        gr.spatial_neighbors(a, coord_type="hexagonal")
