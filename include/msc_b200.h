@@ -238,6 +238,52 @@ size_t msc_trim_graph_workspace_bytes(int64_t n);
 int msc_trim_graph(const int64_t* indptr_dev, const int32_t* indices_dev, const float* data_dev,
                    int64_t n, int32_t trim, int64_t* out_indptr_dev, int32_t* out_indices_dev,
                    float* out_data_dev, void* workspace, size_t workspace_bytes, void* stream);
+/* ---- spatial (2-D / 3-D) uniform-grid search: replaces metalsinglecell
+ *      neighbors._knn_grid (neighbors.py:333-417) and neighbors._radius_grid (neighbors.py:255-330),
+ *      which gr.spatial_neighbors_knn / _radius (gr.py:186-255) and spatial.spatial_neighbors
+ *      (spatial.py:13-44) call.  Coordinates are row-major float32 (n, d), d = 2 or 3.
+ *      Arithmetic: d² = fl(fl(dx²) + fl(dy²)) [+ fl(dz²)], dx = fl(x_p - x_q), no fused
+ *      multiply-add; distance = correctly rounded float32 sqrt(d²).  Exact for every row. ---- */
+#define MSC_SPATIAL_MAX_K        65  /* largest k of msc_spatial_knn (self + 64 others)         */
+#define MSC_SPATIAL_MAX_N        (1LL << 29)
+#define MSC_SP_STAT_NONFINITE    0   /* non-finite coordinates (nothing is computed)             */
+#define MSC_SP_STAT_STATUS       1   /* 0 ok, 1 non-finite input, 2 no cell plan                */
+#define MSC_SP_STAT_CELLS        2   /* cells of the grid                                        */
+#define MSC_SP_STAT_CHUNKS       3   /* query chunks (<= 32 points of one cell)                  */
+#define MSC_SP_STAT_EVALS        4   /* candidate distances evaluated                            */
+#define MSC_SP_STAT_EXPANDED     5   /* kNN rows that needed more than one ring of cells         */
+#define MSC_SP_STAT_RING         6   /* radius search: rings of cells around the query's cell    */
+#define MSC_SP_STAT_CELL_SIDE    7   /* cell side, the bits of a float64                         */
+#define MSC_SP_STATS_LEN         8
+
+/* k nearest points of every point (self first, then (distance, index) order): knn_idx (n, k)
+ * int32 and knn_dist (n, k) float32, row-major.  1 <= k <= min(n, MSC_SPATIAL_MAX_K).
+ * Replaces _knn_grid (neighbors.py:333-417), whose lists are self-inclusive and distance-sorted. */
+size_t msc_spatial_knn_workspace_bytes(int64_t n, int32_t d, int32_t k);
+int msc_spatial_knn(const float* coords_dev, int64_t n, int32_t d, int32_t k, int32_t* knn_idx_dev,
+                    float* knn_dist_dev, int64_t* stats_dev, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+/* Every other point with min_radius² <= d² <= radius² (the two squares rounded to float32):
+ * the two Metal passes of _radius_grid (neighbors.py:255-330).  The count call builds the grid
+ * in the workspace and writes indptr (n + 1 int64); the fill call, given the same workspace
+ * unchanged and indptr[n] = nnz, writes the columns (ascending in every row) and float32
+ * distances. */
+size_t msc_spatial_radius_workspace_bytes(int64_t n, int32_t d);
+int msc_spatial_radius_count(const float* coords_dev, int64_t n, int32_t d, double radius,
+                             double min_radius, int64_t* indptr_dev, int64_t* stats_dev,
+                             void* workspace, size_t workspace_bytes, void* stream);
+size_t msc_spatial_radius_scratch_bytes(int64_t nnz);
+int msc_spatial_radius_fill(int64_t n, int32_t d, double radius, double min_radius,
+                            const int64_t* indptr_dev, int64_t nnz, int32_t* indices_dev,
+                            float* dist_dev, void* workspace, size_t workspace_bytes,
+                            void* scratch, size_t scratch_bytes, void* stream);
+
+/* Euclidean length of every edge of a CSR graph from float64 coordinates (n, d): squares summed
+ * axis by axis in order, correctly rounded sqrt (gr._edge_lengths, gr.py:32-34). */
+int msc_spatial_edge_lengths(const double* coords64_dev, int64_t n, int32_t d,
+                             const int64_t* indptr_dev, const int32_t* indices_dev,
+                             double* out_dev, void* stream);
 
 #ifdef __cplusplus
 }

@@ -962,4 +962,101 @@ int msc_trim_graph(const int64_t* indptr_dev, const int32_t* indices_dev, const 
                      out_data_dev, workspace, as_stream(stream));
 }
 
+namespace {
+int check_spatial(int64_t n, int32_t d, const void* coords, const void* stats, const void* ws,
+                  size_t ws_bytes, size_t need) {
+  if (n < 1 || n > MSC_SPATIAL_MAX_N) { set_error("n=%lld out of range", (long long)n); return MSC_ERR_INVALID_ARG; }
+  if (d != 2 && d != 3) {
+    set_error("spatial search expects 2-D or 3-D coordinates, got %d-D", d);
+    return MSC_ERR_UNSUPPORTED;
+  }
+  if (bad_ptr(coords, "coords") || bad_ptr(stats, "stats") || bad_ptr(ws, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (ws_bytes < need) {
+    set_error("workspace of %zu bytes, %zu needed", ws_bytes, need);
+    return MSC_ERR_WORKSPACE;
+  }
+  return MSC_OK;
+}
+int check_radius(double radius, double min_radius) {
+  if (!(radius >= 0) || !std::isfinite(radius) || !(min_radius >= 0) || !(min_radius <= radius)) {
+    set_error("radius interval [%g, %g] is not a finite interval of non-negative values",
+              min_radius, radius);
+    return MSC_ERR_INVALID_ARG;
+  }
+  return MSC_OK;
+}
+}  // namespace
+
+size_t msc_spatial_knn_workspace_bytes(int64_t n, int32_t d, int32_t k) {
+  (void)d;
+  (void)k;
+  return n < 1 ? 0 : spatial_knn_workspace_bytes(n);
+}
+
+int msc_spatial_knn(const float* coords_dev, int64_t n, int32_t d, int32_t k, int32_t* knn_idx_dev,
+                    float* knn_dist_dev, int64_t* stats_dev, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+  MSC_TRY(check_spatial(n, d, coords_dev, stats_dev, workspace, workspace_bytes,
+                        n < 1 ? 0 : spatial_knn_workspace_bytes(n)));
+  if (k < 1 || k > MSC_SPATIAL_MAX_K || k > n) {
+    set_error("k=%d must be in [1, min(n=%lld, %d)]", k, (long long)n, MSC_SPATIAL_MAX_K);
+    return k > MSC_SPATIAL_MAX_K && k <= n ? MSC_ERR_UNSUPPORTED : MSC_ERR_INVALID_ARG;
+  }
+  if (bad_ptr(knn_idx_dev, "knn_idx") || bad_ptr(knn_dist_dev, "knn_dist")) return MSC_ERR_INVALID_ARG;
+  return launch_spatial_knn(coords_dev, n, d, k, knn_idx_dev, knn_dist_dev, stats_dev, workspace,
+                            as_stream(stream));
+}
+
+size_t msc_spatial_radius_workspace_bytes(int64_t n, int32_t d) {
+  (void)d;
+  return n < 1 ? 0 : spatial_radius_workspace_bytes(n);
+}
+
+int msc_spatial_radius_count(const float* coords_dev, int64_t n, int32_t d, double radius,
+                             double min_radius, int64_t* indptr_dev, int64_t* stats_dev,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  MSC_TRY(check_spatial(n, d, coords_dev, stats_dev, workspace, workspace_bytes,
+                        n < 1 ? 0 : spatial_radius_workspace_bytes(n)));
+  MSC_TRY(check_radius(radius, min_radius));
+  if (bad_ptr(indptr_dev, "indptr")) return MSC_ERR_INVALID_ARG;
+  return launch_spatial_radius_count(coords_dev, n, d, radius, min_radius, indptr_dev, stats_dev,
+                                     workspace, as_stream(stream));
+}
+
+size_t msc_spatial_radius_scratch_bytes(int64_t nnz) {
+  return spatial_radius_fill_scratch_bytes(nnz < 0 ? 0 : nnz);
+}
+
+int msc_spatial_radius_fill(int64_t n, int32_t d, double radius, double min_radius,
+                            const int64_t* indptr_dev, int64_t nnz, int32_t* indices_dev,
+                            float* dist_dev, void* workspace, size_t workspace_bytes,
+                            void* scratch, size_t scratch_bytes, void* stream) {
+  MSC_TRY(check_spatial(n, d, indptr_dev, workspace, workspace, workspace_bytes,
+                        n < 1 ? 0 : spatial_radius_workspace_bytes(n)));
+  MSC_TRY(check_radius(radius, min_radius));
+  if (nnz < 0) { set_error("nnz < 0"); return MSC_ERR_INVALID_ARG; }
+  if (nnz > 0 && (bad_ptr(indices_dev, "indices") || bad_ptr(dist_dev, "dist") ||
+                  bad_ptr(scratch, "scratch")))
+    return MSC_ERR_INVALID_ARG;
+  if (scratch_bytes < spatial_radius_fill_scratch_bytes(nnz)) {
+    set_error("scratch of %zu bytes, %zu needed", scratch_bytes,
+              spatial_radius_fill_scratch_bytes(nnz));
+    return MSC_ERR_WORKSPACE;
+  }
+  return launch_spatial_radius_fill(n, d, radius, min_radius, indptr_dev, nnz, indices_dev,
+                                    dist_dev, workspace, scratch, as_stream(stream));
+}
+
+int msc_spatial_edge_lengths(const double* coords64_dev, int64_t n, int32_t d,
+                             const int64_t* indptr_dev, const int32_t* indices_dev,
+                             double* out_dev, void* stream) {
+  if (n < 1 || d < 1 || d > 3) { set_error("bad n/d"); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(coords64_dev, "coords64") || bad_ptr(indptr_dev, "indptr") ||
+      bad_ptr(indices_dev, "indices") || bad_ptr(out_dev, "out"))
+    return MSC_ERR_INVALID_ARG;
+  return launch_spatial_edge_lengths(coords64_dev, n, d, indptr_dev, indices_dev, out_dev,
+                                     as_stream(stream));
+}
+
 }  // extern "C"

@@ -309,5 +309,18 @@ size_t trim_workspace_bytes(int64_t n);
 int launch_trim(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n,
                 int trim, int64_t* out_ptr, int32_t* out_idx, float* out_data, void* ws,
                 cudaStream_t st);
+// ---- spatial.cu ----
+size_t spatial_knn_workspace_bytes(int64_t n);
+int launch_spatial_knn(const float* X, int64_t n, int d, int k, int32_t* idx, float* dist,
+                       int64_t* stats, void* ws, cudaStream_t st);
+size_t spatial_radius_workspace_bytes(int64_t n);
+int launch_spatial_radius_count(const float* X, int64_t n, int d, double radius, double min_radius,
+                                int64_t* indptr, int64_t* stats, void* ws, cudaStream_t st);
+size_t spatial_radius_fill_scratch_bytes(int64_t nnz);
+int launch_spatial_radius_fill(int64_t n, int d, double radius, double min_radius,
+                               const int64_t* indptr, int64_t nnz, int32_t* cols, float* dist,
+                               void* ws, void* scratch, cudaStream_t st);
+int launch_spatial_edge_lengths(const double* X, int64_t n, int d, const int64_t* indptr,
+                                const int32_t* cols, double* out, cudaStream_t st);
 
 }  // namespace msc

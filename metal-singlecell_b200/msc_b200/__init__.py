@@ -7,11 +7,14 @@ GPU through the C ABI in ``include/msc_b200.h``.
     import msc_b200 as msc
     msc.pp.neighbors(adata, n_neighbors=15)
     msc.pp.bbknn(adata, batch_key="batch")      # batch-balanced graph
+
+``msc_b200.gr`` / ``msc_b200.spatial`` carry the spatial (2-D / 3-D) kNN and radius graphs on a
+uniform-grid search.
 """
 
-from . import pp, neighbors, bbknn, synth, _lib
+from . import pp, neighbors, bbknn, synth, spatial, gr, _lib
 from .anndata_lite import AnnDataLite
 
 __version__ = "0.1.0"
 
-__all__ = ["pp", "neighbors", "bbknn", "synth", "AnnDataLite", "__version__"]
+__all__ = ["pp", "neighbors", "bbknn", "synth", "spatial", "gr", "AnnDataLite", "__version__"]

@@ -10,7 +10,7 @@ metalsinglecell pp.py:768-769, neighbors.py:724).
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_float, c_int32, c_int64, c_size_t, c_void_p, c_char_p
+from ctypes import c_double, c_float, c_int32, c_int64, c_size_t, c_void_p, c_char_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libmsc_b200.so"
@@ -30,8 +30,13 @@ MAX_K_KNN = 513
 MAX_D = 128
 BBKNN_MAX_WIDTH = 128
 
+SP_STAT_NONFINITE, SP_STAT_STATUS, SP_STAT_CELLS, SP_STAT_CHUNKS, SP_STAT_EVALS, \
+    SP_STAT_EXPANDED, SP_STAT_RING, SP_STAT_CELL_SIDE = range(8)
+SP_STATS_LEN = 8
+SPATIAL_MAX_K = 65
+
 P = c_void_p
-I32, I64, SZ, F32 = c_int32, c_int64, c_size_t, c_float
+I32, I64, SZ, F32, F64 = c_int32, c_int64, c_size_t, c_float, c_double
 
 # name -> (restype, argtypes); mirrors include/msc_b200.h
 SIGNATURES = {
@@ -67,6 +72,13 @@ SIGNATURES = {
     "msc_bbknn_distances_csr": (I32, [P, P, I64, I32, P, P, P, P, SZ, P]),
     "msc_trim_graph_workspace_bytes": (SZ, [I64]),
     "msc_trim_graph": (I32, [P, P, P, I64, I32, P, P, P, P, SZ, P]),
+    "msc_spatial_knn_workspace_bytes": (SZ, [I64, I32, I32]),
+    "msc_spatial_knn": (I32, [P, I64, I32, I32, P, P, P, P, SZ, P]),
+    "msc_spatial_radius_workspace_bytes": (SZ, [I64, I32]),
+    "msc_spatial_radius_count": (I32, [P, I64, I32, F64, F64, P, P, P, SZ, P]),
+    "msc_spatial_radius_scratch_bytes": (SZ, [I64]),
+    "msc_spatial_radius_fill": (I32, [I64, I32, F64, F64, P, I64, P, P, P, SZ, P, SZ, P]),
+    "msc_spatial_edge_lengths": (I32, [P, I64, I32, P, P, P, P]),
 }
 
 _lib = None
@@ -113,6 +125,16 @@ def check_stats(stats) -> None:
         raise RuntimeError("msc_b200: a device-side wait timed out; results are invalid")
     if int(stats[STAT_NONFINITE]):
         raise ValueError(f"msc_b200: input holds {int(stats[STAT_NONFINITE])} non-finite values")
+
+
+def check_spatial_stats(stats) -> None:
+    """Device-side failures of the spatial search (read after the stream completed)."""
+    if int(stats[SP_STAT_NONFINITE]):
+        raise ValueError(f"msc_b200: coordinates hold {int(stats[SP_STAT_NONFINITE])} "
+                         "non-finite values")
+    if int(stats[SP_STAT_STATUS]):
+        raise RuntimeError(f"msc_b200: spatial grid plan failed (status "
+                           f"{int(stats[SP_STAT_STATUS])})")
 
 
 def ptr(t) -> int:

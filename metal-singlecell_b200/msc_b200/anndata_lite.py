@@ -1,8 +1,9 @@
 """A minimal AnnData stand-in: the slots ``pp.neighbors`` and ``pp.bbknn`` read and write.
 
-They work on any object exposing ``X``, ``n_obs``, ``n_vars``, ``obs`` (per-cell columns),
-``obsm``, ``obsp``, ``uns`` and ``copy()`` — a real ``anndata.AnnData`` included.  This class
-provides exactly that for environments without anndata; ``obs`` is a dict of per-cell arrays.
+``pp.neighbors`` and ``pp.bbknn`` work on any object exposing ``X``, ``n_obs``, ``n_vars``,
+``obs`` (per-cell columns), ``obsm``, ``obsp``, ``uns`` and ``copy()`` — a real ``anndata.AnnData``
+included; the spatial builders also read ``obs`` (a mapping or DataFrame of per-observation
+columns).  This class provides exactly that for environments without anndata.
 """
 
 from __future__ import annotations
@@ -14,7 +15,7 @@ class AnnDataLite:
     def __init__(self, X=None, *, obs=None, obsm=None, obsp=None, uns=None, n_obs=None,
                  n_vars=None):
         self.X = X
-        self.obs = dict(obs or {})
+        self.obs = obs if obs is not None else {}
         self.obsm = dict(obsm or {})
         self.obsp = dict(obsp or {})
         self.uns = dict(uns or {})

@@ -56,6 +56,46 @@ def test_argument_checks(n, d, k, metric, prec, kprime, code):
         _lib.check(rc)
 
 
+def test_spatial_argument_checks():
+    """The spatial entry points refuse bad requests before anything reaches a device: the
+    address below is never dereferenced, since every case fails a host-side check first."""
+    lib = _lib.load()
+    F, big = 4096, 1 << 40
+    E = _lib
+    cases = [
+        (lib.msc_spatial_knn(F, 100, 4, 5, F, F, F, F, big, None), E.MSC_ERR_UNSUPPORTED),  # 4-D
+        (lib.msc_spatial_knn(F, 100, 2, 0, F, F, F, F, big, None), E.MSC_ERR_INVALID_ARG),  # k=0
+        (lib.msc_spatial_knn(F, 100, 2, 101, F, F, F, F, big, None), E.MSC_ERR_INVALID_ARG),
+        (lib.msc_spatial_knn(F, 100, 2, 66, F, F, F, F, big, None), E.MSC_ERR_UNSUPPORTED),
+        (lib.msc_spatial_knn(None, 100, 2, 5, F, F, F, F, big, None), E.MSC_ERR_INVALID_ARG),
+        (lib.msc_spatial_knn(F, 100, 2, 5, F, F, F, F, 16, None), E.MSC_ERR_WORKSPACE),
+        (lib.msc_spatial_knn(F, 0, 2, 1, F, F, F, F, big, None), E.MSC_ERR_INVALID_ARG),
+        (lib.msc_spatial_radius_count(F, 100, 2, -1.0, 0.0, F, F, F, big, None),
+         E.MSC_ERR_INVALID_ARG),
+        (lib.msc_spatial_radius_count(F, 100, 2, 1.0, 2.0, F, F, F, big, None),
+         E.MSC_ERR_INVALID_ARG),                                                       # min > max
+        (lib.msc_spatial_radius_count(F, 100, 2, float("inf"), 0.0, F, F, F, big, None),
+         E.MSC_ERR_INVALID_ARG),
+        (lib.msc_spatial_radius_count(F, 100, 3, 1.0, 0.0, F, F, F, 16, None),
+         E.MSC_ERR_WORKSPACE),
+        (lib.msc_spatial_radius_fill(100, 2, 1.0, 0.0, F, -1, F, F, F, big, F, big, None),
+         E.MSC_ERR_INVALID_ARG),                                                       # nnz < 0
+        (lib.msc_spatial_radius_fill(100, 2, 1.0, 0.0, F, 10, F, F, F, big, F, 8, None),
+         E.MSC_ERR_WORKSPACE),                                                         # scratch
+        (lib.msc_spatial_edge_lengths(F, 100, 4, F, F, F, None), E.MSC_ERR_INVALID_ARG),
+    ]
+    for i, (rc, code) in enumerate(cases):
+        assert rc == code, (i, rc, _lib.last_error())
+    text = HEADER.read_text()
+    for name, val in [("MSC_SPATIAL_MAX_K", _lib.SPATIAL_MAX_K),
+                      ("MSC_SP_STATS_LEN", _lib.SP_STATS_LEN),
+                      ("MSC_SP_STAT_EXPANDED", _lib.SP_STAT_EXPANDED),
+                      ("MSC_SP_STAT_CELL_SIDE", _lib.SP_STAT_CELL_SIDE)]:
+        assert re.search(rf"#define {name}\s+{val}\b", text), name
+    assert lib.msc_spatial_knn_workspace_bytes(1_000_000, 2, 7) > 0
+    assert lib.msc_spatial_radius_scratch_bytes(0) >= 0
+
+
 def test_workspace_queries_are_host_only():
     lib = _lib.load()
     a = lib.msc_neighbors_workspace_bytes(1_300_000, 50, 15, 0, 0, 1, 0)     # BF16x3
