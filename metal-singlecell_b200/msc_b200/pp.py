@@ -17,34 +17,42 @@ import numpy as np
 from .neighbors import neighbors as _nb, DEFAULT_PRECISION
 from .bbknn import bbknn as _bbknn
 
-_N_PCS_DEFAULT = 50            # scanpy's settings.N_PCS
+# Width below which scanpy builds the graph on ``.X`` itself rather than on a PCA (the default
+# component count of its settings object).
+_WIDE = 50
 
 
-def _dense(X):
-    import scipy.sparse as sp
-    return X.toarray() if sp.issparse(X) else np.asarray(X)
+def _as_f32(M):
+    """A dense float32 array of ``M``, which may be a SciPy sparse matrix."""
+    if hasattr(M, "toarray") and not isinstance(M, np.ndarray):
+        M = M.toarray()
+    return np.asarray(M, dtype=np.float32)
 
 
 def _choose_representation(adata, use_rep, n_pcs):
-    """scanpy's representation rule as the reference applies it (pp.py:722-745): ``.X`` when
-    ``n_pcs == 0`` or the object has at most 50 variables, ``X_pca`` otherwise, ``obsm[use_rep]``
-    when given (``'X'`` = ``.X``).  Computing a missing PCA (pp.py:735-737) is a preprocessing step
-    outside this library: run PCA first."""
-    if use_rep is None and n_pcs == 0:
-        return np.asarray(_dense(adata.X), dtype=np.float32), None
-    if use_rep is None:
-        if adata.n_vars > _N_PCS_DEFAULT:
-            if "X_pca" not in adata.obsm or adata.obsm["X_pca"].shape[1] < (n_pcs or _N_PCS_DEFAULT):
-                raise ValueError("obsm['X_pca'] with enough components is missing: run PCA "
-                                 "(e.g. msc.pp.pca) before pp.neighbors")
-            return np.asarray(adata.obsm["X_pca"], dtype=np.float32), "X_pca"
-        return np.asarray(_dense(adata.X), dtype=np.float32), None
+    """The embedding the graph is built on, with the name it is recorded under (pp.py:722-745).
+
+    * ``use_rep`` given: ``'X'`` selects ``.X``; any other name must be a key of ``.obsm``, else
+      ``ValueError`` with the reference's message.
+    * ``use_rep`` absent: ``.X`` when ``n_pcs == 0`` or the object has at most 50 variables;
+      otherwise ``obsm['X_pca']``, which must hold at least ``n_pcs`` (default 50) components.
+      The reference computes that PCA itself when it is missing (pp.py:735-737); PCA is a
+      preprocessing step outside this library, so here the caller is asked to run it first.
+    """
     if use_rep == "X":
-        return np.asarray(_dense(adata.X), dtype=np.float32), "X"
-    if use_rep not in adata.obsm:
-        raise ValueError(f"Did not find {use_rep} in .obsm.keys(). "
-                         f"You need to compute it first.")
-    return np.asarray(adata.obsm[use_rep], dtype=np.float32), use_rep
+        return _as_f32(adata.X), "X"
+    if use_rep is not None:
+        if use_rep not in adata.obsm:
+            raise ValueError(f"Did not find {use_rep} in .obsm.keys(). "
+                             f"You need to compute it first.")
+        return _as_f32(adata.obsm[use_rep]), use_rep
+    if n_pcs == 0 or adata.n_vars <= _WIDE:
+        return _as_f32(adata.X), None
+    pcs = adata.obsm["X_pca"] if "X_pca" in adata.obsm else None
+    if pcs is None or pcs.shape[1] < (n_pcs or _WIDE):
+        raise ValueError("obsm['X_pca'] with enough components is missing: run PCA "
+                         "(e.g. msc.pp.pca) before pp.neighbors")
+    return _as_f32(pcs), "X_pca"
 
 
 def neighbors(adata, n_neighbors: int = 15, n_pcs: int | None = None, *,
@@ -52,30 +60,32 @@ def neighbors(adata, n_neighbors: int = 15, n_pcs: int | None = None, *,
               key_added: str | None = None, random_state: int = 0, copy: bool = False,
               precision: str = DEFAULT_PRECISION):
     """kNN graph (``sc.pp.neighbors``); writes ``obsp['distances']``/``['connectivities']`` and
-    ``uns['neighbors']`` (pp.py:753-788).  Returns ``None``, or the modified copy if ``copy``."""
+    ``uns['neighbors']`` (pp.py:753-788).  Returns ``None``, or the modified copy if ``copy``.
+
+    ``key_added`` renames all three slots (``f'{key}_distances'``, ``f'{key}_connectivities'``,
+    ``uns[key]``).  ``uns[...]['params']`` holds ``n_neighbors``, ``method``, ``random_state`` and
+    ``metric`` always, and ``use_rep`` / ``n_pcs`` only when the caller passed them."""
     if metric not in ("euclidean", "cosine"):
         raise NotImplementedError(f"metric={metric!r} is not implemented (euclidean, cosine)")
     if method not in ("umap", "gauss"):
         raise ValueError(f"method={method!r} must be 'umap' or 'gauss'")
-    adata = adata.copy() if copy else adata
-    rep, _ = _choose_representation(adata, use_rep, n_pcs)
-    if n_pcs is not None:                            # scanpy truncates the rep to the first n_pcs
-        rep = rep[:, :n_pcs]
+    target = adata.copy() if copy else adata
+    rep, _ = _choose_representation(target, use_rep, n_pcs)
+    if n_pcs is not None:
+        rep = rep[:, :n_pcs]          # only the leading n_pcs columns take part
     dist, conn = _nb(rep, n_neighbors=n_neighbors, random_state=random_state, metric=metric,
                      method=method, precision=precision)
-    ck = "connectivities" if key_added is None else f"{key_added}_connectivities"
-    dk = "distances" if key_added is None else f"{key_added}_distances"
-    adata.obsp[dk] = dist
-    adata.obsp[ck] = conn
-    params = {"n_neighbors": n_neighbors, "method": method,
-              "random_state": random_state, "metric": metric}
-    if use_rep is not None:            # scanpy records only what the caller asked for
-        params["use_rep"] = use_rep
-    if n_pcs is not None:
-        params["n_pcs"] = n_pcs
-    adata.uns["neighbors" if key_added is None else key_added] = {
-        "connectivities_key": ck, "distances_key": dk, "params": params}
-    return adata if copy else None
+    prefix = "" if key_added is None else f"{key_added}_"
+    slots = {"connectivities_key": prefix + "connectivities",
+             "distances_key": prefix + "distances"}
+    target.obsp[slots["distances_key"]] = dist
+    target.obsp[slots["connectivities_key"]] = conn
+    params = dict(n_neighbors=n_neighbors, method=method, random_state=random_state,
+                  metric=metric)
+    params.update({name: val for name, val in (("use_rep", use_rep), ("n_pcs", n_pcs))
+                   if val is not None})
+    target.uns["neighbors" if key_added is None else key_added] = {**slots, "params": params}
+    return target if copy else None
 
 
 def _obs_column(adata, key):

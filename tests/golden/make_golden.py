@@ -23,19 +23,26 @@ maps every ``mx.*`` call those functions make onto its NumPy equivalent):
   oracle's grid kNN and radius search (oracle/spatial.py) in place of the Metal grid kernels: the edge
   selection, FP64 edge lengths, the lattice median correction and ring expansion, the
   percentile / set_diag / transform tail and the per-library blocks are the reference's code,
-  on jittered and exact hex lattices, a 3-D point cloud and interleaved sections.
+  on jittered and exact hex lattices, a 3-D point cloud and interleaved sections;
+* the UMAP layout's edge preparation ``embedding._prune_weak_edges`` and
+  ``_make_epochs_per_sample`` (embedding.py:100-137, 255-267), pure NumPy/SciPy, run as is on
+  connectivities built by the oracle, at several epoch counts.
 
-Run from the repository root with the reference mounted:  python tests/golden/make_golden.py
+Run from the repository root, naming the reference project's ``src`` directory (the one that
+holds the ``metalsinglecell`` package), as an argument or in ``MSC_REFERENCE_SRC``:
+
+    python tests/golden/make_golden.py <reference>/src
+
 Writes tests/golden/reference_knn_500x20.npz, reference_rho_sigma.npz, reference_distances_csr.npz,
-reference_trim.npz and reference_spatial.npz.
+reference_trim.npz, reference_spatial.npz and reference_umap_edges.npz.
 """
+import os
 import sys
 import types
 from pathlib import Path
 
 import numpy as np
 
-REF = Path("/root/reference/src")
 OUT = Path(__file__).resolve().parent
 sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
 sys.path.insert(0, str(Path(__file__).resolve().parents[2] / "metal-singlecell_b200"))
@@ -83,9 +90,21 @@ def numpy_mlx():
     return mx
 
 
+def reference_src(argv) -> Path:
+    """The reference's ``src`` directory: the first argument, else ``MSC_REFERENCE_SRC``."""
+    src = argv[1] if len(argv) > 1 else os.environ.get("MSC_REFERENCE_SRC")
+    if not src:
+        sys.exit("usage: make_golden.py <reference src directory> (or set MSC_REFERENCE_SRC)")
+    src = Path(src)
+    if not (src / "metalsinglecell").is_dir():
+        sys.exit(f"{src} holds no metalsinglecell package")
+    return src
+
+
 def main():
+    ref = reference_src(sys.argv)
     mx = numpy_mlx()
-    sys.path.insert(0, str(REF))
+    sys.path.insert(0, str(ref))
     from metalsinglecell import neighbors as ref_nb
     from metalsinglecell._vendor.mlx_vis.umap import UMAP as RefUMAP
 
@@ -195,6 +214,7 @@ def main():
     from metalsinglecell import gr as ref_gr
     from oracle import spatial as osp
     spatial_golden(ref_nb, ref_gr, osp)
+    umap_edges_golden()
     print("wrote", sorted(p.name for p in OUT.glob("reference_*.npz")))
 
 
@@ -280,6 +300,40 @@ def spatial_golden(ref_nb, ref_gr, osp):
     finally:
         ref_nb._knn_grid, ref_nb._radius_grid = saved
     np.savez_compressed(OUT / "reference_spatial.npz", n_cases=len(SPATIAL_CASES), **out)
+
+
+def umap_edges_golden():
+    """The reference UMAP's edge preparation (embedding.py:100-137, 255-267) run as is on
+    connectivities the oracle builds: `_prune_weak_edges` at several n_epochs, the kept graph as
+    COO (embedding.py:115) and `_make_epochs_per_sample` of its weights.  Pure NumPy/SciPy."""
+    import oracle
+    from metalsinglecell import embedding as ref_emb
+    out = {}
+    X = oracle_input_mixture()
+    C = oracle.neighbors_graph(X, 15)["connectivities"]
+    # the lowest weights of this graph (~1e-3) sit between max/1000 and max/200, so the epochs
+    # below drop some edges (200, 500) or none (3)
+    cases = (3, 200, 500, 5000)
+    out["indptr"] = C.indptr.astype(np.int64)
+    out["indices"] = C.indices.astype(np.int64)
+    out["data"] = C.data.astype(np.float32)
+    out["epochs"] = np.asarray(cases, np.int64)
+    for e in cases:
+        G = ref_emb._prune_weak_edges(C, e)
+        coo = G.tocoo()
+        out[f"e{e}_rows"] = coo.row.astype(np.int64)
+        out[f"e{e}_cols"] = coo.col.astype(np.int64)
+        out[f"e{e}_weights"] = coo.data.astype(np.float32)
+        out[f"e{e}_eps"] = ref_emb._make_epochs_per_sample(np.asarray(coo.data, np.float64), e)
+    np.savez_compressed(OUT / "reference_umap_edges.npz", **out)
+
+
+def oracle_input_mixture():
+    """2,000 cells × 10 dims from 6 Gaussian clusters (seeded), for the UMAP edge golden."""
+    rng = np.random.default_rng(77)
+    centres = rng.normal(0, 4, (6, 10))
+    lab = rng.integers(0, 6, 2000)
+    return (centres[lab] + rng.standard_normal((2000, 10))).astype(np.float32)
 
 
 if __name__ == "__main__":
