@@ -182,8 +182,11 @@ int msc_fuzzy_union(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, i
  * process exits), so it accepts only n <= MSC_NOALLOC_MAX_CELLS and n*k <= MSC_NOALLOC_MAX_ENTRIES
  * and answers MSC_ERR_INVALID_ARG beyond that.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) with that device current; make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the GPU (other streams,
- * other host threads) race and corrupt each other's results — serialise them. */
+ * stream capture.  The address is kept for the life of the process, so a cudaDeviceReset (or any
+ * other teardown of the device's primary context) after that first call is not supported: the
+ * kept address would no longer name the array.  All calls share the one array: calls that overlap
+ * on the GPU (other streams, other host threads) race and corrupt each other's results —
+ * serialise them. */
 #define MSC_NOALLOC_MAX_CELLS   65536
 #define MSC_NOALLOC_MAX_ENTRIES 1048576
 int msc_fuzzy_union_noalloc(const int32_t* knn_idx_dev, const float* w_dev, int64_t n, int32_t k,
@@ -201,6 +204,20 @@ int msc_gauss_connectivities(const int32_t* knn_idx_dev, const float* knn_dist_d
 int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int64_t n,
                       int32_t k, int64_t* indptr_dev, int32_t* indices_dev, float* data_dev,
                       void* stream);
+
+/* Edge preparation of the UMAP layout from a connectivities CSR already on the device (the graph
+ * hand-off to its first consumer).  Replaces the host steps of metalsinglecell `embedding.umap`:
+ * `_prune_weak_edges` (embedding.py:255-267: keep w >= fl32(max w / n_epochs)), the kept graph
+ * as COO in CSR order (embedding.py:115) and `_make_epochs_per_sample` (embedding.py:123-137:
+ * n_epochs / (n_epochs · (w / max w)) in FP64, -1 for an edge never sampled).
+ *   input : CSR (indptr n+1 int64, indices int32, data float32), n_epochs >= 1
+ *   output: the kept graph's indptr (n+1 int64; nnz = out_indptr[n]) and, per kept edge in CSR
+ *           order, its row, column, weight and sampling period; capacity = the input's nnz */
+size_t msc_umap_edges_workspace_bytes(int64_t n);
+int msc_umap_edges(const int64_t* indptr_dev, const int32_t* indices_dev, const float* data_dev,
+                   int64_t n, int32_t n_epochs, int64_t* out_indptr_dev, int32_t* rows_dev,
+                   int32_t* cols_dev, float* weights_dev, double* epochs_per_sample_dev,
+                   void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * Batch-balanced kNN — replaces metalsinglecell `neighbors.bbknn` (neighbors.py:491-559), called

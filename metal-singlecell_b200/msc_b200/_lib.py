@@ -29,6 +29,8 @@ MAX_K = 129
 MAX_K_KNN = 513
 MAX_D = 128
 BBKNN_MAX_WIDTH = 128
+NOALLOC_MAX_CELLS = 65536
+NOALLOC_MAX_ENTRIES = 1 << 20
 
 SP_STAT_NONFINITE, SP_STAT_STATUS, SP_STAT_CELLS, SP_STAT_CHUNKS, SP_STAT_EVALS, \
     SP_STAT_EXPANDED, SP_STAT_RING, SP_STAT_CELL_SIDE = range(8)
@@ -65,6 +67,8 @@ SIGNATURES = {
     "msc_gauss_workspace_bytes": (SZ, [I64, I32]),
     "msc_gauss_connectivities": (I32, [P, P, I64, I32, P, P, P, P, P, SZ, P]),
     "msc_distances_csr": (I32, [P, P, I64, I32, P, P, P, P]),
+    "msc_umap_edges_workspace_bytes": (SZ, [I64]),
+    "msc_umap_edges": (I32, [P, P, P, I64, I32, P, P, P, P, P, P, SZ, P]),
     "msc_bbknn_width": (I32, [P, I32, I32]),
     "msc_bbknn_workspace_bytes": (SZ, [I64, I32, P, I32, I32, I32]),
     "msc_bbknn_knn": (I32, [P, I64, I32, P, P, I32, I32, I32, P, P, P, P, SZ, P]),

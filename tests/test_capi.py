@@ -160,3 +160,16 @@ def test_bbknn_argument_checks():
     assert lib.msc_trim_graph_workspace_bytes(1000) > 0
     text = HEADER.read_text()
     assert re.search(rf"#define MSC_BBKNN_MAX_WIDTH\s+{_lib.BBKNN_MAX_WIDTH}\b", text)
+
+
+def test_no_alloc_limits_match_the_header_and_fit_its_array():
+    # the fixed array of msc_fuzzy_union_noalloc is 20 MiB; the workspace the union needs at the
+    # corners of the accepted region must fit in it, or accepted calls would be refused
+    lib = _lib.load()
+    text = HEADER.read_text()
+    assert re.search(rf"#define MSC_NOALLOC_MAX_CELLS\s+{_lib.NOALLOC_MAX_CELLS}\b", text)
+    assert re.search(rf"#define MSC_NOALLOC_MAX_ENTRIES\s+{_lib.NOALLOC_MAX_ENTRIES}\b", text)
+    for n, k in ((_lib.NOALLOC_MAX_CELLS, _lib.NOALLOC_MAX_ENTRIES // _lib.NOALLOC_MAX_CELLS),
+                 (_lib.NOALLOC_MAX_ENTRIES // _lib.MAX_K, _lib.MAX_K),
+                 (_lib.NOALLOC_MAX_CELLS, 2)):
+        assert 0 < lib.msc_fuzzy_union_workspace_bytes(n, k) <= 20 << 20, (n, k)

@@ -92,3 +92,16 @@ def test_no_alloc_union_rejects_sizes_beyond_its_scratch():
     assert "scratch" in _lib.last_error()
     rc = lib.msc_fuzzy_union_noalloc(1, 1, 60_000, 20, 1, 1, 1, 1, None)   # n*k > 2^20
     assert rc == _lib.MSC_ERR_INVALID_ARG
+
+
+def test_no_alloc_union_at_its_largest_documented_sizes():
+    # the two corners of the accepted region: every cell at the cell limit, and the widest lists
+    # at the entry limit; both must be accepted and equal the workspace entry point
+    for n, k, seed in ((_lib.NOALLOC_MAX_CELLS, 16, 3),
+                       (_lib.NOALLOC_MAX_ENTRIES // _lib.MAX_K, _lib.MAX_K, 4)):
+        assert n * k <= _lib.NOALLOC_MAX_ENTRIES
+        idx, w = _graph(n, k, seed)
+        ref = _with_workspace(idx, w, n, k)
+        got = _no_alloc(idx, w, n, k)
+        for a, b, what in zip(got, ref, ("indptr", "indices", "data")):
+            assert np.array_equal(a, b), f"n={n} k={k}: {what} differs"
