@@ -44,6 +44,8 @@ class Request:
     result: dict = field(default_factory=dict)
     error: BaseException | None = None
     event: threading.Event = field(default_factory=threading.Event)
+    # a CUDA embedding is read only after the work queued on its producer stream at submit time
+    ready: object = None
 
     @property
     def n(self) -> int:
@@ -94,6 +96,13 @@ class GraphServer:
         return time.perf_counter() - self.t0
 
     def submit(self, req: Request) -> Request:
+        """Queue ``req``.  A CUDA embedding may still be in the making on the caller's current
+        stream: an event recorded there now is waited on by the request's own stream before it
+        reads the tensor, and the tensor is kept alive for that stream until the graph is done."""
+        torch = self.torch
+        if isinstance(req.X, torch.Tensor) and req.X.is_cuda:
+            req.ready = torch.cuda.Event()
+            req.ready.record(torch.cuda.current_stream(req.X.device))
         with self.lock:
             req.arrival = self.now()
             req.rid = self._next_id
@@ -131,7 +140,13 @@ class GraphServer:
             X = req.X
             if not isinstance(X, torch.Tensor):
                 X = torch.from_numpy(np.ascontiguousarray(X, np.float32))
-            Xd = X.to(self.device, non_blocking=True) if not X.is_cuda else X
+            if X.is_cuda:
+                if req.ready is not None:
+                    st.wait_event(req.ready)          # the producer's writes come first
+                X.record_stream(st)                   # its memory stays live for this stream
+                Xd = X if X.device == self.device else X.to(self.device)
+            else:
+                Xd = X.to(self.device, non_blocking=True)
             res = neighbors_device(Xd, req.n_neighbors, metric=req.metric, method=req.method,
                                    precision=req.precision)
             res["X"] = Xd
