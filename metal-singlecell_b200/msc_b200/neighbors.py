@@ -240,6 +240,10 @@ def neighbors_host(Xh, n_neighbors: int = 15, *, metric: str = "euclidean",
     return dict(h, conn_nnz=nnz)
 
 
+def _index_dtype(n: int, nnz: int):
+    return np.int32 if max(n, nnz) < 2 ** 31 else np.int64
+
+
 def graph_to_host(res: dict, n: int, k: int):
     """Device result of ``neighbors_device`` → (distances CSR, connectivities CSR) on the host,
     in SciPy's canonical layout with int32 index arrays (what SciPy itself produces for
@@ -250,10 +254,11 @@ def graph_to_host(res: dict, n: int, k: int):
     _lib.check_stats(stats)
     nnz = int(stats[_lib.STAT_CONN_NNZ])
     m = max(k - 1, 0)
-    d_ptr = res["dist_indptr"].cpu().numpy().astype(np.int32)
+    # SciPy's own choice of index type: int32 while every index and nnz fit, else int64
+    d_ptr = res["dist_indptr"].cpu().numpy().astype(_index_dtype(n, n * m))
     d_ind = res["dist_indices"][: n * m].cpu().numpy()
     d_dat = res["dist_data"][: n * m].cpu().numpy()
-    c_ptr = res["conn_indptr"].cpu().numpy().astype(np.int32)
+    c_ptr = res["conn_indptr"].cpu().numpy().astype(_index_dtype(n, nnz))
     c_ind = res["conn_indices"][:nnz].cpu().numpy()
     c_dat = res["conn_data"][:nnz].cpu().numpy()
     dist = sp.csr_matrix((d_dat, d_ind, d_ptr), shape=(n, n))
@@ -298,10 +303,85 @@ def graph_arrays(res: dict, n: int, which: str = "connectivities") -> dict:
     consumers (Leiden, UMAP epochs) that the reference feeds through a host CSR."""
     import torch
     indptr, indices, data = csr_device(res, n, which)
+    if indices.numel() >= 2 ** 32:
+        raise ValueError("the graph container's uint32 row pointers hold at most 2^32 - 1 edges")
     deg = indptr[1:] - indptr[:-1]
     src = torch.repeat_interleave(torch.arange(n, device=indptr.device, dtype=torch.int32), deg)
-    return {"indptr": indptr.to(torch.int32), "indices": indices, "weights": data,
-            "edge_src": src, "n": n}
+    # the container keeps its row pointers as uint32 (csr_graph.py:32); torch's uint32 type has
+    # few operators, so the words are taken as they lie: an int64 value below 2^32 has that
+    # uint32 value as its low (first, little-endian) word
+    lo = indptr.view(torch.int32).view(n + 1, 2)[:, 0].contiguous().view(torch.uint32)
+    return {"indptr": lo, "indices": indices, "weights": data, "edge_src": src, "n": n}
+
+
+def umap_edges(res: dict, n: int, n_epochs: int | None = None, *, stream=None) -> dict:
+    """The edge list the UMAP layout samples, prepared on the device from a ``neighbors_device``
+    result (metalsinglecell embedding.py:100-116, 123-137, 255-267): edges with weight below
+    max(w) / n_epochs dropped, the kept graph as COO in CSR order, and each edge's sampling period
+    ``epochs_per_sample`` (FP64; -1 never sampled).  ``n_epochs`` defaults as the reference's
+    ``umap`` does: 500 up to 10,000 cells, else 200.
+
+    Returns device tensors ``indptr`` (the kept graph's int64 row pointers), ``rows``, ``cols``
+    (int32), ``weights`` (float32), ``epochs_per_sample`` (float64) and ``n_epochs``."""
+    torch = _torch()
+    lib = _lib.load()
+    if n_epochs is None:
+        n_epochs = 500 if n <= 10_000 else 200
+    indptr = res["conn_indptr"]
+    dev = indptr.device
+    cap = max(int(res["conn_indices"].numel()), 1)
+    out_ptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    rows = torch.empty(cap, dtype=torch.int32, device=dev)
+    cols = torch.empty(cap, dtype=torch.int32, device=dev)
+    w = torch.empty(cap, dtype=torch.float32, device=dev)
+    eps = torch.empty(cap, dtype=torch.float64, device=dev)
+    nbytes = lib.msc_umap_edges_workspace_bytes(n)
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    st = _stream(torch, dev) if stream is None else stream
+    _lib.check(lib.msc_umap_edges(indptr.data_ptr(), res["conn_indices"].data_ptr(),
+                                  res["conn_data"].data_ptr(), n, int(n_epochs),
+                                  out_ptr.data_ptr(), rows.data_ptr(), cols.data_ptr(),
+                                  w.data_ptr(), eps.data_ptr(), ws.data_ptr(), nbytes, st),
+               "msc_umap_edges")
+    m = int(out_ptr[n].item())
+    return {"indptr": out_ptr, "rows": rows[:m], "cols": cols[:m], "weights": w[:m],
+            "epochs_per_sample": eps[:m], "n_epochs": int(n_epochs)}
+
+
+_HOST_STATE: dict = {}           # the buffers of the last shape the host-level call saw
+
+
+def _host_state(n: int, d: int, k: int, device) -> HostGraphState:
+    key = (n, d, k, str(device))
+    st = _HOST_STATE.get(key)
+    if st is None:
+        _HOST_STATE.clear()                    # keep one shape's pinned buffers at most
+        st = HostGraphState(n, d, k, device=device)
+        _HOST_STATE[key] = st
+    return st
+
+
+def _host_csr(h: dict, n: int, k: int):
+    """SciPy CSR matrices owning their arrays, from the pinned host tensors of
+    ``neighbors_host``; index arrays int32 while they fit, as SciPy itself chooses."""
+    import scipy.sparse as sp
+    torch = _torch()
+    m = max(k - 1, 0)
+
+    def own(t, count, dtype):
+        out = np.empty(count, dtype=dtype)
+        if count:
+            torch.from_numpy(out).copy_(t[:count])     # multi-threaded host copy
+        return out
+
+    nnz = int(h["conn_nnz"])
+    d_ptr = h["dist_indptr"].numpy().astype(_index_dtype(n, n * m))
+    c_ptr = h["conn_indptr"].numpy().astype(_index_dtype(n, nnz))
+    dist = sp.csr_matrix((own(h["dist_data"], n * m, np.float32),
+                          own(h["dist_indices"], n * m, np.int32), d_ptr), shape=(n, n))
+    conn = sp.csr_matrix((own(h["conn_data"], nnz, np.float32),
+                          own(h["conn_indices"], nnz, np.int32), c_ptr), shape=(n, n))
+    return dist, conn
 
 
 def neighbors(X_pca: np.ndarray, n_neighbors: int = 15, random_state: int = 0,
@@ -314,18 +394,31 @@ def neighbors(X_pca: np.ndarray, n_neighbors: int = 15, random_state: int = 0,
     them in the reference), ``connectivities`` the symmetric fuzzy graph (method='umap') or the
     Gaussian-kernel graph (method='gauss').  ``random_state`` and ``approx`` are accepted for
     compatibility; the graph is exact and deterministic.
+
+    The embedding is uploaded, the graph built on the GPU and both matrices copied back, the
+    distances while the connectivities are still being computed (``neighbors_host``).  Device and
+    pinned host buffers of the last shape are kept for the next call of that shape.
     """
     torch = _torch()
     X = np.ascontiguousarray(X_pca, dtype=np.float32)
     if X.ndim != 2:
         raise ValueError("X_pca must be 2-D")
+    n, d = X.shape
+    k = int(n_neighbors)
     dev = torch.device(device) if device is not None else torch.device("cuda",
                                                                        torch.cuda.current_device())
-    Xd = torch.from_numpy(X).to(dev, non_blocking=False)
-    res = neighbors_device(Xd, n_neighbors, metric=metric, method=method, precision=precision,
-                           kprime=kprime)
-    torch.cuda.current_stream(dev).synchronize()
-    return graph_to_host(res, X.shape[0], int(n_neighbors))
+    # argument errors are raised before any buffer of this shape is made
+    mid, meth, pid = _ids(metric, method, precision)
+    lib = _lib.load()
+    if lib.msc_neighbors_workspace_bytes(n, d, k, mid, meth, pid, int(kprime)) == 0:
+        _lib.check(lib.msc_neighbors(0, n, d, k, mid, meth, pid, int(kprime), *([0] * 10), 0, 0),
+                   "msc_neighbors")
+        raise ValueError("msc_neighbors: invalid arguments")
+    st = _host_state(n, d, k, dev)
+    with torch.cuda.device(dev):
+        h = neighbors_host(torch.from_numpy(X), k, metric=metric, method=method,
+                           precision=precision, kprime=kprime, state=st)
+    return _host_csr(h, n, k)
 
 
 def _knn(X_pca: np.ndarray, n_neighbors: int, random_state: int = 0,

@@ -19,12 +19,15 @@ This package restates, in NumPy/SciPy on the host, what the reference computes f
 * ``spatial.grid_knn`` / ``spatial.grid_radius`` / ``spatial.knn_edges`` — the uniform-grid
   spatial kNN and radius search of 2-D/3-D coordinates (``neighbors.py:143-417``, used by
   ``gr.py:186-255``), pinned against sklearn by the reference's own known-answer criteria.
+* ``handoff.umap_edges`` — the UMAP layout's edge preparation (weak-edge pruning and
+  epochs-per-sample, ``embedding.py:100-137, 255-267``), the first consumer of the graph.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import this
 package, and only as the checker.  The product (``metal-singlecell_b200/``) never imports it.
 
-Pinning: ``bbknn.trim_graph`` equals the reference's own ``_trim_graph`` bit for bit on the
-fixtures of ``tests/golden/make_golden.py``.  The kNN restatement is pinned by the reference's own known-answer tests
+Pinning: ``bbknn.trim_graph`` and ``handoff.umap_edges`` equal the reference's own
+``_trim_graph`` and ``_prune_weak_edges`` / ``_make_epochs_per_sample`` bit for bit on the fixtures
+of ``tests/golden/make_golden.py``.  The kNN restatement is pinned by the reference's own known-answer tests
 (``tests/test_postfix_fixes.py:108-121``, 500×20 recall vs NumPy brute force;
 ``tests/test_postfix_fixes.py:197-207``, coincident points stay finite) and by fixtures generated
 from the reference's NumPy-expressible code (``tests/golden/make_golden.py``).  Connectivity

@@ -122,3 +122,20 @@ def test_oracle_spatial_graphs_vs_reference():
             np.testing.assert_array_equal(M.data, ref, err_msg=f"{c} {tag}")
         checked += 1
     assert checked == 13
+
+
+def test_oracle_umap_edges_vs_reference():
+    # the reference's own _prune_weak_edges + tocoo + _make_epochs_per_sample (embedding.py)
+    import scipy.sparse as sp
+    from oracle import handoff
+    g = np.load(G / "reference_umap_edges.npz")
+    n = g["indptr"].size - 1
+    C = sp.csr_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
+    for e in g["epochs"]:
+        o = handoff.umap_edges(C, int(e))
+        np.testing.assert_array_equal(o["rows"], g[f"e{e}_rows"])
+        np.testing.assert_array_equal(o["cols"], g[f"e{e}_cols"])
+        np.testing.assert_array_equal(o["weights"], g[f"e{e}_weights"])
+        np.testing.assert_array_equal(o["epochs_per_sample"], g[f"e{e}_eps"])
+        assert o["indptr"][-1] == o["rows"].size
+        np.testing.assert_array_equal(np.diff(o["indptr"]), np.bincount(o["rows"], minlength=n))

@@ -44,7 +44,7 @@ def test_csr_views_and_torch_tensor(result):
 def test_graph_container_layout(result):
     res, C, _ = result
     g = nbm.graph_arrays(res, 300)
-    assert g["n"] == 300 and g["indptr"].dtype == torch.int32
+    assert g["n"] == 300 and g["indptr"].dtype == torch.uint32     # csr_graph.py:32
     np.testing.assert_array_equal(g["indptr"].numpy(), C.indptr)
     np.testing.assert_array_equal(g["indices"].numpy(), C.indices)
     np.testing.assert_array_equal(g["weights"].numpy(), C.data)
