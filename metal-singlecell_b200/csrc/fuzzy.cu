@@ -8,13 +8,15 @@
 // pair is the symmetric locally scaled Gaussian kernel.
 //
 // Stages (all integer work is exact, so the CSR structure is bit-exact):
-//   1. count: fwd[i] = kept entries of row i; indeg[j] += 1 per kept edge i→j;
-//   2. exclusive scan of fwd+indeg → per-row segment offsets;
-//   3. fill: row i's own entries, then every edge i→j scattered into row j's segment as a
-//      "reverse" record (slot from an atomic cursor — order within the segment is arbitrary);
-//   4. per row: sort the records by key = (column << 1 | reverse) — warp rank sort up to 256,
-//      block bitonic beyond — then merge the pairs (a column present in both directions) and
-//      write the unique entries left-justified;
+//   1. count: indeg[j] += 1 per kept edge i→j (a warp walks 32 rows' lists in memory order);
+//   2. exclusive scan of the in-degrees → row i's segment of the record array at i·k + rptr[i]:
+//      k slots for its own list, then its reverse records;
+//   3. fill: every kept edge i→j written into row j's segment as one 8-byte reverse record
+//      (slot from an atomic cursor — order within the segment is arbitrary);
+//   4. per row: its own list (read straight from the kNN arrays) and its reverse records sorted by
+//      key = (column << 1 | reverse) — a warp bitonic network in registers up to 256 entries,
+//      a block network beyond — then the pairs merged (a column present in both directions) and
+//      the unique entries written left-justified into the segment;
 //   5. exclusive scan of the unique counts → indptr; 6. copy into indices / data.
 #include "kernels.cuh"
 
@@ -23,7 +25,6 @@ namespace msc {
 namespace {
 
 constexpr int UW = 8;            // warps per block in the warp-per-row kernels
-constexpr int WARP_MAX = 256;    // longest row the warp tier sorts
 constexpr int BLK_SMEM_MAX = 8192;
 
 // ------------------------------------------------------------------------------------------------
@@ -123,59 +124,59 @@ int scan_excl(const T* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream
 }
 
 // ------------------------------------------------------------------------------------------------
-// stages 1 and 3
+// stages 1 and 3: flat passes over the kNN lists, a warp per 32 rows
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ bool kept(int mode, int t, float v) {
   // umap: memberships > 0 (self has 0); gauss: every neighbour but self (column 0)
   return mode == 0 ? (v > 0.f) : (t > 0);
 }
 
-__global__ void count_kernel(int mode, const int32_t* __restrict__ idx,
-                             const float* __restrict__ vals, int64_t n, int k,
-                             int32_t* __restrict__ fwd, int32_t* __restrict__ indeg) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    int c = 0;
-    for (int t = 0; t < k; ++t) {
-      const int64_t e = i * k + t;
-      const int32_t j = idx[e];
-      if (j != i && j >= 0 && j < n && kept(mode, t, vals[e])) {
-        ++c;
-        atomicAdd(&indeg[j], 1);
-      }
+// The lanes of a warp walk the k·32 list entries of 32 consecutive rows in memory order (coalesced
+// loads).  Entry x of the group is row x / k, position x % k; the division is a multiply-shift,
+// exact for x < 32·k and k <= 129 (x·ceil(2^22 / k) >> 22 = floor(x / k), checked exhaustively).
+__host__ __device__ __forceinline__ uint32_t div_magic(int k) {
+  return uint32_t(((uint64_t(1) << 22) + uint64_t(k) - 1) / uint64_t(k));
+}
+
+template <class F>
+__device__ __forceinline__ void for_each_kept_edge(int mode, const int32_t* __restrict__ idx,
+                                                   const float* __restrict__ vals, int64_t n, int k,
+                                                   uint32_t magic, F&& f) {
+  const int lane = lane_id();
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t g = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; g * 32 < n;
+       g += nwarps) {
+    const int64_t r0 = g * 32;
+    const int ne = int(min64(32, n - r0)) * k;
+    const int64_t e0 = r0 * k;
+    for (int x = lane; x < ne; x += 32) {
+      const int r = int((uint32_t(x) * magic) >> 22);
+      const int t = x - r * k;
+      const int64_t i = r0 + r;
+      const int32_t j = idx[e0 + x];
+      const float v = vals[e0 + x];
+      if (j != i && j >= 0 && j < n && kept(mode, t, v)) f(i, j, v);
     }
-    fwd[i] = c;
   }
 }
 
-__global__ void seglen_kernel(const int32_t* __restrict__ fwd, const int32_t* __restrict__ indeg,
-                              int64_t n, int32_t* __restrict__ len) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x)
-    len[i] = fwd[i] + indeg[i];
+__global__ void __launch_bounds__(256)
+rev_count_kernel(int mode, const int32_t* __restrict__ idx, const float* __restrict__ vals,
+                 int64_t n, int k, uint32_t magic, int32_t* __restrict__ indeg) {
+  for_each_kept_edge(mode, idx, vals, n, k, magic,
+                     [&](int64_t, int32_t j, float) { atomicAdd(&indeg[j], 1); });
 }
 
-__global__ void fill_kernel(int mode, const int32_t* __restrict__ idx,
-                            const float* __restrict__ vals, int64_t n, int k,
-                            const int64_t* __restrict__ segptr, const int32_t* __restrict__ fwd,
-                            int32_t* __restrict__ cursor, uint32_t* __restrict__ rkey,
-                            float* __restrict__ rval) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    int64_t own = segptr[i];
-    for (int t = 0; t < k; ++t) {
-      const int64_t e = i * k + t;
-      const int32_t j = idx[e];
-      const float v = vals[e];
-      if (j == i || j < 0 || j >= n || !kept(mode, t, v)) continue;
-      rkey[own] = uint32_t(j) << 1;
-      rval[own] = v;
-      ++own;
-      const int64_t slot = segptr[j] + fwd[j] + atomicAdd(&cursor[j], 1);
-      rkey[slot] = (uint32_t(i) << 1) | 1u;
-      rval[slot] = v;
-    }
-  }
+// Row i's segment of the record array starts at i·k + rptr[i] (rptr = exclusive scan of the
+// in-degrees): k slots for its own list, then its reverse records (i' → i, in any order).
+__global__ void __launch_bounds__(256)
+rev_fill_kernel(int mode, const int32_t* __restrict__ idx, const float* __restrict__ vals,
+                int64_t n, int k, uint32_t magic, const int64_t* __restrict__ rptr,
+                int32_t* __restrict__ cursor, int2* __restrict__ rec) {
+  for_each_kept_edge(mode, idx, vals, n, k, magic, [&](int64_t i, int32_t j, float v) {
+    const int64_t slot = int64_t(j) * k + rptr[j] + k + atomicAdd(&cursor[j], 1);
+    rec[slot] = make_int2(int((uint32_t(i) << 1) | 1u), __float_as_int(v));
+  });
 }
 
 // value of a merged entry (row i, column c); a/b = forward/reverse record values
@@ -195,91 +196,160 @@ __device__ __forceinline__ float pair_value(int mode, int64_t i, uint32_t c, boo
 }
 
 // ------------------------------------------------------------------------------------------------
-// stage 4, warp tier: rows of length <= WARP_MAX; longer rows are queued for the block tier
+// stage 4, warp tier: a row of L <= 32·W entries (its k list positions + its reverse records) is
+// held W keys per lane, sorted by a warp bitonic network (registers and shuffles), merged and
+// written back left-justified into its own segment.  Key = column << 1 | reverse, so the forward
+// and the reverse record of one column sort next to each other, forward first.
 // ------------------------------------------------------------------------------------------------
+constexpr uint32_t SENT = 0xffffffffu;    // empty position: sorts last, never written
+
+template <int W>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&key)[W], float (&val)[W]) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int size = 2; size <= 32 * W; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {                      // partner in the same lane, another register
+        const int rs = stride >> 5;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          if ((w & rs) == 0) {
+            const int w2 = w | rs;
+            const bool up = ((w * 32 + lane) & size) == 0;
+            if ((key[w] > key[w2]) == up) {
+              const uint32_t tk = key[w]; key[w] = key[w2]; key[w2] = tk;
+              const float tv = val[w]; val[w] = val[w2]; val[w2] = tv;
+            }
+          }
+        }
+      } else {                                 // partner in lane ^ stride, same register
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          const uint32_t ok = __shfl_xor_sync(FULL, key[w], stride);
+          const float ov = __shfl_xor_sync(FULL, val[w], stride);
+          const bool up = ((w * 32 + lane) & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          if (lower == up ? ok < key[w] : ok > key[w]) { key[w] = ok; val[w] = ov; }
+        }
+      }
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ int merge_row_regs(int mode, int64_t i, int k, int L, int64_t n,
+                                              const int32_t* __restrict__ idx,
+                                              const float* __restrict__ vals, int2* seg,
+                                              const double* __restrict__ sig2) {
+  const int lane = lane_id();
+  uint32_t key[W];
+  float val[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const int p = w * 32 + lane;
+    key[w] = SENT;
+    val[w] = 0.f;
+    if (p < k) {
+      const int32_t j = idx[i * k + p];
+      const float v = vals[i * k + p];
+      if (j != i && j >= 0 && j < n && kept(mode, p, v)) { key[w] = uint32_t(j) << 1; val[w] = v; }
+    } else if (p < L) {
+      const int2 r = seg[p];
+      key[w] = uint32_t(r.x);
+      val[w] = __int_as_float(r.y);
+    }
+  }
+  __syncwarp();                                 // every record is read before any is rewritten
+  warp_bitonic<W>(key, val);
+  int written = 0;
+  uint32_t carry_col = SENT;                     // column of the previous register's lane 31
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const uint32_t kk = key[w];
+    const uint32_t col = kk >> 1;
+    uint32_t left = __shfl_up_sync(FULL, kk == SENT ? SENT : col, 1);
+    if (lane == 0) left = carry_col;
+    uint32_t rk = __shfl_down_sync(FULL, kk, 1);
+    float rv = __shfl_down_sync(FULL, val[w], 1);
+    if (w + 1 < W) {
+      const uint32_t nk = __shfl_sync(FULL, key[w + 1 < W ? w + 1 : w], 0);
+      const float nv = __shfl_sync(FULL, val[w + 1 < W ? w + 1 : w], 0);
+      if (lane == 31) { rk = nk; rv = nv; }
+    } else if (lane == 31) {
+      rk = SENT;
+    }
+    carry_col = __shfl_sync(FULL, kk == SENT ? SENT : col, 31);
+    const bool first = kk != SENT && left != col;
+    float out = 0.f;
+    if (first) {
+      if (rk != SENT && (rk >> 1) == col) {
+        out = pair_value(mode, i, col, true, val[w], true, rv, sig2);
+      } else {
+        const bool rev = kk & 1u;
+        out = pair_value(mode, i, col, !rev, val[w], rev, val[w], sig2);
+      }
+    }
+    const unsigned m = __ballot_sync(FULL, first);
+    if (first) seg[written + __popc(m & ((1u << lane) - 1u))] = make_int2(int(col), __float_as_int(out));
+    written += __popc(m);
+  }
+  return written;
+}
+
+constexpr int WARP_MAX = 256;    // longest row the warp tier sorts (8 keys per lane)
+
 __global__ void __launch_bounds__(UW * 32)
-merge_warp_kernel(int mode, int64_t n, const int64_t* __restrict__ segptr,
-                  uint32_t* __restrict__ rkey, float* __restrict__ rval,
-                  const double* __restrict__ sig2, int32_t* __restrict__ uniq,
-                  int32_t* __restrict__ big_rows, int32_t* __restrict__ n_big) {
-  __shared__ uint32_t sk_all[UW][WARP_MAX];
-  __shared__ float sv_all[UW][WARP_MAX];
-  const int lane = lane_id(), wib = warp_id();
-  uint32_t* sk = sk_all[wib];
-  float* sv = sv_all[wib];
+merge_warp_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
+                  const float* __restrict__ vals, const int64_t* __restrict__ rptr,
+                  int2* __restrict__ rec, const double* __restrict__ sig2,
+                  int32_t* __restrict__ uniq, int32_t* __restrict__ big_rows,
+                  int32_t* __restrict__ n_big) {
+  const int lane = lane_id();
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < n; i += nwarps) {
-    const int64_t b = segptr[i];
-    const int L = int(segptr[i + 1] - b);
-    if (L > WARP_MAX) {
+    const int64_t b = i * k + rptr[i];
+    const int L = k + int(rptr[i + 1] - rptr[i]);
+    int2* seg = rec + b;
+    int u;
+    if (L <= 32) u = merge_row_regs<1>(mode, i, k, L, n, idx, vals, seg, sig2);
+    else if (L <= 64) u = merge_row_regs<2>(mode, i, k, L, n, idx, vals, seg, sig2);
+    else if (L <= 128) u = merge_row_regs<4>(mode, i, k, L, n, idx, vals, seg, sig2);
+    else if (L <= WARP_MAX) u = merge_row_regs<8>(mode, i, k, L, n, idx, vals, seg, sig2);
+    else {
+      // a long row goes to the block tier: its own list into the first k slots of its segment
+      for (int t = lane; t < k; t += 32) {
+        const int32_t j = idx[i * k + t];
+        const float v = vals[i * k + t];
+        const bool ok = j != i && j >= 0 && j < n && kept(mode, t, v);
+        seg[t] = make_int2(int(ok ? (uint32_t(j) << 1) : SENT), __float_as_int(v));
+      }
       if (lane == 0) big_rows[atomicAdd(n_big, 1)] = int32_t(i);
       continue;
     }
-    // rank sort into shared memory (keys are distinct within a row)
-    for (int e = lane; e < L; e += 32) {
-      const uint32_t key = rkey[b + e];
-      int r = 0;
-      for (int f = 0; f < L; ++f) r += rkey[b + f] < key;
-      sk[r] = key;
-      sv[r] = rval[b + e];
-    }
-    __syncwarp();
-    // merge pairs and write unique entries left-justified
-    int written = 0;
-    uint32_t prev_col = 0xffffffffu;               // column of the previous chunk's last entry
-    for (int e0 = 0; e0 < L; e0 += 32) {
-      const int e = e0 + lane;
-      bool uniq_e = false;
-      uint32_t col = 0xffffffffu;
-      float val = 0.f;
-      const uint32_t left = __shfl_up_sync(FULL, e < L ? (sk[e] >> 1) : 0xffffffffu, 1);
-      if (e < L) {
-        const uint32_t key = sk[e];
-        col = key >> 1;
-        const bool second = (lane == 0 ? prev_col : left) == col;
-        if (!second) {
-          uniq_e = true;
-          const bool rev = key & 1u;
-          const bool nxt = e + 1 < L && (sk[e + 1] >> 1) == col;
-          if (nxt) val = pair_value(mode, i, col, true, sv[e], true, sv[e + 1], sig2);
-          else val = pair_value(mode, i, col, !rev, sv[e], rev, sv[e], sig2);
-        }
-      }
-      const unsigned m = __ballot_sync(FULL, uniq_e);
-      const int pos = written + __popc(m & ((1u << lane) - 1u));
-      prev_col = __shfl_sync(FULL, col, 31);
-      __syncwarp();
-      if (uniq_e) {
-        rkey[b + pos] = col;
-        rval[b + pos] = val;
-      }
-      written += __popc(m);
-    }
-    if (lane == 0) uniq[i] = written;
-    __syncwarp();
+    if (lane == 0) uniq[i] = u;
   }
 }
 
 // block tier: one block per long row; ascending-only bitonic network over the next power of two
 // (positions >= L act as +inf and never move), in shared memory when the row fits, else in place
-// in global memory
+// in its segment
 __global__ void __launch_bounds__(1024)
-merge_block_kernel(int mode, const int32_t* __restrict__ big_rows, const int32_t* __restrict__ n_big,
-                   const int64_t* __restrict__ segptr, uint32_t* __restrict__ rkey,
-                   float* __restrict__ rval, const double* __restrict__ sig2,
+merge_block_kernel(int mode, int k, const int32_t* __restrict__ big_rows,
+                   const int32_t* __restrict__ n_big, const int64_t* __restrict__ rptr,
+                   int2* __restrict__ rec, const double* __restrict__ sig2,
                    int32_t* __restrict__ uniq) {
   extern __shared__ unsigned char smem[];
   const int nb = *n_big;
   for (int r = blockIdx.x; r < nb; r += gridDim.x) {
     const int64_t i = big_rows[r];
-    const int64_t b = segptr[i];
-    const int64_t L = segptr[i + 1] - b;
+    const int64_t b = i * k + rptr[i];
+    const int64_t L = k + (rptr[i + 1] - rptr[i]);
+    int2* seg = rec + b;
     const bool in_smem = L <= BLK_SMEM_MAX;
-    uint32_t* K = in_smem ? reinterpret_cast<uint32_t*>(smem) : rkey + b;
-    float* V = in_smem ? reinterpret_cast<float*>(smem + BLK_SMEM_MAX * 4) : rval + b;
-    if (in_smem) {
-      for (int64_t e = threadIdx.x; e < L; e += blockDim.x) { K[e] = rkey[b + e]; V[e] = rval[b + e]; }
-    }
+    int2* S = in_smem ? reinterpret_cast<int2*>(smem) : seg;
+    if (in_smem)
+      for (int64_t e = threadIdx.x; e < L; e += blockDim.x) S[e] = seg[e];
     __syncthreads();
     int64_t P = 1;
     while (P < L) P <<= 1;
@@ -289,9 +359,8 @@ merge_block_kernel(int mode, const int32_t* __restrict__ big_rows, const int32_t
         for (int64_t q = threadIdx.x; q < P / 2; q += blockDim.x) {
           const int64_t lo = (q / j) * 2 * j + (q % j);
           const int64_t hi = flip ? (lo ^ (kk - 1)) : lo + j;
-          if (hi < L && K[hi] < K[lo]) {
-            uint32_t tk = K[lo]; K[lo] = K[hi]; K[hi] = tk;
-            float tv = V[lo]; V[lo] = V[hi]; V[hi] = tv;
+          if (hi < L && uint32_t(S[hi].x) < uint32_t(S[lo].x)) {
+            const int2 t = S[lo]; S[lo] = S[hi]; S[hi] = t;
           }
         }
         __syncthreads();
@@ -301,30 +370,29 @@ merge_block_kernel(int mode, const int32_t* __restrict__ big_rows, const int32_t
     if (threadIdx.x < 32) {
       const int lane = threadIdx.x;
       int64_t written = 0;
-      uint32_t prev_col = 0xffffffffu;             // the previous chunk may already be rewritten
+      uint32_t prev_col = SENT;                    // the previous chunk may already be rewritten
       for (int64_t e0 = 0; e0 < L; e0 += 32) {
         const int64_t e = e0 + lane;
-        bool uniq_e = false;
-        uint32_t col = 0xffffffffu;
-        float val = 0.f;
-        const uint32_t left = __shfl_up_sync(FULL, e < L ? (K[e] >> 1) : 0xffffffffu, 1);
-        if (e < L) {
-          const uint32_t key = K[e];
-          col = key >> 1;
-          const bool second = (lane == 0 ? prev_col : left) == col;
-          if (!second) {
-            uniq_e = true;
-            const bool rev = key & 1u;
-            const bool nxt = e + 1 < L && (K[e + 1] >> 1) == col;
-            if (nxt) val = pair_value(mode, i, col, true, V[e], true, V[e + 1], sig2);
-            else val = pair_value(mode, i, col, !rev, V[e], rev, V[e], sig2);
+        const uint32_t kk = e < L ? uint32_t(S[e].x) : SENT;
+        const float v = e < L ? __int_as_float(S[e].y) : 0.f;
+        const uint32_t col = kk >> 1;
+        uint32_t left = __shfl_up_sync(FULL, kk == SENT ? SENT : col, 1);
+        if (lane == 0) left = prev_col;
+        const bool first = kk != SENT && left != col;
+        float out = 0.f;
+        if (first) {
+          const uint32_t nk = e + 1 < L ? uint32_t(S[e + 1].x) : SENT;
+          if (nk != SENT && (nk >> 1) == col) {
+            out = pair_value(mode, i, col, true, v, true, __int_as_float(S[e + 1].y), sig2);
+          } else {
+            const bool rev = kk & 1u;
+            out = pair_value(mode, i, col, !rev, v, rev, v, sig2);
           }
         }
-        const unsigned m = __ballot_sync(FULL, uniq_e);
-        const int64_t pos = written + __popc(m & ((1u << lane) - 1u));
-        prev_col = __shfl_sync(FULL, col, 31);
+        const unsigned m = __ballot_sync(FULL, first);
+        prev_col = __shfl_sync(FULL, kk == SENT ? SENT : col, 31);
         __syncwarp();                       // all reads of this chunk precede its writes
-        if (uniq_e) { rkey[b + pos] = col; rval[b + pos] = val; }
+        if (first) seg[written + __popc(m & ((1u << lane) - 1u))] = make_int2(int(col), __float_as_int(out));
         __syncwarp();
         written += __popc(m);
       }
@@ -336,17 +404,19 @@ merge_block_kernel(int mode, const int32_t* __restrict__ big_rows, const int32_t
 
 // stage 6: copy the unique entries of every row to the output CSR
 __global__ void __launch_bounds__(UW * 32)
-emit_kernel(int64_t n, const int64_t* __restrict__ segptr, const int64_t* __restrict__ outptr,
-            const uint32_t* __restrict__ rkey, const float* __restrict__ rval,
+emit_kernel(int64_t n, int k, const int64_t* __restrict__ rptr,
+            const int64_t* __restrict__ outptr, const int2* __restrict__ rec,
             int32_t* __restrict__ indices, float* __restrict__ data) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < n; i += nwarps) {
-    const int64_t b = segptr[i], o = outptr[i];
+    const int2* seg = rec + i * k + rptr[i];
+    const int64_t o = outptr[i];
     const int64_t m = outptr[i + 1] - o;
     for (int64_t e = lane; e < m; e += 32) {
-      indices[o + e] = int32_t(rkey[b + e]);
-      data[o + e] = rval[b + e];
+      const int2 r = seg[e];
+      indices[o + e] = r.x;
+      data[o + e] = __int_as_float(r.y);
     }
   }
 }
@@ -357,26 +427,23 @@ __global__ void copy_nnz_kernel(const int64_t* __restrict__ outptr, int64_t n,
 }
 
 struct UnionWs {
-  int32_t *fwd, *indeg, *cursor, *len, *uniq, *big, *nbig;
-  int64_t *segptr, *scan;
-  uint32_t* rkey;
-  float* rval;
+  int32_t *indeg, *cursor, *nbig, *uniq, *big;
+  int64_t *rptr, *scan;
+  int2* rec;
 };
 
 UnionWs carve_union(Carver& c, int64_t n, int k) {
   UnionWs w;
-  w.fwd = c.take<int32_t>(n);
   w.indeg = c.take<int32_t>(n);
   w.cursor = c.take<int32_t>(n);
   w.nbig = c.take<int32_t>(8);
-  w.len = c.take<int32_t>(n);
   w.uniq = c.take<int32_t>(n);
   w.big = c.take<int32_t>(n);
-  w.segptr = c.take<int64_t>(n + 1);
+  w.rptr = c.take<int64_t>(n + 1);
   w.scan = c.take<int64_t>(scan_scratch_elems(n));
-  const size_t e2 = size_t(2) * size_t(n) * size_t(std::max(k - 1, 1));
-  w.rkey = c.take<uint32_t>(e2);
-  w.rval = c.take<float>(e2);
+  // every row's k own slots plus at most n·k reverse records in all (n·(k-1) when every list
+  // holds its own cell, as kNN lists do)
+  w.rec = c.take<int2>(size_t(2) * size_t(n) * size_t(k));
   return w;
 }
 
@@ -396,32 +463,30 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
     return MSC_ERR_WORKSPACE;
   }
   if (n >= (int64_t(1) << 31)) { set_error("n >= 2^31"); return MSC_ERR_UNSUPPORTED; }
+  if (k < 1 || k > MSC_MAX_K) { set_error("fuzzy union: k=%d out of range", k); return MSC_ERR_INVALID_ARG; }
   Carver c(ws);
   UnionWs w = carve_union(c, n, k);
-  // fwd, indeg, cursor and the big-row counter are contiguous at the start: one memset
-  MSC_CUDA_TRY(cudaMemsetAsync(w.fwd, 0, reinterpret_cast<char*>(w.len) - reinterpret_cast<char*>(w.fwd), st));
+  // in-degrees, cursors and the long-row counter are contiguous at the start: one memset
+  MSC_CUDA_TRY(cudaMemsetAsync(w.indeg, 0, reinterpret_cast<char*>(w.uniq) - reinterpret_cast<char*>(w.indeg), st));
   const int sms = num_sms();
-  const int g1 = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), sms * 8)));
-  count_kernel<<<g1, 256, 0, st>>>(mode, idx, vals, n, k, w.fwd, w.indeg);
+  const uint32_t magic = div_magic(k);
+  const int g1 = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), int64_t(sms) * 8)));
+  rev_count_kernel<<<g1, 256, 0, st>>>(mode, idx, vals, n, k, magic, w.indeg);
   MSC_LAUNCH_CHECK();
-  seglen_kernel<<<g1, 256, 0, st>>>(w.fwd, w.indeg, n, w.len);
+  MSC_TRY(scan_excl<int32_t>(w.indeg, n, w.rptr, w.scan, st));
+  rev_fill_kernel<<<g1, 256, 0, st>>>(mode, idx, vals, n, k, magic, w.rptr, w.cursor, w.rec);
   MSC_LAUNCH_CHECK();
-  MSC_TRY(scan_excl<int32_t>(w.len, n, w.segptr, w.scan, st));
-  fill_kernel<<<g1, 256, 0, st>>>(mode, idx, vals, n, k, w.segptr, w.fwd, w.cursor, w.rkey,
-                                  w.rval);
-  MSC_LAUNCH_CHECK();
-  const int g2 = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, UW), sms * 16)));
-  merge_warp_kernel<<<g2, UW * 32, 0, st>>>(mode, n, w.segptr, w.rkey, w.rval, sig2, w.uniq,
+  const int g2 = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, UW), int64_t(sms) * 16)));
+  merge_warp_kernel<<<g2, UW * 32, 0, st>>>(mode, n, k, idx, vals, w.rptr, w.rec, sig2, w.uniq,
                                              w.big, w.nbig);
   MSC_LAUNCH_CHECK();
-  const size_t bsm = size_t(BLK_SMEM_MAX) * 8;
+  const size_t bsm = size_t(BLK_SMEM_MAX) * sizeof(int2);
   MSC_CUDA_TRY(cudaFuncSetAttribute(merge_block_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(bsm)));
-  merge_block_kernel<<<sms, 1024, bsm, st>>>(mode, w.big, w.nbig, w.segptr, w.rkey, w.rval, sig2,
-                                             w.uniq);
+  merge_block_kernel<<<sms, 1024, bsm, st>>>(mode, k, w.big, w.nbig, w.rptr, w.rec, sig2, w.uniq);
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl<int32_t>(w.uniq, n, indptr, w.scan, st));
-  emit_kernel<<<g2, UW * 32, 0, st>>>(n, w.segptr, indptr, w.rkey, w.rval, indices, data);
+  emit_kernel<<<g2, UW * 32, 0, st>>>(n, k, w.rptr, indptr, w.rec, indices, data);
   MSC_LAUNCH_CHECK();
   if (nnz_dev) {
     copy_nnz_kernel<<<1, 32, 0, st>>>(indptr, n, nnz_dev);
