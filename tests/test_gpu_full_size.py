@@ -7,7 +7,10 @@ rows (the oracle scans all 1.3M cells for each sampled row).
   and bit-identical to the oracle, ties included, on 192 seeded rows;
 * distances CSR: row i holds exactly knn row i's columns 1..k-1, column-sorted (the oracle's
   ``distances_csr`` of those rows);
-* connectivities: symmetric, no diagonal, values in (0, 1], n(k-1) <= nnz <= 2n(k-1).
+* connectivities: symmetric, no diagonal, values in (0, 1], n(k-1) <= nnz <= 2n(k-1);
+* the whole graph: the oracle's ρ/σ, memberships, fuzzy union and distances CSR, run on the host
+  over all 1.3M of the GPU's kNN lists (which the sampled rows pin to the oracle's exact kNN),
+  equal the GPU's connectivities and distances CSR bit for bit — every row, not a sample.
 """
 import numpy as np
 import pytest
@@ -85,3 +88,22 @@ def test_full_size_connectivities(scale_graph):
     D = (C - C.T).tocsr()
     D.eliminate_zeros()
     assert D.nnz == 0                                     # symmetric, values bit-equal
+
+
+def test_full_size_whole_graph_matches_oracle(scale_graph):
+    import scipy.sparse as sp
+    X, k, g = scale_graph
+    n = X.shape[0]
+    idx, dist = g["knn_idx"], g["knn_dist"]
+    sigma, rho = oracle.smooth_knn_dist(dist, k)
+    w = oracle.membership_strengths(idx, dist, sigma, rho)
+    ref_conn = oracle.fuzzy_union(idx, w, n)
+    ref_dist = oracle.distances_csr(idx, dist, n)
+    for what, (ptr, ind, dat), ref in (
+            ("connectivities", (g["conn_indptr"], g["conn_indices"], g["conn_data"]), ref_conn),
+            ("distances", (g["dist_indptr"], g["dist_indices"], g["dist_data"]), ref_dist)):
+        nnz = int(ptr[n])
+        assert nnz == ref.nnz, what
+        np.testing.assert_array_equal(ptr.astype(np.int64), ref.indptr.astype(np.int64), what)
+        np.testing.assert_array_equal(ind[:nnz], ref.indices.astype(np.int32), what)
+        np.testing.assert_array_equal(dat[:nnz], ref.data, what)
