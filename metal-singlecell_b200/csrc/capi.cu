@@ -380,6 +380,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       stage_mark(st, 1);
       const uint32_t* mask = nullptr;
       int words = 0;
+      bool ordered = false;
       const NearInit init{w.pr.cand_val, w.cand_idx, w.pr.iperm, w.pr.excl};
       if (prune) {
         // near pass -> per-row radius -> outliers to the end of each sample -> operands of the
@@ -398,15 +399,20 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
         MSC_TRY(launch_prune_plan(Xu, P.d, P.npacked, w.perm, w.items, n_items, cfg.bn, w.ctl,
                                   P.prec, w.pr, words, st));
         mask = w.pr.mask;
+        MSC_TRY(launch_visit_order(w.items, n_items, cfg.bn, P.d, P.npacked, w.perm, w.ctl,
+                                   w.ctl, P.prec, P.L.kmma, w.qs, w.km, w.pr, words, st,
+                                   &ordered));
       } else {
         stage_mark(st, 2);
       }
       stage_mark(st, 3);
+      const VisitOrder order{w.pr.vlist, w.pr.voff, w.pr.roff, &w.ctl->ordered_ok};
       MSC_TRY(launch_knn_tc(P.prec, cfg, w.Aop, w.Bop, P.npacked, P.npacked, P.L.kp, P.L.kmma,
                             w.items, n_items, w.perm, nullptr, nullptr, &w.ctl->tc_counter[0],
                             w.ctl, P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask, words,
                             false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr,
-                            prune ? &init : nullptr));
+                            prune ? &init : nullptr, nullptr,
+                            ordered ? &order : nullptr));
     }
   }
   stage_mark(st, 4);
@@ -840,6 +846,30 @@ int msc_distances_csr(const int32_t* knn_idx_dev, const float* knn_dist_dev, int
     return MSC_ERR_INVALID_ARG;
   return launch_distances_csr(knn_idx_dev, knn_dist_dev, n, k, indptr_dev, indices_dev, data_dev,
                               as_stream(stream));
+}
+
+// ---- UMAP edge preparation on the device (embedding.py:115-137, 255-267) ----
+
+size_t msc_umap_edges_workspace_bytes(int64_t n) { return n < 1 ? 0 : umap_edges_workspace_bytes(n); }
+
+int msc_umap_edges(const int64_t* indptr_dev, const int32_t* indices_dev, const float* data_dev,
+                   int64_t n, int32_t n_epochs, int64_t* out_indptr_dev, int32_t* rows_dev,
+                   int32_t* cols_dev, float* weights_dev, double* epochs_per_sample_dev,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 1 || n >= (int64_t(1) << 31)) { set_error("n=%lld out of range", (long long)n); return MSC_ERR_INVALID_ARG; }
+  if (n_epochs < 1) { set_error("n_epochs=%d must be >= 1", n_epochs); return MSC_ERR_INVALID_ARG; }
+  if (bad_ptr(indptr_dev, "indptr") || bad_ptr(indices_dev, "indices") ||
+      bad_ptr(data_dev, "data") || bad_ptr(out_indptr_dev, "out_indptr") ||
+      bad_ptr(rows_dev, "rows") || bad_ptr(cols_dev, "cols") || bad_ptr(weights_dev, "weights") ||
+      bad_ptr(epochs_per_sample_dev, "epochs_per_sample") || bad_ptr(workspace, "workspace"))
+    return MSC_ERR_INVALID_ARG;
+  if (workspace_bytes < umap_edges_workspace_bytes(n)) {
+    set_error("workspace %zu < %zu bytes", workspace_bytes, umap_edges_workspace_bytes(n));
+    return MSC_ERR_WORKSPACE;
+  }
+  return launch_umap_edges(indptr_dev, indices_dev, data_dev, n, n_epochs, out_indptr_dev,
+                           rows_dev, cols_dev, weights_dev, epochs_per_sample_dev, workspace,
+                           as_stream(stream));
 }
 
 // ---- batch-balanced kNN (neighbors.py:491-559, 465-488) ----

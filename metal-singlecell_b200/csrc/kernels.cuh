@@ -141,6 +141,13 @@ struct PruneWs {
   int2* part;         // refine split: k' (value, row) per row per work item
   float* part_thr;
   int max_split_items;
+  // sorted visit lists of the main scan (see VisitOrder)
+  double* roff;       // per packed row (final layout): |z|² + 3·eps
+  int32_t* vcnt;      // per work item: kept far tiles
+  int64_t* voff;      // per work item: first entry (n_items + 1)
+  int64_t* vscan;     // scan scratch over the work items
+  unsigned long long* vlist;
+  int64_t vcap;       // entries vlist holds
 };
 int prune_mask_words(int64_t max_seg, int bn);
 PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words,
@@ -155,6 +162,12 @@ int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, 
 int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* perm,
                       const WorkItem* items, int64_t n_items, int bn, const Ctl* ctl, int prec,
                       const PruneWs& w, int words, cudaStream_t st);
+// sorted visit lists of the main scan from the plan's masks (after launch_prune_plan): false in
+// *built when the shape does not allow them (the mask walk is used)
+int launch_visit_order(const WorkItem* items, int64_t n_items, int bn, int d, int64_t npacked,
+                       const int32_t* perm, const Ctl* ctl, Ctl* ctl_w, int prec, int kmma,
+                       const QStat* qs, const KeyMax* km, const PruneWs& w, int words,
+                       cudaStream_t st, bool* built);
 // visit masks of the refine pass's work items (from the main pass's masks)
 int launch_refine_mask(const WorkItem* items3, const int32_t* n_items3, const int32_t* qmap,
                        int64_t max_items, const SegDesc* seg, int nseg, int bn, int words,
@@ -193,6 +206,19 @@ struct RefineSplit {
   float* part_thr;
 };
 
+// Main scan after a pruning plan: every work item's kept far key tiles sorted by a lower bound on
+// the squared operand-space distance between the query tile's rows and the key tile's keys
+// (entry = bound bits << 32 | key tile; bound = -inf: unsorted, never stops the walk).  The
+// producer walks the near tiles and then this list, and ends the item's walk at the first tile
+// whose bound exceeds every row's current radius R = threshold + roff (all later tiles are
+// farther still).
+struct VisitOrder {
+  const unsigned long long* list;
+  const int64_t* off;
+  const double* roff;
+  const int32_t* ok;      // device flag: the lists were built (else the mask walk)
+};
+
 // ---- knn_tc.cu ----
 // Work items are claimed dynamically by the persistent CTAs, in index order or (reverse) from the
 // last one down.  Batches pack their largest samples first, so index order starts the longest
@@ -220,7 +246,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask = nullptr, int mask_words = 0, bool near_only = false,
                   bool reverse = false, const float* seed = nullptr,
-                  const NearInit* init = nullptr, const RefineSplit* split = nullptr);
+                  const NearInit* init = nullptr, const RefineSplit* split = nullptr,
+                  const VisitOrder* order = nullptr);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,
@@ -253,6 +280,11 @@ int launch_distances_csr(const int32_t* idx, const float* dist, int64_t n, int k
 int launch_gauss_sigma(const float* dist, int64_t n, int k, double* sig2, cudaStream_t st);
 
 // ---- fuzzy.cu ----
+// ---- handoff.cu ----
+size_t umap_edges_workspace_bytes(int64_t n);
+int launch_umap_edges(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n,
+                      int n_epochs, int64_t* out_ptr, int32_t* rows, int32_t* cols,
+                      float* weights, double* eps, void* ws, cudaStream_t st);
 size_t union_workspace_bytes(int64_t n, int k);
 // mode 0: umap fuzzy union of memberships w; mode 1: gauss kernel from distances + sig2
 int launch_union(int mode, const int32_t* idx, const float* vals, const double* sig2,

@@ -330,6 +330,13 @@ struct TcParams {
   const int32_t* init_idx;
   const int32_t* iperm;
   const int4* excl;
+  // main pass after a pruning plan: every work item's far tiles sorted by their distance bound
+  // (VisitOrder in kernels.cuh), each row's fixed radius part roff, and the flag that the lists
+  // were built; null: the mask walk
+  const unsigned long long* vlist;
+  const int64_t* voff;
+  const double* roff;
+  const int32_t* vok;
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -491,7 +498,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 40);
   uint64_t* item_full = bars + 41;         // [ITEM_RING] a claimed work item is in item_ring
   uint64_t* item_empty = bars + 45;        // [ITEM_RING] every consumer has read it
-  int* item_ring = reinterpret_cast<int*>(bars + 49);   // [ITEM_RING]; 51 x 8 B < 512 B
+  int* item_ring = reinterpret_cast<int*>(bars + 49);   // [ITEM_RING]
+  // ordered walk (main pass with sorted visit lists): the key tile a stage / an accumulator holds
+  // (-1: the item's walk ends there), and per epilogue warp the largest radius R of its rows,
+  // tagged with the work item (item << 32 | float bits); bytes 408..512 of the 512-byte block
+  int* stage_meta = item_ring + ITEM_RING;                  // [stages <= 8]
+  int* acc_meta = stage_meta + 8;                           // [2]
+  unsigned long long* rq_pub = reinterpret_cast<unsigned long long*>(bars + 56);   // [NEPI]
   float* pub = reinterpret_cast<float*>(smem + sp.pub_off);
 
   const int warp = warp_id(), lane = lane_id();
@@ -503,12 +516,17 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   const size_t b_bytes = size_t(brows) * 128;           // one K atom of this CTA's key rows
   const uint32_t tmem_cols = uint32_t(2 * P.bn);
   const int n_items = P.n_items_dev ? *P.n_items_dev : P.n_items;
+  // the producer drives the walk from the sorted list and ends it early (single CTAs only)
+  const bool ordered = !PAIR && !P.near_only && P.qmap == nullptr && P.vlist != nullptr &&
+                       *P.vok != 0;
 
   if (threadIdx.x == 0) {
+    for (int i = 0; i < NEPI; ++i) rq_pub[i] = ~0ull;       // no item yet
     for (int i = 0; i < 2; ++i) {
       mbar_init(&a_full[i], 1);
       mbar_init(&a_empty[i], 1);
-      mbar_init(&acc_full[i], 1);
+      // ordered: the MMA commit and the MMA thread's own arrive (after it wrote acc_meta)
+      mbar_init(&acc_full[i], ordered ? 2 : 1);
       mbar_init(&acc_empty[i], PAIR ? 2 * NEPI : NEPI);
       mbar_init(&a_peer[i], 1);
     }
@@ -612,7 +630,23 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         int stage = 0, abuf = 0;
         uint32_t sphase = 0, aphase = 0;
         bool ok = true;
-        long long c_wait = 0;
+        long long c_wait = 0, n_far = 0, n_stop = 0;
+        // ordered walk: the largest radius over the item's rows, from the epilogue warps' latest
+        // figures for this item (+inf while a warp has none yet); a warp quarter's two column
+        // groups both bound its rows' final thresholds, so the smaller of the two counts
+        auto radius_bound = [&](int it) -> double {
+          float rmax = -F_INF;
+          for (int q = 0; q < 4; ++q) {
+            float r = F_INF;
+            for (int hh = 0; hh < NH; ++hh) {
+              const unsigned long long v =
+                  *reinterpret_cast<volatile unsigned long long*>(&rq_pub[hh * 4 + q]);
+              if (int(uint32_t(v >> 32)) == it) r = fminf(r, __uint_as_float(uint32_t(v)));
+            }
+            rmax = fmaxf(rmax, r);
+          }
+          return double(rmax) * (1.0 + 1e-9);
+        };
         for (;;) {
           int it;
           if (!claim(it)) { ok = false; break; }
@@ -627,21 +661,52 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
           KeyTileWalk walk;
           walk_init(walk, w, it);
-          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+          // ordered: the near tiles, then the sorted far tiles until one is provably beyond every
+          // row's current radius (then so are all later ones)
+          int64_t vo = 0, vn = 0;
+          int jn = 0;
+          if (ordered) { vo = P.voff[it]; vn = P.voff[it + 1] - vo; }
+          auto next_tile = [&]() -> int {
+            if (!ordered) return walk.next();
+            if (jn < walk.np) return key_tile_at(jn++, walk.diag, walk.nkt);
+            const int64_t jf = jn - walk.np;
+            if (jf >= vn) return -1;
+            const unsigned long long e = P.vlist[vo + jf];
+            const float need = __uint_as_float(uint32_t(e >> 32));
+            if (need > 0.f && double(need) > radius_bound(it)) { ++n_stop; return -1; }
+            ++jn;
+            ++n_far;
+            return int(uint32_t(e));
+          };
+          for (int kt = next_tile(); kt >= 0 && ok; kt = next_tile()) {
             for (int kb = 0; kb < P.kb; ++kb) {           // one pipeline stage per K atom
               const long long tw = P.prof ? clock64() : 0;
               ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
               if (P.prof) c_wait += clock64() - tw;
               if (!ok) break;
+              if (ordered && kb == 0) *reinterpret_cast<volatile int*>(&stage_meta[stage]) = kt;
               mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
               tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
                           w.key0 + kt * P.bn + int(rank) * brows);
               if (++stage == P.stages) { stage = 0; sphase ^= 1; }
             }
           }
+          if (ok && ordered) {
+            // the end of the item's walk: a stage that carries no keys, tile -1
+            ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
+            if (ok) {
+              *reinterpret_cast<volatile int*>(&stage_meta[stage]) = -1;
+              mbar_arrive(&b_full[stage]);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+            }
+          }
           if (!ok) break;
         }
-        if (P.prof) atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
+        if (P.prof) {
+          atomicAdd(&g_tc_prof[P.prof_slot][0], (unsigned long long)c_wait);
+          atomicAdd(&g_tc_prof[P.prof_slot][13], (unsigned long long)n_far);
+          atomicAdd(&g_tc_prof[P.prof_slot][14], (unsigned long long)n_stop);
+        }
         // drain: every load this thread armed completes on its own; wait for them (bounded)
         for (int s = 0; s < P.stages; ++s) {
           // stages armed in the current lap have parity sphase for indices < stage
@@ -694,21 +759,42 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           if (!ok) break;
           const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
           KeyTileWalk walk;
-          walk_init(walk, w, it);
-          for (int kt = walk.next(); kt >= 0 && ok; kt = walk.next()) {
+          if (!ordered) walk_init(walk, w, it);
+          for (;;) {
+            int kt_meta = 0;
+            if (!ordered) {
+              if (walk.next() < 0) break;
+            } else {
+              // ordered: the next stage names the tile, or ends the item (a stage without keys)
+              const long long t1 = P.prof ? clock64() : 0;
+              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+              if (P.prof) c_b += clock64() - t1;
+              if (!ok) break;
+              const int kt = *reinterpret_cast<volatile int*>(&stage_meta[stage]);
+              if (kt < 0) {
+                mbar_arrive(&b_empty[stage]);
+                if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+                break;
+              }
+              kt_meta = kt;
+            }
             const long long t2 = P.prof ? clock64() : 0;
             ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
                       : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
             if (P.prof) c_acc += clock64() - t2;
             if (!ok) break;
+            // the epilogue read this accumulator's previous tile before it released it
+            if (ordered) *reinterpret_cast<volatile int*>(&acc_meta[acc]) = kt_meta;
             tc_fence_after();
             const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
             for (int kb = 0; kb < P.kb; ++kb) {
-              const long long t1 = P.prof ? clock64() : 0;
-              ok = mbar_wait(&b_full[stage], sphase, abort_flag);
-              if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
-              if (P.prof) c_b += clock64() - t1;
-              if (!ok) break;
+              if (!(ordered && kb == 0)) {                 // ordered: the first stage is waited for
+                const long long t1 = P.prof ? clock64() : 0;
+                ok = mbar_wait(&b_full[stage], sphase, abort_flag);
+                if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
+                if (P.prof) c_b += clock64() - t1;
+                if (!ok) break;
+              }
               const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
               const int ks1 = min(P.ksteps, 4 * kb + 4);
               for (int ks = 4 * kb; ks < ks1; ++ks) {
@@ -722,9 +808,19 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (!ok) break;
             issued = true;
             umma_commit_g<PAIR>(&acc_full[acc]);
+            if (ordered) mbar_arrive(&acc_full[acc]);     // releases acc_meta to the epilogue
             if (++acc == 2) { acc = 0; accphase ^= 1; }
           }
           if (!ok) break;
+          if (ordered) {
+            // the end of the item for the epilogue: an accumulator turn without a tile
+            ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+            if (!ok) break;
+            *reinterpret_cast<volatile int*>(&acc_meta[acc]) = -1;
+            mbar_arrive(&acc_full[acc]);
+            mbar_arrive(&acc_full[acc]);
+            if (++acc == 2) { acc = 0; accphase ^= 1; }
+          }
           umma_commit_g<PAIR>(&a_empty[abuf]);
           if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
         }
@@ -792,12 +888,28 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       }
       const int limit = w.key0 + w.nkeys;
       KeyTileWalk walk;
-      walk_init(walk, w, it);
-      for (int kt = walk.next(); kt >= 0; kt = walk.next()) {
+      if (!ordered) walk_init(walk, w, it);
+      // ordered: R = threshold + roff of this row, published per warp after every tile
+      const double roff_row = (ordered && row < nq) ? P.roff[qrow + row] : 0.0;
+      for (;;) {
+        int kt = 0;
+        if (!ordered) {
+          kt = walk.next();
+          if (kt < 0) break;
+        }
         const long long te = P.prof ? clock64() : 0;
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
         if (P.prof) c_ew += clock64() - te;
         if (!ok) break;
+        if (ordered) {
+          kt = *reinterpret_cast<volatile int*>(&acc_meta[acc]);
+          if (kt < 0) {                    // the item's walk ended: hand the turn back
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[acc]);
+            if (++acc == 2) { acc = 0; accphase ^= 1; }
+            break;
+          }
+        }
         tc_fence_after();
         sel.refresh();
         const uint32_t t0 =
@@ -874,6 +986,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           }
         }
         if (++acc == 2) { acc = 0; accphase ^= 1; }
+        if (ordered) {
+          // an upper bound on R over this warp's rows: thr_f (the filter threshold) bounds the
+          // row's final k'-th value, roff is the fixed part; rows past the tile's end do not count
+          float rr = -F_INF;
+          if (row < nq) rr = __double2float_ru(double(sel.thr_f) + roff_row);
+          for (int o = 16; o > 0; o >>= 1) rr = fmaxf(rr, __shfl_xor_sync(FULL, rr, o));
+          if (lane == 0)
+            *reinterpret_cast<volatile unsigned long long*>(&rq_pub[warp - EPI_WARP0]) =
+                (static_cast<unsigned long long>(uint32_t(it)) << 32) | __float_as_uint(rr);
+        }
       }
       if (!ok) break;
       const int wrow0 = q * 32;
@@ -1137,7 +1259,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   const int32_t* n_items_dev, int32_t* counter, Ctl* ctl, int kprime,
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask, int mask_words, bool near_only, bool reverse,
-                  const float* seed, const NearInit* init, const RefineSplit* split) {
+                  const float* seed, const NearInit* init, const RefineSplit* split,
+                  const VisitOrder* order) {
   const int prof_slot = near_only ? 0 : (qmap ? 2 : 1);
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
@@ -1179,6 +1302,11 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.init_idx = load ? init->idx : nullptr;
   P.iperm = load ? init->iperm : nullptr;
   P.excl = load ? init->excl : nullptr;
+  const bool ord = order && order->list && !near_only && !qmap && !cfg.pair;
+  P.vlist = ord ? order->list : nullptr;
+  P.voff = ord ? order->off : nullptr;
+  P.roff = ord ? order->roff : nullptr;
+  P.vok = ord ? order->ok : nullptr;
   if (cfg.pair && (mask || near_only)) {
     set_error("pruned scans run on single CTAs only");
     return MSC_ERR_INVALID_ARG;

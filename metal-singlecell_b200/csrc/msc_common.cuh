@@ -120,7 +120,8 @@ struct Ctl {
   int32_t tc_counter[3];    // item counters of the tensor-core launches (main, refine, near)
   int32_t refine_split;     // work items per refine item (key ranges), 1 = not split
   int32_t n_items_refine_eff;   // n_items_refine × refine_split
-  int32_t pad2[3];
+  int32_t ordered_ok;           // 1: every work item's sorted visit list fits (prune.cu)
+  int32_t pad2[2];
 };
 
 // ------------------------------------------------------------------------------------------------

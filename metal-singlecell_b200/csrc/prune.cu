@@ -573,6 +573,139 @@ __global__ void refine_merge_kernel(const WorkItem* __restrict__ items3,
   }
 }
 
+// ---- sorted visit lists of the main scan ----
+
+// |z|² + 3·eps of every packed row of the final layout: the part of the row's radius
+// R = threshold + roff that stays fixed while the scan lowers the threshold (as R is formed from
+// the near pass's threshold in row_radius_kernel)
+__global__ void row_offset_kernel(const int32_t* __restrict__ perm, int64_t npacked,
+                                  const QStat* __restrict__ qs, const KeyMax* __restrict__ km,
+                                  int prec, int kmma, int d, double* __restrict__ roff) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    if (perm[p] < 0) { roff[p] = 0.0; continue; }
+    const QStat q = qs[p];
+    roff[p] = q.sq + 3.0 * cert_eps(q, *km, prec, kmma, d);
+  }
+}
+
+// kept far tiles per work item (warp per item)
+__global__ void visit_count_kernel(const uint32_t* __restrict__ mask, int64_t n_items, int words,
+                                   int32_t* __restrict__ cnt) {
+  const int lane = lane_id();
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t it = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; it < n_items;
+       it += warps) {
+    int c = 0;
+    for (int wi = lane; wi < words; wi += 32) c += __popc(mask[it * words + wi]);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL, c, o);
+    if (lane == 0) cnt[it] = c;
+  }
+}
+
+constexpr int VO_T = 256;            // threads per block of the order kernel
+constexpr int VO_SORT_MAX = 8192;    // longest list sorted (longer ones keep tile order)
+
+// One block per work item: its kept far tiles (the set bits of its mask), each with the bound
+// need = f²·L², L = |c_Q − c_K|·sqrt(1 − e) − r_Q − r_K (the 128-row query tile's ball and the
+// 256-row key ball, the float distance lowered by its rounding bound e as in separated()), rounded
+// down, 0 when L <= 0; sorted ascending (ties by tile).  need <= f²·|x − y|² for every row x of
+// the tile and key y of the key tile (both in unscaled coordinates; f = the operand scale).
+__global__ void __launch_bounds__(VO_T)
+visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
+                   const Ctl* __restrict__ ctl, int prec, const float* __restrict__ qc,
+                   const float* __restrict__ qr, const float* __restrict__ kc,
+                   const float* __restrict__ kr, const uint32_t* __restrict__ mask, int words,
+                   const int64_t* __restrict__ voff, int64_t cap,
+                   unsigned long long* __restrict__ vlist, int32_t* __restrict__ ok_flag) {
+  extern __shared__ unsigned long long vo_keys[];                 // [VO_SORT_MAX]
+  float* qcen = reinterpret_cast<float*>(vo_keys + VO_SORT_MAX);   // [dp]
+  int32_t* wpre = reinterpret_cast<int32_t*>(qcen + dp);           // [words + 1]
+  const bool fits = voff[n_items] <= cap;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ok_flag = fits ? 1 : 0;
+  if (!fits) return;
+  const double f = op_scale(prec, ctl);
+  const double f2 = f * f;
+  const double e = double(d + 8) * 0x1p-23;
+  const int n4 = dp / 4;
+  for (int64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const WorkItem w = items[it];
+    const int64_t o = voff[it];
+    const int c = int(voff[it + 1] - o);
+    if (c == 0) continue;                                         // block-uniform
+    const int64_t qt = w.qrow0 / QTILE;
+    __syncthreads();
+    for (int t = threadIdx.x; t < dp; t += VO_T) qcen[t] = qc[qt * dp + t];
+    // exclusive prefix of the words' bit counts (one thread; words is small)
+    if (threadIdx.x == 0) {
+      int a = 0;
+      for (int wi = 0; wi < words; ++wi) { wpre[wi] = a; a += __popc(mask[it * words + wi]); }
+      wpre[words] = a;
+    }
+    __syncthreads();
+    const float rq = qr[qt];
+    const bool sorted = c <= VO_SORT_MAX;
+    for (int wi = threadIdx.x; wi < words; wi += VO_T) {
+      uint32_t bits = mask[it * words + wi];
+      int pos = wpre[wi];
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1u;
+        const int kt = wi * 32 + b;
+        float need = -F_INF;
+        if (sorted) {
+          const int64_t g = (int64_t(w.key0) + int64_t(kt) * bn) / 256;
+          const float rk = kr[g];
+          if (rq < 0.f || rk < 0.f) {
+            need = F_INF;
+          } else {
+            const float4* a4 = reinterpret_cast<const float4*>(qcen);
+            const float4* b4 = reinterpret_cast<const float4*>(kc + g * dp);
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+            for (int t = 0; t < n4; ++t) {
+              const float4 x = a4[t], y = b4[t];
+              const float e0 = x.x - y.x, e1 = x.y - y.y, e2 = x.z - y.z, e3 = x.w - y.w;
+              s0 = fmaf(e0, e0, s0);
+              s1 = fmaf(e1, e1, s1);
+              s2 = fmaf(e2, e2, s2);
+              s3 = fmaf(e3, e3, s3);
+            }
+            const double lo = double((s0 + s1) + (s2 + s3)) * (1.0 - e);
+            const double L = sqrt(lo) - double(rq) - double(rk);
+            need = L > 0.0 ? __double2float_rd(f2 * L * L * (1.0 - 1e-12)) : 0.f;
+          }
+        }
+        const unsigned long long key =
+            (static_cast<unsigned long long>(__float_as_uint(need)) << 32) | uint32_t(kt);
+        if (sorted) vo_keys[pos] = key;
+        else vlist[o + pos] = key;
+        ++pos;
+      }
+    }
+    if (!sorted) continue;                                        // block-uniform
+    int P2 = 1;
+    while (P2 < c) P2 <<= 1;
+    __syncthreads();
+    for (int t = c + threadIdx.x; t < P2; t += VO_T) vo_keys[t] = ~0ull;
+    __syncthreads();
+    // need >= 0 here, so the float bits order as the values do
+    for (int kk = 2; kk <= P2; kk <<= 1) {
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        for (int t = threadIdx.x; t < P2; t += VO_T) {
+          const int u = t ^ jj;
+          if (u > t) {
+            const unsigned long long a = vo_keys[t], b = vo_keys[u];
+            const bool up = (t & kk) == 0;
+            if ((a > b) == up) { vo_keys[t] = b; vo_keys[u] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int t = threadIdx.x; t < c; t += VO_T) vlist[o + t] = vo_keys[t];
+  }
+}
+
 int grid_for(int64_t n) {
   return int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, PR_T), int64_t(num_sms()) * 8)));
 }
@@ -614,6 +747,15 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.part = c.take<int2>(size_t(prow) * kprime);
   w.part_thr = c.take<float>(prow);
   w.seed = c.take<float>(npacked);
+  w.roff = c.take<double>(npacked);
+  w.vcnt = c.take<int32_t>(n_items);
+  w.voff = c.take<int64_t>(n_items + 1);
+  w.vscan = c.take<int64_t>(scan_i32_scratch_elems(n_items));
+  // kept far tiles of all work items: at most every key tile of every work item; beyond a
+  // quarter of that (pruning keeps a few percent on large samples) the mask walk takes over
+  const int64_t all = n_items * int64_t(words) * 32;
+  w.vcap = std::min<int64_t>(all, std::max<int64_t>(int64_t(16) << 20, all / 4));
+  w.vlist = c.take<unsigned long long>(w.vcap);
   return w;
 }
 
@@ -683,6 +825,35 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
                                                     w.mask, profiling_enabled() ? 1 : 0,
                                                     max_pairs);
   MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_visit_order(const WorkItem* items, int64_t n_items, int bn, int d, int64_t npacked,
+                       const int32_t* perm, const Ctl* ctl, Ctl* ctl_w, int prec, int kmma,
+                       const QStat* qs, const KeyMax* km, const PruneWs& w, int words,
+                       cudaStream_t st, bool* built) {
+  *built = false;
+  const char* env = std::getenv("MSC_B200_ORDERED");
+  if (env && *env == '0') return MSC_OK;
+  const int dp = int(round_up(d, 4));
+  const size_t smem = size_t(VO_SORT_MAX) * 8 + size_t(dp) * 4 + size_t(words + 1) * 4;
+  if (bn != 256 || d > 128 || smem > size_t(200) * 1024) return MSC_OK;
+  row_offset_kernel<<<grid_for(npacked), PR_T, 0, st>>>(perm, npacked, qs, km, prec, kmma, d,
+                                                        w.roff);
+  MSC_LAUNCH_CHECK();
+  const int cgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, 8),
+                                                              int64_t(num_sms()) * 8)));
+  visit_count_kernel<<<cgrid, PR_T, 0, st>>>(w.mask, n_items, words, w.vcnt);
+  MSC_LAUNCH_CHECK();
+  MSC_TRY(scan_excl_i32(w.vcnt, n_items, w.voff, w.vscan, st));
+  MSC_CUDA_TRY(cudaFuncSetAttribute(visit_order_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int ogrid = int(std::max<int64_t>(1, std::min<int64_t>(n_items, int64_t(num_sms()) * 4)));
+  visit_order_kernel<<<ogrid, VO_T, smem, st>>>(items, n_items, bn, d, dp, ctl, prec, w.qc, w.qr,
+                                                w.kc, w.kr, w.mask, words, w.voff, w.vcap,
+                                                w.vlist, &ctl_w->ordered_ok);
+  MSC_LAUNCH_CHECK();
+  *built = true;
   return MSC_OK;
 }
 
