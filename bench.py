@@ -43,6 +43,17 @@ for p in (ROOT, ROOT / "metal-singlecell_b200"):
 import numpy as np
 
 METRIC = "kNN-graph cells/s at 1.3M×50 k=15, BF16+rerank vs FP32 GPU; serve p50/p99 ms"
+FORM_STEPS = 3            # graphs timed for each comparison form
+# DRAM bytes (read + written) of one main-scan launch of the candidate kernel, from a one-pass
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of this bench's own command; a
+# profiler cannot run inside the timed bench, so the figure is carried here with its source
+MAIN_SCAN_TRAFFIC = {
+    "scale:fp16": (11_273_000_000,
+                   "copied from a one-pass ncu capture of knn_tc_kernel's main-scan launch at "
+                   "1.3M cells: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,"
+                   "gpu__time_duration.sum --clock-control none -k regex:knn_tc -s 1 -c 1 "
+                   "python bench.py --steps 1 --warmup 3 --skip-cpu --skip-fp32"),
+}
 
 
 def workload(name: str, n: int | None = None):
@@ -193,6 +204,173 @@ def cpu_baseline(X, k, metric, budget_s: float = 15.0):
                       f"{n} cells + rho/sigma + memberships), {t_total:.1f} s on {cores} threads"}
 
 
+def error_vs_fp64(X, idx, dist, k, metric, n_rows: int = 512, seed: int = 20261204):
+    """Distance error of the returned float32 distances against the FP64 oracle on a seeded
+    sample of rows, and whether those rows' neighbour lists equal the oracle's exactly."""
+    import oracle
+    n = X.shape[0]
+    rows = np.sort(np.random.default_rng(seed).choice(n, min(n_rows, n), replace=False))
+    ridx, rd2, _ = oracle.knn_exact(X, k, metric=metric, rows=rows,
+                                    threads=len(os.sched_getaffinity(0)))
+    exact = rd2 * 0.5 if metric == "cosine" else np.sqrt(rd2)
+    got = np.asarray(dist[rows], np.float64)
+    nz = exact > 0
+    rel = np.abs(got[nz] - exact[nz]) / exact[nz]
+    same = (np.asarray(idx[rows]) == ridx).all(axis=1)
+    return {"rows": int(rows.size), "rows_identical_to_oracle": int(same.sum()),
+            "max_rel_error": float(rel.max()) if rel.size else 0.0,
+            "mean_rel_error": float(rel.mean()) if rel.size else 0.0,
+            "bound": 2.0 ** -24,
+            "note": "float32 distance vs FP64 sqrt of the FP64 squared distance (cosine: d2/2); "
+                    "target 1e-5 relative"}
+
+
+def events_ms(torch, fn, reps: int, warm: int = 1) -> float:
+    """Mean device time of ``fn`` over ``reps`` calls, CUDA events on the current stream."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def config_leg(name: str, uuid, steps: int = 5):
+    """One configuration of the workload list at its stated size: the default form, the
+    three-term BF16 form and the plain FP32 form of the same exact graph, each timed over
+    ``steps`` graphs with its own clock record, the forms' kNN lists compared with each other,
+    and the distance error against the FP64 oracle on sampled rows."""
+    import torch
+    from msc_b200 import neighbors as nbm, _lib
+    X, p, desc = workload(name)
+    n = X.shape[0]
+    k, metric, method = p["n_neighbors"], p["metric"], p.get("method", "umap")
+    kprime = p.get("kprime", 0)
+    Xd = torch.from_numpy(X).cuda()
+    out = {"workload": desc, "n_neighbors": k, "metric": metric, "method": method,
+           "kprime": int(kprime) or "auto", "forms": {}}
+    lists = {}
+    for prec in ("fp16", "bf16x3", "fp32"):
+        ws, buf = nbm.Workspace(Xd.device), {}
+
+        def step():
+            return nbm.neighbors_device(Xd, k, metric=metric, method=method, precision=prec,
+                                        kprime=kprime, workspace=ws, out=buf)
+        res = step()
+        torch.cuda.synchronize()
+        _lib.check_stats(res["stats"].cpu().numpy())
+        with ClockSampler(uuid) as clk:
+            ms = events_ms(torch, step, steps, warm=1)
+        lists[prec] = (res["knn_idx"].clone(), res["knn_dist"].clone())
+        out["forms"][prec] = {"ms_per_graph": ms, "cells_per_s": n / (ms / 1000.0),
+                              "steps": steps, "clocks": clk.summary()}
+    ref_i, ref_d = lists["fp32"]
+    out["forms_identical"] = all(bool(torch.equal(i, ref_i) and torch.equal(d, ref_d))
+                                 for i, d in lists.values())
+    out["speedup_fp16_over_fp32"] = out["forms"]["fp32"]["ms_per_graph"] / \
+        out["forms"]["fp16"]["ms_per_graph"]
+    out["speedup_bf16x3_over_fp32"] = out["forms"]["fp32"]["ms_per_graph"] / \
+        out["forms"]["bf16x3"]["ms_per_graph"]
+    idx, dist = (t.cpu().numpy() for t in lists["fp16"])
+    out["error_vs_fp64"] = error_vs_fp64(X, idx, dist, k, metric)
+    del Xd, lists
+    torch.cuda.empty_cache()
+    return out
+
+
+def batch_leg(uuid, n_samples: int = 64, steps: int = 5):
+    """The batching configuration, reduced to ``n_samples`` samples: one persistent launch under
+    a captured CUDA graph with autotuned tiles against the per-sample launch loop."""
+    import torch
+    from msc_b200 import batch, synth, _lib
+    X, offsets, p = synth.batch_samples(n_samples, seed=3, d=30)
+    n, d = X.shape
+    k = p["n_neighbors"]
+    Xd = torch.from_numpy(X).cuda()
+    loop_out = batch.per_sample_loop(Xd, offsets, k)
+    tune = batch.autotune(Xd, offsets, k, reps=1, use_cache=False)
+    bt = batch.BatchedKnn(offsets, d, k, tile_config=tune["tile_config"])
+    bt.capture(Xd)
+    with ClockSampler(uuid) as clk:
+        loop_ms = events_ms(torch, lambda: batch.per_sample_loop(Xd, offsets, k, out=loop_out),
+                            steps)
+        graph_ms = events_ms(torch, bt.replay, steps)
+    stats = bt.check()
+    sizes = np.diff(offsets)
+    same = bool(torch.equal(bt.idx, loop_out[0]) and torch.equal(bt.dist, loop_out[1]))
+    out = {"workload": f"{len(sizes)} samples, {n:,} cells (min {int(sizes.min())}, max "
+                       f"{int(sizes.max())}), 30 PCs, k=15, euclidean (the 256-sample "
+                       f"configuration's first {n_samples} samples)",
+           "graph_ms": graph_ms, "cells_per_s": n / (graph_ms / 1000.0),
+           "per_sample_loop_ms": loop_ms, "speedup_vs_loop": loop_ms / graph_ms,
+           "identical_to_loop": same, "tile": batch.decode_tile_code(tune["tile_config"]),
+           "certified": int(stats[_lib.STAT_CERTIFIED]),
+           "rescanned": int(stats[_lib.STAT_RESCANNED]), "steps": steps,
+           "clocks": clk.summary()}
+    del Xd, bt, loop_out
+    torch.cuda.empty_cache()
+    return out
+
+
+def serve_leg(uuid, args, load_fracs=(0.5, 0.7, 0.85), pool_size: int = 64):
+    """The serving configuration: Poisson arrivals of ``args.serve_requests`` graph requests per
+    load point (1k-500k cells, 30/50/100 PCs, k in {10, 15, 30}, euclidean / cosine), admitted by
+    HBM budget into concurrent slots; p50 / p99 latency (arrival to the result complete in HBM
+    and handed to the caller) and cells/s at arrival rates set to fractions of the batched-offline
+    throughput of the same requests.  The requests cycle through ``pool_size`` distinct seeded
+    embeddings (host memory), each request uploading its own."""
+    import torch
+    from msc_b200 import serve, synth
+    spec = synth.serving_requests(1.0, args.serve_requests, seed=5)
+    pool = [synth.request_embedding(r) for r in spec[:pool_size]]
+    reqs_spec = [spec[i % pool_size] for i in range(len(spec))]
+    data = [pool[i % pool_size] for i in range(len(spec))]
+    total_cells = sum(x.shape[0] for x in data)
+    budget = int(args.hbm_budget_gb * (1 << 30))
+
+    def fresh():
+        return [serve.Request(X=x, n_neighbors=r["k"], metric=r["metric"])
+                for x, r in zip(data, reqs_spec)]
+
+    serve.run_offline(fresh()[:16], budget, args.slots)            # warm-up
+    with ClockSampler(uuid) as clk:
+        off = serve.run_offline(fresh(), budget, args.slots)
+    off["clocks"] = clk.summary()
+    mean_cells = total_cells / len(data)
+    sweep = []
+    for frac in load_fracs:
+        rate = frac * off["cells_per_s"] / mean_cells
+        rng = np.random.default_rng(7)
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(data))).tolist()
+        with ClockSampler(uuid) as clk:
+            rep = serve.run_trace(fresh(), arr, budget, args.slots)
+        rep.update({"load_frac_of_offline": frac, "rate_req_per_s": rate,
+                    "throughput_frac_of_offline": rep["cells_per_s"] / off["cells_per_s"],
+                    "clocks": clk.summary()})
+        sweep.append(rep)
+    kept_up = [r for r in sweep if r["failed"] == 0 and
+               r["throughput_frac_of_offline"] >= 0.95 * r["load_frac_of_offline"]]
+    best = max(kept_up, key=lambda r: r["load_frac_of_offline"], default=None)
+    sizes = np.array([x.shape[0] for x in pool])
+    return {"requests_per_point": len(data), "distinct_embeddings": pool_size,
+            "cells_total_per_point": int(total_cells),
+            "pool_cells": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                           "max": int(sizes.max())},
+            "slots": args.slots, "hbm_budget_gb": args.hbm_budget_gb,
+            "distribution": "cells LogNormal(ln 20000, 1) clipped 1k-500k; PCs {30,50,100}; "
+                            "k {10,15,30}; metric {euclidean, cosine}",
+            "latency": "arrival -> result complete on the device and handed to the caller",
+            "offline": off, "sweep": sweep,
+            "sustained": None if best is None else {
+                "throughput_frac_of_offline": best["throughput_frac_of_offline"],
+                "load_frac_of_offline": best["load_frac_of_offline"],
+                "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"]}}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -300,7 +478,8 @@ def run_ours(args):
                 "hot_chunks_per_warp": c[6] / ctas / nepi,
                 "insertions_per_row": c[8] / max(n, 1), "ctas": c[9], "epilogue_warps": nepi,
                 "insert_rounds_per_warp": c[11] / ctas / nepi,
-                "hot_path_cycles_per_warp": c[12] / ctas / nepi}
+                "hot_path_cycles_per_warp": c[12] / ctas / nepi,
+                "far_tiles_scanned": c[13], "walks_ended_early": c[14]}
     pipeline = {"near_pass": pipe(16), "main": pipe(32), "refine": pipe(48)}
     # key tiles beyond the near ones: kept by the pruning plan / all of them
     pruning = {"far_tiles_visited": int(cnt[10]), "far_tiles_total": int(cnt[11]),
@@ -312,30 +491,30 @@ def run_ours(args):
     cand_ms = stages.get("candidates")
     # Work of the main candidate launch: the (128-row query tile, 256-key tile) pairs it computes
     # -- every query tile's near tiles (its own key tile and two either side) plus the far tiles
-    # the pruning plan kept -- each 2·d·128·256 FLOP (d unpadded).  Without pruning every pair of
-    # the n×n matrix is computed.
+    # it scanned: those the pruning plan kept, minus those an ordered walk left after ending
+    # early -- each 2·d·128·256 FLOP (d unpadded).  Without pruning every pair of the n×n matrix
+    # is computed.
     dense_flop = 2.0 * d * float(n) * float(n)
     if cnt[11]:
         nkt = -(-n // 256)
         q = np.arange(-(-n // 128))
         diag = (128 * q) // 256
         near_tiles = int((np.minimum(nkt - 1, diag + 2) - np.maximum(0, diag - 2) + 1).sum())
-        tile_pairs = near_tiles + int(cnt[10])
+        # far tiles the main scan computed: the ordered walk counts its own (it ends walks
+        # early), else every tile the plan kept
+        ordered = cnt[32 + 13] + cnt[32 + 14] > 0
+        tile_pairs = near_tiles + int(cnt[32 + 13] if ordered else cnt[10])
         alg_flop = min(dense_flop, 2.0 * d * 128.0 * 256.0 * tile_pairs)
     else:
         tile_pairs = None
         alg_flop = dense_flop
     achieved = alg_flop / (cand_ms / 1000.0) / 1e12 if cand_ms else None
     peak = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops")
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get(f"{args.workload}:{args.precision}")
-        except Exception:
-            traffic = None
+    traffic, traffic_src = MAIN_SCAN_TRAFFIC.get(f"{args.workload}:{args.precision}",
+                                                 (None, None))
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_source": traffic_src,
                 "kernel": "knn_tc_kernel" if args.precision != "fp32" else "knn_fp32_kernel",
                 "algorithmic_flop_per_launch": alg_flop, "kernel_ms": cand_ms,
                 "tile_pairs_computed": tile_pairs,
@@ -344,68 +523,92 @@ def run_ours(args):
                 "peak_kind": f"{pk_kind} bf16 sustained (kernel timed inside a full step)",
                 "stage_ms": stages, "pipeline_cycles_per_cta": pipeline, "pruning": pruning}
 
-    # e2e through the public host call: pinned host in, both CSR matrices back to pinned host,
-    # the distances CSR copied out while the connectivities are computed (neighbors_host)
-    Xh = torch.from_numpy(X).pin_memory()
+    # e2e through the drop-in call itself (neighbors.neighbors, neighbors.py:727-760 in the
+    # reference): a host NumPy embedding in, SciPy CSR matrices out; the upload, the graph, the
+    # copies back (distances while the connectivities run) and the SciPy construction are all
+    # inside the timed region
     m = k - 1
+
+    def dropin_step():
+        dist_csr, conn_csr = nbm.neighbors(X, k, metric=metric, method=method,
+                                           precision=args.precision, kprime=kprime, device=dev)
+        return conn_csr.nnz
+
+    for _ in range(max(1, args.warmup // 2)):
+        dropin_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nnzs = [dropin_step() for _ in range(args.steps)]
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    barrier()
+    h2d = X.nbytes
+    d2h = 8 * (n + 1) * 2 + n * m * 8 + nnzs[-1] * 8 + 8 * _lib.STATS_LEN
+    e2e = {"value": reps.rate(n, e2e_s), "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_s,
+           "path": "msc_b200.neighbors.neighbors(X_pca): host NumPy in, SciPy CSR out"}
+
+    # the same through the pinned-buffer host call (neighbors_host): no pageable copies
+    Xh = torch.from_numpy(X).pin_memory()
     hstate = nbm.HostGraphState(n, d, k, device=dev)
 
-    def e2e_step():
+    def pinned_step():
         r = nbm.neighbors_host(Xh, k, metric=metric, method=method, precision=args.precision,
                                kprime=kprime, state=hstate)
         return r["conn_nnz"]
 
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
+    pinned_step()
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    nnzs = [e2e_step() for _ in range(args.steps)]
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    for _ in range(args.steps):
+        pinned_step()
+    pin_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     barrier()
-    h2d = X.nbytes
-    d2h = 8 + 2 * (n + 1) * 8 + n * m * 8 + nnzs[-1] * 8
-    e2e = {"value": reps.rate(n, e2e_s), "unit": "cells/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_s}
+    e2e_pinned = {"value": reps.rate(n, pin_s), "unit": "cells/s", "ms_per_step": 1000 * pin_s,
+                  "path": "msc_b200.neighbors.neighbors_host: pinned torch CPU tensors"}
+    del hstate, Xh
 
-    # the plain FP32 GPU form of the same graph (the comparison the metric names)
-    fp32 = None
-    if not args.skip_fp32 and args.precision != "fp32":
-        step("fp32")
-        torch.cuda.synchronize()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(st)
-        step("fp32")
-        f1.record(st)
-        torch.cuda.synchronize()
-        fms = max_over_ranks(f0.elapsed_time(f1))
-        fp32 = {"value": reps.rate(n, fms / 1000.0), "unit": "cells/s", "ms_per_step": fms,
-                "speedup_of_headline": fms / ms}
+    # the plain FP32 GPU form and the three-term BF16 form of the same exact graph, each over
+    # FORM_STEPS graphs (the FP32 form scans every key; the 16-bit forms are pruned)
+    fp32 = bf16x3 = None
+    if not args.skip_fp32:
+        forms = {}
+        for prec in ("fp32", "bf16x3"):
+            if prec == args.precision:
+                continue
+            fms = max_over_ranks(events_ms(torch, lambda: step(prec), FORM_STEPS, warm=1))
+            forms[prec] = {"value": reps.rate(n, fms / 1000.0), "unit": "cells/s",
+                           "ms_per_step": fms, "steps": FORM_STEPS}
+        fp32, bf16x3 = forms.get("fp32"), forms.get("bf16x3")
+        if fp32:
+            fp32["speedup_of_headline"] = fp32["ms_per_step"] / ms
+            fp32["pruning"] = "none: every key tile of every query tile is scanned"
+        if bf16x3:
+            bf16x3["speedup_over_fp32_form"] = (fp32["ms_per_step"] / bf16x3["ms_per_step"]) \
+                if fp32 else None
 
-    # the three-term BF16 form of the same exact graph (the metric's "BF16+rerank"; the default
-    # takes one-term FP16 candidates and refines the rows it cannot certify with this form)
-    bf16x3 = None
-    if not args.skip_fp32 and args.precision != "bf16x3":
-        try:
-            step("bf16x3")
-            torch.cuda.synchronize()
-            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            b0.record(st)
-            step("bf16x3")
-            b1.record(st)
-            torch.cuda.synchronize()
-            bms = b0.elapsed_time(b1)
-            # no collective inside this optional block (a rank that failed here would leave the
-            # others waiting): the figure is this rank's own
-            bf16x3 = {"value": n / (bms / 1000.0), "unit": "cells/s", "ms_per_step": bms,
-                      "scope": "one replica",
-                      "speedup_over_fp32_form": (fp32["ms_per_step"] / bms) if fp32 else None}
-        except Exception as e:          # an optional comparison: report it, keep the line
-            bf16x3 = {"error": f"{type(e).__name__}: {e}"}
+    err = None
+    if rank == 0 and not args.skip_cpu:
+        res = step()
+        torch.cuda.synchronize()
+        err = error_vs_fp64(X, res["knn_idx"].cpu().numpy(), res["knn_dist"].cpu().numpy(), k,
+                            metric)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         cpu = cpu_baseline(X, k, metric, budget_s=args.ref_budget)
+
+    # the other configurations of the workload list, each at its stated size with its own clock
+    # record (one GPU only: under torchrun every rank is a replica of the headline graph)
+    configs = None
+    if world == 1 and args.workload == "scale" and not args.skip_configs:
+        del Xd, ws, out
+        torch.cuda.empty_cache()
+        configs = {"plain_10k": config_leg("plain", uuid),
+                   "precision_200k": config_leg("precision", uuid),
+                   "batch_64": batch_leg(uuid, args.batch_samples),
+                   "serve": serve_leg(uuid, args)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
@@ -417,8 +620,9 @@ def run_ours(args):
                            "kprime": int(kprime) or "auto",
                            "l2": "inputs larger than L2 (embedding 260 MB + packed operands)",
                            "parallelism": f"replicas x{world}"},
-                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
-                "cpu_baseline": cpu, "fp32_form": fp32, "bf16x3_form": bf16x3,
+                "e2e": e2e, "e2e_pinned": e2e_pinned, "gpu_launches": int(launches),
+                "roofline": roofline, "cpu_baseline": cpu, "fp32_form": fp32,
+                "bf16x3_form": bf16x3, "error_vs_fp64": err, "configs": configs,
                 "stats": {"certified": int(stats[_lib.STAT_CERTIFIED]),
                           "refined": int(stats[_lib.STAT_REFINED]),
                           "rescanned": int(stats[_lib.STAT_RESCANNED]),
@@ -746,6 +950,12 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16x3", "bf16", "fp32"])
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-configs", action="store_true",
+                    help="headline graph only: no plain / precision / batching / serving legs")
+    ap.add_argument("--batch-samples", type=int, default=64,
+                    help="samples of the batching leg of the default run")
+    ap.add_argument("--serve-requests", type=int, default=1000,
+                    help="requests per load point of the serving leg of the default run")
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--n", type=int, default=None, help="cells of the scale workload (profiling)")
     ap.add_argument("--samples", type=int, default=256, help="batch workload: samples")
