@@ -580,6 +580,17 @@ def run_ours(args):
             fms = max_over_ranks(events_ms(torch, lambda: step(prec), FORM_STEPS, warm=1))
             forms[prec] = {"value": reps.rate(n, fms / 1000.0), "unit": "cells/s",
                            "ms_per_step": fms, "steps": FORM_STEPS}
+        # the FP32 form under the same locality order, near pass and pruning plan as the 16-bit
+        # forms: the gain of the 16-bit candidates alone
+        os.environ["MSC_B200_PRUNE_FP32"] = "1"
+        try:
+            fms = max_over_ranks(events_ms(torch, lambda: step("fp32"), FORM_STEPS, warm=1))
+        finally:
+            del os.environ["MSC_B200_PRUNE_FP32"]
+        forms["fp32_pruned"] = {"value": reps.rate(n, fms / 1000.0), "unit": "cells/s",
+                                "ms_per_step": fms, "steps": FORM_STEPS,
+                                "speedup_of_headline": fms / ms,
+                                "pruning": "the same plan as the headline form"}
         fp32, bf16x3 = forms.get("fp32"), forms.get("bf16x3")
         if fp32:
             fp32["speedup_of_headline"] = fp32["ms_per_step"] / ms
@@ -622,7 +633,9 @@ def run_ours(args):
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "e2e_pinned": e2e_pinned, "gpu_launches": int(launches),
                 "roofline": roofline, "cpu_baseline": cpu, "fp32_form": fp32,
-                "bf16x3_form": bf16x3, "error_vs_fp64": err, "configs": configs,
+                "bf16x3_form": bf16x3,
+                "fp32_pruned_form": forms.get("fp32_pruned") if not args.skip_fp32 else None,
+                "error_vs_fp64": err, "configs": configs,
                 "stats": {"certified": int(stats[_lib.STAT_CERTIFIED]),
                           "refined": int(stats[_lib.STAT_REFINED]),
                           "rescanned": int(stats[_lib.STAT_RESCANNED]),

@@ -244,8 +244,13 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
     P.refine = tc_config_ok(tc_default_config(PREC_BF16X3, d, P.kprime), P.L3.kp, P.kprime);
   }
   // Pruning pays once a sample spans many key tiles beyond the near ones; its mask (one bit per
-  // 256-key tile per 128-row query tile) is capped at 2 GB.  MSC_B200_PRUNE=0 turns it off.
-  if (P.candidates && k > 1 && P.prec != PREC_FP32 && P.max_seg >= PRUNE_MIN_CELLS) {
+  // 256-key tile per 128-row query tile) is capped at 2 GB.  MSC_B200_PRUNE=0 turns it off.  The
+  // plain FP32 form scans every key unless MSC_B200_PRUNE_FP32=1 (the same plan, for comparing
+  // the forms at equal pruning).
+  const char* env32 = std::getenv("MSC_B200_PRUNE_FP32");
+  const bool prune32 = env32 && *env32 == '1';
+  if (P.candidates && k > 1 && (P.prec != PREC_FP32 || prune32) &&
+      P.max_seg >= PRUNE_MIN_CELLS) {
     const char* env = std::getenv("MSC_B200_PRUNE");
     const int words = prune_mask_words(P.max_seg, PRUNE_BN);
     if (!(env && *env == '0') && double(P.ntiles) * words * 4.0 <= double(PRUNE_MASK_MAX)) {
@@ -351,10 +356,12 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   const int64_t n_items = pair_items ? P.nptiles : P.ntiles;
   MSC_TRY(launch_build_items(w.seg, P.nseg, n_items, pair_items ? 2 * QTILE : QTILE, w.items, w.ctl,
                              st));
-  // pruning needs single-CTA work items over 256-key tiles
+  // pruning needs single-CTA work items over 256-key tiles (or the FP32 SIMT kernel)
   const bool prune = P.prune && tc && !cfg.pair && cfg.bn == PRUNE_BN;
-  MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc), ORDER_LEAF,
-                       w.perm, prune ? w.pr.leaf : nullptr, w.order_ws, w.order_ws_bytes, st));
+  const bool prune32 = P.prune && P.candidates && P.k > 1 && P.prec == PREC_FP32;
+  MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc || prune32),
+                       ORDER_LEAF, w.perm, (prune || prune32) ? w.pr.leaf : nullptr, w.order_ws,
+                       w.order_ws_bytes, st));
   if (!P.candidates) {
     MSC_TRY(launch_all_rows_fail(w.perm, P.npacked, w.fail_rows, w.ctl, st));
     MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,
@@ -368,10 +375,30 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       MSC_TRY(launch_pack_fp32(Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked, w.A32,
                                w.sq32, w.qs, w.km, st));
       stage_mark(st, 1);
-      stage_mark(st, 2);
-      stage_mark(st, 3);
-      MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
-                              P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
+      if (prune32) {
+        // the same near pass -> radius -> outliers -> re-pack -> plan as the tensor-core forms
+        const FpPrune near{nullptr, 0, true, nullptr, &w.ctl->tc_counter[2]};
+        MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
+                                P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, &near));
+        stage_mark(st, 2);
+        MSC_TRY(launch_prune_partition(Xu, P.d, w.seg, P.nseg, P.npacked, w.perm, w.cand_thr,
+                                       w.qs, w.km, P.prec, P.L.kmma, PRUNE_BN, w.pr, st));
+        MSC_CUDA_TRY(cudaMemsetAsync(w.km, 0, sizeof(KeyMax), st));
+        MSC_TRY(launch_pack_fp32(Xu, w.perm, w.seg, P.nseg, w.mean, P.d, P.dpad, P.npacked,
+                                 w.A32, w.sq32, w.qs, w.km, st));
+        const int words32 = prune_mask_words(P.max_seg, PRUNE_BN);
+        MSC_TRY(launch_prune_plan(Xu, P.d, P.npacked, w.perm, w.items, P.ntiles, PRUNE_BN, w.ctl,
+                                  P.prec, w.pr, words32, st));
+        stage_mark(st, 3);
+        const FpPrune main32{w.pr.mask, words32, false, w.pr.seed, &w.ctl->tc_counter[0]};
+        MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
+                                P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, &main32));
+      } else {
+        stage_mark(st, 2);
+        stage_mark(st, 3);
+        MSC_TRY(launch_knn_fp32(w.A32, w.sq32, P.d, P.dpad, w.items, P.ntiles, w.perm, w.ctl,
+                                P.kprime, w.cand_idx, w.cand_thr, P.kprime, st));
+      }
     } else {
       if (P.prec == PREC_FP16)
         MSC_TRY(launch_maxnorm(Xu, w.seg, P.nseg, w.mean, P.d, P.npacked, w.ctl, st));

@@ -184,9 +184,20 @@ int prune_counters(unsigned long long* out);
 int prune_counters_clear();
 
 // ---- knn_fp32.cu ----
+// the FP32 SIMT form under a pruning plan: a near pass (own 256-key tile only), or a main pass
+// over the near 256-key tiles and the mask's far ones with per-row seeds; counter: the launch's
+// work-item counter (zeroed by the launcher)
+struct FpPrune {
+  const uint32_t* mask;
+  int words;
+  bool near_only;
+  const float* seed;
+  int32_t* counter;
+};
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
                     int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
-                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st);
+                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
+                    const FpPrune* prune = nullptr);
 
 // The near pass's candidates handed to the main pass: the near pass writes val (and the usual
 // candidate rows); the main pass loads them as every row's starting list and never offers the

@@ -5,6 +5,11 @@
 // so the n×n matrix never leaves shared memory.  Persistent: one block per SM takes 128-row query
 // tiles from a device work list and sweeps the tile's sample key by key tile.
 //
+// With a pruning plan (prune.cu) the same kernel runs as a near pass (every query tile against its
+// own 256-key tile) and then as a pruned main pass (the near 256-key tiles and those the plan's
+// mask keeps, each swept as four 64-key tiles), so that the FP32 form can be compared with the
+// 16-bit tensor-core forms at the same pruning.
+//
 // Reference counterpart: the fp16 Gram tile + `topk_rows` kernel of metalsinglecell
 // neighbors.py:114-119 (which materialises a block×n distance matrix in device memory).
 #include "kernels.cuh"
@@ -18,6 +23,73 @@ constexpr int F_BM = 128;     // query rows per tile
 constexpr int F_BN = 64;      // keys per tile
 constexpr int F_THREADS = 256;
 constexpr int V_STRIDE = F_BN + 4;
+
+constexpr int F_BIG = 256;    // key tiles of the pruning plan
+constexpr int F_SUB = F_BIG / F_BN;
+
+// The 64-key tiles of one work item: every tile in order (plain form), or the plan's 256-key
+// tiles — the near ones first (the query tile's own, then alternately right and left, two each
+// side), then the far ones whose mask bit is set — each split into its 64-key tiles; the near
+// pass takes the own 256-key tile only.
+struct FpWalk {
+  int nkeys, nsmall, nbig, diag, lo, hi, np, j;
+  const uint32_t* mask;
+  int words, w;
+  uint32_t cur;
+  int big, sub;
+  bool plain;
+  __device__ __forceinline__ void init(const WorkItem& item, const uint32_t* m, int nw, bool near) {
+    nkeys = item.nkeys;
+    nsmall = (nkeys + F_BN - 1) / F_BN;
+    plain = m == nullptr && !near;
+    nbig = (nkeys + F_BIG - 1) / F_BIG;
+    diag = (item.qrow0 - item.key0) / F_BIG;
+    lo = max(0, diag - 2);
+    hi = min(nbig - 1, diag + 2);
+    np = near ? 1 : hi - lo + 1;
+    j = 0;
+    mask = near ? nullptr : m;
+    words = nw;
+    w = 0;
+    cur = mask ? mask[0] : 0u;
+    big = -1;
+    sub = F_SUB;
+  }
+  __device__ __forceinline__ int near_at(int t) const {
+    const int left = diag - lo, right = hi - diag, m = min(left, right);
+    if (t == 0) return diag;
+    if (t <= 2 * m) return (t & 1) ? diag + ((t + 1) >> 1) : diag - (t >> 1);
+    return right > left ? diag + (t - m) : diag - (t - m);
+  }
+  __device__ __forceinline__ int next_big() {
+    if (j < np) return near_at(j++);
+    if (!mask) return -1;
+    for (;;) {
+      while (cur == 0u) {
+        if (++w >= words) return -1;
+        cur = mask[w];
+      }
+      const int b = __ffs(cur) - 1;
+      cur &= cur - 1u;
+      const int bt = w * 32 + b;
+      if (bt < nbig) return bt;
+    }
+  }
+  // the next 64-key tile, or -1
+  __device__ __forceinline__ int next() {
+    if (plain) return j < nsmall ? j++ : -1;
+    for (;;) {
+      if (big >= 0 && sub < F_SUB) {
+        const int kt = big * F_SUB + sub++;
+        if (kt < nsmall) return kt;
+        continue;
+      }
+      big = next_big();
+      sub = 0;
+      if (big < 0) return -1;
+    }
+  }
+};
 
 template <int KPL, int CB>
 struct FpSmem {
@@ -35,7 +107,9 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, int dpad,
                 const WorkItem* __restrict__ items, const int32_t* __restrict__ perm,
                 Ctl* __restrict__ ctl, int kprime, int32_t* __restrict__ cand_idx,
-                float* __restrict__ cand_thr, int cand_stride) {
+                float* __restrict__ cand_thr, int cand_stride, const uint32_t* __restrict__ mask,
+                int words, int near_only, const float* __restrict__ seed,
+                int32_t* __restrict__ counter, int n_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float* As = reinterpret_cast<float*>(smem_raw);
   float* Bs = As + size_t(dpad) * F_BM;
@@ -49,10 +123,8 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
   const bool selector = tid < F_BM;              // warps 0-3 own one row each
   RowSelect<KPL, CB, F_BM> sel;
   sel.bind(sel_mem, selector ? tid : 0, kprime);
-  const int n_items = ctl->n_items;
-
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(&ctl->item_counter, 1);
+    if (tid == 0) s_item = atomicAdd(counter, 1);
     __syncthreads();
     const int it = s_item;
     if (it >= n_items) break;
@@ -68,8 +140,12 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       As[(4 * tq + 2) * F_BM + r] = a.z;
       As[(4 * tq + 3) * F_BM + r] = a.w;
     }
-    if (selector) sel.reset();
-    const int nkt = (w.nkeys + F_BN - 1) / F_BN;
+    if (selector) {
+      sel.reset();
+      if (seed && tid < w.nq) sel.set_seed(seed[int64_t(w.qrow0) + tid]);
+    }
+    FpWalk walk;
+    walk.init(w, mask ? mask + int64_t(it) * words : nullptr, words, near_only != 0);
     // first key tile
     auto load_b = [&](int kt, int buf) {
       const int64_t k0 = int64_t(w.key0) + int64_t(kt) * F_BN;
@@ -84,13 +160,15 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
       }
       if ((tid & 127) < F_BN) Sq[buf * F_BN + (tid & 127)] = sq32[k0 + (tid & 127)];
     };
-    if (tid >= F_BM) load_b(0, 0);
+    int kt = walk.next();
+    if (tid >= F_BM && kt >= 0) load_b(kt, 0);
     __syncthreads();
     // neighbour ids are packed positions here; finish() maps them to original rows
     const int self_base = w.qrow0;
     const int limit = w.key0 + w.nkeys;
-    for (int kt = 0; kt < nkt; ++kt) {
-      const int buf = kt & 1;
+    for (int step = 0; kt >= 0; ++step) {
+      const int nxt = walk.next();                 // every thread walks the same sequence
+      const int buf = step & 1;
       const float* B = Bs + size_t(buf) * dpad * F_BN;
       float acc[8][4];
 #pragma unroll
@@ -131,10 +209,11 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
           }
           sel.push32(v, col0 + h, self_base + tid, limit);
         }
-      } else if (kt + 1 < nkt) {
-        load_b(kt + 1, buf ^ 1);
+      } else if (nxt >= 0) {
+        load_b(nxt, buf ^ 1);
       }
       __syncthreads();
+      kt = nxt;
     }
     if (selector) {
       const int wrow0 = tid & ~31;
@@ -152,15 +231,18 @@ knn_fp32_kernel(const float* __restrict__ A32, const float* __restrict__ sq32, i
 template <int KPL, int CB>
 int launch_fp32_t(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
                   int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime, int32_t* cand_idx,
-                  float* cand_thr, int cand_stride, cudaStream_t st) {
+                  float* cand_thr, int cand_stride, cudaStream_t st, const FpPrune& pr) {
   (void)d;
   const size_t smem = FpSmem<KPL, CB>::bytes(dpad);
   auto kern = knn_fp32_kernel<KPL, CB>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(smem)));
   int grid = int(std::min<int64_t>(n_items, num_sms()));
+  MSC_CUDA_TRY(cudaMemsetAsync(pr.counter, 0, sizeof(int32_t), st));
   kern<<<std::max(grid, 1), F_THREADS, smem, st>>>(A32, sq32, dpad, items, perm, ctl, kprime,
-                                                   cand_idx, cand_thr, cand_stride);
+                                                   cand_idx, cand_thr, cand_stride, pr.mask,
+                                                   pr.words, pr.near_only ? 1 : 0, pr.seed,
+                                                   pr.counter, int(n_items));
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
@@ -169,13 +251,17 @@ int launch_fp32_t(const float* A32, const float* sq32, int d, int dpad, const Wo
 
 int launch_knn_fp32(const float* A32, const float* sq32, int d, int dpad, const WorkItem* items,
                     int64_t n_items, const int32_t* perm, Ctl* ctl, int kprime,
-                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st) {
+                    int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
+                    const FpPrune* prune) {
+  FpPrune pr{};
+  if (prune) pr = *prune;
+  if (!pr.counter) pr.counter = &ctl->item_counter;
   if (kprime <= 32)
     return launch_fp32_t<32, 32>(A32, sq32, d, dpad, items, n_items, perm, ctl, kprime, cand_idx,
-                                 cand_thr, cand_stride, st);
+                                 cand_thr, cand_stride, st, pr);
   if (kprime <= 64)
     return launch_fp32_t<64, 32>(A32, sq32, d, dpad, items, n_items, perm, ctl, kprime, cand_idx,
-                                 cand_thr, cand_stride, st);
+                                 cand_thr, cand_stride, st, pr);
   set_error("kprime=%d > 64 is not supported by the candidate kernels", kprime);
   return MSC_ERR_UNSUPPORTED;
 }

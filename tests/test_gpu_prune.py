@@ -72,3 +72,28 @@ def test_pruned_equals_full_scan_and_oracle(n, d, c, noise, k, metric, precision
     np.testing.assert_array_equal(pd[rows], rdist, err_msg="oracle: distances")
     frac = _visited_fraction(X, k, precision, metric)
     assert frac < 0.6, f"pruning kept {frac:.2f} of the far key tiles"
+
+
+def test_fp32_form_under_the_same_plan_equals_its_full_scan():
+    # MSC_B200_PRUNE_FP32=1: the plain FP32 SIMT form runs the same near pass, outlier partition
+    # and pruning plan as the tensor-core forms (the comparison of the forms at equal pruning)
+    X = synth.gaussian_mixture(60_000, 50, 40, seed=12, sizes="lognormal", noise_frac=0.01)
+    fi, fd, fs = _knn(X, 15, "fp32", prune=False)
+    old = os.environ.get("MSC_B200_PRUNE_FP32")
+    os.environ["MSC_B200_PRUNE_FP32"] = "1"
+    try:
+        pi, pd, ps = _knn(X, 15, "fp32", prune=True)
+        frac = _visited_fraction(X, 15, "fp32")
+    finally:
+        if old is None:
+            del os.environ["MSC_B200_PRUNE_FP32"]
+        else:
+            os.environ["MSC_B200_PRUNE_FP32"] = old
+    assert int(ps[_lib.STAT_TIMEOUT]) == 0
+    np.testing.assert_array_equal(pi, fi, err_msg="pruned vs full FP32 scan: indices")
+    np.testing.assert_array_equal(pd, fd, err_msg="pruned vs full FP32 scan: distances")
+    rows = np.sort(np.random.default_rng(6).choice(X.shape[0], 1000, replace=False))
+    ridx, _, rdist = oracle.knn_exact(X, 15, rows=rows)
+    np.testing.assert_array_equal(pi[rows], ridx.astype(np.int32))
+    np.testing.assert_array_equal(pd[rows], rdist)
+    assert frac < 0.6, f"pruning kept {frac:.2f} of the far key tiles"

@@ -58,3 +58,22 @@ def test_scrublet_above_the_supported_width_is_refused():
     assert k_adj + 1 == 514
     with pytest.raises(NotImplementedError):
         nbm._knn(X, k_adj + 1)
+
+
+def test_scrublet_knn_call_at_30k_cells():
+    # a typical sample: n = 30,000 observed cells and 60,000 simulated doublets, k_adj + 1 = 262
+    n = 30_000
+    X, n_sim = scrublet_embedding(n, seed=3)
+    k_adj = k_adj_of(n, n_sim)
+    assert k_adj + 1 == 262
+    idx, dist = nbm._knn(X, k_adj + 1, random_state=0)
+    assert idx.shape == (X.shape[0], k_adj + 1)
+    assert (idx[:, 0] == np.arange(X.shape[0])).all()
+    rows = np.sort(np.random.default_rng(30).choice(X.shape[0], 1000, replace=False))
+    ridx, _, rdist = oracle.knn_exact(X, k_adj + 1, rows=rows)
+    np.testing.assert_array_equal(idx[rows], ridx.astype(np.int32))
+    np.testing.assert_array_equal(dist[rows], rdist)
+    # the doublet score of a sampled observed cell is that of the oracle's list
+    obs = rows[rows < n]
+    np.testing.assert_array_equal(scores(idx[obs], n, k_adj),
+                                  scores(ridx[: obs.size], n, k_adj))
