@@ -217,12 +217,12 @@ struct RefineSplit {
   float* part_thr;
 };
 
-// Main scan after a pruning plan: every work item's kept far key tiles sorted by a lower bound on
-// the squared operand-space distance between the query tile's rows and the key tile's keys
-// (entry = bound bits << 32 | key tile; bound = -inf: unsorted, never stops the walk).  The
-// producer walks the near tiles and then this list, and ends the item's walk at the first tile
-// whose bound exceeds every row's current radius R = threshold + roff (all later tiles are
-// farther still).
+// Main scan after a pruning plan: every work item's kept far key tiles, nearest (by ball centres)
+// first, each entry carrying a stop bound (bound bits << 32 | key tile): a lower bound on the
+// squared operand-space distance between the query tile's rows and the keys of that tile and of
+// every later tile (-inf: the list is unsorted and never ends a walk).  The producer walks the
+// near tiles and then this list, and ends the item's walk at the first entry whose bound exceeds
+// every row's current radius R = threshold + roff.
 struct VisitOrder {
   const unsigned long long* list;
   const int64_t* off;

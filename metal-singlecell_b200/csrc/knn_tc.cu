@@ -40,6 +40,17 @@ namespace msc {
 namespace {
 
 constexpr int EPI_WARP0 = 4;
+// Epilogue variants of the eight-epilogue-warp kernels, fixed at build time (-D...=0 builds the
+// other variant for comparison): the register split between warpgroup 0 and the epilogue
+// warpgroups, and three TMEM chunk buffers with two chunks per wait (else two buffers, one each)
+#ifndef MSC_TC_REGSPLIT
+#define MSC_TC_REGSPLIT 1
+#endif
+#ifndef MSC_TC_TRIBUF
+#define MSC_TC_TRIBUF 1
+#endif
+constexpr bool kRegSplit = MSC_TC_REGSPLIT != 0;
+constexpr bool kTriBuf = MSC_TC_TRIBUF != 0;
 // register split of the eight-epilogue-warp kernels (see knn_tc_kernel)
 constexpr int REG_LOW = 56, REG_HIGH = 224;
 constexpr int REG_LAUNCH = (REG_LOW * 128 + REG_HIGH * 256) / 384;     // 168
@@ -623,7 +634,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   if (warp < EPI_WARP0) {
     // warpgroup 0: one register decrease for the whole warpgroup (the split needs one
     // setmaxnreg per warpgroup), then the roles; warp 2 (TMEM owner) waits for the teardown
-    if constexpr (NEPI == 8) reg_dec();
+    if constexpr (NEPI == 8 && kRegSplit) reg_dec();
     if (warp == 0) {
       // ------------------------------------------------------------------ TMA producer (each CTA)
       if (lane == 0) {
@@ -838,7 +849,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
   } else {
     // ------------------------------------------------------------------ epilogue (each CTA)
-    if constexpr (NEPI == 8) reg_inc();
+    if constexpr (NEPI == 8 && kRegSplit) reg_inc();
     const int q = warp & 3;                        // TMEM lane quarter this warp may access
     const int h = (warp - EPI_WARP0) >> 2;         // column group
     const int row = q * 32 + lane;
@@ -926,7 +937,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             else mbar_arrive(&acc_empty[acc]);
           }
         };
-        if constexpr (NEPI == 8) {
+        if constexpr (NEPI == 8 && kTriBuf) {
           // With the register split: three chunk buffers.  tcgen05.wait::ld waits for all of a
           // thread's loads, so chunks go two per wait: a cycle starts with chunks c, c+1 loaded
           // and a free third buffer, loads c+2 (free buffer) and c+3 (c's buffer, once c is
@@ -1147,7 +1158,7 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
   auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
   MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  if (NEPI == 8) {
+  if (NEPI == 8 && kRegSplit) {
     // the register split needs the block's pool at REG_LAUNCH registers per thread
     cudaFuncAttributes fa{};
     MSC_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));

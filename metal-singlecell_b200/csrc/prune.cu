@@ -606,11 +606,14 @@ __global__ void visit_count_kernel(const uint32_t* __restrict__ mask, int64_t n_
 constexpr int VO_T = 256;            // threads per block of the order kernel
 constexpr int VO_SORT_MAX = 8192;    // longest list sorted (longer ones keep tile order)
 
-// One block per work item: its kept far tiles (the set bits of its mask), each with the bound
-// need = f²·L², L = |c_Q − c_K|·sqrt(1 − e) − r_Q − r_K (the 128-row query tile's ball and the
-// 256-row key ball, the float distance lowered by its rounding bound e as in separated()), rounded
-// down, 0 when L <= 0; sorted ascending (ties by tile).  need <= f²·|x − y|² for every row x of
-// the tile and key y of the key tile (both in unscaled coordinates; f = the operand scale).
+// One block per work item: its kept far tiles (the set bits of its mask) in order of the distance
+// between the 128-row query tile's ball centre and the 256-row key ball's centre (ties by tile):
+// nearest first, so the rows' thresholds fall early and later tiles rarely insert.  Each entry
+// carries a stop bound: the smallest need over it and every later entry, need = f²·L²,
+// L = |c_Q − c_K|·sqrt(1 − e) − r_Q − r_K (the float distance lowered by its rounding bound e as in
+// separated()), rounded down, 0 when L <= 0; need <= f²·|x − y|² for every row x of the tile and
+// key y of the key tile (unscaled coordinates, f = the operand scale), so once an entry's bound
+// exceeds every row's radius, no later tile can give a row a candidate.
 __global__ void __launch_bounds__(VO_T)
 visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
                    const Ctl* __restrict__ ctl, int prec, const float* __restrict__ qc,
@@ -618,9 +621,11 @@ visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, 
                    const float* __restrict__ kr, const uint32_t* __restrict__ mask, int words,
                    const int64_t* __restrict__ voff, int64_t cap,
                    unsigned long long* __restrict__ vlist, int32_t* __restrict__ ok_flag) {
-  extern __shared__ unsigned long long vo_keys[];                 // [VO_SORT_MAX]
-  float* qcen = reinterpret_cast<float*>(vo_keys + VO_SORT_MAX);   // [dp]
-  int32_t* wpre = reinterpret_cast<int32_t*>(qcen + dp);           // [words + 1]
+  extern __shared__ unsigned long long vo_keys[];                 // [VO_SORT_MAX] dist | pos
+  int32_t* vo_kt = reinterpret_cast<int32_t*>(vo_keys + VO_SORT_MAX);   // [VO_SORT_MAX]
+  float* vo_need = reinterpret_cast<float*>(vo_kt + VO_SORT_MAX);       // [VO_SORT_MAX]
+  float* qcen = vo_need + VO_SORT_MAX;                                  // [dp]
+  int32_t* wpre = reinterpret_cast<int32_t*>(qcen + dp);                // [words + 1]
   const bool fits = voff[n_items] <= cap;
   if (blockIdx.x == 0 && threadIdx.x == 0) *ok_flag = fits ? 1 : 0;
   if (!fits) return;
@@ -652,33 +657,38 @@ visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, 
         const int b = __ffs(bits) - 1;
         bits &= bits - 1u;
         const int kt = wi * 32 + b;
-        float need = -F_INF;
-        if (sorted) {
-          const int64_t g = (int64_t(w.key0) + int64_t(kt) * bn) / 256;
-          const float rk = kr[g];
-          if (rq < 0.f || rk < 0.f) {
-            need = F_INF;
-          } else {
-            const float4* a4 = reinterpret_cast<const float4*>(qcen);
-            const float4* b4 = reinterpret_cast<const float4*>(kc + g * dp);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-            for (int t = 0; t < n4; ++t) {
-              const float4 x = a4[t], y = b4[t];
-              const float e0 = x.x - y.x, e1 = x.y - y.y, e2 = x.z - y.z, e3 = x.w - y.w;
-              s0 = fmaf(e0, e0, s0);
-              s1 = fmaf(e1, e1, s1);
-              s2 = fmaf(e2, e2, s2);
-              s3 = fmaf(e3, e3, s3);
-            }
-            const double lo = double((s0 + s1) + (s2 + s3)) * (1.0 - e);
-            const double L = sqrt(lo) - double(rq) - double(rk);
-            need = L > 0.0 ? __double2float_rd(f2 * L * L * (1.0 - 1e-12)) : 0.f;
-          }
+        if (!sorted) {                  // tile order, no stop bound (-inf never ends a walk)
+          vlist[o + pos] = (static_cast<unsigned long long>(__float_as_uint(-F_INF)) << 32) |
+                           uint32_t(kt);
+          ++pos;
+          continue;
         }
-        const unsigned long long key =
-            (static_cast<unsigned long long>(__float_as_uint(need)) << 32) | uint32_t(kt);
-        if (sorted) vo_keys[pos] = key;
-        else vlist[o + pos] = key;
+        const int64_t g = (int64_t(w.key0) + int64_t(kt) * bn) / 256;
+        const float rk = kr[g];
+        float dist = 0.f, need = F_INF;
+        if (rq >= 0.f && rk >= 0.f) {
+          const float4* a4 = reinterpret_cast<const float4*>(qcen);
+          const float4* b4 = reinterpret_cast<const float4*>(kc + g * dp);
+          float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+          for (int t = 0; t < n4; ++t) {
+            const float4 x = a4[t], y = b4[t];
+            const float e0 = x.x - y.x, e1 = x.y - y.y, e2 = x.z - y.z, e3 = x.w - y.w;
+            s0 = fmaf(e0, e0, s0);
+            s1 = fmaf(e1, e1, s1);
+            s2 = fmaf(e2, e2, s2);
+            s3 = fmaf(e3, e3, s3);
+          }
+          const float sum = (s0 + s1) + (s2 + s3);
+          dist = sum;
+          const double L = sqrt(double(sum) * (1.0 - e)) - double(rq) - double(rk);
+          need = L > 0.0 ? __double2float_rd(f2 * L * L * (1.0 - 1e-12)) : 0.f;
+        } else {
+          dist = F_INF;                 // a ball without rows: no candidate, last
+        }
+        vo_kt[pos] = kt;
+        vo_need[pos] = need;
+        vo_keys[pos] = (static_cast<unsigned long long>(__float_as_uint(dist)) << 32) |
+                       uint32_t(pos);
         ++pos;
       }
     }
@@ -688,7 +698,7 @@ visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, 
     __syncthreads();
     for (int t = c + threadIdx.x; t < P2; t += VO_T) vo_keys[t] = ~0ull;
     __syncthreads();
-    // need >= 0 here, so the float bits order as the values do
+    // dist >= 0, so the float bits order as the values do; pos breaks ties in tile order
     for (int kk = 2; kk <= P2; kk <<= 1) {
       for (int jj = kk >> 1; jj > 0; jj >>= 1) {
         for (int t = threadIdx.x; t < P2; t += VO_T) {
@@ -702,7 +712,16 @@ visit_order_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, 
         __syncthreads();
       }
     }
-    for (int t = threadIdx.x; t < c; t += VO_T) vlist[o + t] = vo_keys[t];
+    // suffix minimum of the stop bounds along the sorted order (one thread), then the entries
+    if (threadIdx.x == 0) {
+      float m = F_INF;
+      for (int j = c - 1; j >= 0; --j) {
+        const int p = int(uint32_t(vo_keys[j]));
+        m = fminf(m, vo_need[p]);
+        vlist[o + j] = (static_cast<unsigned long long>(__float_as_uint(m)) << 32) |
+                       uint32_t(vo_kt[p]);
+      }
+    }
   }
 }
 
@@ -836,7 +855,7 @@ int launch_visit_order(const WorkItem* items, int64_t n_items, int bn, int d, in
   const char* env = std::getenv("MSC_B200_ORDERED");
   if (env && *env == '0') return MSC_OK;
   const int dp = int(round_up(d, 4));
-  const size_t smem = size_t(VO_SORT_MAX) * 8 + size_t(dp) * 4 + size_t(words + 1) * 4;
+  const size_t smem = size_t(VO_SORT_MAX) * 16 + size_t(dp) * 4 + size_t(words + 1) * 4;
   if (bn != 256 || d > 128 || smem > size_t(200) * 1024) return MSC_OK;
   row_offset_kernel<<<grid_for(npacked), PR_T, 0, st>>>(perm, npacked, qs, km, prec, kmma, d,
                                                         w.roff);

@@ -177,6 +177,11 @@ def gauss_connectivities(knn_idx: np.ndarray, knn_dist: np.ndarray, n: int) -> s
     (i→j or j→i): W_ij = sqrt(2σ_iσ_j/(σ_i²+σ_j²))·exp(-d_ij²/(σ_i²+σ_j²)), in FP64, rounded to
     float32.  The kernel is symmetric, so W is.  The reference has no ``method`` parameter
     (``pp.py:780`` always records 'umap'), so this is an addition: parity unpinned.
+
+    Two deliberate departures from scanpy's implementation: an edge to a coincident cell
+    (distance 0) is kept, where scanpy's ``eliminate_zeros()`` on the distance matrix drops it
+    (and takes that row's median over fewer entries); and the medians and the kernel are FP64,
+    rounded once, where scanpy computes in float32.
     """
     k = knn_idx.shape[1]
     D = np.asarray(knn_dist, np.float32)[:, 1:].astype(np.float64)
