@@ -40,14 +40,17 @@ namespace msc {
 namespace {
 
 constexpr int EPI_WARP0 = 4;
-// Epilogue variants of the eight-epilogue-warp kernels, fixed at build time (-D...=0 builds the
-// other variant for comparison): the register split between warpgroup 0 and the epilogue
-// warpgroups, and three TMEM chunk buffers with two chunks per wait (else two buffers, one each)
+// Epilogue variants of the eight-epilogue-warp kernels, fixed at build time: the register split
+// between warpgroup 0 and the epilogue warpgroups (setmaxnreg), and three TMEM chunk buffers with
+// two chunks per wait (else two buffers, one chunk per wait).  Both are off: measured at
+// 1.3M × 50 on one B200, the main scan took 74.0 ms with both, 81.1 ms with the three buffers
+// alone and 64.1 ms with neither (the three-buffer epilogue spills under the 168-register launch
+// budget; the split moves the spills, it does not remove them).
 #ifndef MSC_TC_REGSPLIT
-#define MSC_TC_REGSPLIT 1
+#define MSC_TC_REGSPLIT 0
 #endif
 #ifndef MSC_TC_TRIBUF
-#define MSC_TC_TRIBUF 1
+#define MSC_TC_TRIBUF 0
 #endif
 constexpr bool kRegSplit = MSC_TC_REGSPLIT != 0;
 constexpr bool kTriBuf = MSC_TC_TRIBUF != 0;

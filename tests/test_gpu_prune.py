@@ -97,3 +97,26 @@ def test_fp32_form_under_the_same_plan_equals_its_full_scan():
     np.testing.assert_array_equal(pi[rows], ridx.astype(np.int32))
     np.testing.assert_array_equal(pd[rows], rdist)
     assert frac < 0.6, f"pruning kept {frac:.2f} of the far key tiles"
+
+
+def test_ordered_walk_equals_full_scan():
+    # MSC_B200_ORDERED=1: far tiles nearest ball first, walks ended once every row's radius is
+    # passed; the lists must equal the full scan's and the oracle's
+    X = synth.gaussian_mixture(60_000, 50, 40, seed=13, sizes="lognormal", noise_frac=0.01)
+    fi, fd, _ = _knn(X, 15, "fp16", prune=False)
+    old = os.environ.get("MSC_B200_ORDERED")
+    os.environ["MSC_B200_ORDERED"] = "1"
+    try:
+        oi, od, os_ = _knn(X, 15, "fp16", prune=True)
+    finally:
+        if old is None:
+            del os.environ["MSC_B200_ORDERED"]
+        else:
+            os.environ["MSC_B200_ORDERED"] = old
+    assert int(os_[_lib.STAT_TIMEOUT]) == 0
+    np.testing.assert_array_equal(oi, fi, err_msg="ordered vs full scan: indices")
+    np.testing.assert_array_equal(od, fd, err_msg="ordered vs full scan: distances")
+    rows = np.sort(np.random.default_rng(7).choice(X.shape[0], 1000, replace=False))
+    ridx, _, rdist = oracle.knn_exact(X, 15, rows=rows)
+    np.testing.assert_array_equal(oi[rows], ridx.astype(np.int32))
+    np.testing.assert_array_equal(od[rows], rdist)
