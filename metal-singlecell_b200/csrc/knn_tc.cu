@@ -31,6 +31,7 @@
 // abort flag that every role polls, the kernel records MSC_STAT_TIMEOUT and all roles leave their
 // loops, so a fault in the pipeline returns an error instead of hanging the GPU.
 #include <cuda.h>
+#include <cstdlib>
 
 #include "kernels.cuh"
 #include "msc_select.cuh"
@@ -103,7 +104,7 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of `parity` to complete.  false = gave up (abort raised).
-__device__ __forceinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity,
                                             volatile int* abort_flag,
                                             uint64_t limit_ns = WAIT_LIMIT_NS) {
   const uint64_t t0 = globaltimer();
@@ -123,7 +124,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
 }
 // Teardown wait for work this thread itself started (copies, MMAs): ignores the abort flag
 // because such work completes on its own, but is still bounded in time.
-__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+__device__ __noinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 0;; ++it) {
     if (mbar_test(bar, parity)) return true;
@@ -228,7 +229,7 @@ __device__ __forceinline__ bool mbar_test_cl(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
+__device__ __noinline__ bool mbar_wait_cl_slow(uint64_t* bar, uint32_t parity,
                                                volatile int* abort_flag) {
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
@@ -351,6 +352,9 @@ struct TcParams {
   const int64_t* voff;
   const double* roff;
   const int32_t* vok;
+  // single CTAs: the producer alone walks the key tiles and hands each tile to the MMA thread and
+  // the epilogue warps with the data (stage and accumulator tags); else every role walks
+  int meta_walk;
 };
 
 // Key-tile order of a query tile whose own rows lie in key tile `diag`: first the NEAR tiles
@@ -373,34 +377,18 @@ __device__ __forceinline__ int key_tile_at(int j, int diag, int nkt) {
   return right > left ? diag + (j - m) : diag - (j - m);
 }
 
-// Mask word of a pruned walk at position k: the word holding the query tile's own key tile
-// first, then outward, alternating right and left (dw, dw+1, dw-1, dw+2, ...), clipped to the
-// sample.  In the locality order, key tiles near in packed position are mostly near in space, so
-// the rows' thresholds fall early and fewer candidates are inserted.
-__device__ __forceinline__ int mask_word_at(int k, int dw, int nw) {
-  const int left = dw, right = nw - 1 - dw;
-  const int m = min(left, right);
-  if (k == 0) return dw;
-  if (k <= 2 * m) return (k & 1) ? dw + ((k + 1) >> 1) : dw - (k >> 1);
-  return right > left ? dw + (k - m) : dw - (k - m);
-}
-
 // The key tiles of one work item in the order every role walks them: the near tiles
 // (key_tile_at), then all other tiles in plain order, or only those whose bit is set in the
-// item's visit mask (the pruned scan; its words from the query tile's own word outward), or none
-// (the near pass).  Every role of the CTA walks the same sequence, so the tiles need no hand-off
-// between them.
+// item's visit mask (the pruned scan), or none (the near pass).  Every role of the CTA walks the
+// same sequence, so the tiles need no hand-off between them.
 struct KeyTileWalk {
   int nkt, diag, np, j;
   const uint32_t* mask;
-  int w, nw;             // position in the word sequence, words in the mask
-  int dw;                // first word of the outward order
+  int w, nw;
   uint32_t cur, nxt;
   bool near_only;
   int khi = 1 << 30;     // range walks stop before this tile
   bool range = false;
-  // the mask word at position k: outward from dw, or in plain order for range walks
-  __device__ __forceinline__ int word(int k) const { return range ? k : mask_word_at(k, dw, nw); }
   __device__ __forceinline__ void init(const WorkItem& item, int qref, int bn,
                                        const uint32_t* m, int words, bool near) {
     nkt = (item.nkeys + bn - 1) / bn;
@@ -415,9 +403,8 @@ struct KeyTileWalk {
     mask = m;
     w = 0;
     nw = words;
-    dw = min(max(diag >> 5, 0), max(words - 1, 0));
-    cur = m ? m[word(0)] : 0u;
-    nxt = (m && words > 1) ? m[word(1)] : 0u;   // one word ahead: its load overlaps the near tiles
+    cur = m ? m[0] : 0u;
+    nxt = (m && words > 1) ? m[1] : 0u;     // one word ahead: its load overlaps the near tiles
   }
   // A range walk (the refine pass): no near phase, only the tiles [lo, hi), in plain order or
   // as the mask's bits.
@@ -443,11 +430,11 @@ struct KeyTileWalk {
     while (cur == 0u) {
       if (++w >= nw) return -1;
       cur = nxt;
-      nxt = w + 1 < nw ? mask[word(w + 1)] : 0u;
+      nxt = w + 1 < nw ? mask[w + 1] : 0u;
     }
     const int b = __ffs(cur) - 1;
     cur &= cur - 1u;
-    const int kt = word(w) * 32 + b;
+    const int kt = w * 32 + b;
     return kt < khi ? kt : -1;
   }
 };
@@ -513,9 +500,9 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   uint64_t* item_full = bars + 41;         // [ITEM_RING] a claimed work item is in item_ring
   uint64_t* item_empty = bars + 45;        // [ITEM_RING] every consumer has read it
   int* item_ring = reinterpret_cast<int*>(bars + 49);   // [ITEM_RING]
-  // ordered walk (main pass with sorted visit lists): the key tile a stage / an accumulator holds
-  // (-1: the item's walk ends there), and per epilogue warp the largest radius R of its rows,
-  // tagged with the work item (item << 32 | float bits); bytes 408..512 of the 512-byte block
+  // tagged walk: the key tile a stage / an accumulator holds (-1: the item's walk ends there);
+  // ordered walk: per epilogue warp the largest radius R of its rows, tagged with the work item
+  // (item << 32 | float bits); bytes 408..512 of the 512-byte block
   int* stage_meta = item_ring + ITEM_RING;                  // [stages <= 8]
   int* acc_meta = stage_meta + 8;                           // [2]
   unsigned long long* rq_pub = reinterpret_cast<unsigned long long*>(bars + 56);   // [NEPI]
@@ -533,14 +520,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   // the producer drives the walk from the sorted list and ends it early (single CTAs only)
   const bool ordered = !PAIR && !P.near_only && P.qmap == nullptr && P.vlist != nullptr &&
                        *P.vok != 0;
+  // the producer alone walks (from the list, or the mask) and tags stages and accumulators
+  const bool meta = !PAIR && (ordered || P.meta_walk != 0);
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < NEPI; ++i) rq_pub[i] = ~0ull;       // no item yet
     for (int i = 0; i < 2; ++i) {
       mbar_init(&a_full[i], 1);
       mbar_init(&a_empty[i], 1);
-      // ordered: the MMA commit and the MMA thread's own arrive (after it wrote acc_meta)
-      mbar_init(&acc_full[i], ordered ? 2 : 1);
+      // tagged walk: the MMA commit and the MMA thread's own arrive (after it wrote acc_meta)
+      mbar_init(&acc_full[i], meta ? 2 : 1);
       mbar_init(&acc_empty[i], PAIR ? 2 * NEPI : NEPI);
       mbar_init(&a_peer[i], 1);
     }
@@ -698,14 +687,14 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
               ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
               if (P.prof) c_wait += clock64() - tw;
               if (!ok) break;
-              if (ordered && kb == 0) *reinterpret_cast<volatile int*>(&stage_meta[stage]) = kt;
+              if (meta && kb == 0) *reinterpret_cast<volatile int*>(&stage_meta[stage]) = kt;
               mbar_expect_tx(&b_full[stage], uint32_t(b_bytes));
               tma_load_2d(Bsm + stage * b_bytes, &tmB, &b_full[stage], kb * 64,
                           w.key0 + kt * P.bn + int(rank) * brows);
               if (++stage == P.stages) { stage = 0; sphase ^= 1; }
             }
           }
-          if (ok && ordered) {
+          if (ok && meta) {
             // the end of the item's walk: a stage that carries no keys, tile -1
             ok = mbar_wait(&b_empty[stage], sphase ^ 1, abort_flag);
             if (ok) {
@@ -773,13 +762,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           if (!ok) break;
           const uint32_t a_base = smem_u32(Asm + abuf * a_bytes);
           KeyTileWalk walk;
-          if (!ordered) walk_init(walk, w, it);
+          if (!meta) walk_init(walk, w, it);
           for (;;) {
             int kt_meta = 0;
-            if (!ordered) {
+            if (!meta) {
               if (walk.next() < 0) break;
             } else {
-              // ordered: the next stage names the tile, or ends the item (a stage without keys)
+              // tagged walk: the next stage names the tile, or ends the item (a stage without keys)
               const long long t1 = P.prof ? clock64() : 0;
               ok = mbar_wait(&b_full[stage], sphase, abort_flag);
               if (P.prof) c_b += clock64() - t1;
@@ -798,11 +787,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (P.prof) c_acc += clock64() - t2;
             if (!ok) break;
             // the epilogue read this accumulator's previous tile before it released it
-            if (ordered) *reinterpret_cast<volatile int*>(&acc_meta[acc]) = kt_meta;
+            if (meta) *reinterpret_cast<volatile int*>(&acc_meta[acc]) = kt_meta;
             tc_fence_after();
             const uint32_t d_tmem = tmem_base + uint32_t(acc * P.bn);
             for (int kb = 0; kb < P.kb; ++kb) {
-              if (!(ordered && kb == 0)) {                 // ordered: the first stage is waited for
+              if (!(meta && kb == 0)) {                    // tagged: the first stage is waited for
                 const long long t1 = P.prof ? clock64() : 0;
                 ok = mbar_wait(&b_full[stage], sphase, abort_flag);
                 if (ok && PAIR) ok = mbar_wait_cl(&b_peer[stage], sphase, abort_flag);
@@ -822,11 +811,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (!ok) break;
             issued = true;
             umma_commit_g<PAIR>(&acc_full[acc]);
-            if (ordered) mbar_arrive(&acc_full[acc]);     // releases acc_meta to the epilogue
+            if (meta) mbar_arrive(&acc_full[acc]);        // releases acc_meta to the epilogue
             if (++acc == 2) { acc = 0; accphase ^= 1; }
           }
           if (!ok) break;
-          if (ordered) {
+          if (meta) {
             // the end of the item for the epilogue: an accumulator turn without a tile
             ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
             if (!ok) break;
@@ -902,12 +891,12 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
       }
       const int limit = w.key0 + w.nkeys;
       KeyTileWalk walk;
-      if (!ordered) walk_init(walk, w, it);
+      if (!meta) walk_init(walk, w, it);
       // ordered: R = threshold + roff of this row, published per warp after every tile
       const double roff_row = (ordered && row < nq) ? P.roff[qrow + row] : 0.0;
       for (;;) {
         int kt = 0;
-        if (!ordered) {
+        if (!meta) {
           kt = walk.next();
           if (kt < 0) break;
         }
@@ -915,7 +904,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
         if (P.prof) c_ew += clock64() - te;
         if (!ok) break;
-        if (ordered) {
+        if (meta) {
           kt = *reinterpret_cast<volatile int*>(&acc_meta[acc]);
           if (kt < 0) {                    // the item's walk ended: hand the turn back
             __syncwarp();
@@ -1321,6 +1310,10 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.voff = ord ? order->off : nullptr;
   P.roff = ord ? order->roff : nullptr;
   P.vok = ord ? order->ok : nullptr;
+  {
+    const char* env = std::getenv("MSC_B200_META_WALK");
+    P.meta_walk = (env && *env == '1') ? 1 : 0;
+  }
   if (cfg.pair && (mask || near_only)) {
     set_error("pruned scans run on single CTAs only");
     return MSC_ERR_INVALID_ARG;

@@ -274,44 +274,25 @@ __global__ void sub_ball_kernel(const float* __restrict__ X, int d, int dp,
 // R over u's rows (z-space), f2 = square of the operand scale.  An empty ball is separated from
 // everything; an unknown R (inf / NaN) from nothing.  Centres are n4 float4 (zero padded); the
 // FP32 distance is lowered by its rounding bound (d+8 units of 2^-23 relative) before the test.
-// The part of the separation bound that depends on the query ball alone: ru + sqrt(R'/f²),
-// R' = R·(1 + 1e-9).  Hoisted out of the tests (one per query ball and task).
-__device__ __forceinline__ double sep_reach(float ru, double R, double f2) {
-  return double(ru) + sqrt(R * (1.0 + 1e-9) / f2);
-}
-
-// Balls (cu, ru) and (cw, rw) are separated when every point of one is farther than sqrt(R)/f
-// from every point of the other: |cu - cw|·(1 - e)^(1/2) - ru - rw > sqrt(R'/f²), with the
-// float sum of squared centre differences and e its relative error bound.  The partial sums only
-// grow, so a partial sum above (reach + rw)²/(1 - e) (rounded up) already proves it and the test
-// stops there; the decision is the one the full sum gives.  reach = sep_reach(ru, R, f2).
 __device__ __forceinline__ bool separated(const float* __restrict__ cu, float ru, double R,
                                           const float* __restrict__ cw, float rw, int n4, int d,
-                                          double f2, double reach) {
+                                          double f2) {
   if (ru < 0.f || rw < 0.f) return true;
   if (!(R < 1e300)) return false;
-  const double e = double(d + 8) * 0x1p-23;
-  const double tr = reach + double(rw);
-  const float need = __double2float_ru(tr * tr / (1.0 - e) * (1.0 + 1e-12));
   const float4* a = reinterpret_cast<const float4*>(cu);
   const float4* b = reinterpret_cast<const float4*>(cw);
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-  auto add = [&](const float4 x, const float4 y) {
+#pragma unroll 4
+  for (int t = 0; t < n4; ++t) {
+    const float4 x = a[t], y = b[t];
     const float e0 = x.x - y.x, e1 = x.y - y.y, e2 = x.z - y.z, e3 = x.w - y.w;
     s0 = fmaf(e0, e0, s0);
     s1 = fmaf(e1, e1, s1);
     s2 = fmaf(e2, e2, s2);
     s3 = fmaf(e3, e3, s3);
-  };
-  int t = 0;
-  for (; t + 4 <= n4; t += 4) {                  // 16 dimensions, then the early exit
-#pragma unroll
-    for (int j = 0; j < 4; ++j) add(a[t + j], b[t + j]);
-    if (t + 4 < n4 && (s0 + s1) + (s2 + s3) > need) return true;
   }
-  for (; t < n4; ++t) add(a[t], b[t]);
   const float s = (s0 + s1) + (s2 + s3);
-  const double lo = double(s) * (1.0 - e);
+  const double lo = double(s) * (1.0 - double(d + 8) * 0x1p-23);
   const double L = sqrt(lo) - double(ru) - double(rw);
   return L > 0.0 && f2 * L * L > R * (1.0 + 1e-9);
 }
@@ -337,10 +318,8 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
   __shared__ unsigned ubits_all[PLAN_WARPS][32], wbits_all[PLAN_WARPS][32];
   const int lane = lane_id(), wib = warp_id();
   float* qball = reinterpret_cast<float*>(sm4) + wib * (9 * dp);   // [0]: tile, [1..8]: sub-balls
-  __shared__ double reach_all[PLAN_WARPS][8];
   unsigned* ubits = ubits_all[wib];
   unsigned* wbits = wbits_all[wib];
-  double* reach_u = reach_all[wib];              // per query sub-ball of the task's tile
   const int n4 = dp / 4;
   const double f = op_scale(prec, ctl);
   const double f2 = f * f;
@@ -367,9 +346,6 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
     const float rq = qr[qt];
     double Rq = 0.0;
     for (int j = 0; j < 4; ++j) Rq = fmax(Rq, rsub[sb0 + j]);    // rsub is >= 0 or +inf
-    const double reach_q = sep_reach(rq, Rq, f2);
-    if (lane < 8) reach_u[lane] = sep_reach(sr[2 * sb0 + lane], rsub[sb0 + (lane >> 1)], f2);
-    __syncwarp();
     const int nkt = (w.nkeys + bn - 1) / bn;
     const int diag = (w.qrow0 - w.key0) / bn;
     const int lo = max(0, diag - 2), hi = min(nkt - 1, diag + 2);
@@ -380,7 +356,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
       bool l1 = false;                           // not separated at level 1
       if (kt < nkt && (kt < lo || kt > hi)) {
         const int64_t g = (int64_t(w.key0) + int64_t(kt) * bn) / 256;
-        l1 = !separated(qball, rq, Rq, kc + g * dp, kr[g], n4, d, f2, reach_q);
+        l1 = !separated(qball, rq, Rq, kc + g * dp, kr[g], n4, d, f2);
       }
       const uint32_t fm = __ballot_sync(FULL, l1);
       uint32_t bits = 0u;
@@ -396,7 +372,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
           const int kti = base + __fns(fm, 0, i + 1);
           const int64_t g = (int64_t(w.key0) + int64_t(kti) * bn) / 256;
           if (!separated(qball + (1 + u) * dp, sr[2 * sb0 + u], rsub[sb0 + (u >> 1)],
-                         kc + g * dp, kr[g], n4, d, f2, reach_u[u]))
+                         kc + g * dp, kr[g], n4, d, f2))
             atomicOr(&ubits[i], 1u << u);
         }
         // (b) key sub-ball v of failing tile i
@@ -405,8 +381,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
           const int kti = base + __fns(fm, 0, i + 1);
           const int64_t kb0 = (int64_t(w.key0) + int64_t(kti) * bn) / SUB;
           const float rw = sr[2 * kb0 + v];
-          if (rw >= 0.f &&
-              !separated(qball, rq, Rq, sc + (2 * kb0 + v) * dp, rw, n4, d, f2, reach_q))
+          if (rw >= 0.f && !separated(qball, rq, Rq, sc + (2 * kb0 + v) * dp, rw, n4, d, f2))
             atomicOr(&wbits[i], 1u << v);
         }
         __syncwarp();
@@ -428,7 +403,7 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
           for (int pr = lane; pr < npair && !hit; pr += 32) {
             const int u = __fns(ub, 0, pr % nu + 1), vv = __fns(wb, 0, pr / nu + 1);
             hit = !separated(qball + (1 + u) * dp, sr[2 * sb0 + u], rsub[sb0 + (u >> 1)],
-                             sc + (2 * kb0 + vv) * dp, sr[2 * kb0 + vv], n4, d, f2, reach_u[u]);
+                             sc + (2 * kb0 + vv) * dp, sr[2 * kb0 + vv], n4, d, f2);
           }
           if (__any_sync(FULL, hit)) bits |= 1u << (kti - base);
         }
