@@ -14,7 +14,7 @@
 //   3. fill: every kept edge i→j written into row j's segment as one 8-byte reverse record
 //      (slot from an atomic cursor — order within the segment is arbitrary);
 //   4. per row: its own list (read straight from the kNN arrays) and its reverse records sorted by
-//      key = (column << 1 | reverse) — a warp bitonic network in registers up to 256 entries,
+//      key = (column << 1 | reverse) — a warp bitonic network in registers up to 128 entries,
 //      a block network beyond — then the pairs merged (a column present in both directions) and
 //      the unique entries written left-justified into the segment;
 //   5. exclusive scan of the unique counts → indptr; 6. copy into indices / data.
@@ -297,8 +297,19 @@ __device__ __forceinline__ int merge_row_regs(int mode, int64_t i, int k, int L,
   return written;
 }
 
-constexpr int WARP_MAX = 256;    // longest row the warp tier sorts (8 keys per lane)
+constexpr int WARP_MAX = 128;    // longest row the warp tier sorts (4 keys per lane)
 
+// rows of 65..128 entries are rare: their sort stays out of line, so that the common paths (one or
+// two keys per lane) keep a small instruction footprint
+__device__ __noinline__ int merge_row_regs4(int mode, int64_t i, int k, int L, int64_t n,
+                                            const int32_t* __restrict__ idx,
+                                            const float* __restrict__ vals, int2* seg,
+                                            const double* __restrict__ sig2) {
+  return merge_row_regs<4>(mode, i, k, L, n, idx, vals, seg, sig2);
+}
+
+// A warp takes 32 consecutive rows at a time: their segment offsets come in one coalesced load,
+// then the rows are merged one after another.
 __global__ void __launch_bounds__(UW * 32)
 merge_warp_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
                   const float* __restrict__ vals, const int64_t* __restrict__ rptr,
@@ -307,27 +318,41 @@ merge_warp_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
                   int32_t* __restrict__ n_big) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < n; i += nwarps) {
-    const int64_t b = i * k + rptr[i];
-    const int L = k + int(rptr[i + 1] - rptr[i]);
-    int2* seg = rec + b;
-    int u;
-    if (L <= 32) u = merge_row_regs<1>(mode, i, k, L, n, idx, vals, seg, sig2);
-    else if (L <= 64) u = merge_row_regs<2>(mode, i, k, L, n, idx, vals, seg, sig2);
-    else if (L <= 128) u = merge_row_regs<4>(mode, i, k, L, n, idx, vals, seg, sig2);
-    else if (L <= WARP_MAX) u = merge_row_regs<8>(mode, i, k, L, n, idx, vals, seg, sig2);
-    else {
-      // a long row goes to the block tier: its own list into the first k slots of its segment
-      for (int t = lane; t < k; t += 32) {
-        const int32_t j = idx[i * k + t];
-        const float v = vals[i * k + t];
-        const bool ok = j != i && j >= 0 && j < n && kept(mode, t, v);
-        seg[t] = make_int2(int(ok ? (uint32_t(j) << 1) : SENT), __float_as_int(v));
+  for (int64_t g = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; g * 32 < n;
+       g += nwarps) {
+    const int64_t r0 = g * 32;
+    const int nr = int(min64(32, n - r0));
+    const int64_t my_p0 = lane < nr ? rptr[r0 + lane] : 0;
+    const int64_t my_p1 = lane < nr ? rptr[r0 + lane + 1] : 0;
+    int my_u = 0;
+    for (int j = 0; j < nr; ++j) {
+      const int64_t i = r0 + j;
+      const int64_t p0 = __shfl_sync(FULL, my_p0, j);
+      const int L = k + int(__shfl_sync(FULL, my_p1, j) - p0);
+      int2* seg = rec + i * k + p0;
+      int u;
+      if (L <= 32) {
+        u = merge_row_regs<1>(mode, i, k, L, n, idx, vals, seg, sig2);
+      } else if (L <= 64) {
+        u = merge_row_regs<2>(mode, i, k, L, n, idx, vals, seg, sig2);
+      } else if (L <= WARP_MAX) {
+        u = merge_row_regs4(mode, i, k, L, n, idx, vals, seg, sig2);
+      } else {
+        // a long row goes to the block tier: its own list into the first k slots of its segment
+        for (int t = lane; t < k; t += 32) {
+          const int32_t jj = idx[i * k + t];
+          const float v = vals[i * k + t];
+          const bool ok = jj != i && jj >= 0 && jj < n && kept(mode, t, v);
+          seg[t] = make_int2(int(ok ? (uint32_t(jj) << 1) : SENT), __float_as_int(v));
+        }
+        if (lane == 0) big_rows[atomicAdd(n_big, 1)] = int32_t(i);
+        continue;
       }
-      if (lane == 0) big_rows[atomicAdd(n_big, 1)] = int32_t(i);
-      continue;
+      if (lane == j) my_u = u;
     }
-    if (lane == 0) uniq[i] = u;
+    // rows of the block tier write their own count there
+    const int64_t p0 = my_p0, p1 = my_p1;
+    if (lane < nr && k + int(p1 - p0) <= WARP_MAX) uniq[r0 + lane] = my_u;
   }
 }
 

@@ -32,6 +32,7 @@
 // loops, so a fault in the pipeline returns an error instead of hanging the GPU.
 #include <cuda.h>
 #include <cstdlib>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "msc_select.cuh"
@@ -54,6 +55,17 @@ constexpr int EPI_WARP0 = 4;
 #define MSC_TC_TRIBUF 0
 #endif
 constexpr bool kRegSplit = MSC_TC_REGSPLIT != 0;
+// The per-row candidate lists of the epilogue: 1 = RowTopK (every passing value replaces the
+// row's largest at once), 2 = RowTopKD (passing values are buffered per row and merged into the
+// sorted list by the whole warp when the buffer is full)
+#ifndef MSC_TC_SELECT
+#define MSC_TC_SELECT 1
+#endif
+template <int KH>
+struct SelectorOf {
+  using type = typename std::conditional<MSC_TC_SELECT == 2, RowTopKD<KH, 128, 16>,
+                                         RowTopK<KH, 128>>::type;
+};
 constexpr bool kTriBuf = MSC_TC_TRIBUF != 0;
 // register split of the eight-epilogue-warp kernels (see knn_tc_kernel)
 constexpr int REG_LOW = 56, REG_HIGH = 224;
@@ -459,7 +471,7 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
   p.a_off = 0;
   p.b_off = p.a_off + size_t(na) * kb * BM * 128;
   p.sel_off = p.b_off + size_t(stages) * brows * 128;
-  p.pub_off = p.sel_off + size_t(nh) * RowTopK<KH, BM>::smem_bytes();
+  p.pub_off = p.sel_off + size_t(nh) * SelectorOf<KH>::type::smem_bytes();
   p.bar_off = p.pub_off + (nh > 1 ? size_t(2) * BM * sizeof(float) : 0);
   p.total = p.bar_off + 512 + 1024;          // barriers + slack for 1024-byte alignment
   return p;
@@ -476,7 +488,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
   static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
   constexpr int NH = NEPI / 4;
-  using Sel = RowTopK<KH, BM>;
+  using Sel = typename SelectorOf<KH>::type;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~uintptr_t(1023));

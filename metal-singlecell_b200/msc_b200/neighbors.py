@@ -361,26 +361,100 @@ def _host_state(n: int, d: int, k: int, device) -> HostGraphState:
     return st
 
 
-def _host_csr(h: dict, n: int, k: int):
-    """SciPy CSR matrices owning their arrays, from the pinned host tensors of
-    ``neighbors_host``; index arrays int32 while they fit, as SciPy itself chooses."""
+_STAGE_BYTES = 32 << 20              # pinned staging chunk of the upload
+
+
+def _upload(torch, st: HostGraphState, X: np.ndarray):
+    """Copy a pageable host embedding into ``st.X`` through two pinned staging chunks: the host
+    copy of one chunk (multi-threaded) overlaps the DMA of the other, at pinned-copy speed."""
+    if getattr(st, "stage", None) is None:
+        st.stage = [torch.empty(_STAGE_BYTES, dtype=torch.uint8).pin_memory() for _ in range(2)]
+        st.stage_ev = [None, None]
+    src = torch.from_numpy(X).view(-1).view(torch.uint8)
+    dst = st.X.view(-1).view(torch.uint8)
+    main = torch.cuda.current_stream(st.device)
+    total = src.numel()
+    for c, off in enumerate(range(0, total, _STAGE_BYTES)):
+        b = c & 1
+        m = min(_STAGE_BYTES, total - off)
+        if st.stage_ev[b] is not None:
+            st.stage_ev[b].synchronize()           # its previous chunk has left the buffer
+        st.stage[b][:m].copy_(src[off:off + m])
+        dst[off:off + m].copy_(st.stage[b][:m], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(main)
+        st.stage_ev[b] = ev
+
+
+def _owned(torch, t, count: int, dtype):
+    """A new NumPy array holding the first ``count`` elements of pinned tensor ``t``."""
+    out = np.empty(count, dtype=dtype)
+    if count:
+        torch.from_numpy(out).copy_(t[:count])          # multi-threaded host copy
+    return out
+
+
+def _graph_host(X: np.ndarray, k: int, metric: str, method: str, precision: str, kprime: int,
+                st: HostGraphState):
+    """The drop-in's path: upload, graph, and both matrices back as SciPy CSR owning their arrays.
+    The distances CSR is final before the connectivities are computed (``msc_neighbors_ex``
+    records an event there): it is copied to pinned memory on a second stream and from there into
+    its NumPy arrays while the GPU still computes the connectivities."""
     import scipy.sparse as sp
     torch = _torch()
+    lib = _lib.load()
+    n, d = X.shape
+    mid, meth, pid = _ids(metric, method, precision)
+    nbytes = lib.msc_neighbors_workspace_bytes(n, d, k, mid, meth, pid, int(kprime))
+    ws = st.workspace.get(nbytes)
+    main = torch.cuda.current_stream(st.device)
+    _upload(torch, st, X)
+    o = st.dev_out
+
+    def buf(name, shape, dtype):
+        t = o.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=st.device)
+            o[name] = t
+        return t
     m = max(k - 1, 0)
-
-    def own(t, count, dtype):
-        out = np.empty(count, dtype=dtype)
-        if count:
-            torch.from_numpy(out).copy_(t[:count])     # multi-threaded host copy
-        return out
-
-    nnz = int(h["conn_nnz"])
-    d_ptr = h["dist_indptr"].numpy().astype(_index_dtype(n, n * m))
-    c_ptr = h["conn_indptr"].numpy().astype(_index_dtype(n, nnz))
-    dist = sp.csr_matrix((own(h["dist_data"], n * m, np.float32),
-                          own(h["dist_indices"], n * m, np.int32), d_ptr), shape=(n, n))
-    conn = sp.csr_matrix((own(h["conn_data"], nnz, np.float32),
-                          own(h["conn_indices"], nnz, np.int32), c_ptr), shape=(n, n))
+    knn_idx, knn_dist = buf("knn_idx", (n, k), torch.int32), buf("knn_dist", (n, k), torch.float32)
+    d_ptr = buf("dist_indptr", (n + 1,), torch.int64)
+    d_ind = buf("dist_indices", (max(n * m, 1),), torch.int32)
+    d_dat = buf("dist_data", (max(n * m, 1),), torch.float32)
+    c_ptr = buf("conn_indptr", (n + 1,), torch.int64)
+    c_ind = buf("conn_indices", (max(2 * n * m, 1),), torch.int32)
+    c_dat = buf("conn_data", (max(2 * n * m, 1),), torch.float32)
+    stats = buf("stats", (_lib.STATS_LEN,), torch.int64)
+    _lib.check(lib.msc_neighbors_ex(st.X.data_ptr(), n, d, k, mid, meth, pid, int(kprime),
+                                    knn_idx.data_ptr(), knn_dist.data_ptr(), d_ptr.data_ptr(),
+                                    d_ind.data_ptr(), d_dat.data_ptr(), c_ptr.data_ptr(),
+                                    c_ind.data_ptr(), c_dat.data_ptr(), stats.data_ptr(),
+                                    ws.data_ptr(), ws.numel(), main.cuda_stream,
+                                    st.ready.cuda_event), "msc_neighbors_ex")
+    h = st.host
+    cs = st.copy_stream
+    with torch.cuda.stream(cs):
+        cs.wait_event(st.ready)
+        h["dist_indptr"].copy_(d_ptr, non_blocking=True)
+        h["dist_indices"][: n * m].copy_(d_ind[: n * m], non_blocking=True)
+        h["dist_data"][: n * m].copy_(d_dat[: n * m], non_blocking=True)
+    h["stats"].copy_(stats, non_blocking=True)
+    h["conn_indptr"].copy_(c_ptr, non_blocking=True)
+    cs.synchronize()                              # the distances are on the host; the GPU goes on
+    d_ptr_h = h["dist_indptr"].numpy().astype(_index_dtype(n, n * m))
+    dist = sp.csr_matrix((_owned(torch, h["dist_data"], n * m, np.float32),
+                          _owned(torch, h["dist_indices"], n * m, np.int32), d_ptr_h),
+                         shape=(n, n))
+    main.synchronize()
+    _lib.check_stats(h["stats"].numpy())
+    nnz = int(h["conn_indptr"][n])
+    h["conn_indices"][:nnz].copy_(c_ind[:nnz], non_blocking=True)
+    h["conn_data"][:nnz].copy_(c_dat[:nnz], non_blocking=True)
+    main.synchronize()
+    conn = sp.csr_matrix((_owned(torch, h["conn_data"], nnz, np.float32),
+                          _owned(torch, h["conn_indices"], nnz, np.int32),
+                          h["conn_indptr"].numpy().astype(_index_dtype(n, nnz))), shape=(n, n))
     return dist, conn
 
 
@@ -395,9 +469,10 @@ def neighbors(X_pca: np.ndarray, n_neighbors: int = 15, random_state: int = 0,
     Gaussian-kernel graph (method='gauss').  ``random_state`` and ``approx`` are accepted for
     compatibility; the graph is exact and deterministic.
 
-    The embedding is uploaded, the graph built on the GPU and both matrices copied back, the
-    distances while the connectivities are still being computed (``neighbors_host``).  Device and
-    pinned host buffers of the last shape are kept for the next call of that shape.
+    The embedding is uploaded through pinned staging chunks, the graph built on the GPU, and the
+    distances matrix copied back and assembled on the host while the connectivities are still
+    being computed.  Device and pinned buffers of the last shape are kept for the next call of
+    that shape.
     """
     torch = _torch()
     X = np.ascontiguousarray(X_pca, dtype=np.float32)
@@ -416,9 +491,7 @@ def neighbors(X_pca: np.ndarray, n_neighbors: int = 15, random_state: int = 0,
         raise ValueError("msc_neighbors: invalid arguments")
     st = _host_state(n, d, k, dev)
     with torch.cuda.device(dev):
-        h = neighbors_host(torch.from_numpy(X), k, metric=metric, method=method,
-                           precision=precision, kprime=kprime, state=st)
-    return _host_csr(h, n, k)
+        return _graph_host(X, k, metric, method, precision, kprime, st)
 
 
 def _knn(X_pca: np.ndarray, n_neighbors: int, random_state: int = 0,
