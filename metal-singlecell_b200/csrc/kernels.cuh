@@ -128,6 +128,7 @@ struct PruneWs {
   double* rpos;       // R per packed position
   double* rpos2;
   double* mean;       // per sample
+  double2* mean_part; // per sample and slice: partial sums of R and counts
   float *qc, *qr;     // 128-row balls: centres [npacked/128][d], radii
   float *kc, *kr;     // 256-row balls
   float *sc, *sr;     // two balls per 32-row block

@@ -536,398 +536,4 @@ struct RowTopK {
 };
 
 
-// --- the row top-k' with deferred, warp-merged insertions -------------------------------------
-//
-// The same filter as RowTopK, but a value that passes is only appended to its row's buffer of
-// CAP pairs (two shared-memory stores, no list update), and the row's threshold stays what it was
-// at the last merge.  When a row's buffer is full, or when the list is read, the whole warp merges
-// that row: the buffer (one pair per lane) is sorted by a bitonic network over shuffles, its
-// reversal is laid against the upper half of the row's sorted list (a half-cleaner: each slot keeps
-// the smaller of the two), and a 64-pair bitonic merge (two pairs per lane) restores the order —
-// 22 shuffle stages for up to CAP pairs, where RowTopK spends one lockstep round of dependent
-// shared-memory updates on every pair.  Lists are sorted ascending; the threshold is slot k'-1.
-//
-// Shared memory, row-major with odd strides so that a warp reading one row's slots, and the 32
-// lanes appending to their own rows, both spread over the banks:
-//   lv/lc[ROWS][KH+1]   sorted list (+inf / -1 padding)      bv/bc[ROWS][CAP+1]   buffer
-template <int KH, int ROWS, int CAP = 16>
-struct RowTopKD {
-  static_assert(KH == 32 || KH == 48 || KH == 64, "32, 48 or 64 slots");
-  static_assert(CAP >= 1 && CAP <= 32, "buffer of 1..32 pairs");
-  static constexpr int LS = KH + 1, BS = CAP + 1;
-  __host__ __device__ static constexpr size_t smem_bytes() { return size_t(ROWS) * (LS + BS) * 8; }
-
-  float* lv;
-  int* lc;
-  float* bv;
-  int* bc;
-  int row;        // this thread's row within the ROWS rows
-  int kp;         // k' (<= KH)
-  int cnt;        // pairs in this row's buffer
-  float thr;      // the list's k'-th value (+inf while fewer than k' are kept)
-  float thr_f;    // filter threshold: min(thr, seed, the partner's published threshold)
-  // An upper bound on the row's final k'-th value known before the scan, +inf if none (see
-  // RowTopK::seed): values at or above it are never kept; finish() reports min(thr, seed).
-  float seed = F_INF;
-  float* pub_own = nullptr;           // see RowTopK::pub_own
-  const float* pub_other = nullptr;
-  int ex_r0 = 0, ex_r1 = 0, ex_o0 = 0, ex_o1 = 0;   // columns never offered again (RowTopK)
-  int n_hot = 0, n_compact = 0, n_append = 0;        // hot chunks, merges, appended pairs
-  bool prof = false;
-  long long c_hot = 0, n_rounds = 0;
-
-  __device__ __forceinline__ void bind(void* smem, int row_, int kprime) {
-    lv = static_cast<float*>(smem);
-    lc = reinterpret_cast<int*>(lv + ROWS * LS);
-    bv = reinterpret_cast<float*>(lc + ROWS * LS);
-    bc = reinterpret_cast<int*>(bv + ROWS * BS);
-    row = row_;
-    kp = kprime;
-  }
-
-  __device__ __forceinline__ void reset() {
-    for (int t = 0; t < KH; ++t) {
-      lv[row * LS + t] = F_INF;
-      lc[row * LS + t] = -1;
-    }
-    cnt = 0;
-    thr = F_INF;
-    thr_f = F_INF;
-    seed = F_INF;
-  }
-
-  __device__ __forceinline__ void set_seed(float sd) {
-    seed = sd;
-    thr_f = fminf(thr_f, sd);
-  }
-
-  __device__ __forceinline__ void refresh() {
-    thr_f = fminf(thr, seed);
-    if (pub_other) thr_f = fminf(thr_f, *reinterpret_cast<const volatile float*>(pub_other));
-  }
-
-  // one compare-exchange stage over lanes lane ^ j: the lower lane keeps the smaller pair when up
-  __device__ __forceinline__ static void cx(float& v, int& c, int j, bool keep_min) {
-    const float ov = __shfl_xor_sync(FULL, v, j);
-    const int oc = __shfl_xor_sync(FULL, c, j);
-    if (keep_min ? (ov < v) : (v < ov)) { v = ov; c = oc; }
-  }
-  __device__ __forceinline__ static void sort32(float& v, int& c) {
-    const int lane = lane_id();
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1)
-#pragma unroll
-      for (int j = k >> 1; j > 0; j >>= 1) cx(v, c, j, ((lane & j) == 0) == ((lane & k) == 0));
-  }
-  // a bitonic 64-sequence (a: positions lane, b: positions 32 + lane) into ascending order
-  __device__ __forceinline__ static void merge64(float& a, int& ac, float& b, int& bc_) {
-    if (b < a) {
-      const float t = a; a = b; b = t;
-      const int u = ac; ac = bc_; bc_ = u;
-    }
-    const int lane = lane_id();
-#pragma unroll
-    for (int j = 16; j > 0; j >>= 1) {
-      cx(a, ac, j, (lane & j) == 0);
-      cx(b, bc_, j, (lane & j) == 0);
-    }
-  }
-  // the pair at sorted position kp-1 of (a, b)
-  __device__ __forceinline__ float kth(float a, float b) const {
-    return kp - 1 < 32 ? __shfl_sync(FULL, a, kp - 1) : __shfl_sync(FULL, b, kp - 1 - 32);
-  }
-  __device__ __forceinline__ void load_list(int r, float& a, int& ac, float& b, int& bc_) const {
-    const int lane = lane_id();
-    a = lv[r * LS + lane];
-    ac = lc[r * LS + lane];
-    b = 32 + lane < KH ? lv[r * LS + 32 + lane] : F_INF;
-    bc_ = 32 + lane < KH ? lc[r * LS + 32 + lane] : -1;
-  }
-  __device__ __forceinline__ void store_list(int r, float a, int ac, float b, int bc_) {
-    const int lane = lane_id();
-    lv[r * LS + lane] = a;
-    lc[r * LS + lane] = ac;
-    if (32 + lane < KH) {
-      lv[r * LS + 32 + lane] = b;
-      lc[r * LS + 32 + lane] = bc_;
-    }
-  }
-
-  // warp-collective: merge the cj buffered pairs of warp row j into its list; the new k'-th
-  // value for every lane
-  __device__ __forceinline__ float merge_row(int j, int cj) {
-    const int lane = lane_id();
-    const int r = row - lane + j;
-    float a, b;
-    int ac, bcl;
-    load_list(r, a, ac, b, bcl);
-    float x = lane < cj ? bv[r * BS + lane] : F_INF;
-    int xc = lane < cj ? bc[r * BS + lane] : -1;
-    sort32(x, xc);
-    // half-cleaner of (list ascending, buffer padded to 64 and reversed): the buffer's reversal
-    // meets the list's upper half; the lower 64 of the 128 are the list's lower half and the
-    // elementwise minima, a bitonic sequence
-    const float rx = __shfl_sync(FULL, x, 31 - lane);
-    const int rxc = __shfl_sync(FULL, xc, 31 - lane);
-    if (rx < b) { b = rx; bcl = rxc; }
-    merge64(a, ac, b, bcl);
-    store_list(r, a, ac, b, bcl);
-    ++n_compact;
-    return kth(a, b);
-  }
-
-  // the rows (bits of `rows`) merge their buffers; their owners take the new thresholds
-  __device__ __forceinline__ void merge_rows(unsigned rows) {
-    const int lane = lane_id();
-    while (rows) {
-      const int j = __ffs(rows) - 1;
-      rows &= rows - 1u;
-      const float t = merge_row(j, __shfl_sync(FULL, cnt, j));
-      if (lane == j) {
-        thr = t;
-        cnt = 0;
-        if (pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
-      }
-    }
-    refresh();
-  }
-
-  // warp-collective: the lists an earlier pass wrote (RowTopK::load_warp), each sorted on load
-  __device__ __forceinline__ void load_warp(const float* __restrict__ vals,
-                                            const int32_t* __restrict__ idx,
-                                            const int32_t* __restrict__ iperm,
-                                            const int32_t* __restrict__ perm, int64_t first_row,
-                                            int nvalid_rows, int stride) {
-    const int lane = lane_id();
-    const int row0 = row - lane;
-    const int64_t my_orow = lane < nvalid_rows ? int64_t(perm[first_row + lane]) : 0;
-    for (int r = 0; r < nvalid_rows; ++r) {
-      const int64_t orow = __shfl_sync(FULL, my_orow, r);
-      float a = F_INF, b = F_INF;
-      int ac = -1, bcl = -1;
-      if (lane < kp) {
-        const int32_t c = idx[orow * stride + lane];
-        if (c >= 0) { a = vals[orow * stride + lane]; ac = iperm[c]; }
-      }
-      if (32 + lane < kp) {
-        const int32_t c = idx[orow * stride + 32 + lane];
-        if (c >= 0) { b = vals[orow * stride + 32 + lane]; bcl = iperm[c]; }
-      }
-      sort32(a, ac);
-      sort32(b, bcl);
-      // (a ascending, b ascending): laying b's reversal against a gives the lower and the upper
-      // 32 as two bitonic halves; each sorts by a 32-merge
-      const float rb = __shfl_sync(FULL, b, 31 - lane);
-      const int rbc = __shfl_sync(FULL, bcl, 31 - lane);
-      float lo = a, hi = rb;
-      int loc = ac, hic = rbc;
-      if (rb < a) { lo = rb; loc = rbc; hi = a; hic = ac; }
-#pragma unroll
-      for (int j = 16; j > 0; j >>= 1) {
-        cx(lo, loc, j, (lane & j) == 0);
-        cx(hi, hic, j, (lane & j) == 0);
-      }
-      store_list(row0 + r, lo, loc, hi, hic);
-      const float t = kth(lo, hi);
-      if (lane == r) thr = t;
-    }
-    __syncwarp();
-    if (lane < nvalid_rows && pub_own) *reinterpret_cast<volatile float*>(pub_own) = thr;
-    refresh();
-  }
-
-  __device__ __forceinline__ static unsigned span_bits(int col0, int a, int b) {
-    const int lo = max(a - col0, 0), hi = min(b - col0, 32);
-    if (hi <= lo) return 0u;
-    const unsigned upto = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
-    return upto & ~((1u << lo) - 1u);
-  }
-
-  __device__ __forceinline__ static float pick32(const float (&v)[32], int e) {
-    float a[16], b[8], c[4], d[2];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) a[i] = (e & 1) ? v[2 * i + 1] : v[2 * i];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) b[i] = (e & 2) ? a[2 * i + 1] : a[2 * i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) c[i] = (e & 4) ? b[2 * i + 1] : b[2 * i];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) d[i] = (e & 8) ? c[2 * i + 1] : c[2 * i];
-    return (e & 16) ? d[1] : d[0];
-  }
-
-  // Offer 32 consecutive candidate columns col0..col0+31 of this row (warp-collective); columns
-  // equal to `self`, >= `limit` or in the excluded ranges are never kept.  Every lane marks its
-  // values below the threshold, then the lanes append their next marked value together; a row
-  // whose buffer is full is merged first (and its marks re-tested against the new threshold).
-  __device__ __forceinline__ void push32(const float (&v)[32], int col0, int self, int limit) {
-    float g[11];
-#pragma unroll
-    for (int q = 0; q < 10; ++q) g[q] = min3f(v[3 * q], v[3 * q + 1], v[3 * q + 2]);
-    g[10] = fminf(v[30], v[31]);
-    const float n0 = min3f(g[0], g[1], g[2]), n1 = min3f(g[3], g[4], g[5]);
-    const float n2 = min3f(g[6], g[7], g[8]), n3 = fminf(g[9], g[10]);
-    const float mn = fminf(min3f(n0, n1, n2), n3);
-    if (!__any_sync(FULL, mn < thr_f)) return;
-    ++n_hot;
-    const long long t_hot = prof ? clock64() : 0;
-    unsigned keep = ~0u;
-    {
-      const int ds = self - col0;
-      if (ds >= 0 && ds < 32) keep &= ~(1u << ds);
-      const int dl = limit - col0;
-      if (dl < 32) keep &= dl <= 0 ? 0u : ((1u << dl) - 1u);
-      keep &= ~(span_bits(col0, ex_r0, ex_r1) | span_bits(col0, ex_o0, ex_o1));
-    }
-    auto marks = [&]() {
-      unsigned m = 0u;
-      if (mn < thr_f) {
-#pragma unroll
-        for (int e = 0; e < 32; ++e) m |= (v[e] < thr_f ? 1u : 0u) << e;
-      }
-      return m & keep;
-    };
-    unsigned m = marks();
-    while (__any_sync(FULL, m != 0u)) {
-      ++n_rounds;
-      const unsigned full = __ballot_sync(FULL, m != 0u && cnt == CAP);
-      if (full) {
-        merge_rows(full);
-        if ((full >> lane_id()) & 1u) m &= marks();
-      }
-      if (m) {
-        const int e = __ffs(m) - 1;
-        m &= m - 1u;
-        const float x = pick32(v, e);
-        if (x < thr_f) {
-          bv[row * BS + cnt] = x;
-          bc[row * BS + cnt] = col0 + e;
-          ++cnt;
-          ++n_append;
-        }
-      }
-    }
-    if (prof) c_hot += clock64() - t_hot;
-  }
-
-  __device__ __forceinline__ void push1(float v, int c, int self, int limit) {
-    const bool ok = v < thr_f && c != self && c < limit;
-    const unsigned full = __ballot_sync(FULL, ok && cnt == CAP);
-    if (full) merge_rows(full);
-    if (ok && v < thr_f) {
-      bv[row * BS + cnt] = v;
-      bc[row * BS + cnt] = c;
-      ++cnt;
-    }
-  }
-
-  // warp-collective: every row with buffered pairs merges them
-  __device__ __forceinline__ void flush() {
-    const unsigned pend = __ballot_sync(FULL, cnt > 0);
-    if (pend) merge_rows(pend);
-  }
-
-  // warp-collective: merge the partner group's lists (same layout at `other`, flushed) into these
-  // (flushed), keeping the k' smallest; the partner's copies of keys in the excluded ranges are
-  // dropped (both groups loaded the same earlier candidates)
-  __device__ __forceinline__ void merge_from(const void* other) {
-    flush();
-    const int lane = lane_id();
-    const int row0 = row - lane;
-    const float* OV = static_cast<const float*>(other);
-    const int* OC = reinterpret_cast<const int*>(OV + ROWS * LS);
-    float* keep_pub = pub_own;
-    pub_own = nullptr;
-    for (int j = 0; j < 32; ++j) {
-      const int r = row0 + j;
-      const int er0 = __shfl_sync(FULL, ex_r0, j), er1 = __shfl_sync(FULL, ex_r1, j);
-      const int eo0 = __shfl_sync(FULL, ex_o0, j), eo1 = __shfl_sync(FULL, ex_o1, j);
-      float a, b;
-      int ac, bcl;
-      load_list(r, a, ac, b, bcl);
-      float x = OV[r * LS + lane], y = 32 + lane < KH ? OV[r * LS + 32 + lane] : F_INF;
-      int xc = OC[r * LS + lane], yc = 32 + lane < KH ? OC[r * LS + 32 + lane] : -1;
-      auto loaded = [&](int c) { return (c >= er0 && c < er1) || (c >= eo0 && c < eo1); };
-      if (loaded(xc)) { x = F_INF; xc = -1; }
-      if (loaded(yc)) { y = F_INF; yc = -1; }
-      // the partner's list with holes: sort it again (64 = two 32-sorts and a merge)
-      sort32(x, xc);
-      sort32(y, yc);
-      {
-        const float ry = __shfl_sync(FULL, y, 31 - lane);
-        const int ryc = __shfl_sync(FULL, yc, 31 - lane);
-        float lo = x, hi = ry;
-        int loc = xc, hic = ryc;
-        if (ry < x) { lo = ry; loc = ryc; hi = x; hic = xc; }
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-          cx(lo, loc, s, (lane & s) == 0);
-          cx(hi, hic, s, (lane & s) == 0);
-        }
-        x = lo; xc = loc; y = hi; yc = hic;
-      }
-      // half-cleaner of (own ascending, partner ascending reversed): slot p meets partner 63-p
-      const float ry = __shfl_sync(FULL, y, 31 - lane), rx = __shfl_sync(FULL, x, 31 - lane);
-      const int ryc = __shfl_sync(FULL, yc, 31 - lane), rxc = __shfl_sync(FULL, xc, 31 - lane);
-      if (ry < a) { a = ry; ac = ryc; }
-      if (rx < b) { b = rx; bcl = rxc; }
-      merge64(a, ac, b, bcl);
-      store_list(r, a, ac, b, bcl);
-      const float t = kth(a, b);
-      if (lane == j) thr = t;
-    }
-    pub_own = keep_pub;
-    thr_f = fminf(thr, seed);
-  }
-
-  // warp-collective: RowTopK::finish_partial (flushes first)
-  __device__ __forceinline__ void finish_partial(int2* part, float* part_thr, int64_t part_row0,
-                                                 const int32_t* __restrict__ perm, int nvalid_rows,
-                                                 int kout) {
-    flush();
-    __syncwarp();
-    const int lane = lane_id();
-    const int row0 = row - lane;
-    for (int r = 0; r < nvalid_rows; ++r) {
-      const int rr = row0 + r;
-      const float sd = __shfl_sync(FULL, seed, r);
-      int2* out = part + (part_row0 + r) * kout;
-      for (int s = lane; s < kout; s += 32) {
-        const int c = lc[rr * LS + s];
-        out[s] = make_int2(__float_as_int(lv[rr * LS + s]), c >= 0 ? perm[c] : -1);
-      }
-      const float th = __shfl_sync(FULL, thr, r);
-      if (lane == 0) part_thr[part_row0 + r] = fminf(th, sd);
-    }
-    __syncwarp();
-  }
-
-  // warp-collective: RowTopK::finish (flushes first)
-  __device__ __forceinline__ void finish(int* out_idx, float* out_thr, int out_stride,
-                                         const int32_t* __restrict__ perm,
-                                         const int32_t* __restrict__ qmap, int64_t first_row,
-                                         int nvalid_rows, int kout, float* out_val = nullptr) {
-    flush();
-    __syncwarp();
-    const int lane = lane_id();
-    const int row0 = row - lane;
-    int64_t my_orow = 0;
-    if (lane < nvalid_rows)
-      my_orow = perm[qmap ? int64_t(qmap[first_row + lane]) : first_row + lane];
-    for (int r = 0; r < nvalid_rows; ++r) {
-      const int rr = row0 + r;
-      const int64_t orow = __shfl_sync(FULL, my_orow, r);
-      const float sd = __shfl_sync(FULL, seed, r);
-      for (int s = lane; s < kout; s += 32) {
-        const int c = lc[rr * LS + s];
-        out_idx[orow * out_stride + s] = c >= 0 ? perm[c] : -1;
-        if (out_val) out_val[orow * out_stride + s] = lv[rr * LS + s];
-      }
-      const float th = __shfl_sync(FULL, thr, r);
-      if (lane == 0) out_thr[orow] = fminf(th, sd);
-    }
-    __syncwarp();
-  }
-};
-
 }  // namespace msc

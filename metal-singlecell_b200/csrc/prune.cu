@@ -70,24 +70,46 @@ __global__ void row_radius_kernel(const int32_t* __restrict__ perm, int64_t npac
   }
 }
 
-// mean of the finite R of every sample (one block per sample, fixed summation order)
-__global__ void sample_mean_kernel(const SegDesc* __restrict__ seg, const double* __restrict__ rpos,
-                                   double* __restrict__ mean_out) {
+// mean of the finite R of every sample, in two steps with a fixed summation order: MEAN_CHUNKS
+// blocks per sample (grid y = sample) each sum a fixed slice, then one thread per sample adds the
+// slices in order
+constexpr int MEAN_CHUNKS = 64;
+__global__ void sample_mean_partial_kernel(const SegDesc* __restrict__ seg, int nseg,
+                                           const double* __restrict__ rpos,
+                                           double2* __restrict__ part) {
   __shared__ double ssum[PR_T / 32], scnt[PR_T / 32];
-  const SegDesc s = seg[blockIdx.x];
-  double sum = 0.0, cnt = 0.0;
-  for (int64_t j = threadIdx.x; j < s.n; j += blockDim.x) {
-    const double r = rpos[s.poff + j];
-    if (r < 1e300) { sum += r; cnt += 1.0; }
+  for (int sidx = blockIdx.y; sidx < nseg; sidx += gridDim.y) {
+    const SegDesc s = seg[sidx];
+    const int64_t per = (s.n + MEAN_CHUNKS - 1) / MEAN_CHUNKS;
+    const int64_t j0 = int64_t(blockIdx.x) * per, j1 = min64(s.n, j0 + per);
+    double sum = 0.0, cnt = 0.0;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      const double r = rpos[s.poff + j];
+      if (r < 1e300) { sum += r; cnt += 1.0; }
+    }
+    sum = warp_sum_d(sum);
+    cnt = warp_sum_d(cnt);
+    __syncthreads();
+    if (lane_id() == 0) { ssum[warp_id()] = sum; scnt[warp_id()] = cnt; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) { a += ssum[w]; b += scnt[w]; }
+      part[int64_t(sidx) * MEAN_CHUNKS + blockIdx.x] = make_double2(a, b);
+    }
   }
-  sum = warp_sum_d(sum);
-  cnt = warp_sum_d(cnt);
-  if (lane_id() == 0) { ssum[warp_id()] = sum; scnt[warp_id()] = cnt; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+}
+__global__ void sample_mean_final_kernel(const double2* __restrict__ part, int nseg,
+                                         double* __restrict__ mean_out) {
+  for (int sidx = blockIdx.x * blockDim.x + threadIdx.x; sidx < nseg;
+       sidx += gridDim.x * blockDim.x) {
     double a = 0.0, b = 0.0;
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) { a += ssum[w]; b += scnt[w]; }
-    mean_out[blockIdx.x] = b > 0.0 ? a / b : __longlong_as_double(0x7ff0000000000000ll);
+    for (int c = 0; c < MEAN_CHUNKS; ++c) {
+      const double2 v = part[int64_t(sidx) * MEAN_CHUNKS + c];
+      a += v.x;
+      b += v.y;
+    }
+    mean_out[sidx] = b > 0.0 ? a / b : __longlong_as_double(0x7ff0000000000000ll);
   }
 }
 
@@ -722,6 +744,7 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.rpos = c.take<double>(npacked);
   w.rpos2 = c.take<double>(npacked);
   w.mean = c.take<double>(nseg);
+  w.mean_part = c.take<double2>(size_t(nseg) * MEAN_CHUNKS);
   const int64_t nq = npacked / QTILE, nk = npacked / 256, ns = npacked / SUB;
   const int dp = int(round_up(d, 4));
   w.qc = c.take<float>(size_t(nq) * dp);
@@ -761,7 +784,10 @@ int launch_prune_partition(const float* X, int d, const SegDesc* seg, int nseg, 
   const int grid = grid_for(npacked);
   row_radius_kernel<<<grid, PR_T, 0, st>>>(perm, npacked, cand_thr, qs, km, prec, kmma, d, w.rpos);
   MSC_LAUNCH_CHECK();
-  sample_mean_kernel<<<nseg, PR_T, 0, st>>>(seg, w.rpos, w.mean);
+  sample_mean_partial_kernel<<<dim3(MEAN_CHUNKS, std::min(nseg, 65535)), PR_T, 0, st>>>(
+      seg, nseg, w.rpos, w.mean_part);
+  MSC_LAUNCH_CHECK();
+  sample_mean_final_kernel<<<(nseg + 127) / 128, 128, 0, st>>>(w.mean_part, nseg, w.mean);
   MSC_LAUNCH_CHECK();
   double factor = OUTLIER_FACTOR;
   if (const char* env = std::getenv("MSC_B200_OUTLIER_FACTOR")) {
