@@ -312,7 +312,11 @@ int order_levels(const Problem& P, bool tc) {
   if (env && *env == '0') return 0;
   int l = 0;
   while ((int64_t(ORDER_LEAF) << l) < P.max_seg) ++l;
-  return std::min(28, l + 4);
+  // uneven 2-means splits leave some nodes above the leaf size after l levels; four more levels
+  // split them (MSC_B200_ORDER_EXTRA overrides the four: tuning)
+  int extra = 4;
+  if (const char* e = std::getenv("MSC_B200_ORDER_EXTRA")) extra = std::max(0, std::atoi(e));
+  return std::min(28, l + extra);
 }
 
 int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {

@@ -1,15 +1,16 @@
 """Continuous-batching request loop for neighbour-graph jobs.
 
-Requests (an embedding plus n_neighbors / metric / method) arrive at any time.  A single scheduler
-thread admits them as soon as an execution slot is free and their device memory fits the HBM
-budget.  Admitted requests run on their own CUDA streams, so the work of requests that arrive
+Requests (an embedding plus n_neighbors / metric / method) arrive at any time.  A scheduler
+thread admits them, in arrival order, as soon as an execution slot is free and their device memory
+fits the HBM budget; each slot's worker thread enqueues and completes its request.  Admitted requests run on their own CUDA streams, so the work of requests that arrive
 while others are on the GPU overlaps on the device: small graphs share the SMs, and a large one
 yields slots as its neighbours finish.  Embeddings are uploaded once and results stay in HBM as
 device CSR tensors, ready for GPU consumers; a host copy is optional.
 
 Every request's result is the exact graph, so it does not depend on what else was running
 (``tests/test_gpu_serve.py`` checks alone-vs-mixed equality).  ``run_trace`` replays a Poisson
-arrival trace and reports p50/p99 latency (arrival → result complete on the device) and cells/s;
+arrival trace and reports p50/p99 latency (arrival → result complete on the device and handed to
+the caller; with ``to_host``, after the host copy) and cells/s;
 ``run_offline`` pushes the same requests back to back at full concurrency, the batched-offline
 throughput that the served throughput is compared against.
 """
@@ -68,7 +69,12 @@ def request_bytes(lib, n, d, k, metric, method, precision) -> int:
 
 
 class GraphServer:
-    """Admission by HBM budget and free slots; one CUDA stream per slot."""
+    """Admission by HBM budget and free slots; one CUDA stream and one worker thread per slot.
+
+    The scheduler thread admits pending requests in arrival order and hands each to a free slot's
+    worker.  The worker enqueues the graph on its slot's stream (the library call releases the
+    GIL, so the host work of several slots runs on several cores), waits for it, checks it and
+    completes the request, then frees the slot and the bytes."""
 
     def __init__(self, hbm_budget: int, slots: int = 8, device=None, poll_s: float = 2e-4):
         torch = _torch()
@@ -77,18 +83,26 @@ class GraphServer:
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         self.budget = int(hbm_budget)
+        self.poll_s = poll_s
         self.slots = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.free_slots = collections.deque(range(slots))
         self.pending: collections.deque[Request] = collections.deque()
-        self.inflight: dict[int, tuple[Request, object, int]] = {}
+        self.inflight: dict[int, tuple[Request, int]] = {}
         self.in_use = 0
         self.lock = threading.Lock()
+        self.cv = threading.Condition(self.lock)       # pending work, freed slots, stop
         self.t0 = time.perf_counter()
         self.completed: list[Request] = []
         self._next_id = 0
         self._stop = False
         self.peak_in_use = 0
         self.peak_inflight = 0
+        self._work = [collections.deque() for _ in range(slots)]
+        self._work_cv = [threading.Condition(threading.Lock()) for _ in range(slots)]
+        self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True)
+                         for i in range(slots)]
+        for t in self._workers:
+            t.start()
         self._thread = threading.Thread(target=self._loop, daemon=True)
         self._thread.start()
 
@@ -103,17 +117,18 @@ class GraphServer:
         if isinstance(req.X, torch.Tensor) and req.X.is_cuda:
             req.ready = torch.cuda.Event()
             req.ready.record(torch.cuda.current_stream(req.X.device))
-        with self.lock:
+        with self.cv:
             req.arrival = self.now()
             req.rid = self._next_id
             self._next_id += 1
             self.pending.append(req)
+            self.cv.notify_all()
         return req
 
     def cancel(self, req: Request) -> bool:
         """Withdraw a request that has not been admitted yet: it completes at once with a
         ``CancelledError`` and never reaches the GPU.  False if it was already admitted or done."""
-        with self.lock:
+        with self.cv:
             for i, r in enumerate(self.pending):
                 if r is req:
                     del self.pending[i]
@@ -127,12 +142,20 @@ class GraphServer:
         return True
 
     def close(self):
-        self._stop = True
+        with self.cv:
+            self._stop = True
+            self.cv.notify_all()
         self._thread.join()
+        for i, cv in enumerate(self._work_cv):
+            with cv:
+                self._work[i].append(None)             # the worker's sentinel
+                cv.notify()
+        for t in self._workers:
+            t.join()
 
-    # -- scheduler ------------------------------------------------------------------------------
+    # -- workers ------------------------------------------------------------------------------
 
-    def _start(self, req: Request, slot: int, need: int):
+    def _start(self, req: Request, slot: int):
         torch = self.torch
         st = self.slots[slot]
         from .neighbors import neighbors_device
@@ -155,75 +178,97 @@ class GraphServer:
             ev = torch.cuda.Event()
             ev.record(st)
         req.result = res
-        req.admitted = self.now()
-        self.inflight[slot] = (req, ev, need)
+        return ev
 
-    def _finish(self, slot: int):
-        req, ev, need = self.inflight.pop(slot)
-        req.done = self.now()
-        try:
-            stats = req.result["stats"].cpu().numpy()
-            _lib.check_stats(stats)
-            if req.to_host:
-                from .neighbors import graph_to_host
-                req.result["host"] = graph_to_host(req.result, req.n, req.n_neighbors)
-        except BaseException as e:      # report per request, keep serving
-            req.error = e
-        self.in_use -= need
-        self.free_slots.append(slot)
-        self.completed.append(req)
+    def _wait(self, ev):
+        if hasattr(ev, "synchronize"):
+            ev.synchronize()                          # blocks without holding the GIL
+            return
+        while not ev.query():
+            time.sleep(self.poll_s)
+
+    def _release(self, req: Request, slot: int, need: int):
+        with self.cv:
+            self.inflight.pop(slot, None)
+            self.in_use -= need
+            self.free_slots.append(slot)
+            self.completed.append(req)
+            self.cv.notify_all()
         req.event.set()
 
-    def _loop(self):
+    def _worker(self, slot: int):
         torch = self.torch
         torch.cuda.set_device(self.device)
-        while not self._stop or self.pending or self.inflight:
-            progressed = False
-            for slot in list(self.inflight):
-                if self.inflight[slot][1].query():
-                    self._finish(slot)
-                    progressed = True
-            while self.free_slots:
-                with self.lock:
-                    if not self.pending:
+        q, cv = self._work[slot], self._work_cv[slot]
+        while True:
+            with cv:
+                while not q:
+                    cv.wait()
+                item = q.popleft()
+            if item is None:
+                return
+            req, need = item
+            try:
+                ev = self._start(req, slot)
+            except BaseException as e:               # e.g. an allocation failure at start
+                req.error = e
+                req.done = self.now()
+                self._release(req, slot, need)
+                continue
+            self._wait(ev)
+            req.done = self.now()
+            try:
+                stats = req.result["stats"].cpu().numpy()
+                _lib.check_stats(stats)
+                if req.to_host:
+                    from .neighbors import graph_to_host
+                    req.result["host"] = graph_to_host(req.result, req.n, req.n_neighbors)
+                    req.done = self.now()
+            except BaseException as e:                # report per request, keep serving
+                req.error = e
+            self._release(req, slot, need)
+
+    # -- scheduler ------------------------------------------------------------------------------
+
+    def _loop(self):
+        while True:
+            with self.cv:
+                while True:
+                    if self._stop and not self.pending and not self.inflight:
+                        return
+                    if self.pending and self.free_slots:
                         break
-                    req = self.pending[0]
-                need = request_bytes(self.lib, req.n, int(req.X.shape[1]), req.n_neighbors,
-                                     req.metric, req.method, req.precision)
+                    self.cv.wait(0.05)
+                req = self.pending[0]
+            need = request_bytes(self.lib, req.n, int(req.X.shape[1]), req.n_neighbors,
+                                 req.metric, req.method, req.precision)
+            with self.cv:
+                if not self.pending or self.pending[0] is not req:
+                    continue                           # cancelled meanwhile
                 if need < 0 or need > self.budget:
-                    with self.lock:
-                        if not self.pending or self.pending[0] is not req:
-                            continue           # cancelled meanwhile
-                        self.pending.popleft()
-                        req.error = ValueError(f"request needs {need} bytes > budget "
-                                               f"{self.budget}")
-                        req.done = self.now()
-                        self.completed.append(req)
-                    req.event.set()
-                    continue
-                if self.in_use + need > self.budget:
-                    break                      # wait for memory to free up (FIFO admission)
-                with self.lock:
-                    if not self.pending or self.pending[0] is not req:
-                        continue               # cancelled meanwhile
                     self.pending.popleft()
-                slot = self.free_slots.popleft()
-                self.in_use += need
-                self.peak_in_use = max(self.peak_in_use, self.in_use)
-                try:
-                    self._start(req, slot, need)
-                except BaseException as e:
-                    self.in_use -= need
-                    self.free_slots.append(slot)
-                    req.error = e
+                    req.error = ValueError(f"request needs {need} bytes > budget {self.budget}")
                     req.done = self.now()
                     self.completed.append(req)
                     req.event.set()
                     continue
+                while self.in_use + need > self.budget or not self.free_slots:
+                    self.cv.wait(0.05)                 # FIFO: the head waits for memory
+                    if not self.pending or self.pending[0] is not req:
+                        break
+                if not self.pending or self.pending[0] is not req:
+                    continue
+                self.pending.popleft()
+                slot = self.free_slots.popleft()
+                self.in_use += need
+                self.peak_in_use = max(self.peak_in_use, self.in_use)
+                self.inflight[slot] = (req, need)
                 self.peak_inflight = max(self.peak_inflight, len(self.inflight))
-                progressed = True
-            if not progressed:
-                time.sleep(2e-4)
+                req.admitted = self.now()
+            cv = self._work_cv[slot]
+            with cv:
+                self._work[slot].append((req, need))
+                cv.notify()
 
 
 def _percentile(v, q):
