@@ -179,13 +179,20 @@ rev_fill_kernel(int mode, const int32_t* __restrict__ idx, const float* __restri
   });
 }
 
-// value of a merged entry (row i, column c); a/b = forward/reverse record values
+// value of a merged entry (row i, column c); a/b = forward/reverse record values.  The gauss
+// kernel is kept out of line: the umap merge paths stay small
+__device__ __noinline__ float gauss_pair(int64_t i, uint32_t c, bool has_a, float a, float b,
+                                         const double* __restrict__ sig2);
 __device__ __forceinline__ float pair_value(int mode, int64_t i, uint32_t c, bool has_a, float a,
                                             bool has_b, float b, const double* __restrict__ sig2) {
   if (mode == 0) {
     if (has_a && has_b) return __fsub_rn(__fadd_rn(a, b), __fmul_rn(a, b));
     return has_a ? a : b;
   }
+  return gauss_pair(i, c, has_a, a, b, sig2);
+}
+__device__ __noinline__ float gauss_pair(int64_t i, uint32_t c, bool has_a, float a, float b,
+                                         const double* __restrict__ sig2) {
   const float dd = has_a ? a : b;                 // the pair's distance (same from both ends)
   const double d2 = double(dd) * double(dd);
   const double si2 = sig2[i], sc2 = sig2[c];

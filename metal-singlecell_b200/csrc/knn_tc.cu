@@ -1251,12 +1251,13 @@ TcConfig tc_default_config(int prec, int d, int kprime) {
   // Single CTAs first: CTA pairs halve the key bytes per SM and double the K-atom stages that
   // fit, but measured slower at 1.3M × 50 (1057 vs 819 ms for the candidate stage), so they are
   // taken only when nothing else fits.  N=256 key tiles (one MMA costs the same ~186 cycles at
-  // N = 64..256, so only N=256 reaches the tensor peak); eight epilogue warps (a warp's TMEM reads
-  // are serialised, so read bandwidth grows with the number of reading warps), else four; then
-  // the deepest K-atom pipeline that fits
+  // N = 64..256, so only N=256 reaches the tensor peak); four epilogue warps, one list per row
+  // (measured at 1.3M × 50: main scan 55.1 ms and near pass 3.9 ms, against 56.9 and 5.0 with
+  // eight warps whose two column halves each keep a list), else eight; then the deepest K-atom
+  // pipeline that fits
   for (int pair : {0, 1})
     for (int bn : {256, 128, 64, 32})
-      for (int epi : {8, 4})
+      for (int epi : {4, 8})
         for (int stages = 8; stages >= 2; --stages) {
           TcConfig c{bn, stages, kpl, 16, epi, pair};
           if (tc_config_ok(c, L.kp, kprime)) return c;

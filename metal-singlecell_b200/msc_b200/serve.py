@@ -97,6 +97,7 @@ class GraphServer:
         self._stop = False
         self.peak_in_use = 0
         self.peak_inflight = 0
+        self._pinned = [None] * slots
         self._work = [collections.deque() for _ in range(slots)]
         self._work_cv = [threading.Condition(threading.Lock()) for _ in range(slots)]
         self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True)
@@ -169,7 +170,7 @@ class GraphServer:
                 X.record_stream(st)                   # its memory stays live for this stream
                 Xd = X if X.device == self.device else X.to(self.device)
             else:
-                Xd = X.to(self.device, non_blocking=True)
+                Xd = self._upload(X, slot)
             res = neighbors_device(Xd, req.n_neighbors, metric=req.metric, method=req.method,
                                    precision=req.precision)
             res["X"] = Xd
@@ -179,6 +180,22 @@ class GraphServer:
             ev.record(st)
         req.result = res
         return ev
+
+    def _upload(self, X, slot: int):
+        """Host embedding -> device on the slot's stream through the slot's pinned buffer (grown
+        on demand, reused: the slot's previous request finished before this one started), so the
+        copy is asynchronous instead of a blocking copy from pageable memory."""
+        torch = self.torch
+        if not hasattr(torch, "empty") or not hasattr(X, "numel"):
+            return X.to(self.device, non_blocking=True)          # stand-ins in host-only tests
+        buf = self._pinned[slot]
+        nbytes = X.numel() * 4
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8).pin_memory()
+            self._pinned[slot] = buf
+        staged = buf[:nbytes].view(torch.float32).view(X.shape)
+        staged.copy_(X)
+        return staged.to(self.device, non_blocking=True)
 
     def _wait(self, ev):
         if hasattr(ev, "synchronize"):
