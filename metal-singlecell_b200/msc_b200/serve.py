@@ -68,6 +68,13 @@ def request_bytes(lib, n, d, k, metric, method, precision) -> int:
     return int(ws + n * d * 4 + outs)
 
 
+# pinned staging buffers of closed servers, handed to the next server of this process
+# (page-locking host memory costs milliseconds per call; a new server would otherwise pay it
+# again for every slot); a buffer belongs to one slot of one server at a time
+_PINNED_POOL: list = []
+_PINNED_LOCK = threading.Lock()
+
+
 class GraphServer:
     """Admission by HBM budget and free slots; one CUDA stream and one worker thread per slot.
 
@@ -97,7 +104,9 @@ class GraphServer:
         self._stop = False
         self.peak_in_use = 0
         self.peak_inflight = 0
-        self._pinned = [None] * slots
+        with _PINNED_LOCK:                            # buffers of earlier servers, largest first
+            _PINNED_POOL.sort(key=lambda b: b.numel())
+            self._pinned = [_PINNED_POOL.pop() if _PINNED_POOL else None for _ in range(slots)]
         self._work = [collections.deque() for _ in range(slots)]
         self._work_cv = [threading.Condition(threading.Lock()) for _ in range(slots)]
         self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True)
@@ -153,6 +162,9 @@ class GraphServer:
                 cv.notify()
         for t in self._workers:
             t.join()
+        with _PINNED_LOCK:                            # hand the staging buffers on
+            _PINNED_POOL.extend(b for b in self._pinned if b is not None)
+            self._pinned = [None] * len(self._pinned)
 
     # -- workers ------------------------------------------------------------------------------
 
@@ -307,6 +319,8 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
         r.event.wait()
     srv.close()
     ok = [r for r in reqs if r.error is None]
+    errors = [f"request {r.rid}: {type(r.error).__name__}: {str(r.error)[:300]}"
+              for r in reqs if r.error is not None][:5]
     lat = [r.latency * 1e3 for r in ok]
     makespan = max(r.done for r in reqs) - t_start
     cells = sum(r.n for r in ok)
@@ -314,7 +328,8 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
             "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
             "mean_ms": float(np.mean(lat)) if lat else float("nan"),
             "cells_per_s": cells / makespan, "makespan_s": makespan,
-            "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_in_use}
+            "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_in_use,
+            "errors": errors}
 
 
 def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None) -> dict:
