@@ -109,6 +109,17 @@ int num_sms() {
   return v;
 }
 
+cudaError_t raise_smem_cap_fn(const void* func, size_t bytes) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, func);
+  if (e != cudaSuccess) return e;
+  if (fa.maxDynamicSharedSizeBytes >= 0 && size_t(fa.maxDynamicSharedSizeBytes) >= bytes)
+    return cudaSuccess;
+  return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
 namespace {
 
 constexpr int COLMEAN_NB = 256;

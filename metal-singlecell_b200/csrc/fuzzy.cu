@@ -513,8 +513,7 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
                                              w.big, w.nbig);
   MSC_LAUNCH_CHECK();
   const size_t bsm = size_t(BLK_SMEM_MAX) * sizeof(int2);
-  MSC_CUDA_TRY(cudaFuncSetAttribute(merge_block_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(bsm)));
+  MSC_CUDA_TRY(raise_smem_cap(merge_block_kernel, bsm));
   merge_block_kernel<<<sms, 1024, bsm, st>>>(mode, k, w.big, w.nbig, w.rptr, w.rec, sig2, w.uniq);
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl<int32_t>(w.uniq, n, indptr, w.scan, st));

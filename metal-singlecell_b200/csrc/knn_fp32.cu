@@ -235,8 +235,7 @@ int launch_fp32_t(const float* A32, const float* sq32, int d, int dpad, const Wo
   (void)d;
   const size_t smem = FpSmem<KPL, CB>::bytes(dpad);
   auto kern = knn_fp32_kernel<KPL, CB>;
-  MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem)));
+  MSC_CUDA_TRY(raise_smem_cap(kern, smem));
   int grid = int(std::min<int64_t>(n_items, num_sms()));
   MSC_CUDA_TRY(cudaMemsetAsync(pr.counter, 0, sizeof(int32_t), st));
   kern<<<std::max(grid, 1), F_THREADS, smem, st>>>(A32, sq32, dpad, items, perm, ctl, kprime,

@@ -1105,15 +1105,16 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiledFn get_encode() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  // looked up once; the initialisation of a function-local static is thread-safe
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+      return reinterpret_cast<EncodeTiledFn>(p);
+    return nullptr;
+  }();
   return fn;
 }
 
@@ -1157,7 +1158,7 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   const int brows = PAIR ? P.bn / 2 : P.bn;
   const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
   auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
-  MSC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  MSC_CUDA_TRY(raise_smem_cap(kern, smem));
   if (NEPI == 8 && kRegSplit) {
     // the register split needs the block's pool at REG_LAUNCH registers per thread
     cudaFuncAttributes fa{};

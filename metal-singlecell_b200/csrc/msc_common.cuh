@@ -151,4 +151,15 @@ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 // number of SMs of the current device (cached per device)
 int num_sms();
 
+// Raise a kernel's dynamic shared-memory cap (cudaFuncAttributeMaxDynamicSharedMemorySize) to at
+// least `bytes`, never lowering it.  The attribute is per function and process-wide: when host
+// threads launch the same kernel with different sizes, one thread setting a smaller cap between
+// another's set and launch makes that launch fail ("too many resources requested").  Raising only,
+// under one lock, leaves every cap at the largest size any caller asked for.
+cudaError_t raise_smem_cap_fn(const void* func, size_t bytes);
+template <typename K>
+inline cudaError_t raise_smem_cap(K* kern, size_t bytes) {
+  return raise_smem_cap_fn(reinterpret_cast<const void*>(kern), bytes);
+}
+
 }  // namespace msc

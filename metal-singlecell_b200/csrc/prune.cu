@@ -869,8 +869,7 @@ int launch_visit_order(const WorkItem* items, int64_t n_items, int bn, int d, in
   visit_count_kernel<<<cgrid, PR_T, 0, st>>>(w.mask, n_items, words, w.vcnt);
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl_i32(w.vcnt, n_items, w.voff, w.vscan, st));
-  MSC_CUDA_TRY(cudaFuncSetAttribute(visit_order_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  MSC_CUDA_TRY(raise_smem_cap(visit_order_kernel, smem));
   const int ogrid = int(std::max<int64_t>(1, std::min<int64_t>(n_items, int64_t(num_sms()) * 4)));
   visit_order_kernel<<<ogrid, VO_T, smem, st>>>(items, n_items, bn, d, dp, ctl, prec, w.qc, w.qr,
                                                 w.kc, w.kr, w.mask, words, w.voff, w.vcap,

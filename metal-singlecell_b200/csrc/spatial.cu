@@ -568,20 +568,10 @@ SpWs carve(Carver& c, int64_t n) {
   return w;
 }
 
-int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-      sms = 148;
-  }
-  return sms;
-}
 
 unsigned flat_grid(int64_t items, int threads) {
   const int64_t b = (items + threads - 1) / threads;
-  return unsigned(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(sm_count()) * 16)));
+  return unsigned(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(num_sms()) * 16)));
 }
 
 // The grid: bounding box, plan, binning, cell-ordered points, chunks.  The cell table is sized
@@ -619,7 +609,7 @@ unsigned search_grid(int64_t n) {
   // persistent: enough warps for every chunk of a uniform layout, at most 8 blocks per SM
   const int64_t warps = n / 16 + 1;
   const int64_t blocks = (warps + SP_W - 1) / SP_W;
-  return unsigned(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(sm_count()) * 8)));
+  return unsigned(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(num_sms()) * 8)));
 }
 
 template <int K>

@@ -207,8 +207,7 @@ int launch_smooth_knn(const float* dist, int64_t n, int k, float local_connectiv
   MSC_LAUNCH_CHECK();
   const size_t smem = size_t(SK_THREADS) * k * sizeof(float);
   if (smem > 48 * 1024)
-    MSC_CUDA_TRY(cudaFuncSetAttribute(smooth_knn_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    MSC_CUDA_TRY(raise_smem_cap(smooth_knn_kernel, smem));
   smooth_knn_kernel<<<unsigned(ceil_div(n, SK_THREADS)), SK_THREADS, smem, st>>>(
       dist, n, k, local_connectivity, gsum, sigma, rho);
   MSC_LAUNCH_CHECK();

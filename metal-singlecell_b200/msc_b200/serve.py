@@ -188,7 +188,9 @@ class GraphServer:
             res["X"] = Xd
             if req.to_host:
                 res["host_stats"] = res["stats"].to("cpu", non_blocking=True)
-            ev = torch.cuda.Event()
+            # a blocking-sync event: the slot's worker sleeps while it waits instead of spinning
+            # on a host core (with a spin per slot the workers starve the threads enqueuing work)
+            ev = torch.cuda.Event(blocking=True)
             ev.record(st)
         req.result = res
         return ev
@@ -203,7 +205,9 @@ class GraphServer:
         buf = self._pinned[slot]
         nbytes = X.numel() * 4
         if buf is None or buf.numel() < nbytes:
-            buf = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8).pin_memory()
+            # grown to a power of two, so that a slot re-pins only a few times as sizes vary
+            size = 1 << max(20, (nbytes - 1).bit_length())
+            buf = torch.empty(size, dtype=torch.uint8).pin_memory()
             self._pinned[slot] = buf
         staged = buf[:nbytes].view(torch.float32).view(X.shape)
         staged.copy_(X)
@@ -322,11 +326,15 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
     errors = [f"request {r.rid}: {type(r.error).__name__}: {str(r.error)[:300]}"
               for r in reqs if r.error is not None][:5]
     lat = [r.latency * 1e3 for r in ok]
+    queue = [(r.admitted - r.arrival) * 1e3 for r in ok]        # waiting for a slot / memory
+    service = [(r.done - r.admitted) * 1e3 for r in ok]         # admitted -> handed back
     makespan = max(r.done for r in reqs) - t_start
     cells = sum(r.n for r in ok)
     return {"requests": len(reqs), "failed": len(reqs) - len(ok),
             "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
             "mean_ms": float(np.mean(lat)) if lat else float("nan"),
+            "queue_p50_ms": _percentile(queue, 50), "queue_p99_ms": _percentile(queue, 99),
+            "service_p50_ms": _percentile(service, 50), "service_p99_ms": _percentile(service, 99),
             "cells_per_s": cells / makespan, "makespan_s": makespan,
             "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_in_use,
             "errors": errors}

@@ -66,3 +66,44 @@ def test_admission_respects_budget():
     too_big = serve.Request(X=synth.gaussian_mixture(30000, 50, 5, seed=9), n_neighbors=15)
     rep2 = serve.run_trace([too_big], [0.0], 1 << 20, slots=2)
     assert rep2["failed"] == 1 and isinstance(too_big.error, ValueError)
+
+
+def test_concurrent_launches_of_different_widths():
+    """Host threads on their own streams launch graphs of different widths d (hence different
+    shared-memory sizes of the same kernels) at once.  A kernel's shared-memory cap is one
+    process-wide attribute: a thread lowering it between another thread's set and launch made
+    that launch fail.  Every call must succeed and match its single-thread result."""
+    import threading
+    import torch
+    shapes = [(700, 30, 10), (900, 50, 15), (800, 100, 30), (600, 50, 10)]
+    Xs = [torch.from_numpy(synth.gaussian_mixture(n, d, 4, seed=40 + i)).cuda()
+          for i, (n, d, _) in enumerate(shapes)]
+    alone = []
+    for X, (_, _, k) in zip(Xs, shapes):
+        r = nbm.neighbors_device(X, k)
+        torch.cuda.synchronize()
+        alone.append((r["knn_idx"].cpu(), r["knn_dist"].cpu()))
+    errors, mismatches = [], []
+
+    def worker(t):
+        st = torch.cuda.Stream()
+        ws = nbm.Workspace(torch.device("cuda", 0))
+        try:
+            for it in range(24):
+                j = (t + it) % len(shapes)
+                with torch.cuda.stream(st):
+                    r = nbm.neighbors_device(Xs[j], shapes[j][2], workspace=ws)
+                st.synchronize()
+                if not (torch.equal(r["knn_idx"].cpu(), alone[j][0])
+                        and torch.equal(r["knn_dist"].cpu(), alone[j][1])):
+                    mismatches.append((t, it, j))
+        except Exception as e:                      # noqa: BLE001 (reported below)
+            errors.append(f"thread {t}: {type(e).__name__}: {e}")
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(8)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors[:3]
+    assert not mismatches, mismatches[:5]

@@ -33,7 +33,7 @@ class _Event:
     """Completes a fixed time after it is recorded (the fake request's device time)."""
     work_s = 0.02
 
-    def __init__(self):
+    def __init__(self, **flags):
         self.t = None
 
     def record(self, stream):
