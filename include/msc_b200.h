@@ -142,10 +142,11 @@ int msc_knn(const float* X_dev, int64_t n, int32_t d, int32_t k, int32_t metric,
  *   msc_batched_prepare  writes the sample table into the workspace and waits for that copy;
  *   msc_batched_knn      only enqueues kernels (capturable in a CUDA graph); call it with the
  *                        same offsets / shapes as the prepare call.
- * tile_config: 0 = automatic, else bn | stages<<12 | cb<<20 | epi8<<27 | pair<<28 (key tile
- * rows, pipeline depth in 64-element K atoms, selector buffer, eight instead of four epilogue
- * warps, two-CTA clusters on 256-row query tiles) as chosen by the Python autotuner.  With 0, the environment variable MSC_B200_TILE_CONFIG (same
- * encoding) overrides the automatic choice for every entry point. */
+ * tile_config: 0 = automatic, else bn | stages<<12 | cb<<20 | epi8<<27 | pair<<28 | dual<<29
+ * (key tile rows, pipeline depth in 64-element K atoms, selector buffer, eight instead of four
+ * epilogue warps, two-CTA clusters on 256-row query tiles, two CTAs per SM with one accumulator
+ * each) as chosen by the Python autotuner.  With 0, the environment variable
+ * MSC_B200_TILE_CONFIG (same encoding) overrides the automatic choice for every entry point. */
 size_t msc_batched_workspace_bytes(const int64_t* offsets_host, int32_t n_samples, int32_t d,
                                    int32_t k, int32_t metric, int32_t precision, int32_t kprime);
 int msc_batched_prepare(const int64_t* offsets_host, int32_t n_samples, int32_t d, int32_t k,

@@ -339,10 +339,10 @@ int decode_tile_config(int32_t code, const Problem& P, TcConfig& cfg) {
   }
   if (code == 0) return MSC_OK;
   TcConfig c{code & 0xfff, (code >> 12) & 0xff, list_slots(P.kprime), (code >> 20) & 0x7f,
-             (code >> 27) & 1 ? 8 : 4, (code >> 28) & 1};
+             (code >> 27) & 1 ? 8 : 4, (code >> 28) & 1, (code >> 29) & 1 ? 2 : 1};
   if (!tc_config_ok(c, P.L.kp, P.kprime)) {
-    set_error("tile_config 0x%x (bn=%d stages=%d cb=%d epi=%d pair=%d) is not valid here", code,
-              c.bn, c.stages, c.cb, c.epi, c.pair);
+    set_error("tile_config 0x%x (bn=%d stages=%d cb=%d epi=%d pair=%d ctas=%d) is not valid here",
+              code, c.bn, c.stages, c.cb, c.epi, c.pair, c.ctas);
     return MSC_ERR_INVALID_ARG;
   }
   cfg = c;

@@ -243,6 +243,9 @@ struct TcConfig {
   int cb;        // 16 or 32; kept in the tile code for compatibility, no longer used
   int epi;       // epilogue warps: 4 (one per TMEM lane quarter) or 8 (two, splitting the columns)
   int pair;      // 1: CTA pairs (cta_group::2, M=256, each CTA stages half of every key tile)
+  // CTAs per SM: 1, or 2 (one accumulator and one query buffer each, at most 128 registers per
+  // thread), so that every scheduler runs two epilogue warps of different rows
+  int ctas = 1;
 };
 bool tc_config_ok(const TcConfig& c, int kp, int kprime);
 int list_slots(int kprime);

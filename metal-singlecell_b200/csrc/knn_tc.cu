@@ -77,6 +77,8 @@ constexpr int BM = 128;
 constexpr int ITEM_RING = 4;                        // claimed work items in flight per CTA
 constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;   // 4 s per wait
 constexpr size_t SMEM_LIMIT = 232448;               // 227 KB opt-in per block
+constexpr size_t SMEM_PER_SM = 233472;              // 228 KB per SM
+constexpr size_t SMEM_BLOCK_RESERVE = 1024;         // reserved by the system per resident block
 
 // ------------------------------------------------------------------------------------------------
 // PTX wrappers
@@ -477,13 +479,17 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
 // quarter, each filtering half of the columns into its own list; the two lists of a row share
 // their thresholds while filtering and are merged when the query tile is done).
 // PAIR: two-CTA clusters, 256-row work items (see the file comment).
-template <int KH, int NEPI, bool PAIR>
-__global__ void __launch_bounds__(128 + 32 * NEPI, 1)
+// DUAL: two CTAs per SM, each with one accumulator (the MMA of a CTA's next tile waits for its
+// epilogue to release the last one, while the other CTA's warps use the SM).
+template <int KH, int NEPI, bool PAIR, bool DUAL>
+__global__ void __launch_bounds__(128 + 32 * NEPI, DUAL ? 2 : 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const TcParams P, const WorkItem* __restrict__ items, Ctl* __restrict__ ctl,
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
   static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
+  static_assert(!DUAL || (NEPI == 4 && !PAIR), "two CTAs per SM: single CTAs, four epilogue warps");
   constexpr int NH = NEPI / 4;
+  constexpr int NACC = DUAL ? 1 : 2;                    // accumulators in TMEM
   using Sel = typename SelectorOf<KH>::type;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -523,7 +529,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   const int nunits = PAIR ? int(gridDim.x >> 1) : int(gridDim.x);
   const size_t a_bytes = size_t(P.kb) * BM * 128;
   const size_t b_bytes = size_t(brows) * 128;           // one K atom of this CTA's key rows
-  const uint32_t tmem_cols = uint32_t(2 * P.bn);
+  const uint32_t tmem_cols = uint32_t(NACC * P.bn);
   const int n_items = P.n_items_dev ? *P.n_items_dev : P.n_items;
   // the producer drives the walk from the sorted list and ends it early (single CTAs only)
   const bool ordered = !PAIR && !P.near_only && P.qmap == nullptr && P.vlist != nullptr &&
@@ -820,7 +826,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             issued = true;
             umma_commit_g<PAIR>(&acc_full[acc]);
             if (meta) mbar_arrive(&acc_full[acc]);        // releases acc_meta to the epilogue
-            if (++acc == 2) { acc = 0; accphase ^= 1; }
+            if (++acc == NACC) { acc = 0; accphase ^= 1; }
           }
           if (!ok) break;
           if (meta) {
@@ -830,7 +836,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             *reinterpret_cast<volatile int*>(&acc_meta[acc]) = -1;
             mbar_arrive(&acc_full[acc]);
             mbar_arrive(&acc_full[acc]);
-            if (++acc == 2) { acc = 0; accphase ^= 1; }
+            if (++acc == NACC) { acc = 0; accphase ^= 1; }
           }
           umma_commit_g<PAIR>(&a_empty[abuf]);
           if (++abuf == P.na) { abuf = 0; aphase ^= 1; }
@@ -917,7 +923,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           if (kt < 0) {                    // the item's walk ended: hand the turn back
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[acc]);
-            if (++acc == 2) { acc = 0; accphase ^= 1; }
+            if (++acc == NACC) { acc = 0; accphase ^= 1; }
             break;
           }
         }
@@ -974,6 +980,16 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (!cycle(c + 2, rc, ra, rb)) break;
             if (!cycle(c + 4, rb, rc, ra)) break;
           }
+        } else if constexpr (DUAL) {
+          // one chunk buffer (the register cap of two CTAs per SM): load, wait, filter; the
+          // other CTA's warp on this scheduler runs while this one waits for TMEM
+          (void)rb;
+          for (int c = 0; c < nch; ++c) {
+            tmem_ld32_async(t0 + uint32_t(c * 32), ra);
+            tmem_wait(ra);
+            if (c == nch - 1) release();
+            sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
+          }
         } else {
           tmem_ld32_async(t0, ra);
           tmem_wait(ra);
@@ -996,7 +1012,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             }
           }
         }
-        if (++acc == 2) { acc = 0; accphase ^= 1; }
+        if (++acc == NACC) { acc = 0; accphase ^= 1; }
         if (ordered) {
           // an upper bound on R over this warp's rows: thr_f (the filter threshold) bounds the
           // row's final k'-th value, roff is the fixed part; rows past the tile's end do not count
@@ -1149,15 +1165,18 @@ size_t config_smem(const TcConfig& c, int kb, int na) {
   return SIZE_MAX;
 }
 
-int pick_na(const TcConfig& c, int kb) { return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1; }
+int pick_na(const TcConfig& c, int kb) {
+  if (c.ctas == 2) return 1;
+  return config_smem(c, kb, 2) <= SMEM_LIMIT ? 2 : 1;
+}
 
-template <int KH, int NEPI, bool PAIR>
+template <int KH, int NEPI, bool PAIR, bool DUAL>
 int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
                 const WorkItem* items, Ctl* ctl, int32_t* cand_idx, float* cand_thr,
                 cudaStream_t st) {
   const int brows = PAIR ? P.bn / 2 : P.bn;
   const size_t smem = smem_plan<KH>(P.kb, brows, P.stages, P.na, NEPI / 4).total;
-  auto kern = knn_tc_kernel<KH, NEPI, PAIR>;
+  auto kern = knn_tc_kernel<KH, NEPI, PAIR, DUAL>;
   MSC_CUDA_TRY(raise_smem_cap(kern, smem));
   if (NEPI == 8 && kRegSplit) {
     // the register split needs the block's pool at REG_LAUNCH registers per thread
@@ -1170,7 +1189,7 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
     }
   }
   if (!PAIR) {
-    const int grid = std::max(1, std::min(P.n_items, num_sms()));
+    const int grid = std::max(1, std::min(P.n_items, (DUAL ? 2 : 1) * num_sms()));
     kern<<<grid, 128 + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
     MSC_LAUNCH_CHECK();
     return MSC_OK;
@@ -1194,15 +1213,15 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   return MSC_OK;
 }
 
-template <int NEPI, bool PAIR>
+template <int NEPI, bool PAIR, bool DUAL = false>
 int launch_tc_epi(const TcConfig& cfg, const TcParams& P, const CUtensorMap& ma,
                   const CUtensorMap& mb, const WorkItem* items, Ctl* ctl, int32_t* cand_idx,
                   float* cand_thr, cudaStream_t st) {
   if (cfg.kpl == 32)
-    return launch_tc_t<32, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+    return launch_tc_t<32, NEPI, PAIR, DUAL>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
   if (cfg.kpl == 48)
-    return launch_tc_t<48, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
-  return launch_tc_t<64, NEPI, PAIR>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+    return launch_tc_t<48, NEPI, PAIR, DUAL>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
+  return launch_tc_t<64, NEPI, PAIR, DUAL>(P, ma, mb, items, ctl, cand_idx, cand_thr, st);
 }
 
 }  // namespace
@@ -1233,6 +1252,15 @@ int launch_wait_selftest(uint64_t limit_ns, int32_t* out, cudaStream_t st) {
 
 bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;
+  if (c.ctas != 1 && c.ctas != 2) return false;
+  if (c.ctas == 2) {
+    // two CTAs per SM: single CTAs with four epilogue warps; both CTAs' shared memory (and the
+    // per-block reserve) within the SM's
+    if (c.pair || c.epi != 4 || c.stages < 1 || c.stages > 8) return false;
+    if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 48 && c.kpl != 64)) return false;
+    if (c.cb != 16 && c.cb != 32) return false;
+    return 2 * (config_smem(c, kp / 64, 1) + SMEM_BLOCK_RESERVE) <= SMEM_PER_SM;
+  }
   if (c.stages < 2 || c.stages > 8) return false;
   if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 48 && c.kpl != 64)) return false;
   if (c.cb != 16 && c.cb != 32) return false;
@@ -1256,6 +1284,14 @@ TcConfig tc_default_config(int prec, int d, int kprime) {
   // (measured at 1.3M × 50: main scan 55.1 ms and near pass 3.9 ms, against 56.9 and 5.0 with
   // eight warps whose two column halves each keep a list), else eight; then the deepest K-atom
   // pipeline that fits
+  {
+    const char* env = std::getenv("MSC_B200_DUAL");
+    if (env && *env == '1')
+      for (int stages = 8; stages >= 1; --stages) {
+        TcConfig c{256, stages, kpl, 16, 4, 0, 2};
+        if (tc_config_ok(c, L.kp, kprime)) return c;
+      }
+  }
   for (int pair : {0, 1})
     for (int bn : {256, 128, 64, 32})
       for (int epi : {4, 8})
@@ -1335,6 +1371,8 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
       return launch_tc_epi<8, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
     return launch_tc_epi<4, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
   }
+  if (cfg.ctas == 2)
+    return launch_tc_epi<4, false, true>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
   if (cfg.epi == 8)
     return launch_tc_epi<8, false>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);
   return launch_tc_epi<4, false>(cfg, P, ma, mb, items, ctl, cand_idx, cand_thr, st);

@@ -83,7 +83,8 @@ class GraphServer:
     GIL, so the host work of several slots runs on several cores), waits for it, checks it and
     completes the request, then frees the slot and the bytes."""
 
-    def __init__(self, hbm_budget: int, slots: int = 8, device=None, poll_s: float = 2e-4):
+    def __init__(self, hbm_budget: int, slots: int = 8, device=None, poll_s: float = 2e-4,
+                 pinned_bytes: int = 0):
         torch = _torch()
         self.torch = torch
         self.lib = _lib.load()
@@ -107,6 +108,13 @@ class GraphServer:
         with _PINNED_LOCK:                            # buffers of earlier servers, largest first
             _PINNED_POOL.sort(key=lambda b: b.numel())
             self._pinned = [_PINNED_POOL.pop() if _PINNED_POOL else None for _ in range(slots)]
+        if pinned_bytes > 0 and hasattr(torch, "empty"):
+            # staging for host embeddings up to pinned_bytes, page-locked now rather than while
+            # requests wait
+            size = 1 << max(20, (int(pinned_bytes) - 1).bit_length())
+            for i, b in enumerate(self._pinned):
+                if b is None or b.numel() < size:
+                    self._pinned[i] = torch.empty(size, dtype=torch.uint8).pin_memory()
         self._work = [collections.deque() for _ in range(slots)]
         self._work_cv = [threading.Condition(threading.Lock()) for _ in range(slots)]
         self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True)
@@ -309,10 +317,11 @@ def _percentile(v, q):
 
 
 def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots: int = 8,
-              device=None) -> dict:
+              device=None, pinned_bytes: int = 0) -> dict:
     """Submit ``reqs`` at ``arrivals`` (seconds from start); wait for all; report latency and
-    throughput."""
-    srv = GraphServer(hbm_budget, slots, device)
+    throughput.  ``pinned_bytes``: page-lock each slot's staging buffer for host embeddings of up
+    to that size before the first arrival."""
+    srv = GraphServer(hbm_budget, slots, device, pinned_bytes=pinned_bytes)
     t_start = srv.now()
     for r, a in zip(reqs, arrivals):
         delay = a - (srv.now() - t_start)
@@ -340,6 +349,7 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
             "errors": errors}
 
 
-def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None) -> dict:
+def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None,
+                pinned_bytes: int = 0) -> dict:
     """All requests available at t=0: the batched-offline throughput."""
-    return run_trace(reqs, [0.0] * len(reqs), hbm_budget, slots, device)
+    return run_trace(reqs, [0.0] * len(reqs), hbm_budget, slots, device, pinned_bytes)
