@@ -479,8 +479,10 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
 // quarter, each filtering half of the columns into its own list; the two lists of a row share
 // their thresholds while filtering and are merged when the query tile is done).
 // PAIR: two-CTA clusters, 256-row work items (see the file comment).
-// DUAL: two CTAs per SM, each with one accumulator (the MMA of a CTA's next tile waits for its
-// epilogue to release the last one, while the other CTA's warps use the SM).
+// DUAL: two CTAs per SM.  Each CTA holds 256 TMEM columns: every 256-key tile is computed as two
+// N=128 halves into two 128-column accumulators, so the MMA of the next half runs while the
+// epilogue filters the current one; the two CTAs' epilogue warps share each scheduler.  Needs
+// one K atom per row (the halves read the same key stage) and the tagged walk.
 template <int KH, int NEPI, bool PAIR, bool DUAL>
 __global__ void __launch_bounds__(128 + 32 * NEPI, DUAL ? 2 : 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -489,7 +491,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   static_assert(NEPI == 4 || NEPI == 8, "four or eight epilogue warps");
   static_assert(!DUAL || (NEPI == 4 && !PAIR), "two CTAs per SM: single CTAs, four epilogue warps");
   constexpr int NH = NEPI / 4;
-  constexpr int NACC = DUAL ? 1 : 2;                    // accumulators in TMEM
+  constexpr int NACC = 2;                               // accumulators in TMEM
   using Sel = typename SelectorOf<KH>::type;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -529,13 +531,14 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   const int nunits = PAIR ? int(gridDim.x >> 1) : int(gridDim.x);
   const size_t a_bytes = size_t(P.kb) * BM * 128;
   const size_t b_bytes = size_t(brows) * 128;           // one K atom of this CTA's key rows
-  const uint32_t tmem_cols = uint32_t(NACC * P.bn);
+  const int acc_cols = DUAL ? P.bn / 2 : P.bn;          // TMEM columns of one accumulator
+  const uint32_t tmem_cols = uint32_t(NACC * acc_cols);
   const int n_items = P.n_items_dev ? *P.n_items_dev : P.n_items;
   // the producer drives the walk from the sorted list and ends it early (single CTAs only)
   const bool ordered = !PAIR && !P.near_only && P.qmap == nullptr && P.vlist != nullptr &&
                        *P.vok != 0;
   // the producer alone walks (from the list, or the mask) and tags stages and accumulators
-  const bool meta = !PAIR && (ordered || P.meta_walk != 0);
+  const bool meta = !PAIR && (DUAL || ordered || P.meta_walk != 0);
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < NEPI; ++i) rq_pub[i] = ~0ull;       // no item yet
@@ -795,6 +798,32 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
               }
               kt_meta = kt;
             }
+            if constexpr (DUAL) {
+              // the tile's two N=128 halves, each into the next free accumulator (tagged 2·kt+half);
+              // the key stage is released once both halves have read it
+              const uint32_t b_base = smem_u32(Bsm + stage * b_bytes);
+              for (int hf = 0; hf < 2; ++hf) {
+                const long long t2 = P.prof ? clock64() : 0;
+                ok = mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
+                if (P.prof) c_acc += clock64() - t2;
+                if (!ok) break;
+                *reinterpret_cast<volatile int*>(&acc_meta[acc]) = 2 * kt_meta + hf;
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + uint32_t(acc * acc_cols);
+                const uint32_t bh = b_base + uint32_t(hf * acc_cols * 128);
+                for (int ks = 0; ks < P.ksteps; ++ks)
+                  umma_f16_g<false>(d_tmem, sdesc(a_base + uint32_t((ks & 3) * 32)),
+                                    sdesc(bh + uint32_t((ks & 3) * 32)), P.idesc, ks > 0 ? 1u : 0u);
+                umma_commit_g<false>(&acc_full[acc]);
+                mbar_arrive(&acc_full[acc]);              // releases acc_meta to the epilogue
+                if (++acc == NACC) { acc = 0; accphase ^= 1; }
+              }
+              if (!ok) break;
+              umma_commit_g<false>(&b_empty[stage]);
+              if (++stage == P.stages) { stage = 0; sphase ^= 1; }
+              issued = true;
+              continue;
+            }
             const long long t2 = P.prof ? clock64() : 0;
             ok = PAIR ? mbar_wait_cl(&acc_empty[acc], accphase ^ 1, abort_flag)
                       : mbar_wait(&acc_empty[acc], accphase ^ 1, abort_flag);
@@ -867,7 +896,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
     sel.reset();
     sel.prof = P.prof != 0;
-    const int gcols = P.bn / NH;                   // accumulator columns of this group
+    const int gcols = acc_cols / NH;               // accumulator columns of this group
     const int nch = gcols / 32;
     int acc = 0;
     uint32_t accphase = 0, qphase = 0;
@@ -918,6 +947,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         ok = __all_sync(FULL, mbar_wait(&acc_full[acc], accphase, abort_flag));
         if (P.prof) c_ew += clock64() - te;
         if (!ok) break;
+        int half = 0;                      // DUAL: which N=128 half of key tile kt
         if (meta) {
           kt = *reinterpret_cast<volatile int*>(&acc_meta[acc]);
           if (kt < 0) {                    // the item's walk ended: hand the turn back
@@ -926,12 +956,13 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (++acc == NACC) { acc = 0; accphase ^= 1; }
             break;
           }
+          if constexpr (DUAL) { half = kt & 1; kt >>= 1; }
         }
         tc_fence_after();
         sel.refresh();
         const uint32_t t0 =
-            tmem_base + uint32_t(acc * P.bn + h * gcols) + (uint32_t(q * 32) << 16);
-        const int col_base = w.key0 + kt * P.bn + h * gcols;
+            tmem_base + uint32_t(acc * acc_cols + h * gcols) + (uint32_t(q * 32) << 16);
+        const int col_base = w.key0 + kt * P.bn + half * acc_cols + h * gcols;
         // two register buffers: the next chunk's TMEM load is in flight while the current chunk
         // is filtered; the accumulator is released right after its last load completes
         uint32_t ra[32], rb[32];
@@ -1254,9 +1285,10 @@ bool tc_config_ok(const TcConfig& c, int kp, int kprime) {
   if (c.bn != 32 && c.bn != 64 && c.bn != 128 && c.bn != 256) return false;
   if (c.ctas != 1 && c.ctas != 2) return false;
   if (c.ctas == 2) {
-    // two CTAs per SM: single CTAs with four epilogue warps; both CTAs' shared memory (and the
-    // per-block reserve) within the SM's
-    if (c.pair || c.epi != 4 || c.stages < 1 || c.stages > 8) return false;
+    // two CTAs per SM: single CTAs, four epilogue warps, 256-key tiles computed in two halves,
+    // one K atom per row; both CTAs' shared memory (and the per-block reserve) within the SM's
+    if (c.pair || c.epi != 4 || c.bn != 256 || kp != 64 || c.stages < 1 || c.stages > 8)
+      return false;
     if (c.kpl < kprime || (c.kpl != 32 && c.kpl != 48 && c.kpl != 64)) return false;
     if (c.cb != 16 && c.cb != 32) return false;
     return 2 * (config_smem(c, kp / 64, 1) + SMEM_BLOCK_RESERVE) <= SMEM_PER_SM;
@@ -1285,8 +1317,10 @@ TcConfig tc_default_config(int prec, int d, int kprime) {
   // eight warps whose two column halves each keep a list), else eight; then the deepest K-atom
   // pipeline that fits
   {
+    // two CTAs per SM where they fit (one K atom per row): every scheduler runs two epilogue
+    // warps of different rows.  MSC_B200_DUAL=0 turns this off.
     const char* env = std::getenv("MSC_B200_DUAL");
-    if (env && *env == '1')
+    if (!(env && *env == '0'))
       for (int stages = 8; stages >= 1; --stages) {
         TcConfig c{256, stages, kpl, 16, 4, 0, 2};
         if (tc_config_ok(c, L.kp, kprime)) return c;
@@ -1330,7 +1364,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.cand_stride = cand_stride;
   P.bf16 = bf16;
   P.n_items = int(n_items);
-  P.idesc = idesc_f16(bf16, cfg.pair ? 2 * BM : BM, cfg.bn);
+  P.idesc = idesc_f16(bf16, cfg.pair ? 2 * BM : BM, cfg.ctas == 2 ? cfg.bn / 2 : cfg.bn);
   P.prof = profiling_enabled() ? 1 : 0;
   P.perm = perm;
   P.qmap = qmap;
