@@ -484,7 +484,7 @@ __host__ __device__ inline SmemPlan smem_plan(int kb, int brows, int stages, int
 // epilogue filters the current one; the two CTAs' epilogue warps share each scheduler.  Needs
 // one K atom per row (the halves read the same key stage) and the tagged walk.
 template <int KH, int NEPI, bool PAIR, bool DUAL>
-__global__ void __launch_bounds__(128 + 32 * NEPI, DUAL ? 2 : 1)
+__global__ void __launch_bounds__((DUAL ? 64 : 128) + 32 * NEPI, DUAL ? 2 : 1)
 knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const TcParams P, const WorkItem* __restrict__ items, Ctl* __restrict__ ctl,
               int32_t* __restrict__ cand_idx, float* __restrict__ cand_thr) {
@@ -492,6 +492,11 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   static_assert(!DUAL || (NEPI == 4 && !PAIR), "two CTAs per SM: single CTAs, four epilogue warps");
   constexpr int NH = NEPI / 4;
   constexpr int NACC = 2;                               // accumulators in TMEM
+  // warps: 0 producer, 1 MMA, then (single CTAs) 2 TMEM owner and 3 pair relay, then the
+  // epilogue; DUAL has no warps 2 and 3 (the producer warp owns TMEM), so that two CTAs of six
+  // warps get 168 registers per thread
+  constexpr int EPI0 = DUAL ? 2 : EPI_WARP0;            // first epilogue warp
+  constexpr int TMEM_WARP = DUAL ? 0 : 2;
   using Sel = typename SelectorOf<KH>::type;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -566,7 +571,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   }
   if (NH > 1)
     for (int i = threadIdx.x; i < 2 * BM; i += blockDim.x) pub[i] = F_INF;
-  if (warp == 2) {
+  if (warp == TMEM_WARP) {
     tmem_alloc_g<PAIR>(tmem_slot, tmem_cols);
     tmem_relinquish_g<PAIR>();
   }
@@ -640,7 +645,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     return true;
   };
 
-  if (warp < EPI_WARP0) {
+  if (warp < EPI0) {
     // warpgroup 0: one register decrease for the whole warpgroup (the split needs one
     // setmaxnreg per warpgroup), then the roles; warp 2 (TMEM owner) waits for the teardown
     if constexpr (NEPI == 8 && kRegSplit) reg_dec();
@@ -886,7 +891,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     // ------------------------------------------------------------------ epilogue (each CTA)
     if constexpr (NEPI == 8 && kRegSplit) reg_inc();
     const int q = warp & 3;                        // TMEM lane quarter this warp may access
-    const int h = (warp - EPI_WARP0) >> 2;         // column group
+    const int h = (warp - EPI0) >> 2;              // column group
     const int row = q * 32 + lane;
     Sel sel;
     sel.bind(smem + sp.sel_off + size_t(h) * Sel::smem_bytes(), row, P.kprime);
@@ -1011,16 +1016,6 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             if (!cycle(c + 2, rc, ra, rb)) break;
             if (!cycle(c + 4, rb, rc, ra)) break;
           }
-        } else if constexpr (DUAL) {
-          // one chunk buffer (the register cap of two CTAs per SM): load, wait, filter; the
-          // other CTA's warp on this scheduler runs while this one waits for TMEM
-          (void)rb;
-          for (int c = 0; c < nch; ++c) {
-            tmem_ld32_async(t0 + uint32_t(c * 32), ra);
-            tmem_wait(ra);
-            if (c == nch - 1) release();
-            sel.push32(reinterpret_cast<const float(&)[32]>(ra), col_base + c * 32, self, limit);
-          }
         } else {
           tmem_ld32_async(t0, ra);
           tmem_wait(ra);
@@ -1051,7 +1046,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
           if (row < nq) rr = __double2float_ru(double(sel.thr_f) + roff_row);
           for (int o = 16; o > 0; o >>= 1) rr = fmaxf(rr, __shfl_xor_sync(FULL, rr, o));
           if (lane == 0)
-            *reinterpret_cast<volatile unsigned long long*>(&rq_pub[warp - EPI_WARP0]) =
+            *reinterpret_cast<volatile unsigned long long*>(&rq_pub[warp - EPI0]) =
                 (static_cast<unsigned long long>(uint32_t(it)) << 32) | __float_as_uint(rr);
         }
       }
@@ -1103,7 +1098,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   }
 
   __syncthreads();
-  if (warp == 2) {
+  if (warp == TMEM_WARP) {
     // the even CTA's last commit marks the end of every tensor-core write to TMEM (in a pair it
     // arrives at both CTAs)
     (void)mbar_drain(done_bar, 0);
@@ -1111,7 +1106,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   }
   // a pair leaves together: no remote arrive or MMA operand read can reach a CTA that has exited
   if (PAIR) cluster_sync();
-  if (warp == 2) tmem_dealloc_g<PAIR>(tmem_base, tmem_cols);
+  if (warp == TMEM_WARP) tmem_dealloc_g<PAIR>(tmem_base, tmem_cols);
   if (P.prof && threadIdx.x == 0) {
     atomicAdd(&g_tc_prof[P.prof_slot][5], (unsigned long long)(clock64() - t_kernel0));
     atomicAdd(&g_tc_prof[P.prof_slot][9], 1ull);
@@ -1221,7 +1216,8 @@ int launch_tc_t(const TcParams& P, const CUtensorMap& ma, const CUtensorMap& mb,
   }
   if (!PAIR) {
     const int grid = std::max(1, std::min(P.n_items, (DUAL ? 2 : 1) * num_sms()));
-    kern<<<grid, 128 + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx, cand_thr);
+    kern<<<grid, (DUAL ? 64 : 128) + 32 * NEPI, smem, st>>>(ma, mb, P, items, ctl, cand_idx,
+                                                             cand_thr);
     MSC_LAUNCH_CHECK();
     return MSC_OK;
   }
