@@ -20,6 +20,8 @@
 // may fall on either side from run to run; the graph is the same either way.  A fixed number of
 // levels runs without host synchronisation (graph-capturable); nodes at or below LEAF rows are
 // left as they are and are the leaves of the tree.
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace msc {
@@ -234,14 +236,16 @@ __global__ void __launch_bounds__(OR_T)
 side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                const int32_t* __restrict__ side, double* __restrict__ acc) {
+                const int32_t* __restrict__ side, double* __restrict__ acc, int stride) {
   // Runs that lie inside one node (almost all of them) are first combined across the warps of the
   // block in shared memory, so that at the top levels, where every run belongs to the same one or
   // two nodes, a block issues one set of atomics instead of one per warp.
   __shared__ double part[SUM_WARPS][SUM_SLOT];
   __shared__ int64_t part_node[SUM_WARPS];
   const int lane = lane_id(), wib = warp_id();
-  const int64_t nruns = (npacked + SUM_RUN - 1) / SUM_RUN;
+  // stride > 1: only positions p = q·stride take part (q consecutive along a run)
+  const int64_t npos = (npacked + stride - 1) / stride;
+  const int64_t nruns = (npos + SUM_RUN - 1) / SUM_RUN;
   const int per = (d + 31) / 32;            // dimensions per lane (d <= 128)
   for (int64_t rb = int64_t(blockIdx.x) * SUM_WARPS; rb < nruns;
        rb += int64_t(gridDim.x) * SUM_WARPS) {          // block-uniform
@@ -269,15 +273,16 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
       c0 = 0; c1 = 0;
     };
     if (r < nruns) {                         // warp-uniform
-      const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
+      const int64_t q0 = r * SUM_RUN, q1 = min64(npos, q0 + SUM_RUN);
       // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
       // only loads row data (independent from position to position)
       int32_t idh[2], rowh[2], sdh[2];
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
-        const int64_t p = p0 + 32 * hh + lane;
+        const int64_t q = q0 + 32 * hh + lane;
+        const int64_t p = q * stride;
         idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
-        if (p < p1) {
+        if (q < q1) {
           const int st = ns[p];
           if (ne[p] - st > leaf) {
             idh[hh] = int32_t(S[st]);
@@ -346,17 +351,20 @@ __global__ void __launch_bounds__(OR_T)
 reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                const double* __restrict__ acc, int32_t* __restrict__ side) {
+                const double* __restrict__ acc, int32_t* __restrict__ side, int pstride) {
+  // pstride > 1: only positions p = q·pstride are reassigned
   __shared__ RowTile tiles[OR_W];
   RowTile& tile = tiles[warp_id()];
+  const int64_t npos = (npacked + pstride - 1) / pstride;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npos;
        b += stride) {
-    const int64_t p = b + lane_id();
+    const int64_t q = b + lane_id();
+    const int64_t p = q * pstride;
     const double* a = nullptr;
     double i0 = 0.0, i1 = 0.0;
     int32_t row = -1;
-    if (p < npacked) {
+    if (q < npos) {
       const int st = ns[p];
       if (ne[p] - st > leaf) {
         a = acc + S[st] * (2 * d + 2);
@@ -397,6 +405,15 @@ __global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm
 }
 
 }  // namespace
+
+// Extra 2-means steps on the first LLOYD_LEVELS levels, each on every LLOYD_STRIDE-th position
+// (MSC_B200_LLOYD_LEVELS / MSC_B200_LLOYD_STEPS override the level count and steps: tuning).
+// With one step, a mixture of well-separated clusters is cut into many fragments whose pieces
+// share leaves and tiles; their bounding balls then span clusters and the pruning plan keeps
+// them for almost every query tile.
+constexpr int LLOYD_LEVELS = 8;
+constexpr int LLOYD_STEPS = 5;
+constexpr int LLOYD_STRIDE = 16;
 
 // split nodes at one level: each holds more than `leaf` rows
 inline int64_t max_split_nodes(int64_t npacked, int leaf) { return npacked / (leaf + 1) + 1; }
@@ -445,6 +462,11 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   double* acc = c.take<double>(acc_elems);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(npacked, OR_T),
                                                               int64_t(num_sms()) * 8)));
+  const int sgrid = int(std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(ceil_div(npacked, LLOYD_STRIDE), OR_T), int64_t(num_sms()) * 8)));
+  int lloyd_levels = LLOYD_LEVELS, lloyd_steps = LLOYD_STEPS;
+  if (const char* e = std::getenv("MSC_B200_LLOYD_LEVELS")) lloyd_levels = std::max(0, std::atoi(e));
+  if (const char* e = std::getenv("MSC_B200_LLOYD_STEPS")) lloyd_steps = std::max(0, std::atoi(e));
   order_init_kernel<<<grid, OR_T, 0, st>>>(seg, nseg, npacked, perm, nsA, neA);
   MSC_LAUNCH_CHECK();
   int32_t *pc = perm, *pn = perm2, *sc = nsA, *ec = neA, *sn = nsB, *en = neB;
@@ -462,9 +484,23 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
     MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc, 1);
     MSC_LAUNCH_CHECK();
-    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side);
+    // more 2-means steps on the top levels, where nodes still hold several clusters and a split
+    // through the bisector of two means cuts some of them: every 16th position is reassigned and
+    // the side means re-summed from those positions alone, then every position takes the nearer
+    // of the final means
+    const int steps = l < lloyd_levels ? lloyd_steps : 0;
+    for (int it = 0; it < steps; ++it) {
+      reassign_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side,
+                                              LLOYD_STRIDE);
+      MSC_LAUNCH_CHECK();
+      MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
+      side_sum_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc,
+                                              LLOYD_STRIDE);
+      MSC_LAUNCH_CHECK();
+    }
+    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side, 1);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(side, npacked, S, scratch, st));
     scatter_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, pc, sc, ec, side, S, pn, sn, en);
