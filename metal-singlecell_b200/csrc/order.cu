@@ -351,8 +351,13 @@ __global__ void __launch_bounds__(OR_T)
 reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                const double* __restrict__ acc, int32_t* __restrict__ side, int pstride) {
-  // pstride > 1: only positions p = q·pstride are reassigned
+                const double* __restrict__ acc, int32_t* __restrict__ side, int pstride,
+                double* __restrict__ zero_out, int64_t zero_elems) {
+  // pstride > 1: only positions p = q·pstride are reassigned; zero_out (zero_elems doubles) is
+  // cleared for the side sums that follow
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < zero_elems;
+       i += int64_t(gridDim.x) * blockDim.x)
+    zero_out[i] = 0.0;
   __shared__ RowTile tiles[OR_W];
   RowTile& tile = tiles[warp_id()];
   const int64_t npos = (npacked + pstride - 1) / pstride;
@@ -413,7 +418,7 @@ __global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm
 // them for almost every query tile.
 constexpr int LLOYD_LEVELS = 8;
 constexpr int LLOYD_STEPS = 5;
-constexpr int LLOYD_STRIDE = 16;
+constexpr int LLOYD_STRIDE = 64;
 
 // split nodes at one level: each holds more than `leaf` rows
 inline int64_t max_split_nodes(int64_t npacked, int leaf) { return npacked / (leaf + 1) + 1; }
@@ -434,6 +439,7 @@ size_t order_workspace_bytes(int64_t npacked, int d, int leaf) {
   c.take<int32_t>(npacked);                       // split-node starts
   c.take<int64_t>(npacked + 1);                   // their scan: node ids
   c.take<double>(size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2));   // side sums, counts
+  c.take<double>(size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2));   // and of the next step
   return c.bytes();
 }
 
@@ -460,6 +466,7 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   int64_t* SN = c.take<int64_t>(npacked + 1);
   const size_t acc_elems = size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2);
   double* acc = c.take<double>(acc_elems);
+  double* acc2 = c.take<double>(acc_elems);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(npacked, OR_T),
                                                               int64_t(num_sms()) * 8)));
   const int sgrid = int(std::max<int64_t>(
@@ -491,16 +498,18 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     // the side means re-summed from those positions alone, then every position takes the nearer
     // of the final means
     const int steps = l < lloyd_levels ? lloyd_steps : 0;
+    double *a_cur = acc, *a_next = acc2;
     for (int it = 0; it < steps; ++it) {
-      reassign_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side,
+      reassign_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, a_cur, side,
+                                              LLOYD_STRIDE, a_next, int64_t(acc_elems));
+      MSC_LAUNCH_CHECK();
+      side_sum_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, a_next,
                                               LLOYD_STRIDE);
       MSC_LAUNCH_CHECK();
-      MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-      side_sum_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc,
-                                              LLOYD_STRIDE);
-      MSC_LAUNCH_CHECK();
+      std::swap(a_cur, a_next);
     }
-    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side, 1);
+    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, a_cur, side, 1,
+                                           nullptr, 0);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(side, npacked, S, scratch, st));
     scatter_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, pc, sc, ec, side, S, pn, sn, en);
