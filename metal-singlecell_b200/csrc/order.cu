@@ -30,6 +30,15 @@ namespace {
 
 constexpr int OR_T = 256;
 constexpr int OR_W = OR_T / 32;
+// More 2-means steps on the first LLOYD_LEVELS levels (lloyd_node_kernel), on up to
+// LLOYD_SAMPLES_MAX rows of every split node (MSC_B200_LLOYD_LEVELS / MSC_B200_LLOYD_STEPS override
+// the level count and the steps: tuning).  With one step, a mixture of well-separated clusters is
+// cut into many fragments whose pieces share leaves and tiles; their bounding balls then span
+// clusters and the pruning plan keeps those tiles for almost every query tile.
+constexpr int LLOYD_LEVELS = 10;
+constexpr int LLOYD_STEPS = 8;
+constexpr int LLOYD_SAMPLES_MAX = 512;
+constexpr size_t LLOYD_SMEM_MAX = 200 * 1024;
 
 // One warp's 32 rows, 32 dimensions at a time: row r's dimensions c..c+31 in tile[r][0..31].
 // Lanes load a row together (one coalesced line per row and chunk), then each lane reads its own
@@ -236,16 +245,14 @@ __global__ void __launch_bounds__(OR_T)
 side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                const int32_t* __restrict__ side, double* __restrict__ acc, int stride) {
+                const int32_t* __restrict__ side, double* __restrict__ acc) {
   // Runs that lie inside one node (almost all of them) are first combined across the warps of the
   // block in shared memory, so that at the top levels, where every run belongs to the same one or
   // two nodes, a block issues one set of atomics instead of one per warp.
   __shared__ double part[SUM_WARPS][SUM_SLOT];
   __shared__ int64_t part_node[SUM_WARPS];
   const int lane = lane_id(), wib = warp_id();
-  // stride > 1: only positions p = q·stride take part (q consecutive along a run)
-  const int64_t npos = (npacked + stride - 1) / stride;
-  const int64_t nruns = (npos + SUM_RUN - 1) / SUM_RUN;
+  const int64_t nruns = (npacked + SUM_RUN - 1) / SUM_RUN;
   const int per = (d + 31) / 32;            // dimensions per lane (d <= 128)
   for (int64_t rb = int64_t(blockIdx.x) * SUM_WARPS; rb < nruns;
        rb += int64_t(gridDim.x) * SUM_WARPS) {          // block-uniform
@@ -273,16 +280,15 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
       c0 = 0; c1 = 0;
     };
     if (r < nruns) {                         // warp-uniform
-      const int64_t q0 = r * SUM_RUN, q1 = min64(npos, q0 + SUM_RUN);
+      const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
       // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
       // only loads row data (independent from position to position)
       int32_t idh[2], rowh[2], sdh[2];
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
-        const int64_t q = q0 + 32 * hh + lane;
-        const int64_t p = q * stride;
+        const int64_t p = p0 + 32 * hh + lane;
         idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
-        if (q < q1) {
+        if (p < p1) {
           const int st = ns[p];
           if (ne[p] - st > leaf) {
             idh[hh] = int32_t(S[st]);
@@ -351,25 +357,17 @@ __global__ void __launch_bounds__(OR_T)
 reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                const double* __restrict__ acc, int32_t* __restrict__ side, int pstride,
-                double* __restrict__ zero_out, int64_t zero_elems) {
-  // pstride > 1: only positions p = q·pstride are reassigned; zero_out (zero_elems doubles) is
-  // cleared for the side sums that follow
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < zero_elems;
-       i += int64_t(gridDim.x) * blockDim.x)
-    zero_out[i] = 0.0;
+                const double* __restrict__ acc, int32_t* __restrict__ side) {
   __shared__ RowTile tiles[OR_W];
   RowTile& tile = tiles[warp_id()];
-  const int64_t npos = (npacked + pstride - 1) / pstride;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npos;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
-    const int64_t q = b + lane_id();
-    const int64_t p = q * pstride;
+    const int64_t p = b + lane_id();
     const double* a = nullptr;
     double i0 = 0.0, i1 = 0.0;
     int32_t row = -1;
-    if (q < npos) {
+    if (p < npacked) {
       const int st = ns[p];
       if (ne[p] - st > leaf) {
         a = acc + S[st] * (2 * d + 2);
@@ -401,6 +399,88 @@ reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
   }
 }
 
+// start position of every split node of the level (its id: the scan of the split starts)
+__global__ void node_start_kernel(int64_t npacked, const int32_t* __restrict__ flag,
+                                  const int64_t* __restrict__ SN, int32_t* __restrict__ start) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npacked;
+       p += int64_t(gridDim.x) * blockDim.x)
+    if (flag[p]) start[SN[p]] = int32_t(p);
+}
+
+// More 2-means steps for the split nodes of a top level, one CTA per node: up to m_max of the
+// node's rows (every (size/m)-th position) are staged in shared memory and the two side means,
+// starting from the sums in acc, are moved `steps` times to the means of the staged rows nearer to
+// each; the result replaces the node's sums (as means with counts of one) for the reassignment
+// of every row.  A step that leaves a side empty ends the node's steps with the means before it.
+constexpr int LLOYD_T = 256;
+__global__ void __launch_bounds__(LLOYD_T)
+lloyd_node_kernel(const float* __restrict__ X, int d, int64_t npacked,
+                  const int32_t* __restrict__ perm, const int32_t* __restrict__ ne,
+                  const int64_t* __restrict__ SN, const int32_t* __restrict__ start,
+                  double* __restrict__ acc, int steps, int m_max) {
+  extern __shared__ float xs[];                        // [m][d]
+  __shared__ double mu[2][MSC_MAX_D], sm[2][MSC_MAX_D];
+  __shared__ int sides[LLOYD_SAMPLES_MAX];
+  __shared__ int cnt[2];
+  const int tid = threadIdx.x;
+  const int64_t nodes = SN[npacked];
+  for (int64_t b = blockIdx.x; b < nodes; b += gridDim.x) {     // block-uniform
+    const int64_t s = start[b], size = int64_t(ne[s]) - s;
+    const int m = int(min64(m_max, size));
+    const int64_t stp = size / m;
+    double* a = acc + b * (2 * d + 2);
+    const double n0 = a[2 * d], n1 = a[2 * d + 1];
+    if (n0 == 0.0 || n1 == 0.0) continue;
+    for (int q = tid; q < 2 * d; q += LLOYD_T) {
+      const int h = q >= d, t = q - h * d;
+      mu[h][t] = a[q] / (h ? n1 : n0);
+    }
+    for (int idx = tid; idx < m * d; idx += LLOYD_T) {
+      const int j = idx / d, t = idx - j * d;
+      xs[idx] = X[int64_t(perm[s + int64_t(j) * stp]) * d + t];
+    }
+    __syncthreads();
+    for (int it = 0; it < steps; ++it) {
+      if (tid < 2) cnt[tid] = 0;
+      __syncthreads();
+      for (int j = tid; j < m; j += LLOYD_T) {
+        double d0 = 0.0, d1 = 0.0;
+        for (int t = 0; t < d; ++t) {
+          const double v = xs[j * d + t];
+          const double u0 = v - mu[0][t], u1 = v - mu[1][t];
+          d0 += u0 * u0;
+          d1 += u1 * u1;
+        }
+        const int sd = d0 > d1 ? 1 : 0;
+        sides[j] = sd;
+        atomicAdd(&cnt[sd], 1);
+      }
+      __syncthreads();
+      for (int q = tid; q < 2 * d; q += LLOYD_T) {
+        const int h = q >= d, t = q - h * d;
+        double acc_q = 0.0;
+        for (int j = 0; j < m; ++j)
+          if (sides[j] == h) acc_q += xs[j * d + t];
+        sm[h][t] = acc_q;
+      }
+      __syncthreads();
+      const int c0 = cnt[0], c1 = cnt[1];
+      if (c0 == 0 || c1 == 0) break;                 // block-uniform
+      for (int q = tid; q < 2 * d; q += LLOYD_T) {
+        const int h = q >= d, t = q - h * d;
+        mu[h][t] = sm[h][t] / double(h ? c1 : c0);
+      }
+      __syncthreads();
+    }
+    for (int q = tid; q < 2 * d; q += LLOYD_T) {
+      const int h = q >= d, t = q - h * d;
+      a[q] = mu[h][t];
+    }
+    if (tid == 0) { a[2 * d] = 1.0; a[2 * d + 1] = 1.0; }
+    __syncthreads();
+  }
+}
+
 // leaf of every packed position: the first position of its final node (-1: padding rows)
 __global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm,
                                const int32_t* __restrict__ ns, int32_t* __restrict__ leaf_out) {
@@ -411,14 +491,6 @@ __global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm
 
 }  // namespace
 
-// Extra 2-means steps on the first LLOYD_LEVELS levels, each on every LLOYD_STRIDE-th position
-// (MSC_B200_LLOYD_LEVELS / MSC_B200_LLOYD_STEPS override the level count and steps: tuning).
-// With one step, a mixture of well-separated clusters is cut into many fragments whose pieces
-// share leaves and tiles; their bounding balls then span clusters and the pruning plan keeps
-// them for almost every query tile.
-constexpr int LLOYD_LEVELS = 8;
-constexpr int LLOYD_STEPS = 5;
-constexpr int LLOYD_STRIDE = 64;
 
 // split nodes at one level: each holds more than `leaf` rows
 inline int64_t max_split_nodes(int64_t npacked, int leaf) { return npacked / (leaf + 1) + 1; }
@@ -439,7 +511,7 @@ size_t order_workspace_bytes(int64_t npacked, int d, int leaf) {
   c.take<int32_t>(npacked);                       // split-node starts
   c.take<int64_t>(npacked + 1);                   // their scan: node ids
   c.take<double>(size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2));   // side sums, counts
-  c.take<double>(size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2));   // and of the next step
+  c.take<int32_t>(size_t(max_split_nodes(npacked, leaf)));            // split-node starts by id
   return c.bytes();
 }
 
@@ -466,14 +538,15 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   int64_t* SN = c.take<int64_t>(npacked + 1);
   const size_t acc_elems = size_t(max_split_nodes(npacked, leaf)) * (2 * d + 2);
   double* acc = c.take<double>(acc_elems);
-  double* acc2 = c.take<double>(acc_elems);
+  int32_t* nstart = c.take<int32_t>(size_t(max_split_nodes(npacked, leaf)));
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(npacked, OR_T),
                                                               int64_t(num_sms()) * 8)));
-  const int sgrid = int(std::max<int64_t>(
-      1, std::min<int64_t>(ceil_div(ceil_div(npacked, LLOYD_STRIDE), OR_T), int64_t(num_sms()) * 8)));
   int lloyd_levels = LLOYD_LEVELS, lloyd_steps = LLOYD_STEPS;
   if (const char* e = std::getenv("MSC_B200_LLOYD_LEVELS")) lloyd_levels = std::max(0, std::atoi(e));
   if (const char* e = std::getenv("MSC_B200_LLOYD_STEPS")) lloyd_steps = std::max(0, std::atoi(e));
+  const int m_max = int(std::min<size_t>(LLOYD_SAMPLES_MAX, LLOYD_SMEM_MAX / (sizeof(float) * d)));
+  const size_t lsmem = size_t(m_max) * d * sizeof(float);
+  if (lloyd_levels > 0 && lloyd_steps > 0) MSC_CUDA_TRY(raise_smem_cap(lloyd_node_kernel, lsmem));
   order_init_kernel<<<grid, OR_T, 0, st>>>(seg, nseg, npacked, perm, nsA, neA);
   MSC_LAUNCH_CHECK();
   int32_t *pc = perm, *pn = perm2, *sc = nsA, *ec = neA, *sn = nsB, *en = neB;
@@ -491,25 +564,17 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
     MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc, 1);
+    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
     MSC_LAUNCH_CHECK();
-    // more 2-means steps on the top levels, where nodes still hold several clusters and a split
-    // through the bisector of two means cuts some of them: every 16th position is reassigned and
-    // the side means re-summed from those positions alone, then every position takes the nearer
-    // of the final means
-    const int steps = l < lloyd_levels ? lloyd_steps : 0;
-    double *a_cur = acc, *a_next = acc2;
-    for (int it = 0; it < steps; ++it) {
-      reassign_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, a_cur, side,
-                                              LLOYD_STRIDE, a_next, int64_t(acc_elems));
+    if (l < lloyd_levels && lloyd_steps > 0) {
+      node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
       MSC_LAUNCH_CHECK();
-      side_sum_kernel<<<sgrid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, a_next,
-                                              LLOYD_STRIDE);
+      const int64_t nb = std::min<int64_t>(int64_t(1) << std::min(l, 20), max_split_nodes(npacked, leaf));
+      lloyd_node_kernel<<<unsigned(std::max<int64_t>(1, nb)), LLOYD_T, lsmem, st>>>(
+          X, d, npacked, pc, ec, SN, nstart, acc, lloyd_steps, m_max);
       MSC_LAUNCH_CHECK();
-      std::swap(a_cur, a_next);
     }
-    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, a_cur, side, 1,
-                                           nullptr, 0);
+    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(side, npacked, S, scratch, st));
     scatter_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, pc, sc, ec, side, S, pn, sn, en);
