@@ -419,10 +419,11 @@ lloyd_node_kernel(const float* __restrict__ X, int d, int64_t npacked,
                   const int64_t* __restrict__ SN, const int32_t* __restrict__ start,
                   double* __restrict__ acc, int steps, int m_max) {
   extern __shared__ float xs[];                        // [m][d]
-  __shared__ double mu[2][MSC_MAX_D], sm[2][MSC_MAX_D];
-  __shared__ int sides[LLOYD_SAMPLES_MAX];
+  __shared__ float mu[2][MSC_MAX_D];
+  __shared__ int rows[LLOYD_SAMPLES_MAX], sides[LLOYD_SAMPLES_MAX];
   __shared__ int cnt[2];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = lane_id(), wib = warp_id();
+  constexpr int NW = LLOYD_T / 32;
   const int64_t nodes = SN[npacked];
   for (int64_t b = blockIdx.x; b < nodes; b += gridDim.x) {     // block-uniform
     const int64_t s = start[b], size = int64_t(ne[s]) - s;
@@ -433,48 +434,64 @@ lloyd_node_kernel(const float* __restrict__ X, int d, int64_t npacked,
     if (n0 == 0.0 || n1 == 0.0) continue;
     for (int q = tid; q < 2 * d; q += LLOYD_T) {
       const int h = q >= d, t = q - h * d;
-      mu[h][t] = a[q] / (h ? n1 : n0);
+      mu[h][t] = float(a[q] / (h ? n1 : n0));
     }
-    for (int idx = tid; idx < m * d; idx += LLOYD_T) {
-      const int j = idx / d, t = idx - j * d;
-      xs[idx] = X[int64_t(perm[s + int64_t(j) * stp]) * d + t];
+    for (int j = tid; j < m; j += LLOYD_T) rows[j] = perm[s + int64_t(j) * stp];
+    __syncthreads();
+    // a warp per sample row (coalesced), four rows in flight per warp
+    for (int j0 = wib * 4; j0 < m; j0 += NW * 4) {
+      float v[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int j = j0 + u, t = lane + 32 * c;
+          v[u][c] = (j < m && t < d) ? X[int64_t(rows[j]) * d + t] : 0.f;
+        }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int j = j0 + u, t = lane + 32 * c;
+          if (j < m && t < d) xs[j * d + t] = v[u][c];
+        }
     }
     __syncthreads();
     for (int it = 0; it < steps; ++it) {
       if (tid < 2) cnt[tid] = 0;
       __syncthreads();
       for (int j = tid; j < m; j += LLOYD_T) {
-        double d0 = 0.0, d1 = 0.0;
+        float d0 = 0.f, d1 = 0.f;
         for (int t = 0; t < d; ++t) {
-          const double v = xs[j * d + t];
-          const double u0 = v - mu[0][t], u1 = v - mu[1][t];
-          d0 += u0 * u0;
-          d1 += u1 * u1;
+          const float x = xs[j * d + t];
+          const float u0 = x - mu[0][t], u1 = x - mu[1][t];
+          d0 = fmaf(u0, u0, d0);
+          d1 = fmaf(u1, u1, d1);
         }
         const int sd = d0 > d1 ? 1 : 0;
         sides[j] = sd;
         atomicAdd(&cnt[sd], 1);
       }
       __syncthreads();
-      for (int q = tid; q < 2 * d; q += LLOYD_T) {
-        const int h = q >= d, t = q - h * d;
-        double acc_q = 0.0;
-        for (int j = 0; j < m; ++j)
-          if (sides[j] == h) acc_q += xs[j * d + t];
-        sm[h][t] = acc_q;
-      }
-      __syncthreads();
       const int c0 = cnt[0], c1 = cnt[1];
       if (c0 == 0 || c1 == 0) break;                 // block-uniform
-      for (int q = tid; q < 2 * d; q += LLOYD_T) {
-        const int h = q >= d, t = q - h * d;
-        mu[h][t] = sm[h][t] / double(h ? c1 : c0);
+      float s0 = 0.f, s1 = 0.f;
+      if (tid < d) {
+        for (int j = 0; j < m; ++j) {
+          const float x = xs[j * d + tid];
+          if (sides[j]) s1 += x; else s0 += x;
+        }
+      }
+      __syncthreads();                                // every distance read mu
+      if (tid < d) {
+        mu[0][tid] = s0 / float(c0);
+        mu[1][tid] = s1 / float(c1);
       }
       __syncthreads();
     }
     for (int q = tid; q < 2 * d; q += LLOYD_T) {
       const int h = q >= d, t = q - h * d;
-      a[q] = mu[h][t];
+      a[q] = double(mu[h][t]);
     }
     if (tid == 0) { a[2 * d] = 1.0; a[2 * d + 1] = 1.0; }
     __syncthreads();
