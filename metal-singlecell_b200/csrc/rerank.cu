@@ -79,7 +79,10 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
               int prec, int kmma, int k, int cosine, int32_t* __restrict__ knn_idx,
               float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows,
               const int32_t* __restrict__ rows, const int32_t* __restrict__ nrows,
-              int32_t* __restrict__ fail_flags) {
+              int32_t* __restrict__ fail_flags, const float* __restrict__ Xp,
+              const int32_t* __restrict__ iperm) {
+  // Xp (with iperm: original row -> packed row): the same rows in the locality order; every row
+  // is then read from there (same values, so the same results)
   __shared__ __align__(16) float xs_all[RR_WARPS][MSC_MAX_D];
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
@@ -92,6 +95,9 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
   const double delta = double(d + 4) * 0x1p-24;
   int64_t n_cert = 0, n_ties = 0;
   const int64_t count = rows ? int64_t(*nrows) : npacked;
+  auto row_of = [&](int c) -> const float* {
+    return Xp ? Xp + int64_t(iperm[c]) * d : X + int64_t(c) * d;
+  };
   for (int64_t wq = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; wq < count;
        wq += nwarps) {
     const int64_t p = rows ? int64_t(rows[wq]) : wq;
@@ -99,7 +105,8 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     if (i < 0) continue;                                // padding (warp-uniform)
     const int s = find_seg(seg, nseg, p);
     const int64_t ns = seg[s].n;
-    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
+    const float* xrow = Xp ? Xp + p * d : X + i * d;
+    for (int t = lane; t < d; t += 32) xs[t] = xrow[t];
     __syncwarp();
     if (kk == 0) {
       if (lane == 0) { knn_idx[i * k] = int32_t(i); knn_dist[i * k] = 0.f; ++n_cert; }
@@ -117,7 +124,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
         // the candidate ids sit in lanes c & 31 of c0 (c < 32) or c1
         const int id0 = __shfl_sync(FULL, c0, c & 31), id1 = __shfl_sync(FULL, c1, c & 31);
         const int cid = c < kprime ? (c < 32 ? id0 : id1) : -1;
-        float v = cid >= 0 ? group_part_d2_f32(xs, X + int64_t(cid) * d, d, part) : 0.f;
+        float v = cid >= 0 ? group_part_d2_f32(xs, row_of(cid), d, part) : 0.f;
         v += __shfl_xor_sync(FULL, v, 1);                // the group's four shares
         v += __shfl_xor_sync(FULL, v, 2);
         if (cid < 0) v = __int_as_float(0x7f800000);
@@ -140,8 +147,8 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     const double lim = double(B) * (1.0 + 3.0 * delta) + 1e-300;
     const bool w0 = c0 != INT32_MAX && double(e0) <= lim;
     const bool w1 = c1 != INT32_MAX && double(e1) <= lim;
-    double g0 = w0 ? d2_f64(xs, X + int64_t(c0) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
-    double g1 = w1 ? d2_f64(xs, X + int64_t(c1) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
+    double g0 = w0 ? d2_f64(xs, row_of(c0), d) : __longlong_as_double(0x7ff0000000000000ll);
+    double g1 = w1 ? d2_f64(xs, row_of(c1), d) : __longlong_as_double(0x7ff0000000000000ll);
     const int m = __popc(__ballot_sync(FULL, w0)) + __popc(__ballot_sync(FULL, w1));
     int h0 = c0, h1 = c1;
     warp_sort64_d(g0, h0, g1, h1);
@@ -218,7 +225,8 @@ fp64_scan_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__
     const int sg = find_seg(seg, nseg, p);
     const int64_t off = seg[sg].off, ns = seg[sg].n;
     const int64_t i = perm[p];                           // original row
-    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
+    const float* xrow = Xp ? Xp + p * d : X + i * d;
+    for (int t = lane; t < d; t += 32) xs[t] = xrow[t];
     __syncwarp();
     WarpTop<SLOTS> top;
     top.init();
@@ -301,6 +309,21 @@ __global__ void refine_items_kernel(const SegDesc* __restrict__ seg, int nseg,
 
 }  // namespace
 
+// Xp[p·d + t] = X[perm[p]·d + t] (0 for padding rows): consecutive threads write consecutive
+// elements; the reads are whole rows
+__global__ void gather_packed_kernel(const float* __restrict__ X, int d,
+                                     const int32_t* __restrict__ perm, int64_t npacked,
+                                     float* __restrict__ Xp) {
+  const int64_t total = npacked * d;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t p = e / d;
+    const int t = int(e - p * d);
+    const int32_t i = perm[p];
+    Xp[e] = i >= 0 ? X[int64_t(i) * d + t] : 0.f;
+  }
+}
+
 int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
                          cudaStream_t st) {
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
@@ -315,7 +338,8 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
                   const int32_t* rows, const int32_t* nrows, int64_t max_rows,
-                  int32_t* fail_flags, cudaStream_t st) {
+                  int32_t* fail_flags, cudaStream_t st, const float* Xp,
+                  const int32_t* iperm) {
   if (kprime > 64 || k - 1 > 64) {
     set_error("rerank: kprime=%d / k=%d beyond 64", kprime, k);
     return MSC_ERR_UNSUPPORTED;
@@ -324,7 +348,17 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
   int blocks = int(std::min<int64_t>(ceil_div(n_work, RR_WARPS), int64_t(num_sms()) * 8));
   rerank_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
       X, d, perm, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
-      kmma, k, cosine, knn_idx, knn_dist, fail_rows, rows, nrows, fail_flags);
+      kmma, k, cosine, knn_idx, knn_dist, fail_rows, rows, nrows, fail_flags,
+      (Xp && iperm) ? Xp : nullptr, iperm);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_gather_packed(const float* X, int d, const int32_t* perm, int64_t npacked, float* Xp,
+                         cudaStream_t st) {
+  const int blocks = int(std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(npacked * d, 256), int64_t(num_sms()) * 16)));
+  gather_packed_kernel<<<blocks, 256, 0, st>>>(X, d, perm, npacked, Xp);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
