@@ -225,8 +225,7 @@ fp64_scan_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__
     const int sg = find_seg(seg, nseg, p);
     const int64_t off = seg[sg].off, ns = seg[sg].n;
     const int64_t i = perm[p];                           // original row
-    const float* xrow = Xp ? Xp + p * d : X + i * d;
-    for (int t = lane; t < d; t += 32) xs[t] = xrow[t];
+    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
     __syncwarp();
     WarpTop<SLOTS> top;
     top.init();
