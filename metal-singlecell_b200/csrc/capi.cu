@@ -463,7 +463,8 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   // a copy of the rows in packed order, in the three-term key operand's buffer, which the refine
   // pass fills only afterwards (2·round_up(3d+3, 64) bytes per packed row >= 4d)
   float* Xp = nullptr;
-  if (prune && P.refine && w.pr.iperm) {
+  const char* rp_env = std::getenv("MSC_B200_RERANK_PACKED");      // 0: original order (tuning)
+  if (prune && P.refine && w.pr.iperm && !(rp_env && *rp_env == '0')) {
     Xp = reinterpret_cast<float*>(w.B3);
     MSC_TRY(launch_gather_packed(Xu, P.d, w.perm, P.npacked, Xp, st));
   }

@@ -70,7 +70,7 @@ __device__ __forceinline__ float out_dist(double d2, int cosine) {
   return cosine ? __double2float_rn(d2 * 0.5) : __double2float_rn(sqrt(d2));
 }
 
-__global__ void __launch_bounds__(RR_WARPS * 32, 3)
+__global__ void __launch_bounds__(RR_WARPS * 32, 2)
 rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
               const SegDesc* __restrict__ seg, int nseg,
               int64_t npacked, const int32_t* __restrict__ cand_idx,
@@ -98,6 +98,9 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
   auto row_of = [&](int c) -> const float* {
     return Xp ? Xp + int64_t(iperm[c]) * d : X + int64_t(c) * d;
   };
+  // every row starts on an 8-byte boundary: even d and an 8-byte aligned base
+  const bool pairs_ok = (d % 2 == 0) &&
+      ((reinterpret_cast<uintptr_t>(Xp ? Xp : X) & 7) == 0);
   for (int64_t wq = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; wq < count;
        wq += nwarps) {
     const int64_t p = rows ? int64_t(rows[wq]) : wq;
@@ -118,16 +121,52 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     int c1 = lane + 32 < kprime ? cand_idx[i * cand_stride + lane + 32] : -1;
     float e0 = __int_as_float(0x7f800000), e1 = __int_as_float(0x7f800000);
     {
+      // all rounds' candidate rows first, then their partial sums with the dimension loop outside:
+      // the eight rows' loads of one step are independent and go out together (a round at a time,
+      // a lane waited for one row's loads per round)
       const int part = lane & 3, grp = lane >> 2;
-      for (int r = 0; r < kprime; r += 8) {              // warp-uniform
-        const int c = r + grp;
+      const float* yr[8];
+      int cidr[8];
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int c = rr * 8 + grp;
         // the candidate ids sit in lanes c & 31 of c0 (c < 32) or c1
         const int id0 = __shfl_sync(FULL, c0, c & 31), id1 = __shfl_sync(FULL, c1, c & 31);
         const int cid = c < kprime ? (c < 32 ? id0 : id1) : -1;
-        float v = cid >= 0 ? group_part_d2_f32(xs, row_of(cid), d, part) : 0.f;
+        cidr[rr] = cid;
+        yr[rr] = cid >= 0 ? row_of(cid) : nullptr;
+      }
+      float a0[8], a1[8];
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) { a0[rr] = 0.f; a1[rr] = 0.f; }
+      if (pairs_ok) {
+        // 8-byte pairs (every row 8-byte aligned): the per-lane sums of group_part_d2_f32
+        const float2* x2 = reinterpret_cast<const float2*>(xs);
+        const int h = d >> 1;
+        for (int t = part; t < h; t += 4) {
+          const float2 pv = x2[t];
+#pragma unroll
+          for (int rr = 0; rr < 8; ++rr)
+            if (yr[rr]) {
+              const float2 u = reinterpret_cast<const float2*>(yr[rr])[t];
+              const float f0 = pv.x - u.x, f1 = pv.y - u.y;
+              a0[rr] = fmaf(f0, f0, a0[rr]);
+              a1[rr] = fmaf(f1, f1, a1[rr]);
+            }
+        }
+      } else {
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr)
+          if (yr[rr]) a0[rr] = group_part_d2_f32(xs, yr[rr], d, part);
+      }
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int r = rr * 8;
+        if (r >= kprime) break;                           // warp-uniform
+        float v = a0[rr] + a1[rr];
         v += __shfl_xor_sync(FULL, v, 1);                // the group's four shares
         v += __shfl_xor_sync(FULL, v, 2);
-        if (cid < 0) v = __int_as_float(0x7f800000);
+        if (cidr[rr] < 0) v = __int_as_float(0x7f800000);
         const int rb = r & 31;                            // lanes rb .. rb+7 receive this round
         const float got = __shfl_sync(FULL, v, ((lane - rb) & 7) * 4);
         if (lane >= rb && lane < rb + 8) {
