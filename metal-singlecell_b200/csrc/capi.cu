@@ -459,19 +459,10 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   }
   stage_mark(st, 4);
   if (P.refine) MSC_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(int32_t) * P.npacked, st));
-  // the re-rank reads its rows in the locality order (a row's candidates then share cache lines):
-  // a copy of the rows in packed order, in the three-term key operand's buffer, which the refine
-  // pass fills only afterwards (2·round_up(3d+3, 64) bytes per packed row >= 4d)
-  float* Xp = nullptr;
-  const char* rp_env = std::getenv("MSC_B200_RERANK_PACKED");      // 0: original order (tuning)
-  if (prune && P.refine && w.pr.iperm && !(rp_env && *rp_env == '0')) {
-    Xp = reinterpret_cast<float*>(w.B3);
-    MSC_TRY(launch_gather_packed(Xu, P.d, w.perm, P.npacked, Xp, st));
-  }
   MSC_TRY(launch_rerank(Xu, P.d, w.perm, w.seg, P.nseg, P.npacked, w.cand_idx, w.cand_thr,
                         P.kprime, P.kprime, w.qs, w.km, P.prec, P.L.kmma, P.k, cosine, knn_idx,
                         knn_dist, w.fail_rows, w.ctl, nullptr, nullptr, 0,
-                        P.refine ? w.flags : nullptr, st, Xp, Xp ? w.pr.iperm : nullptr));
+                        P.refine ? w.flags : nullptr, st));
   if (P.refine) {
     // the rows the one-term candidates could not certify, again with the three-term split
     // with pruning, a small refine set is split over key ranges (prune.cu)

@@ -271,12 +271,7 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
                   const int32_t* rows, const int32_t* nrows, int64_t max_rows,
-                  int32_t* fail_flags, cudaStream_t st, const float* Xp = nullptr,
-                  const int32_t* iperm = nullptr);
-// Xp[p] = X[perm[p]] for every packed row p (zero rows for padding): the re-rank's rows in the
-// locality order, so that a row's candidates (mostly its neighbours in that order) share lines
-int launch_gather_packed(const float* X, int d, const int32_t* perm, int64_t npacked, float* Xp,
-                         cudaStream_t st);
+                  int32_t* fail_flags, cudaStream_t st);
 // refine plan: compact the flagged packed rows (sorted) into qmap, count them (ctl->n_refine)
 // and cut them into per-sample query tiles (items, ctl->n_items_refine); S: npacked+1 int64
 // split > 1: when there are at most max_split_items refine items, each becomes `split` work

@@ -70,7 +70,7 @@ __device__ __forceinline__ float out_dist(double d2, int cosine) {
   return cosine ? __double2float_rn(d2 * 0.5) : __double2float_rn(sqrt(d2));
 }
 
-__global__ void __launch_bounds__(RR_WARPS * 32, 2)
+__global__ void __launch_bounds__(RR_WARPS * 32, 3)
 rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
               const SegDesc* __restrict__ seg, int nseg,
               int64_t npacked, const int32_t* __restrict__ cand_idx,
@@ -79,10 +79,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
               int prec, int kmma, int k, int cosine, int32_t* __restrict__ knn_idx,
               float* __restrict__ knn_dist, int32_t* __restrict__ fail_rows,
               const int32_t* __restrict__ rows, const int32_t* __restrict__ nrows,
-              int32_t* __restrict__ fail_flags, const float* __restrict__ Xp,
-              const int32_t* __restrict__ iperm) {
-  // Xp (with iperm: original row -> packed row): the same rows in the locality order; every row
-  // is then read from there (same values, so the same results)
+              int32_t* __restrict__ fail_flags) {
   __shared__ __align__(16) float xs_all[RR_WARPS][MSC_MAX_D];
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
@@ -95,12 +92,6 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
   const double delta = double(d + 4) * 0x1p-24;
   int64_t n_cert = 0, n_ties = 0;
   const int64_t count = rows ? int64_t(*nrows) : npacked;
-  auto row_of = [&](int c) -> const float* {
-    return Xp ? Xp + int64_t(iperm[c]) * d : X + int64_t(c) * d;
-  };
-  // every row starts on an 8-byte boundary: even d and an 8-byte aligned base
-  const bool pairs_ok = (d % 2 == 0) &&
-      ((reinterpret_cast<uintptr_t>(Xp ? Xp : X) & 7) == 0);
   for (int64_t wq = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; wq < count;
        wq += nwarps) {
     const int64_t p = rows ? int64_t(rows[wq]) : wq;
@@ -108,8 +99,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     if (i < 0) continue;                                // padding (warp-uniform)
     const int s = find_seg(seg, nseg, p);
     const int64_t ns = seg[s].n;
-    const float* xrow = Xp ? Xp + p * d : X + i * d;
-    for (int t = lane; t < d; t += 32) xs[t] = xrow[t];
+    for (int t = lane; t < d; t += 32) xs[t] = X[i * d + t];
     __syncwarp();
     if (kk == 0) {
       if (lane == 0) { knn_idx[i * k] = int32_t(i); knn_dist[i * k] = 0.f; ++n_cert; }
@@ -121,52 +111,16 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     int c1 = lane + 32 < kprime ? cand_idx[i * cand_stride + lane + 32] : -1;
     float e0 = __int_as_float(0x7f800000), e1 = __int_as_float(0x7f800000);
     {
-      // all rounds' candidate rows first, then their partial sums with the dimension loop outside:
-      // the eight rows' loads of one step are independent and go out together (a round at a time,
-      // a lane waited for one row's loads per round)
       const int part = lane & 3, grp = lane >> 2;
-      const float* yr[8];
-      int cidr[8];
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int c = rr * 8 + grp;
+      for (int r = 0; r < kprime; r += 8) {              // warp-uniform
+        const int c = r + grp;
         // the candidate ids sit in lanes c & 31 of c0 (c < 32) or c1
         const int id0 = __shfl_sync(FULL, c0, c & 31), id1 = __shfl_sync(FULL, c1, c & 31);
         const int cid = c < kprime ? (c < 32 ? id0 : id1) : -1;
-        cidr[rr] = cid;
-        yr[rr] = cid >= 0 ? row_of(cid) : nullptr;
-      }
-      float a0[8], a1[8];
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) { a0[rr] = 0.f; a1[rr] = 0.f; }
-      if (pairs_ok) {
-        // 8-byte pairs (every row 8-byte aligned): the per-lane sums of group_part_d2_f32
-        const float2* x2 = reinterpret_cast<const float2*>(xs);
-        const int h = d >> 1;
-        for (int t = part; t < h; t += 4) {
-          const float2 pv = x2[t];
-#pragma unroll
-          for (int rr = 0; rr < 8; ++rr)
-            if (yr[rr]) {
-              const float2 u = reinterpret_cast<const float2*>(yr[rr])[t];
-              const float f0 = pv.x - u.x, f1 = pv.y - u.y;
-              a0[rr] = fmaf(f0, f0, a0[rr]);
-              a1[rr] = fmaf(f1, f1, a1[rr]);
-            }
-        }
-      } else {
-#pragma unroll
-        for (int rr = 0; rr < 8; ++rr)
-          if (yr[rr]) a0[rr] = group_part_d2_f32(xs, yr[rr], d, part);
-      }
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int r = rr * 8;
-        if (r >= kprime) break;                           // warp-uniform
-        float v = a0[rr] + a1[rr];
+        float v = cid >= 0 ? group_part_d2_f32(xs, X + int64_t(cid) * d, d, part) : 0.f;
         v += __shfl_xor_sync(FULL, v, 1);                // the group's four shares
         v += __shfl_xor_sync(FULL, v, 2);
-        if (cidr[rr] < 0) v = __int_as_float(0x7f800000);
+        if (cid < 0) v = __int_as_float(0x7f800000);
         const int rb = r & 31;                            // lanes rb .. rb+7 receive this round
         const float got = __shfl_sync(FULL, v, ((lane - rb) & 7) * 4);
         if (lane >= rb && lane < rb + 8) {
@@ -186,8 +140,8 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
     const double lim = double(B) * (1.0 + 3.0 * delta) + 1e-300;
     const bool w0 = c0 != INT32_MAX && double(e0) <= lim;
     const bool w1 = c1 != INT32_MAX && double(e1) <= lim;
-    double g0 = w0 ? d2_f64(xs, row_of(c0), d) : __longlong_as_double(0x7ff0000000000000ll);
-    double g1 = w1 ? d2_f64(xs, row_of(c1), d) : __longlong_as_double(0x7ff0000000000000ll);
+    double g0 = w0 ? d2_f64(xs, X + int64_t(c0) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
+    double g1 = w1 ? d2_f64(xs, X + int64_t(c1) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
     const int m = __popc(__ballot_sync(FULL, w0)) + __popc(__ballot_sync(FULL, w1));
     int h0 = c0, h1 = c1;
     warp_sort64_d(g0, h0, g1, h1);
@@ -347,21 +301,6 @@ __global__ void refine_items_kernel(const SegDesc* __restrict__ seg, int nseg,
 
 }  // namespace
 
-// Xp[p·d + t] = X[perm[p]·d + t] (0 for padding rows): consecutive threads write consecutive
-// elements; the reads are whole rows
-__global__ void gather_packed_kernel(const float* __restrict__ X, int d,
-                                     const int32_t* __restrict__ perm, int64_t npacked,
-                                     float* __restrict__ Xp) {
-  const int64_t total = npacked * d;
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t p = e / d;
-    const int t = int(e - p * d);
-    const int32_t i = perm[p];
-    Xp[e] = i >= 0 ? X[int64_t(i) * d + t] : 0.f;
-  }
-}
-
 int launch_all_rows_fail(const int32_t* perm, int64_t npacked, int32_t* fail_rows, Ctl* ctl,
                          cudaStream_t st) {
   int blocks = int(std::min<int64_t>(ceil_div(npacked, 256), int64_t(num_sms()) * 8));
@@ -376,8 +315,7 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
                   const QStat* qs, const KeyMax* km, int prec, int kmma, int k, int cosine,
                   int32_t* knn_idx, float* knn_dist, int32_t* fail_rows, Ctl* ctl,
                   const int32_t* rows, const int32_t* nrows, int64_t max_rows,
-                  int32_t* fail_flags, cudaStream_t st, const float* Xp,
-                  const int32_t* iperm) {
+                  int32_t* fail_flags, cudaStream_t st) {
   if (kprime > 64 || k - 1 > 64) {
     set_error("rerank: kprime=%d / k=%d beyond 64", kprime, k);
     return MSC_ERR_UNSUPPORTED;
@@ -386,17 +324,7 @@ int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg
   int blocks = int(std::min<int64_t>(ceil_div(n_work, RR_WARPS), int64_t(num_sms()) * 8));
   rerank_kernel<<<std::max(blocks, 1), RR_WARPS * 32, 0, st>>>(
       X, d, perm, seg, nseg, npacked, cand_idx, cand_thr, cand_stride, kprime, qs, km, ctl, prec,
-      kmma, k, cosine, knn_idx, knn_dist, fail_rows, rows, nrows, fail_flags,
-      (Xp && iperm) ? Xp : nullptr, iperm);
-  MSC_LAUNCH_CHECK();
-  return MSC_OK;
-}
-
-int launch_gather_packed(const float* X, int d, const int32_t* perm, int64_t npacked, float* Xp,
-                         cudaStream_t st) {
-  const int blocks = int(std::max<int64_t>(
-      1, std::min<int64_t>(ceil_div(npacked * d, 256), int64_t(num_sms()) * 16)));
-  gather_packed_kernel<<<blocks, 256, 0, st>>>(X, d, perm, npacked, Xp);
+      kmma, k, cosine, knn_idx, knn_dist, fail_rows, rows, nrows, fail_flags);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
