@@ -423,6 +423,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
       const uint32_t* mask = nullptr;
       int words = 0;
       bool ordered = false;
+      const int32_t* claim = nullptr;
       const NearInit init{w.pr.cand_val, w.cand_idx, w.pr.iperm, w.pr.excl};
       if (prune) {
         // near pass -> per-row radius -> outliers to the end of each sample -> operands of the
@@ -441,6 +442,12 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
         MSC_TRY(launch_prune_plan(Xu, P.d, P.npacked, w.perm, w.items, n_items, cfg.bn, w.ctl,
                                   P.prec, w.pr, words, st));
         mask = w.pr.mask;
+        // MSC_B200_CLAIM_ORDER=0: claim in index order (reversed) instead (tuning)
+        const char* co = std::getenv("MSC_B200_CLAIM_ORDER");
+        if (!(co && *co == '0')) {
+          MSC_TRY(launch_claim_order(n_items, words, w.pr, st));
+          claim = w.pr.claim;
+        }
         MSC_TRY(launch_visit_order(w.items, n_items, cfg.bn, P.d, P.npacked, w.perm, w.ctl,
                                    w.ctl, P.prec, P.L.kmma, w.qs, w.km, w.pr, words, st,
                                    &ordered));
@@ -454,7 +461,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
                             w.ctl, P.kprime, w.cand_idx, w.cand_thr, P.kprime, st, mask, words,
                             false, prune && P.nseg == 1, prune ? w.pr.seed : nullptr,
                             prune ? &init : nullptr, nullptr,
-                            ordered ? &order : nullptr));
+                            ordered ? &order : nullptr, claim));
     }
   }
   stage_mark(st, 4);

@@ -149,6 +149,8 @@ struct PruneWs {
   int64_t* vscan;     // scan scratch over the work items
   unsigned long long* vlist;
   int64_t vcap;       // entries vlist holds
+  int32_t* claim;      // main-scan claim order of the work items (costliest first)
+  int32_t* chist;      // its bucket counts / offsets
 };
 int prune_mask_words(int64_t max_seg, int bn);
 PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items, int words,
@@ -165,6 +167,8 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
                       const PruneWs& w, int words, cudaStream_t st);
 // sorted visit lists of the main scan from the plan's masks (after launch_prune_plan): false in
 // *built when the shape does not allow them (the mask walk is used)
+// the main scan's claim order (PruneWs::claim): work items by their kept far tiles, most first
+int launch_claim_order(int64_t n_items, int words, const PruneWs& w, cudaStream_t st);
 int launch_visit_order(const WorkItem* items, int64_t n_items, int bn, int d, int64_t npacked,
                        const int32_t* perm, const Ctl* ctl, Ctl* ctl_w, int prec, int kmma,
                        const QStat* qs, const KeyMax* km, const PruneWs& w, int words,
@@ -262,7 +266,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   const uint32_t* mask = nullptr, int mask_words = 0, bool near_only = false,
                   bool reverse = false, const float* seed = nullptr,
                   const NearInit* init = nullptr, const RefineSplit* split = nullptr,
-                  const VisitOrder* order = nullptr);
+                  const VisitOrder* order = nullptr, const int32_t* claim = nullptr);
 
 // ---- rerank.cu ----
 int launch_rerank(const float* X, int d, const int32_t* perm, const SegDesc* seg, int nseg,

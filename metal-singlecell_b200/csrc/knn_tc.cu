@@ -341,6 +341,7 @@ struct TcParams {
   int mask_words;               // mask words per work item
   int near_only;                // near pass: the near tiles only
   int reverse;                  // claim the work items from the last one down
+  const int32_t* claim;         // else, when set: the claim order of the work items
   const float* seed;            // per packed query row: bound on its final k'-th value, or null
   int prof_slot;                // counter block of this launch (near / main / refine)
   // refine pass split over key ranges: *split_dev work items per refine item (1: no split), each
@@ -606,7 +607,7 @@ knn_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     }
     if (!mbar_wait(&item_empty[r_slot], r_phase ^ 1, abort_flag)) return false;
     int v = atomicAdd(P.counter, 1);
-    v = v < n_items ? (P.reverse ? n_items - 1 - v : v) : -1;
+    v = v < n_items ? (P.claim ? P.claim[v] : (P.reverse ? n_items - 1 - v : v)) : -1;
     item_ring[r_slot] = v;
     mbar_arrive(&item_full[r_slot]);         // release: the ring entry is visible to the waiters
     if (++r_slot == ITEM_RING) { r_slot = 0; r_phase ^= 1; }
@@ -1339,7 +1340,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
                   int32_t* cand_idx, float* cand_thr, int cand_stride, cudaStream_t st,
                   const uint32_t* mask, int mask_words, bool near_only, bool reverse,
                   const float* seed, const NearInit* init, const RefineSplit* split,
-                  const VisitOrder* order) {
+                  const VisitOrder* order, const int32_t* claim) {
   const int prof_slot = near_only ? 0 : (qmap ? 2 : 1);
   if (!tc_config_ok(cfg, kp, kprime)) {
     set_error("tensor-core tile config (bn=%d stages=%d kpl=%d cb=%d epi=%d pair=%d) does not fit",
@@ -1370,6 +1371,7 @@ int launch_knn_tc(int prec, const TcConfig& cfg, const void* Aop, const void* Bo
   P.mask_words = mask_words;
   P.near_only = near_only ? 1 : 0;
   P.reverse = reverse ? 1 : 0;
+  P.claim = claim;
   P.seed = seed;
   P.prof_slot = prof_slot;
   P.split_dev = split ? split->split_dev : nullptr;

@@ -600,6 +600,42 @@ __global__ void visit_count_kernel(const uint32_t* __restrict__ mask, int64_t n_
   }
 }
 
+// Claim order of the main scan's work items, costliest first.  Cost = the far tiles the plan kept
+// (every item also scans its few near tiles), in COST_BUCKETS buckets of 2^shift tiles.  The
+// persistent CTAs claim items in this order, so the long items (rows whose radius reaches many
+// key tiles) start first instead of ending the launch on a few SMs.
+constexpr int COST_BUCKETS = 256;
+__global__ void cost_hist_kernel(const int32_t* __restrict__ cnt, int64_t n_items, int shift,
+                                 int32_t* __restrict__ hist) {
+  __shared__ int32_t h[COST_BUCKETS];
+  for (int b = threadIdx.x; b < COST_BUCKETS; b += blockDim.x) h[b] = 0;
+  __syncthreads();
+  for (int64_t it = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; it < n_items;
+       it += int64_t(gridDim.x) * blockDim.x)
+    atomicAdd(&h[min(COST_BUCKETS - 1, cnt[it] >> shift)], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b < COST_BUCKETS; b += blockDim.x)
+    if (h[b]) atomicAdd(&hist[b], h[b]);
+}
+// one block of COST_BUCKETS threads: hist[b] := items in buckets above b (descending offsets)
+__global__ void cost_offsets_kernel(int32_t* __restrict__ hist) {
+  __shared__ int32_t h[COST_BUCKETS];
+  const int b = threadIdx.x;
+  h[b] = hist[b];
+  __syncthreads();
+  int32_t above = 0;
+  for (int j = b + 1; j < COST_BUCKETS; ++j) above += h[j];
+  hist[b] = above;
+}
+__global__ void cost_scatter_kernel(const int32_t* __restrict__ cnt, int64_t n_items, int shift,
+                                    int32_t* __restrict__ off, int32_t* __restrict__ order) {
+  for (int64_t it = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; it < n_items;
+       it += int64_t(gridDim.x) * blockDim.x) {
+    const int b = min(COST_BUCKETS - 1, cnt[it] >> shift);
+    order[atomicAdd(&off[b], 1)] = int32_t(it);
+  }
+}
+
 constexpr int VO_T = 256;            // threads per block of the order kernel
 constexpr int VO_SORT_MAX = 8192;    // longest list sorted (longer ones keep tile order)
 
@@ -766,6 +802,8 @@ PruneWs carve_prune(Carver& c, int64_t npacked, int nseg, int d, int64_t n_items
   w.seed = c.take<float>(npacked);
   w.roff = c.take<double>(npacked);
   w.vcnt = c.take<int32_t>(n_items);
+  w.claim = c.take<int32_t>(n_items);
+  w.chist = c.take<int32_t>(COST_BUCKETS);
   w.voff = c.take<int64_t>(n_items + 1);
   w.vscan = c.take<int64_t>(scan_i32_scratch_elems(n_items));
   // kept far tiles of all work items: at most every key tile of every work item; beyond a
@@ -844,6 +882,25 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
                                                     w.qr, w.kc, w.kr, w.sc, w.sr, w.rsub, words,
                                                     w.mask, profiling_enabled() ? 1 : 0,
                                                     max_pairs);
+  MSC_LAUNCH_CHECK();
+  return MSC_OK;
+}
+
+int launch_claim_order(int64_t n_items, int words, const PruneWs& w, cudaStream_t st) {
+  const int cgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, 8),
+                                                              int64_t(num_sms()) * 8)));
+  visit_count_kernel<<<cgrid, PR_T, 0, st>>>(w.mask, n_items, words, w.vcnt);
+  MSC_LAUNCH_CHECK();
+  int shift = 0;
+  while ((int64_t(words) * 32 >> shift) >= COST_BUCKETS) ++shift;
+  MSC_CUDA_TRY(cudaMemsetAsync(w.chist, 0, sizeof(int32_t) * COST_BUCKETS, st));
+  const int hgrid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(n_items, PR_T),
+                                                              int64_t(num_sms()) * 2)));
+  cost_hist_kernel<<<hgrid, PR_T, 0, st>>>(w.vcnt, n_items, shift, w.chist);
+  MSC_LAUNCH_CHECK();
+  cost_offsets_kernel<<<1, COST_BUCKETS, 0, st>>>(w.chist);
+  MSC_LAUNCH_CHECK();
+  cost_scatter_kernel<<<hgrid, PR_T, 0, st>>>(w.vcnt, n_items, shift, w.chist, w.claim);
   MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
