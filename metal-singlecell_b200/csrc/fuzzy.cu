@@ -14,8 +14,9 @@
 //   3. fill: every kept edge i→j written into row j's segment as one 8-byte reverse record
 //      (slot from an atomic cursor — order within the segment is arbitrary);
 //   4. per row: its own list (read straight from the kNN arrays) and its reverse records sorted by
-//      key = (column << 1 | reverse) — a warp bitonic network in registers up to 128 entries,
-//      a block network beyond — then the pairs merged (a column present in both directions) and
+//      key = (column << 1 | reverse) — a warp bitonic network in registers up to 128 entries
+//      (inline with the row's neighbours), up to 512 in a second warp-per-row pass, a block
+//      network beyond — then the pairs merged (a column present in both directions) and
 //      the unique entries written left-justified into the segment;
 //   5. exclusive scan of the unique counts → indptr; 6. copy into indices / data.
 #include "kernels.cuh"
@@ -305,6 +306,7 @@ __device__ __forceinline__ int merge_row_regs(int mode, int64_t i, int k, int L,
 }
 
 constexpr int WARP_MAX = 128;    // longest row the warp tier sorts (4 keys per lane)
+constexpr int MID_MAX = 512;     // longest row the mid tier sorts (16 keys per lane)
 
 // rows of 65..128 entries are rare: their sort stays out of line, so that the common paths (one or
 // two keys per lane) keep a small instruction footprint
@@ -345,7 +347,8 @@ merge_warp_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
       } else if (L <= WARP_MAX) {
         u = merge_row_regs4(mode, i, k, L, n, idx, vals, seg, sig2);
       } else {
-        // a long row goes to the block tier: its own list into the first k slots of its segment
+        // a long row goes to the mid or block tier: its own list into the first k slots of its
+        // segment (the block tier sorts the segment in place)
         for (int t = lane; t < k; t += 32) {
           const int32_t jj = idx[i * k + t];
           const float v = vals[i * k + t];
@@ -360,6 +363,39 @@ merge_warp_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
     // rows of the block tier write their own count there
     const int64_t p0 = my_p0, p1 = my_p1;
     if (lane < nr && k + int(p1 - p0) <= WARP_MAX) uniq[r0 + lane] = my_u;
+  }
+}
+
+// mid tier: a warp per listed long row of up to MID_MAX entries, sorted in registers (8 or 16
+// keys per lane); longer rows are listed again for the block tier.  (Rows of 129..512 entries in
+// the block tier -- a 1024-thread block with a barrier per network stage for a few hundred keys --
+// took 1.7 ms at 1.3M cells.)
+constexpr int MID_W = 8;         // warps per block
+__global__ void __launch_bounds__(MID_W * 32)
+merge_mid_kernel(int mode, int64_t n, int k, const int32_t* __restrict__ idx,
+                 const float* __restrict__ vals, const int64_t* __restrict__ rptr,
+                 int2* __restrict__ rec, const double* __restrict__ sig2,
+                 int32_t* __restrict__ uniq, const int32_t* __restrict__ big_rows,
+                 const int32_t* __restrict__ n_big, int32_t* __restrict__ huge_rows,
+                 int32_t* __restrict__ n_huge) {
+  const int lane = lane_id();
+  const int nb = *n_big;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < nb; r += nwarps) {
+    const int64_t i = big_rows[r];
+    const int64_t p0 = rptr[i];
+    const int L = k + int(rptr[i + 1] - p0);
+    int2* seg = rec + i * k + p0;
+    int u;
+    if (L <= 256) {
+      u = merge_row_regs<8>(mode, i, k, L, n, idx, vals, seg, sig2);
+    } else if (L <= MID_MAX) {
+      u = merge_row_regs<16>(mode, i, k, L, n, idx, vals, seg, sig2);
+    } else {
+      if (lane == 0) huge_rows[atomicAdd(n_huge, 1)] = int32_t(i);
+      continue;
+    }
+    if (lane == 0) uniq[i] = u;
   }
 }
 
@@ -459,7 +495,7 @@ __global__ void copy_nnz_kernel(const int64_t* __restrict__ outptr, int64_t n,
 }
 
 struct UnionWs {
-  int32_t *indeg, *cursor, *nbig, *uniq, *big;
+  int32_t *indeg, *cursor, *nbig, *uniq, *big, *huge;
   int64_t *rptr, *scan;
   int2* rec;
 };
@@ -471,6 +507,7 @@ UnionWs carve_union(Carver& c, int64_t n, int k) {
   w.nbig = c.take<int32_t>(8);
   w.uniq = c.take<int32_t>(n);
   w.big = c.take<int32_t>(n);
+  w.huge = c.take<int32_t>(n);
   w.rptr = c.take<int64_t>(n + 1);
   w.scan = c.take<int64_t>(scan_scratch_elems(n));
   // every row's k own slots plus at most n·k reverse records in all (n·(k-1) when every list
@@ -512,9 +549,15 @@ int launch_union(int mode, const int32_t* idx, const float* vals, const double* 
   merge_warp_kernel<<<g2, UW * 32, 0, st>>>(mode, n, k, idx, vals, w.rptr, w.rec, sig2, w.uniq,
                                              w.big, w.nbig);
   MSC_LAUNCH_CHECK();
+  // rows longer than WARP_MAX: a warp each up to MID_MAX (nbig[0] listed), then the longest
+  // (nbig[1] listed) a block each
+  merge_mid_kernel<<<sms * 4, MID_W * 32, 0, st>>>(mode, n, k, idx, vals, w.rptr, w.rec, sig2,
+                                                   w.uniq, w.big, w.nbig, w.huge, w.nbig + 1);
+  MSC_LAUNCH_CHECK();
   const size_t bsm = size_t(BLK_SMEM_MAX) * sizeof(int2);
   MSC_CUDA_TRY(raise_smem_cap(merge_block_kernel, bsm));
-  merge_block_kernel<<<sms, 1024, bsm, st>>>(mode, k, w.big, w.nbig, w.rptr, w.rec, sig2, w.uniq);
+  merge_block_kernel<<<sms, 1024, bsm, st>>>(mode, k, w.huge, w.nbig + 1, w.rptr, w.rec, sig2,
+                                             w.uniq);
   MSC_LAUNCH_CHECK();
   MSC_TRY(scan_excl<int32_t>(w.uniq, n, indptr, w.scan, st));
   emit_kernel<<<g2, UW * 32, 0, st>>>(n, k, w.rptr, indptr, w.rec, indices, data);

@@ -70,7 +70,7 @@ __device__ __forceinline__ float out_dist(double d2, int cosine) {
   return cosine ? __double2float_rn(d2 * 0.5) : __double2float_rn(sqrt(d2));
 }
 
-__global__ void __launch_bounds__(RR_WARPS * 32, 3)
+__global__ void __launch_bounds__(RR_WARPS * 32, 4)
 rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ perm,
               const SegDesc* __restrict__ seg, int nseg,
               int64_t npacked, const int32_t* __restrict__ cand_idx,
