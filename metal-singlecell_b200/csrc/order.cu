@@ -591,7 +591,9 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     if (l < lloyd_levels && lloyd_steps > 0) {
       node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
       MSC_LAUNCH_CHECK();
-      const int64_t nb = std::min<int64_t>(int64_t(1) << std::min(l, 20), max_split_nodes(npacked, leaf));
+      // a CTA per split node (every sample of a batch has its own nodes at every level); CTAs
+      // beyond the level's node count return at once
+      const int64_t nb = std::min<int64_t>(max_split_nodes(npacked, leaf), int64_t(num_sms()) * 4);
       lloyd_node_kernel<<<unsigned(std::max<int64_t>(1, nb)), LLOYD_T, lsmem, st>>>(
           X, d, npacked, pc, ec, SN, nstart, acc, lloyd_steps, m_max);
       MSC_LAUNCH_CHECK();
