@@ -376,7 +376,7 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   const bool prune32 = P.prune && P.candidates && P.k > 1 && P.prec == PREC_FP32;
   MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc || prune32),
                        ORDER_LEAF, w.perm, (prune || prune32) ? w.pr.leaf : nullptr, w.order_ws,
-                       w.order_ws_bytes, st));
+                       w.order_ws_bytes, st, P.max_seg));
   if (!P.candidates) {
     MSC_TRY(launch_all_rows_fail(w.perm, P.npacked, w.fail_rows, w.ctl, st));
     MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,

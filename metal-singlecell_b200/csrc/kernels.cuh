@@ -106,9 +106,10 @@ int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, in
 // near cells are near in packed order; levels = 0 gives the identity order
 // leaf_out (optional): per packed position, the first position of its leaf (-1: padding)
 size_t order_workspace_bytes(int64_t npacked, int d, int leaf);
+// max_seg: the largest sample (the extra 2-means steps run only on levels whose nodes are large)
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
                  int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
-                 cudaStream_t st);
+                 cudaStream_t st, int64_t max_seg);
 size_t scan_i32_scratch_elems(int64_t n);
 int scan_excl_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream_t st);
 int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st);

@@ -44,6 +44,9 @@ constexpr int LLOYD_LEVELS = 8;
 constexpr int LLOYD_STEPS = 5;
 constexpr int LLOYD_SAMPLES_MAX = 512;
 constexpr size_t LLOYD_SMEM_MAX = 200 * 1024;
+// ... and only while the largest sample's nodes hold at least this many cells: smaller nodes are
+// parts of one or a few clusters, and the launches would cost a small graph more than they save
+constexpr int64_t LLOYD_MIN_NODE = 8192;
 
 // One warp's 32 rows, 32 dimensions at a time: row r's dimensions c..c+31 in tile[r][0..31].
 // Lanes load a row together (one coalesced line per row and chunk), then each lane reads its own
@@ -539,7 +542,7 @@ size_t order_workspace_bytes(int64_t npacked, int d, int leaf) {
 
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
                  int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
-                 cudaStream_t st) {
+                 cudaStream_t st, int64_t max_seg) {
   if (ws_bytes < order_workspace_bytes(npacked, d, leaf)) {
     set_error("order: workspace %zu < %zu bytes", ws_bytes, order_workspace_bytes(npacked, d, leaf));
     return MSC_ERR_WORKSPACE;
@@ -588,7 +591,7 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
     side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
     MSC_LAUNCH_CHECK();
-    if (l < lloyd_levels && lloyd_steps > 0) {
+    if (l < lloyd_levels && lloyd_steps > 0 && (max_seg >> l) >= LLOYD_MIN_NODE) {
       node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
       MSC_LAUNCH_CHECK();
       // a CTA per split node (every sample of a batch has its own nodes at every level); CTAs
