@@ -339,6 +339,12 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
     service = [(r.done - r.admitted) * 1e3 for r in ok]         # admitted -> handed back
     makespan = max(r.done for r in reqs) - t_start
     cells = sum(r.n for r in ok)
+    # the five slowest requests: what they were and where their time went
+    slowest = [{"rid": r.rid, "n": r.n, "d": int(r.X.shape[1]), "k": r.n_neighbors,
+                "arrival_s": round(r.arrival - t_start, 4),
+                "queue_ms": round((r.admitted - r.arrival) * 1e3, 2),
+                "service_ms": round((r.done - r.admitted) * 1e3, 2)}
+               for r in sorted(ok, key=lambda r: -r.latency)[:5]]
     return {"requests": len(reqs), "failed": len(reqs) - len(ok),
             "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
             "mean_ms": float(np.mean(lat)) if lat else float("nan"),
@@ -346,7 +352,7 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
             "service_p50_ms": _percentile(service, 50), "service_p99_ms": _percentile(service, 99),
             "cells_per_s": cells / makespan, "makespan_s": makespan,
             "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_in_use,
-            "errors": errors}
+            "errors": errors, "slowest": slowest}
 
 
 def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None,
