@@ -397,9 +397,14 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
                          kc + g * dp, kr[g], n4, d, f2))
             atomicOr(&ubits[i], 1u << u);
         }
-        // (b) key sub-ball v of failing tile i
-        for (int x = lane; x < nv * nf; x += 32) {
-          const int i = x / nv, v = x - i * nv;
+        __syncwarp();
+        // (b) key sub-ball v of failing tile i, only for the tiles (a) left open (a tile with no
+        // open query sub-ball is skipped whatever (b) finds)
+        const uint32_t fo = __ballot_sync(FULL, lane < nf && ubits[lane] != 0u);
+        const int no = __popc(fo);
+        for (int x = lane; x < nv * no; x += 32) {
+          const int io = x / nv, v = x - io * nv;
+          const int i = __fns(fo, 0, io + 1);
           const int kti = base + __fns(fm, 0, i + 1);
           const int64_t kb0 = (int64_t(w.key0) + int64_t(kti) * bn) / SUB;
           const float rw = sr[2 * kb0 + v];
