@@ -50,16 +50,21 @@ def _ids(metric, method, precision):
 
 
 class Workspace:
-    """A reusable device scratch buffer (grown on demand)."""
+    """A reusable device scratch buffer (grown on demand; with ``pow2``, to the next power of two,
+    so that a user of many sizes re-allocates only a few times)."""
 
-    def __init__(self, device=None):
+    def __init__(self, device=None, pow2: bool = False):
         self.device = device
+        self.pow2 = pow2
         self.buf = None
 
     def get(self, nbytes: int):
         torch = _torch()
         if self.buf is None or self.buf.numel() < nbytes:
-            self.buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+            size = max(int(nbytes), 256)
+            if self.pow2:
+                size = 1 << (size - 1).bit_length()
+            self.buf = torch.empty(size, dtype=torch.uint8, device=self.device)
         return self.buf
 
 

@@ -115,6 +115,10 @@ class GraphServer:
             for i, b in enumerate(self._pinned):
                 if b is None or b.numel() < size:
                     self._pinned[i] = torch.empty(size, dtype=torch.uint8).pin_memory()
+        # a scratch workspace per slot, kept across requests (a fresh one per request made the
+        # caching allocator take new device segments for many request sizes on every slot stream)
+        from .neighbors import Workspace
+        self._ws = [Workspace(self.device, pow2=True) for _ in range(slots)]
         self._work = [collections.deque() for _ in range(slots)]
         self._work_cv = [threading.Condition(threading.Lock()) for _ in range(slots)]
         self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True)
@@ -192,7 +196,7 @@ class GraphServer:
             else:
                 Xd = self._upload(X, slot)
             res = neighbors_device(Xd, req.n_neighbors, metric=req.metric, method=req.method,
-                                   precision=req.precision)
+                                   precision=req.precision, workspace=self._ws[slot])
             res["X"] = Xd
             if req.to_host:
                 res["host_stats"] = res["stats"].to("cpu", non_blocking=True)
