@@ -340,9 +340,12 @@ def serve_leg(uuid, args, load_fracs=(0.5, 0.7, 0.85), pool_size: int = 64):
     # every slot stages embeddings up to the largest of the pool; one untimed pass over the
     # pool warms every shape
     pinned = max(x.nbytes for x in pool)
-    serve.run_offline(fresh()[:pool_size], budget, args.slots, pinned_bytes=pinned)
+    # the results are released as requests complete (a consumer that takes each graph)
+    serve.run_offline(fresh()[:pool_size], budget, args.slots, pinned_bytes=pinned,
+                      keep_results=False)
     with ClockSampler(uuid) as clk:
-        off = serve.run_offline(fresh(), budget, args.slots, pinned_bytes=pinned)
+        off = serve.run_offline(fresh(), budget, args.slots, pinned_bytes=pinned,
+                                keep_results=False)
     off["clocks"] = clk.summary()
     mean_cells = total_cells / len(data)
     sweep = []
@@ -351,7 +354,8 @@ def serve_leg(uuid, args, load_fracs=(0.5, 0.7, 0.85), pool_size: int = 64):
         rng = np.random.default_rng(7)
         arr = np.cumsum(rng.exponential(1.0 / rate, len(data))).tolist()
         with ClockSampler(uuid) as clk:
-            rep = serve.run_trace(fresh(), arr, budget, args.slots, pinned_bytes=pinned)
+            rep = serve.run_trace(fresh(), arr, budget, args.slots, pinned_bytes=pinned,
+                                  keep_results=False)
         rep.update({"load_frac_of_offline": frac, "rate_req_per_s": rate,
                     "throughput_frac_of_offline": rep["cells_per_s"] / off["cells_per_s"],
                     "clocks": clk.summary()})

@@ -84,7 +84,7 @@ class GraphServer:
     completes the request, then frees the slot and the bytes."""
 
     def __init__(self, hbm_budget: int, slots: int = 8, device=None, poll_s: float = 2e-4,
-                 pinned_bytes: int = 0):
+                 pinned_bytes: int = 0, keep_results: bool = True):
         torch = _torch()
         self.torch = torch
         self.lib = _lib.load()
@@ -92,6 +92,8 @@ class GraphServer:
             "cuda", torch.cuda.current_device())
         self.budget = int(hbm_budget)
         self.poll_s = poll_s
+        # False: a completed request keeps only its checked stats (result["host_stats"])
+        self.keep_results = keep_results
         self.slots = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
         self.free_slots = collections.deque(range(slots))
         self.pending: collections.deque[Request] = collections.deque()
@@ -262,6 +264,7 @@ class GraphServer:
                 continue
             self._wait(ev)
             req.done = self.now()
+            stats = None
             try:
                 stats = req.result["stats"].cpu().numpy()
                 _lib.check_stats(stats)
@@ -271,6 +274,10 @@ class GraphServer:
                     req.done = self.now()
             except BaseException as e:                # report per request, keep serving
                 req.error = e
+            if not self.keep_results:
+                # a consumer that only needs the outcome: the device buffers go back to the
+                # allocator now instead of piling up until the caller drops the request
+                req.result = {"host_stats": stats}
             self._release(req, slot, need)
 
     # -- scheduler ------------------------------------------------------------------------------
@@ -321,11 +328,13 @@ def _percentile(v, q):
 
 
 def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots: int = 8,
-              device=None, pinned_bytes: int = 0) -> dict:
+              device=None, pinned_bytes: int = 0, keep_results: bool = True) -> dict:
     """Submit ``reqs`` at ``arrivals`` (seconds from start); wait for all; report latency and
     throughput.  ``pinned_bytes``: page-lock each slot's staging buffer for host embeddings of up
-    to that size before the first arrival."""
-    srv = GraphServer(hbm_budget, slots, device, pinned_bytes=pinned_bytes)
+    to that size before the first arrival.  ``keep_results=False``: release every request's
+    device results as soon as it completes (a consumer that takes each result and lets it go)."""
+    srv = GraphServer(hbm_budget, slots, device, pinned_bytes=pinned_bytes,
+                      keep_results=keep_results)
     t_start = srv.now()
     for r, a in zip(reqs, arrivals):
         delay = a - (srv.now() - t_start)
@@ -360,6 +369,7 @@ def run_trace(reqs: list[Request], arrivals: list[float], hbm_budget: int, slots
 
 
 def run_offline(reqs: list[Request], hbm_budget: int, slots: int = 8, device=None,
-                pinned_bytes: int = 0) -> dict:
+                pinned_bytes: int = 0, keep_results: bool = True) -> dict:
     """All requests available at t=0: the batched-offline throughput."""
-    return run_trace(reqs, [0.0] * len(reqs), hbm_budget, slots, device, pinned_bytes)
+    return run_trace(reqs, [0.0] * len(reqs), hbm_budget, slots, device, pinned_bytes,
+                     keep_results)

@@ -155,3 +155,14 @@ def test_cancel_before_admission(fake_gpu):
     assert isinstance(queued[1].error, CancelledError)
     assert first.error is None and queued[0].error is None and queued[2].error is None
     assert fake_gpu == [50, 41, 43]                  # the cancelled request never started
+
+
+def test_results_released_when_not_kept(fake_gpu):
+    srv = serve.GraphServer(hbm_budget=100, slots=2, keep_results=False)
+    reqs = [srv.submit(_req(n)) for n in (20, 30)]
+    _wait(reqs)
+    srv.close()
+    assert all(r.error is None for r in reqs)
+    for r in reqs:
+        assert set(r.result) == {"host_stats"}
+        assert np.array_equal(r.result["host_stats"], np.zeros(8, np.int64))
