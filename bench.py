@@ -627,6 +627,7 @@ def run_ours(args):
         configs = {"plain_10k": config_leg("plain", uuid),
                    "precision_200k": config_leg("precision", uuid),
                    "batch_64": batch_leg(uuid, args.batch_samples),
+                   "bbknn_200k": bbknn_measure(200_000, 8, 3, "fp16", 3, 3, True, 0.0),
                    "serve": serve_leg(uuid, args)}
 
     if rank == 0:
@@ -871,6 +872,12 @@ def bbknn_cpu_baseline(X, batch, kwb, budget_s: float = 15.0):
 
 
 def run_bbknn(args):
+    line = bbknn_measure(args.n, args.batches, args.neighbors_within_batch, args.precision,
+                         args.steps, args.warmup, args.skip_cpu, args.ref_budget)
+    print(json.dumps(line), flush=True)
+
+
+def bbknn_measure(n_cells, batches, kwb, precision, steps, warmup, skip_cpu, ref_budget):
     """Batch-balanced graph (pp.bbknn): every cell's neighbours_within_batch nearest cells of each
     batch, fuzzy set, distances graph and trimming; cells/s with the embedding resident, the kNN
     stage alone, and end to end through the host call."""
@@ -878,16 +885,15 @@ def run_bbknn(args):
     from msc_b200 import bbknn as bbm, neighbors as nbm, _lib
     torch.cuda.set_device(0)
     lib = _lib.load()
-    X, batch, desc = bbknn_workload(args.n, args.batches)
+    X, batch, desc = bbknn_workload(n_cells, batches)
     n, d = X.shape
-    kwb = args.neighbors_within_batch
     _, codes, counts = bbm.batch_codes(batch)
     Xd = torch.from_numpy(X).cuda()
     cd = torch.from_numpy(codes).cuda()
     ws = nbm.Workspace(Xd.device)
 
     def graph():
-        return bbm.bbknn_device(Xd, cd, counts, kwb, precision=args.precision, workspace=ws)
+        return bbm.bbknn_device(Xd, cd, counts, kwb, precision=precision, workspace=ws)
 
     def timed(fn, reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -899,7 +905,7 @@ def run_bbknn(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps, out
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         res = graph()
     uuid = None
     try:
@@ -907,7 +913,7 @@ def run_bbknn(args):
     except Exception:
         uuid = None
     with ClockSampler(uuid) as cs:
-        ms, res = timed(graph, args.steps)
+        ms, res = timed(graph, steps)
     stats = res["stats"].cpu().numpy()
     _lib.check_stats(stats)
     K = res["K"]
@@ -917,28 +923,28 @@ def run_bbknn(args):
     dist = torch.empty((n, K), dtype=torch.float32, device=Xd.device)
     st = torch.cuda.current_stream().cuda_stream
     kbytes = lib.msc_bbknn_workspace_bytes(n, d, cptr, counts.size, kwb,
-                                           _lib.PRECISION[args.precision])
+                                           _lib.PRECISION[precision])
     kws = ws.get(kbytes)
     knn = lambda: _lib.check(lib.msc_bbknn_knn(Xd.data_ptr(), n, d, cd.data_ptr(), cptr,
-                                               counts.size, kwb, _lib.PRECISION[args.precision],
+                                               counts.size, kwb, _lib.PRECISION[precision],
                                                idx.data_ptr(), dist.data_ptr(), 0, kws.data_ptr(),
                                                kws.numel(), st), "msc_bbknn_knn")
     knn()
-    knn_ms, _ = timed(knn, args.steps)
+    knn_ms, _ = timed(knn, steps)
     # end to end through the host call (host embedding in, host CSR matrices out)
-    bbm.bbknn(X, batch, kwb, n_pcs=None, precision=args.precision)
+    bbm.bbknn(X, batch, kwb, n_pcs=None, precision=precision)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        dm, cm, _ = bbm.bbknn(X, batch, kwb, n_pcs=None, precision=args.precision)
-    e2e_ms = 1000.0 * (time.perf_counter() - t0) / args.steps
+    for _ in range(steps):
+        dm, cm, _ = bbm.bbknn(X, batch, kwb, n_pcs=None, precision=precision)
+    e2e_ms = 1000.0 * (time.perf_counter() - t0) / steps
     flop = 2.0 * d * float(n) * float(n)                  # Σ_b 2·d·n·n_b
     pk, pk_kind = peaks()
     peak = pk.get("bf16_tflops_sustained", 1400.0)
     line = {"metric": "bbknn: batch-balanced graph cells/s", "value": n / (ms / 1000),
-            "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "unit": "cells/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": ms, "higher_is_better": True, "data": "synthetic",
-            "dtype": args.precision,
+            "dtype": precision,
             "config": {"workload": desc, "neighbors_within_batch": kwb, "K": K,
                        "batch_sizes": [int(c) for c in counts], "trim": res["trim"]},
             "e2e": {"value": n / (e2e_ms / 1000), "unit": "cells/s", "ms_per_step": e2e_ms,
@@ -954,9 +960,9 @@ def run_bbknn(args):
                       "rescanned": int(stats[_lib.STAT_RESCANNED]),
                       "precision": int(stats[_lib.STAT_PRECISION])},
             "clocks": cs.summary()}
-    if not args.skip_cpu:
-        line["cpu_baseline"] = bbknn_cpu_baseline(X, batch, kwb, args.ref_budget)
-    print(json.dumps(line), flush=True)
+    if not skip_cpu:
+        line["cpu_baseline"] = bbknn_cpu_baseline(X, batch, kwb, ref_budget)
+    return line
 
 
 def main(argv=None):
