@@ -182,6 +182,26 @@ far_b_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
   }
 }
 
+__global__ void __launch_bounds__(OR_T)
+side_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+            const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+            const int32_t* __restrict__ ne, const float* __restrict__ da,
+            const unsigned long long* __restrict__ best_b, int32_t* __restrict__ side) {
+  __shared__ RowTile tiles[OR_W];
+  RowTile& tile = tiles[warp_id()];
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
+       b += stride) {
+    const int64_t p = b + lane_id();
+    int s = 0, e = 0;
+    if (p < npacked) { s = ns[p]; e = ne[p]; }
+    const bool active = p < npacked && e - s > leaf;
+    const int32_t row = active ? perm[p] : -1;
+    const float db = warp_row_d2(X, d, row, active ? perm[far_pos(best_b[s])] : 0, tile);
+    if (p < npacked) side[p] = active && da[p] > db ? 1 : 0;   // nearer to b: second half
+  }
+}
+
 __global__ void scatter_kernel(int64_t npacked, int leaf, const int32_t* __restrict__ perm,
                                const int32_t* __restrict__ ns, const int32_t* __restrict__ ne,
                                const int32_t* __restrict__ side, const int64_t* __restrict__ S,
@@ -233,11 +253,7 @@ __global__ void __launch_bounds__(OR_T)
 side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
-                int32_t* __restrict__ side, double* __restrict__ acc,
-                const float* __restrict__ da, const unsigned long long* __restrict__ best_b) {
-  // With da / best_b the first assignment happens here too: a cell goes to side 1 when it is
-  // nearer to b (the node's second far cell) than to a, its squared distance to a being da; the
-  // row is loaded once for the distance and the sums, and side[] is written for the later passes.
+                const int32_t* __restrict__ side, double* __restrict__ acc) {
   // Runs that lie inside one node (almost all of them) are first combined across the warps of the
   // block in shared memory, so that at the top levels, where every run belongs to the same one or
   // two nodes, a block issues one set of atomics instead of one per warp.
@@ -257,9 +273,7 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
       if (cur < 0) return;
       flushed = true;
       double* a = acc + cur * (2 * d + 2);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (j >= per) break;
+      for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
         if (t < d) {
           if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
@@ -277,23 +291,17 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
       const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
       // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
       // only loads row data (independent from position to position)
-      int32_t idh[2], rowh[2], sdh[2], brh[2];
-      float dah[2];
+      int32_t idh[2], rowh[2], sdh[2];
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
         const int64_t p = p0 + 32 * hh + lane;
-        idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0; brh[hh] = 0; dah[hh] = 0.f;
+        idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
         if (p < p1) {
           const int st = ns[p];
           if (ne[p] - st > leaf) {
             idh[hh] = int32_t(S[st]);
             rowh[hh] = perm[p];
-            if (da) {
-              dah[hh] = da[p];
-              brh[hh] = perm[far_pos(best_b[st])];
-            } else {
-              sdh[hh] = side[p];
-            }
+            sdh[hh] = side[p];
           }
         }
       }
@@ -303,40 +311,13 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
         const int32_t id = __shfl_sync(FULL, hh ? idh[1] : idh[0], jj & 31);
         if (id < 0) continue;                // warp-uniform
         const int32_t rw = __shfl_sync(FULL, hh ? rowh[1] : rowh[0], jj & 31);
-        bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
+        const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
         if (id != cur) { flush(); cur = id; }
         const float* x = X + int64_t(rw) * d;
-        float xv[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (j >= per) break;
-          const int t = lane + 32 * j;
-          xv[j] = t < d ? x[t] : 0.f;
-        }
-        if (da) {                              // warp-uniform
-          const int32_t br = __shfl_sync(FULL, hh ? brh[1] : brh[0], jj & 31);
-          const float dap = __shfl_sync(FULL, hh ? dah[1] : dah[0], jj & 31);
-          const float* y = X + int64_t(br) * d;
-          float db = 0.f;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (j >= per) break;
-            const int t = lane + 32 * j;
-            if (t < d) {
-              const float u = xv[j] - y[t];
-              db = fmaf(u, u, db);
-            }
-          }
-          for (int o = 16; o > 0; o >>= 1) db += __shfl_xor_sync(FULL, db, o);
-          one = dap > db;                      // nearer to b: second half
-          if (lane == 0) side[p0 + jj] = one ? 1 : 0;
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (j >= per) break;
+        for (int j = 0; j < per; ++j) {
           const int t = lane + 32 * j;
           if (t < d) {
-            if (one) s1[j] += xv[j]; else s0[j] += xv[j];
+            if (one) s1[j] += x[t]; else s0[j] += x[t];
           }
         }
         if (one) c1 += 1.0; else c0 += 1.0;
@@ -346,9 +327,7 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     int64_t slot_node = -1;
     if (cur >= 0 && !flushed) {
       slot_node = cur;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (j >= per) break;
+      for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
         if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
       }
@@ -603,16 +582,14 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     MSC_LAUNCH_CHECK();
     far_b_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a, da, best_b);
     MSC_LAUNCH_CHECK();
+    side_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
+    MSC_LAUNCH_CHECK();
     // one 2-means step: side means, then the nearer mean
     split_start_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, sc, ec, sflag);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
     MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-    // the first assignment (nearer of a and b) and the side sums in one pass over the rows; the
-    // positions outside split nodes keep side 0 for the partition scan
-    MSC_CUDA_TRY(cudaMemsetAsync(side, 0, sizeof(int32_t) * npacked, st));
-    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc, da,
-                                           best_b);
+    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
     MSC_LAUNCH_CHECK();
     if (l < lloyd_levels && lloyd_steps > 0 && (max_seg >> l) >= LLOYD_MIN_NODE) {
       node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
