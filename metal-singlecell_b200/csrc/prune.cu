@@ -329,7 +329,7 @@ constexpr int PLAN_WARPS = 4;
 constexpr int PLAN_WORDS = 8;     // mask words (256 key tiles) per warp task
 constexpr int PLAN_MAX_PAIRS = 32;  // sub-ball pairs tested per key tile (one per lane);
                                     // MSC_B200_PLAN_PAIRS overrides (tuning)
-__global__ void __launch_bounds__(PLAN_WARPS * 32)
+__global__ void __launch_bounds__(PLAN_WARPS * 32, 6)
 plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, int dp,
             const Ctl* ctl, int prec, const float* __restrict__ qc, const float* __restrict__ qr,
             const float* __restrict__ kc, const float* __restrict__ kr,
