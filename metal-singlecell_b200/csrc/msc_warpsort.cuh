@@ -49,6 +49,37 @@ __device__ __forceinline__ void warp_sort64_d(double& v0, int& i0, double& v1, i
   v0 = lv; i0 = li; v1 = hv; i1 = hi;
 }
 
+// The same networks on float values alone (no index): fminf / fmaxf, one shuffle per step.  For
+// values without NaN the multiset is sorted exactly; ties need no index since only the values are
+// kept.
+__device__ __forceinline__ void cmpx_f(float& v, int j, bool keep_min) {
+  const float ov = __shfl_xor_sync(FULL, v, j);
+  v = keep_min ? fminf(v, ov) : fmaxf(v, ov);
+}
+__device__ __forceinline__ void warp_sort32_f(float& v) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) cmpx_f(v, j, ((lane & j) == 0) == ((lane & k) == 0));
+}
+__device__ __forceinline__ void warp_merge32_f(float& v) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) cmpx_f(v, j, (lane & j) == 0);
+}
+// 64 values held as v0 (lane-slot 0) and v1 (lane-slot 1), ascending over (slot, lane)
+__device__ __forceinline__ void warp_sort64_f(float& v0, float& v1) {
+  warp_sort32_f(v0);
+  warp_sort32_f(v1);
+  const float r = __shfl_sync(FULL, v1, 31 - lane_id());
+  float lo = fminf(v0, r), hi = fmaxf(v0, r);
+  warp_merge32_f(lo);
+  warp_merge32_f(hi);
+  v0 = lo;
+  v1 = hi;
+}
+
 // The `kk` (<= 32·SLOTS) smallest pairs offered so far, ascending: entry s·32 + lane in slot s of
 // lane `lane`.  offer() takes one pair per lane; a batch with no pair below the current kk-th
 // costs one vote.  A batch is sorted and cascaded through the slots from the last: each step

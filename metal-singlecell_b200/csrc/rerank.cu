@@ -81,6 +81,7 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
               const int32_t* __restrict__ rows, const int32_t* __restrict__ nrows,
               int32_t* __restrict__ fail_flags) {
   __shared__ __align__(16) float xs_all[RR_WARPS][MSC_MAX_D];
+  __shared__ int wsc_all[RR_WARPS][32];                 // a row's window, compacted
   const int lane = lane_id(), wib = warp_id();
   float* xs = xs_all[wib];
   const int kk = k - 1;
@@ -128,24 +129,57 @@ rerank_kernel(const float* __restrict__ X, int d, const int32_t* __restrict__ pe
         }
       }
     }
-    // 2. sort by (FP32 distance, index)
-    {
+    // 2.-3. B = the (k-1)-th smallest FP32 value; the window = the candidates within B's rounding
+    //    bound, recomputed in FP64 (summed in dimension order) and ordered by (FP64 value, index).
+    //    Fast path (no NaN, k-1 <= window <= 32): B from a values-only sort, the window's ids
+    //    compacted into lanes 0..m-1, one FP64 pass and a 32-pair sort.  The window holds the same
+    //    candidates and the same FP64 values as on the general path (two 64-pair sorts), so the
+    //    outputs are the same.
+    const double INF = __longlong_as_double(0x7ff0000000000000ll);
+    double g0 = INF, g1 = INF, Dk = INF;
+    int h0 = INT32_MAX, h1 = INT32_MAX, m = 0;
+    bool fast = false;
+    if (!__any_sync(FULL, isnan(e0) || isnan(e1))) {
+      float s0 = e0, s1 = e1;
+      warp_sort64_f(s0, s1);
+      const float Bf = __shfl_sync(FULL, kk - 1 < 32 ? s0 : s1, (kk - 1) & 31);
+      const double limf = double(Bf) * (1.0 + 3.0 * delta) + 1e-300;
+      const bool w0 = c0 >= 0 && double(e0) <= limf;
+      const bool w1 = c1 >= 0 && double(e1) <= limf;
+      const unsigned b0 = __ballot_sync(FULL, w0), b1 = __ballot_sync(FULL, w1);
+      m = __popc(b0) + __popc(b1);
+      if (m >= kk && m <= 32) {                          // warp-uniform
+        int* wsc = wsc_all[wib];
+        const unsigned lt = (1u << lane) - 1u;
+        if (w0) wsc[__popc(b0 & lt)] = c0;
+        if (w1) wsc[__popc(b0) + __popc(b1 & lt)] = c1;
+        __syncwarp();
+        int cw = lane < m ? wsc[lane] : INT32_MAX;
+        double gw = lane < m ? d2_f64(xs, X + int64_t(cw) * d, d) : INF;
+        __syncwarp();                                    // wsc is read before the next row
+        warp_sort32_d(gw, cw);
+        g0 = gw; h0 = cw;
+        Dk = __shfl_sync(FULL, g0, kk - 1);
+        fast = true;
+      }
+    }
+    if (!fast) {
+      // general path: sort all 64 (FP32 value, index) pairs, then the window's FP64 values
       double v0 = e0, v1 = e1;
       int i0 = c0 >= 0 ? c0 : INT32_MAX, i1 = c1 >= 0 ? c1 : INT32_MAX;
       warp_sort64_d(v0, i0, v1, i1);
-      e0 = float(v0); e1 = float(v1); c0 = i0; c1 = i1;
+      const float se0 = float(v0), se1 = float(v1);
+      const float B = __shfl_sync(FULL, kk - 1 < 32 ? se0 : se1, (kk - 1) & 31);
+      const double lim = double(B) * (1.0 + 3.0 * delta) + 1e-300;
+      const bool w0 = i0 != INT32_MAX && double(se0) <= lim;
+      const bool w1 = i1 != INT32_MAX && double(se1) <= lim;
+      g0 = w0 ? d2_f64(xs, X + int64_t(i0) * d, d) : INF;
+      g1 = w1 ? d2_f64(xs, X + int64_t(i1) * d, d) : INF;
+      m = __popc(__ballot_sync(FULL, w0)) + __popc(__ballot_sync(FULL, w1));
+      h0 = i0; h1 = i1;
+      warp_sort64_d(g0, h0, g1, h1);
+      Dk = __shfl_sync(FULL, kk - 1 < 32 ? g0 : g1, (kk - 1) & 31);
     }
-    const float B = __shfl_sync(FULL, kk - 1 < 32 ? e0 : e1, (kk - 1) & 31);
-    // 3. FP64 for the window
-    const double lim = double(B) * (1.0 + 3.0 * delta) + 1e-300;
-    const bool w0 = c0 != INT32_MAX && double(e0) <= lim;
-    const bool w1 = c1 != INT32_MAX && double(e1) <= lim;
-    double g0 = w0 ? d2_f64(xs, X + int64_t(c0) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
-    double g1 = w1 ? d2_f64(xs, X + int64_t(c1) * d, d) : __longlong_as_double(0x7ff0000000000000ll);
-    const int m = __popc(__ballot_sync(FULL, w0)) + __popc(__ballot_sync(FULL, w1));
-    int h0 = c0, h1 = c1;
-    warp_sort64_d(g0, h0, g1, h1);
-    const double Dk = __shfl_sync(FULL, kk - 1 < 32 ? g0 : g1, (kk - 1) & 31);
     // 4. certificate
     bool cert;
     const int nvalid = int(min64(ns - 1, kprime));
