@@ -273,9 +273,7 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
       if (cur < 0) return;
       flushed = true;
       double* a = acc + cur * (2 * d + 2);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {        // per <= 4: the sums stay in registers
-        if (j >= per) break;
+      for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
         if (t < d) {
           if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
@@ -316,9 +314,7 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
         const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
         if (id != cur) { flush(); cur = id; }
         const float* x = X + int64_t(rw) * d;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {        // per <= 4: the sums stay in registers
-          if (j >= per) break;
+        for (int j = 0; j < per; ++j) {
           const int t = lane + 32 * j;
           if (t < d) {
             if (one) s1[j] += x[t]; else s0[j] += x[t];
@@ -331,9 +327,7 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     int64_t slot_node = -1;
     if (cur >= 0 && !flushed) {
       slot_node = cur;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {        // per <= 4: the sums stay in registers
-        if (j >= per) break;
+      for (int j = 0; j < per; ++j) {
         const int t = lane + 32 * j;
         if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
       }
