@@ -6,10 +6,14 @@
 // and accepts ~0.99 recall; here every row is either proven exact or re-scanned exactly:
 //
 //   1. FP32 direct differences Σ(x_t − y_t)² for all k' candidates (one lane per candidate);
-//   2. warp bitonic sort by FP32 distance; the (k−1)-th value B bounds the answer;
+//   2. the (k−1)-th smallest FP32 value B bounds the answer;
 //   3. candidates within B·(1+3δ) (δ = (d+4)·2⁻²⁴, the FP32 sum's relative error bound) are
 //      recomputed in FP64 and ordered by (FP64 distance, index) — FP64 only breaks ties at the
-//      k-th boundary, and gives the returned distances float32(sqrt(d²₆₄));
+//      k-th boundary, and gives the returned distances float32(sqrt(d²₆₄)).  Usually the window
+//      holds k−1 … 32 candidates: B then comes from a sort of the 64 values alone, the window's
+//      ids are compacted into lanes 0..m−1 for one FP64 pass and a 32-pair sort.  Otherwise (a
+//      wider window, or NaN) all 64 (value, index) pairs are sorted, then the window's FP64
+//      values.  Both give the same set, the same FP64 values and the same order;
 //   4. certificate: every key outside the candidate list has approximate value v̂ ≥ T (the
 //      k'-th smallest kept), so its true squared distance is ≥ (|z_x|² + T − ε)/f² where ε
 //      bounds |v̂ − v| from the operand residual norms recorded by the packing kernel.  If the
