@@ -457,111 +457,97 @@ plan_kernel(const WorkItem* __restrict__ items, int64_t n_items, int bn, int d, 
 // tests for almost every query tile even when no key of it is near.  Here every key is a ball of
 // radius 0: the pair is skipped when every key y satisfies |c_Q − y| − r_Q = L > 0 and
 // f²·L² > R_Q (c_Q, r_Q the query tile's ball, R_Q the largest R of its rows), the plan's own
-// separation rule.  The tile's keys are staged in shared memory once; the query tiles that kept
-// it are tested POINT_BATCH at a time (a thread per key), and a pair every key clears has its bit
-// taken out of the mask.
+// separation rule.  The tile's keys are staged once in shared memory, dimension-major (a warp's
+// 32 keys of one dimension hit 32 banks); the query tiles that kept the tile are listed, and each
+// warp takes whole query tiles from the list: its lanes test 8 keys each and stop at the first key
+// that is not separated.  A pair every key clears has its bit taken out of the mask.
 constexpr int POINT_T = 256;
-constexpr int POINT_BATCH = 8;
-constexpr int POINT_SLICES = 8;    // item slices per key tile (long lists of the outlier tiles)
+constexpr int POINT_SLICES = 2;    // item slices per key tile (the long lists of outlier tiles)
+constexpr int POINT_LIST = 2048;   // listed query tiles per round
 __global__ void __launch_bounds__(POINT_T)
 point_test_kernel(const float* __restrict__ X, int d, int dp, const int32_t* __restrict__ perm,
                   const WorkItem* __restrict__ items, int64_t n_items, int bn, int words,
                   const Ctl* ctl, int prec, const float* __restrict__ qc,
                   const float* __restrict__ qr, const double* __restrict__ rsub,
                   uint32_t* __restrict__ mask, int64_t nkt_all, int prof) {
-  extern __shared__ float ys[];                       // [256][dp] this tile's keys
-  __shared__ float cq[POINT_BATCH][MSC_MAX_D];
-  __shared__ float rq_s[POINT_BATCH];
-  __shared__ double Rq_s[POINT_BATCH];
-  __shared__ int32_t it_s[POINT_BATCH], kt_s[POINT_BATCH];
-  __shared__ int32_t list[POINT_T * 4];
-  __shared__ int nlist;
-  __shared__ unsigned wok[POINT_BATCH][POINT_T / 32];
+  extern __shared__ float ys[];                       // [d][256] this tile's keys
+  __shared__ int32_t list[POINT_LIST];
+  __shared__ int nlist, next;
+  __shared__ unsigned pad_bits[256 / 32];             // keys that are padding rows
   const int tid = threadIdx.x, lane = lane_id(), wib = warp_id();
+  constexpr int NW = POINT_T / 32;
   const double f = op_scale(prec, ctl);
   const double f2 = f * f;
+  const double shrink = 1.0 - double(d + 8) * 0x1p-23;
   long long cleared = 0;
+  if (tid < 256 / 32) pad_bits[tid] = 0u;
   for (int64_t gb = blockIdx.x; gb < nkt_all * POINT_SLICES; gb += gridDim.x) {   // block-uniform
     const int64_t g = gb / POINT_SLICES;
     const int slice = int(gb - g * POINT_SLICES);
     const int64_t p0 = g * 256;
-    // this tile's keys (a padding row never counts: it is marked with a NaN first coordinate)
-    for (int e = tid; e < 256 * dp; e += POINT_T) {
-      const int r = e / dp, t = e - r * dp;
+    __syncthreads();                                   // the previous tile's keys are done with
+    // keys: a warp per row (coalesced), dimension-major in shared memory
+    for (int r = wib; r < 256; r += NW) {
       const int32_t i = perm[p0 + r];
-      ys[e] = i < 0 ? (t == 0 ? __int_as_float(0x7fc00000) : 0.f)
-                    : (t < d ? X[int64_t(i) * d + t] : 0.f);
+      for (int t = lane; t < d; t += 32) ys[t * 256 + r] = i < 0 ? 0.f : X[int64_t(i) * d + t];
+      const unsigned pb = __ballot_sync(FULL, i < 0);  // warp-uniform i: all lanes agree
+      if (lane == 0) atomicOr(&pad_bits[r >> 5], (pb ? 1u : 0u) << (r & 31));
     }
-    // the items of this slice that kept the tile, in chunks of the list size
-    for (int64_t base = slice; base < n_items; base += int64_t(POINT_SLICES) * POINT_T * 4) {
-      __syncthreads();                                 // every thread has read the last count
-      if (tid == 0) nlist = 0;
+    for (int64_t base = slice; base < n_items; base += int64_t(POINT_SLICES) * POINT_LIST) {
       __syncthreads();
-      for (int j = tid; j < POINT_T * 4; j += POINT_T) {
+      if (tid == 0) { nlist = 0; next = 0; }
+      __syncthreads();
+      for (int j = tid; j < POINT_LIST; j += POINT_T) {
         const int64_t it = base + int64_t(j) * POINT_SLICES;
         if (it < n_items) {
           const WorkItem w = items[it];
           const int64_t rel = p0 - w.key0;
           if (rel >= 0 && rel < w.nkeys) {
             const int kt = int(rel / bn);
-            if (mask[it * words + (kt >> 5)] & (1u << (kt & 31))) list[atomicAdd(&nlist, 1)] = int32_t(it);
+            if (mask[it * words + (kt >> 5)] & (1u << (kt & 31)))
+              list[atomicAdd(&nlist, 1)] = int32_t(it);
           }
         }
       }
       __syncthreads();
       const int nl = nlist;
-      for (int b0 = 0; b0 < nl; b0 += POINT_BATCH) {    // block-uniform
-        const int nb = min(POINT_BATCH, nl - b0);
-        if (tid < nb) {
-          const int32_t it = list[b0 + tid];
-          const WorkItem w = items[it];
-          const int64_t qt = w.qrow0 / QTILE, sb0 = w.qrow0 / SUB;
-          double R = 0.0;
-          for (int j = 0; j < 4; ++j) R = fmax(R, rsub[sb0 + j]);
-          it_s[tid] = it;
-          kt_s[tid] = int((p0 - w.key0) / bn);
-          rq_s[tid] = qr[qt];
-          Rq_s[tid] = R;
-        }
-        __syncthreads();
-        for (int e = tid; e < nb * d; e += POINT_T) {
-          const int bb = e / d, t = e - bb * d;
-          cq[bb][t] = qc[int64_t(items[list[b0 + bb]].qrow0 / QTILE) * dp + t];
-        }
-        __syncthreads();
-        const float* y = ys + tid * dp;
-        const bool pad = isnan(y[0]);
-        for (int bb = 0; bb < nb; ++bb) {
+      for (;;) {                                       // warp-uniform: a query tile per warp
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&next, 1);
+        k = __shfl_sync(FULL, k, 0);
+        if (k >= nl) break;
+        const int32_t it = list[k];
+        const WorkItem w = items[it];
+        const int64_t qt = w.qrow0 / QTILE, sb0 = w.qrow0 / SUB;
+        double R = 0.0;
+        for (int j = 0; j < 4; ++j) R = fmax(R, rsub[sb0 + j]);
+        const float rq = qr[qt];
+        if (!(rq >= 0.f) || !(R < 1e300)) continue;     // nothing provable for this tile
+        const float* c = qc + qt * dp;
+        bool all = true;
+        for (int kk = 0; kk < 8 && all; ++kk) {          // keys lane + 32·kk
+          const int key = lane + 32 * kk;
           bool sep = true;
-          if (!pad) {
+          if (!((pad_bits[key >> 5] >> (key & 31)) & 1u)) {
             float acc = 0.f;
             for (int t = 0; t < d; ++t) {
-              const float u = cq[bb][t] - y[t];
+              const float u = c[t] - ys[t * 256 + key];
               acc = fmaf(u, u, acc);
             }
-            const double R = Rq_s[bb];
-            const double lo = double(acc) * (1.0 - double(d + 8) * 0x1p-23);
-            const double L = sqrt(lo) - double(rq_s[bb]);
-            sep = rq_s[bb] >= 0.f && R < 1e300 && L > 0.0 && f2 * L * L > R * (1.0 + 1e-9);
+            const double L = sqrt(double(acc) * shrink) - double(rq);
+            sep = L > 0.0 && f2 * L * L > R * (1.0 + 1e-9);
           }
-          const unsigned all = __all_sync(FULL, sep);
-          if (lane == 0) wok[bb][wib] = all;
+          all = __all_sync(FULL, sep);
         }
-        __syncthreads();
-        if (tid < nb) {
-          bool all = true;
-          for (int w8 = 0; w8 < POINT_T / 32; ++w8) all = all && wok[tid][w8];
-          if (all) {
-            const int64_t it = it_s[tid];
-            const int kt = kt_s[tid];
-            atomicAnd(&mask[it * words + (kt >> 5)], ~(1u << (kt & 31)));
-            ++cleared;
-          }
+        if (all && lane == 0) {
+          const int kt = int((p0 - w.key0) / bn);
+          atomicAnd(&mask[int64_t(it) * words + (kt >> 5)], ~(1u << (kt & 31)));
+          ++cleared;
         }
-        __syncthreads();
       }
     }
-    __syncthreads();                                   // ys is rewritten for the next tile
+    __syncthreads();
+    if (tid < 256 / 32) pad_bits[tid] = 0u;            // for the next tile
   }
   if (prof && cleared) atomicAdd(&g_prune_tiles[0], (unsigned long long)(-cleared));
 }
@@ -1005,7 +991,7 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
   // point test of the kept pairs (MSC_B200_POINT_TEST=0 turns it off: tuning)
   const char* pt_env = std::getenv("MSC_B200_POINT_TEST");
   if (!(pt_env && *pt_env == '0') && bn == 256) {
-    const size_t psmem = size_t(256) * dp * sizeof(float);
+    const size_t psmem = size_t(256) * d * sizeof(float);
     MSC_CUDA_TRY(raise_smem_cap(point_test_kernel, psmem));
     const int64_t nblk = nk * POINT_SLICES;
     const int ptgrid = int(std::max<int64_t>(1, std::min<int64_t>(nblk, int64_t(num_sms()) * 8)));
