@@ -988,9 +988,12 @@ int launch_prune_plan(const float* X, int d, int64_t npacked, const int32_t* per
                                                     w.mask, profiling_enabled() ? 1 : 0,
                                                     max_pairs);
   MSC_LAUNCH_CHECK();
-  // point test of the kept pairs (MSC_B200_POINT_TEST=0 turns it off: tuning)
+  // point test of the kept pairs, opt-in (MSC_B200_POINT_TEST=1).  Measured at 1.3M × 50: far
+  // tiles kept 2.63 M → 1.63 M and main scan 33.4 → 28.0 ms, but the test itself costs ~15 ms
+  // (every key of a separated pair is checked over all d dimensions on the CUDA cores), so the
+  // graph takes 81.0 ms against 72.6 without it
   const char* pt_env = std::getenv("MSC_B200_POINT_TEST");
-  if (!(pt_env && *pt_env == '0') && bn == 256) {
+  if ((pt_env && *pt_env == '1') && bn == 256) {
     const size_t psmem = size_t(256) * d * sizeof(float);
     MSC_CUDA_TRY(raise_smem_cap(point_test_kernel, psmem));
     const int64_t nblk = nk * POINT_SLICES;

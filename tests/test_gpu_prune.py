@@ -120,3 +120,30 @@ def test_ordered_walk_equals_full_scan():
     ridx, _, rdist = oracle.knn_exact(X, 15, rows=rows)
     np.testing.assert_array_equal(oi[rows], ridx.astype(np.int32))
     np.testing.assert_array_equal(od[rows], rdist)
+
+
+def test_point_test_equals_full_scan():
+    # MSC_B200_POINT_TEST=1: kept pairs whose every key is separated from the query tile's ball
+    # are dropped from the plan; the lists must equal the full scan's and the oracle's, and the
+    # plan must keep fewer far tiles than without the test
+    X = synth.gaussian_mixture(60_000, 50, 40, seed=17, sizes="lognormal", noise_frac=0.01)
+    fi, fd, _ = _knn(X, 15, "fp16", prune=False)
+    base = _visited_fraction(X, 15, "fp16")
+    old = os.environ.get("MSC_B200_POINT_TEST")
+    os.environ["MSC_B200_POINT_TEST"] = "1"
+    try:
+        pi, pd, ps = _knn(X, 15, "fp16", prune=True)
+        frac = _visited_fraction(X, 15, "fp16")
+    finally:
+        if old is None:
+            del os.environ["MSC_B200_POINT_TEST"]
+        else:
+            os.environ["MSC_B200_POINT_TEST"] = old
+    assert int(ps[_lib.STAT_TIMEOUT]) == 0
+    np.testing.assert_array_equal(pi, fi, err_msg="point test vs full scan: indices")
+    np.testing.assert_array_equal(pd, fd, err_msg="point test vs full scan: distances")
+    rows = np.sort(np.random.default_rng(8).choice(X.shape[0], 1000, replace=False))
+    ridx, _, rdist = oracle.knn_exact(X, 15, rows=rows)
+    np.testing.assert_array_equal(pi[rows], ridx.astype(np.int32))
+    np.testing.assert_array_equal(pd[rows], rdist)
+    assert frac < base, f"point test kept {frac:.3f} of the far tiles, {base:.3f} without"
