@@ -161,6 +161,7 @@ struct KnnWs {
   float* cand_thr;
   int32_t* fail_rows;
   int32_t* perm;          // packed row -> original row (-1: padding)
+  float* Xo;              // the rows projected for the locality order (d > ORDER_PROJ_D)
   void* order_ws;
   size_t order_ws_bytes;
   // refine pass
@@ -296,7 +297,9 @@ KnnWs carve_knn(Carver& c, const Problem& P) {
   w.cand_thr = c.take<float>(P.n);
   w.fail_rows = c.take<int32_t>(P.n);
   w.perm = c.take<int32_t>(P.npacked);
-  w.order_ws_bytes = order_workspace_bytes(P.npacked, P.d, ORDER_LEAF);
+  // the order's rows: projected when d > ORDER_PROJ_D
+  w.Xo = P.d > ORDER_PROJ_D ? c.take<float>(size_t(P.n) * ORDER_PROJ_D) : nullptr;
+  w.order_ws_bytes = order_workspace_bytes(P.npacked, std::max(P.d, ORDER_PROJ_D), ORDER_LEAF);
   w.order_ws = c.take<unsigned char>(w.order_ws_bytes);
   if (P.refine) {
     w.flags = c.take<int32_t>(P.npacked);
@@ -374,7 +377,19 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   // pruning needs single-CTA work items over 256-key tiles (or the FP32 SIMT kernel)
   const bool prune = P.prune && tc && !cfg.pair && cfg.bn == PRUNE_BN;
   const bool prune32 = P.prune && P.candidates && P.k > 1 && P.prec == PREC_FP32;
-  MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, order_levels(P, tc || prune32),
+  // the tree on projected rows (MSC_B200_ORDER_PROJ=0: on the rows themselves; tuning)
+  const float* Xord = Xu;
+  int dord = P.d;
+  const int levels = order_levels(P, tc || prune32);
+  {
+    const char* pe = std::getenv("MSC_B200_ORDER_PROJ");
+    if (w.Xo && levels > 0 && !(pe && *pe == '0')) {
+      MSC_TRY(launch_project(Xu, P.n, P.d, w.Xo, st));
+      Xord = w.Xo;
+      dord = ORDER_PROJ_D;
+    }
+  }
+  MSC_TRY(launch_order(Xord, dord, w.seg, P.nseg, P.npacked, levels,
                        ORDER_LEAF, w.perm, (prune || prune32) ? w.pr.leaf : nullptr, w.order_ws,
                        w.order_ws_bytes, st, P.max_seg));
   if (!P.candidates) {

@@ -106,6 +106,9 @@ int launch_pack_fp32(const float* X, const int32_t* perm, const SegDesc* seg, in
 // near cells are near in packed order; levels = 0 gives the identity order
 // leaf_out (optional): per packed position, the first position of its leaf (-1: padding)
 size_t order_workspace_bytes(int64_t npacked, int d, int leaf);
+// the tree runs on the rows projected onto ORDER_PROJ_D random sign directions when d is larger
+constexpr int ORDER_PROJ_D = 16;
+int launch_project(const float* X, int64_t n, int d, float* Y, cudaStream_t st);
 // max_seg: the largest sample (the extra 2-means steps run only on levels whose nodes are large)
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
                  int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,

@@ -506,6 +506,34 @@ lloyd_node_kernel(const float* __restrict__ X, int d, int64_t npacked,
   }
 }
 
+// Rows projected onto ORDER_PROJ_D random directions for the tree (entries ±1 from a fixed hash:
+// a random sign matrix keeps the pairwise distances to within a small factor with high
+// probability, which is all that choosing 2-means splits needs).  Each pass of a tree level then
+// reads ORDER_PROJ_D floats per row instead of d; the balls, the plan and every distance of the
+// graph use the exact rows.
+__device__ __forceinline__ float proj_sign(int t, int j) {
+  uint32_t h = uint32_t(t) * 0x9E3779B1u ^ (uint32_t(j) + 0x7F4A7C15u) * 0x85EBCA77u;
+  h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12; h *= 0x297A2D39u; h ^= h >> 15;
+  return (h & 1u) ? 1.f : -1.f;
+}
+__global__ void __launch_bounds__(256)
+project_kernel(const float* __restrict__ X, int64_t n, int d, float* __restrict__ Y) {
+  __shared__ float R[MSC_MAX_D][ORDER_PROJ_D];
+  for (int e = threadIdx.x; e < d * ORDER_PROJ_D; e += blockDim.x)
+    R[e / ORDER_PROJ_D][e % ORDER_PROJ_D] = proj_sign(e / ORDER_PROJ_D, e % ORDER_PROJ_D);
+  __syncthreads();
+  const int64_t total = n * ORDER_PROJ_D;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e / ORDER_PROJ_D;
+    const int j = int(e - i * ORDER_PROJ_D);
+    const float* x = X + i * d;
+    float acc = 0.f;
+    for (int t = 0; t < d; ++t) acc = fmaf(x[t], R[t][j], acc);
+    Y[e] = acc;
+  }
+}
+
 // leaf of every packed position: the first position of its final node (-1: padding rows)
 __global__ void leaf_id_kernel(int64_t npacked, const int32_t* __restrict__ perm,
                                const int32_t* __restrict__ ns, int32_t* __restrict__ leaf_out) {
@@ -616,6 +644,14 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     leaf_id_kernel<<<grid, OR_T, 0, st>>>(npacked, perm, sc, leaf_out);
     MSC_LAUNCH_CHECK();
   }
+  return MSC_OK;
+}
+
+int launch_project(const float* X, int64_t n, int d, float* Y, cudaStream_t st) {
+  const int grid = int(std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(n * ORDER_PROJ_D, 256), int64_t(num_sms()) * 8)));
+  project_kernel<<<grid, 256, 0, st>>>(X, n, d, Y);
+  MSC_LAUNCH_CHECK();
   return MSC_OK;
 }
 
