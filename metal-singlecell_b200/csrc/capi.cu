@@ -275,6 +275,10 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
 
 // leaves of the locality tree (order.cu) hold at most this many rows
 constexpr int ORDER_LEAF = 256;
+// first tree level on the projected rows: the levels above split the sample between clusters, and
+// there the exact rows keep whole clusters together (all levels projected kept 49% more far key
+// tiles at 1.3M × 50)
+constexpr int ORDER_PROJ_FROM = 8;
 
 KnnWs carve_knn(Carver& c, const Problem& P) {
   KnnWs w{};
@@ -377,21 +381,17 @@ int run_knn(const Problem& P, const KnnWs& w, const float* X, int32_t* knn_idx, 
   // pruning needs single-CTA work items over 256-key tiles (or the FP32 SIMT kernel)
   const bool prune = P.prune && tc && !cfg.pair && cfg.bn == PRUNE_BN;
   const bool prune32 = P.prune && P.candidates && P.k > 1 && P.prec == PREC_FP32;
-  // the tree on projected rows (MSC_B200_ORDER_PROJ=0: on the rows themselves; tuning)
-  const float* Xord = Xu;
-  int dord = P.d;
+  // the tree's lower levels on projected rows (MSC_B200_ORDER_PROJ=<level>: the first level on
+  // them, 0 = all, negative = none; tuning)
   const int levels = order_levels(P, tc || prune32);
-  {
-    const char* pe = std::getenv("MSC_B200_ORDER_PROJ");
-    if (w.Xo && levels > 0 && !(pe && *pe == '0')) {
-      MSC_TRY(launch_project(Xu, P.n, P.d, w.Xo, st));
-      Xord = w.Xo;
-      dord = ORDER_PROJ_D;
-    }
-  }
-  MSC_TRY(launch_order(Xord, dord, w.seg, P.nseg, P.npacked, levels,
+  int proj_from = ORDER_PROJ_FROM;
+  if (const char* pe = std::getenv("MSC_B200_ORDER_PROJ")) proj_from = std::atoi(pe);
+  const bool proj = w.Xo && levels > proj_from && proj_from >= 0;
+  if (proj) MSC_TRY(launch_project(Xu, P.n, P.d, w.Xo, st));
+  MSC_TRY(launch_order(Xu, P.d, w.seg, P.nseg, P.npacked, levels,
                        ORDER_LEAF, w.perm, (prune || prune32) ? w.pr.leaf : nullptr, w.order_ws,
-                       w.order_ws_bytes, st, P.max_seg));
+                       w.order_ws_bytes, st, P.max_seg, proj ? w.Xo : nullptr, ORDER_PROJ_D,
+                       proj_from));
   if (!P.candidates) {
     MSC_TRY(launch_all_rows_fail(w.perm, P.npacked, w.fail_rows, w.ctl, st));
     MSC_TRY(launch_fp64_scan(Xu, P.d, w.perm, w.seg, P.nseg, w.fail_rows, P.n, P.k, cosine,

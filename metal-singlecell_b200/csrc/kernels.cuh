@@ -110,9 +110,11 @@ size_t order_workspace_bytes(int64_t npacked, int d, int leaf);
 constexpr int ORDER_PROJ_D = 16;
 int launch_project(const float* X, int64_t n, int d, float* Y, cudaStream_t st);
 // max_seg: the largest sample (the extra 2-means steps run only on levels whose nodes are large)
+// Xp (optional): the rows projected onto dp dimensions, used from level proj_from on
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
                  int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
-                 cudaStream_t st, int64_t max_seg);
+                 cudaStream_t st, int64_t max_seg, const float* Xp = nullptr, int dp = 0,
+                 int proj_from = 0);
 size_t scan_i32_scratch_elems(int64_t n);
 int scan_excl_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* scratch, cudaStream_t st);
 int launch_single_segment(SegDesc* seg, int64_t n, cudaStream_t st);

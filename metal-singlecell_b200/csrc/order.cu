@@ -570,7 +570,9 @@ size_t order_workspace_bytes(int64_t npacked, int d, int leaf) {
 
 int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t npacked, int levels,
                  int leaf, int32_t* perm, int32_t* leaf_out, void* ws, size_t ws_bytes,
-                 cudaStream_t st, int64_t max_seg) {
+                 cudaStream_t st, int64_t max_seg, const float* Xp, int dp, int proj_from) {
+  const float* X0 = X;
+  const int d0 = d;
   if (ws_bytes < order_workspace_bytes(npacked, d, leaf)) {
     set_error("order: workspace %zu < %zu bytes", ws_bytes, order_workspace_bytes(npacked, d, leaf));
     return MSC_ERR_WORKSPACE;
@@ -604,6 +606,9 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   MSC_LAUNCH_CHECK();
   int32_t *pc = perm, *pn = perm2, *sc = nsA, *ec = neA, *sn = nsB, *en = neB;
   for (int l = 0; l < levels; ++l) {
+    // the exact rows on the top levels, where a split separates clusters; the projected rows below
+    X = (Xp && l >= proj_from) ? Xp : X0;
+    d = (Xp && l >= proj_from) ? dp : d0;
     MSC_CUDA_TRY(cudaMemsetAsync(best_a, 0, sizeof(unsigned long long) * npacked, st));
     MSC_CUDA_TRY(cudaMemsetAsync(best_b, 0, sizeof(unsigned long long) * npacked, st));
     far_a_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a);
