@@ -276,9 +276,10 @@ int make_problem(Problem& P, int64_t n, int d, int k, int metric, int prec, int 
 // leaves of the locality tree (order.cu) hold at most this many rows
 constexpr int ORDER_LEAF = 256;
 // first tree level on the projected rows: the levels above split the sample between clusters, and
-// there the exact rows keep whole clusters together (all levels projected kept 49% more far key
-// tiles at 1.3M × 50)
-constexpr int ORDER_PROJ_FROM = 8;
+// there the exact rows keep whole clusters together.  Measured at 1.3M × 50 (graph / far key tiles
+// kept): exact rows throughout 72.3 ms / 2.63 M; projected from level 10 70.95 ms / 2.79 M, from
+// level 8 71.07 ms / 2.84 M, every level 76.0 ms / 3.91 M.
+constexpr int ORDER_PROJ_FROM = 10;
 
 KnnWs carve_knn(Carver& c, const Problem& P) {
   KnnWs w{};
