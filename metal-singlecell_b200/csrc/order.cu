@@ -19,7 +19,9 @@
 // outlying) cells; the extra steps matter at the top of the tree, where a node holds many
 // clusters and the bisector of the first means cuts through some of them (measured at 1.3M × 50,
 // 200 clusters: far key tiles kept by the pruning plan 3.42 M → 2.63 M, main scan 44.8 → 40.9 ms,
-// for 0.6 ms more ordering).
+// for 0.6 ms more ordering).  The caller may give the rows projected onto a few random directions
+// for the lower levels (Xp, from level proj_from on): those levels split inside one cluster, and
+// each of their passes then reads a fraction of a row.
 // A degenerate split (all on one side) halves the range instead; the partition is stable.  The
 // side means are summed with floating-point atomics, so a cell almost equidistant from both means
 // may fall on either side from run to run; the graph is the same either way.  A fixed number of
