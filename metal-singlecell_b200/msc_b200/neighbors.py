@@ -367,6 +367,7 @@ def _host_state(n: int, d: int, k: int, device) -> HostGraphState:
 
 
 _STAGE_BYTES = 32 << 20              # pinned staging chunk of the upload
+_DOWN_CHUNK = 8 << 20                # entries per chunk of the connectivities download
 
 
 def _upload(torch, st: HostGraphState, X: np.ndarray):
@@ -454,11 +455,25 @@ def _graph_host(X: np.ndarray, k: int, metric: str, method: str, precision: str,
     main.synchronize()
     _lib.check_stats(h["stats"].numpy())
     nnz = int(h["conn_indptr"][n])
-    h["conn_indices"][:nnz].copy_(c_ind[:nnz], non_blocking=True)
-    h["conn_data"][:nnz].copy_(c_dat[:nnz], non_blocking=True)
-    main.synchronize()
-    conn = sp.csr_matrix((_owned(torch, h["conn_data"], nnz, np.float32),
-                          _owned(torch, h["conn_indices"], nnz, np.int32),
+    # the connectivities in chunks: every chunk's download is queued at once on the copy stream,
+    # and each chunk is copied into the NumPy arrays as soon as it has arrived, while the later
+    # chunks are still in flight
+    c_data = np.empty(nnz, np.float32)
+    c_indices = np.empty(nnz, np.int32)
+    chunks = []
+    with torch.cuda.stream(cs):
+        for off in range(0, nnz, _DOWN_CHUNK):
+            m = min(_DOWN_CHUNK, nnz - off)
+            h["conn_indices"][off:off + m].copy_(c_ind[off:off + m], non_blocking=True)
+            h["conn_data"][off:off + m].copy_(c_dat[off:off + m], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(cs)
+            chunks.append((off, m, ev))
+    for off, m, ev in chunks:
+        ev.synchronize()
+        torch.from_numpy(c_indices[off:off + m]).copy_(h["conn_indices"][off:off + m])
+        torch.from_numpy(c_data[off:off + m]).copy_(h["conn_data"][off:off + m])
+    conn = sp.csr_matrix((c_data, c_indices,
                           h["conn_indptr"].numpy().astype(_index_dtype(n, nnz))), shape=(n, n))
     return dist, conn
 
