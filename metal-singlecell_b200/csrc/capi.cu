@@ -9,7 +9,9 @@
 //                    connectivities                     (neighbors.py:491-559, 465-488)
 //
 // Nothing here allocates device memory: every buffer is carved out of the caller's workspace.
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 #include <algorithm>
 #include <unordered_map>
@@ -118,6 +120,25 @@ cudaError_t raise_smem_cap_fn(const void* func, size_t bytes) {
   if (fa.maxDynamicSharedSizeBytes >= 0 && size_t(fa.maxDynamicSharedSizeBytes) >= bytes)
     return cudaSuccess;
   return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+int resident_blocks_fn(const void* func, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  const auto key = std::make_tuple(func, dev, threads, smem);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, func, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    v = 1;
+  }
+  v = std::max(1, v);
+  cache[key] = v;
+  return v;
 }
 
 namespace {

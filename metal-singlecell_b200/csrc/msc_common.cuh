@@ -162,4 +162,15 @@ inline cudaError_t raise_smem_cap(K* kern, size_t bytes) {
   return raise_smem_cap_fn(reinterpret_cast<const void*>(kern), bytes);
 }
 
+// Blocks of `threads` threads and `smem` dynamic shared-memory bytes that fit on one SM at once
+// (the occupancy query, cached per kernel, device and shape; at least 1).  A grid-stride kernel
+// launched with more blocks than the SMs hold runs a second, partly filled wave.
+int resident_blocks_fn(const void* func, int threads, size_t smem);
+template <typename K>
+inline int resident_grid(K* kern, int threads, size_t smem, int64_t work_blocks) {
+  const int64_t full = int64_t(num_sms()) *
+                       resident_blocks_fn(reinterpret_cast<const void*>(kern), threads, smem);
+  return int(max64(1, min64(work_blocks, full)));
+}
+
 }  // namespace msc

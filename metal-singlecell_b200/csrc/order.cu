@@ -36,7 +36,6 @@ namespace msc {
 namespace {
 
 constexpr int OR_T = 256;
-constexpr int OR_W = OR_T / 32;
 // More 2-means steps on the first LLOYD_LEVELS levels (lloyd_node_kernel), on up to
 // LLOYD_SAMPLES_MAX rows of every split node (MSC_B200_LLOYD_LEVELS / MSC_B200_LLOYD_STEPS override
 // the level count and the steps: tuning).  With one step, a mixture of well-separated clusters is
@@ -50,14 +49,25 @@ constexpr size_t LLOYD_SMEM_MAX = 200 * 1024;
 // parts of one or a few clusters, and the launches would cost a small graph more than they save
 constexpr int64_t LLOYD_MIN_NODE = 8192;
 
-// One warp's 32 rows, 32 dimensions at a time: row r's dimensions c..c+31 in tile[r][0..31].
-// Lanes load a row together (one coalesced line per row and chunk), then each lane reads its own
-// row back from the tile (stride 33 floats: no bank conflicts).  A thread reading its row alone,
-// one float per load, keeps 32 rows' lines live per warp and thrashes L1.
-using RowTile = float[32][33];
+// The row passes of a level (far_a, far_b, side, reassign, side_sum) run ROW_T-thread blocks:
+// with their row tiles, ten to eleven blocks fit on an SM.
+constexpr int ROW_T = 128;
+constexpr int ROW_W = ROW_T / 32;
 
-// stage dimensions c..c+31 of the lanes' rows (row < 0: not staged); sixteen loads are issued
-// before their stores so that a warp keeps sixteen lines in flight
+// One warp's 32 rows, 32 dimensions at a time: row r's dimensions c..c+31 in tile[r][0..31]
+// (dimensions at or past d, and rows < 0, hold zeros).  Lanes load a row together (one coalesced
+// line per row and chunk), then each lane reads its own row back from the tile in pairs: a stride
+// of 34 floats keeps the rows 8-byte aligned, and the 16 lanes of each half-warp phase of a
+// 64-bit read then cover the 32 banks once.  A thread reading its row alone, one float per load,
+// keeps 32 rows' lines live per warp and thrashes L1.
+constexpr int TILE_S = 34;
+using RowTile = float[32][TILE_S];
+// per warp: one or two rows of reference values (the far cell, or the two side means),
+// zero-padded to whole 32-dimension chunks
+using RefRows = float[2][MSC_MAX_D];
+
+// stage dimensions c..c+31 of the lanes' rows (row < 0: zeros); sixteen loads are issued before
+// their stores so that a warp keeps sixteen lines in flight
 __device__ __forceinline__ void stage_rows(const float* __restrict__ X, int d, int c, int32_t row,
                                            RowTile& tile) {
   const int t = c + lane_id();
@@ -75,21 +85,47 @@ __device__ __forceinline__ void stage_rows(const float* __restrict__ X, int d, i
   __syncwarp();
 }
 
+// Σ_j (tile[lane][j] − ref[c + j])² over the chunk's 32 dimensions, added to acc in order
+__device__ __forceinline__ float chunk_d2(const RowTile& tile, const float* ref, int c, float acc) {
+#pragma unroll
+  for (int j = 0; j < 32; j += 2) {
+    const float2 x = *reinterpret_cast<const float2*>(&tile[lane_id()][j]);
+    const float2 y = *reinterpret_cast<const float2*>(&ref[c + j]);
+    const float dx = x.x - y.x, dy = x.y - y.y;
+    acc = fmaf(dx, dx, acc);
+    acc = fmaf(dy, dy, acc);
+  }
+  return acc;
+}
+
 // squared distance between the lane's row and row `other`, summed over t = 0..d-1 in order
-// (the same sum as a plain loop over the two rows); lanes with row < 0 return 0
+// (the same sum as a plain loop over the two rows: the padding adds exact zeros); lanes with
+// row < 0 return 0.  When the warp's active lanes share `other` (a warp inside one node: all but
+// the warps that straddle a node boundary) that row is staged once in ref[0]; otherwise every
+// lane reads its own through L1.
 __device__ __forceinline__ float warp_row_d2(const float* __restrict__ X, int d, int32_t row,
-                                             int64_t other, RowTile& tile) {
+                                             int64_t other, RowTile& tile, RefRows& ref) {
   const unsigned act = __ballot_sync(FULL, row >= 0);
   float acc = 0.f;
   if (act == 0) return acc;
+  const int64_t o0 = __shfl_sync(FULL, other, __ffs(act) - 1);
+  const bool uni = __all_sync(FULL, row < 0 || other == o0);
+  if (uni) {
+    for (int t = lane_id(); t < MSC_MAX_D; t += 32) ref[0][t] = t < d ? X[o0 * d + t] : 0.f;
+    __syncwarp();
+  }
   for (int c = 0; c < d; c += 32) {
     stage_rows(X, d, c, row, tile);
     if (row >= 0) {
-      const float* y = X + other * d + c;
-      const int tn = min(32, d - c);
-      for (int j = 0; j < tn; ++j) {
-        const float df = tile[lane_id()][j] - y[j];
-        acc = fmaf(df, df, acc);
+      if (uni) {
+        acc = chunk_d2(tile, ref[0], c, acc);
+      } else {
+        const float* y = X + other * d + c;
+        const int tn = min(32, d - c);
+        for (int j = 0; j < tn; ++j) {
+          const float df = tile[lane_id()][j] - y[j];
+          acc = fmaf(df, df, acc);
+        }
       }
     }
     __syncwarp();
@@ -144,12 +180,14 @@ __device__ __forceinline__ void warp_far_max(unsigned long long* best, int s, bo
 
 // The loops below keep the 32 lanes of a warp on 32 consecutive positions (warp-uniform trip
 // counts) so that warp_far_max can combine them and warp_row_d2 can stage their rows.
-__global__ void __launch_bounds__(OR_T)
+__global__ void __launch_bounds__(ROW_T)
 far_a_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
              const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
              const int32_t* __restrict__ ne, unsigned long long* __restrict__ best) {
-  __shared__ RowTile tiles[OR_W];
+  __shared__ __align__(16) RowTile tiles[ROW_W];
+  __shared__ __align__(16) RefRows refs[ROW_W];
   RowTile& tile = tiles[warp_id()];
+  RefRows& ref = refs[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
@@ -158,18 +196,20 @@ far_a_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     if (p < npacked) { s = ns[p]; e = ne[p]; }
     const bool active = p < npacked && e - s > leaf;
     const int32_t row = active ? perm[p] : -1;
-    const float v = warp_row_d2(X, d, row, active ? perm[s] : 0, tile);
+    const float v = warp_row_d2(X, d, row, active ? perm[s] : 0, tile, ref);
     warp_far_max(best, s, active, active ? far_key(v, p) : 0ull);
   }
 }
 
-__global__ void __launch_bounds__(OR_T)
+__global__ void __launch_bounds__(ROW_T)
 far_b_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
              const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
              const int32_t* __restrict__ ne, const unsigned long long* __restrict__ best_a,
              float* __restrict__ da, unsigned long long* __restrict__ best_b) {
-  __shared__ RowTile tiles[OR_W];
+  __shared__ __align__(16) RowTile tiles[ROW_W];
+  __shared__ __align__(16) RefRows refs[ROW_W];
   RowTile& tile = tiles[warp_id()];
+  RefRows& ref = refs[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
@@ -178,19 +218,21 @@ far_b_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     if (p < npacked) { s = ns[p]; e = ne[p]; }
     const bool active = p < npacked && e - s > leaf;
     const int32_t row = active ? perm[p] : -1;
-    const float v = warp_row_d2(X, d, row, active ? perm[far_pos(best_a[s])] : 0, tile);
+    const float v = warp_row_d2(X, d, row, active ? perm[far_pos(best_a[s])] : 0, tile, ref);
     if (active) da[p] = v;
     warp_far_max(best_b, s, active, active ? far_key(v, p) : 0ull);
   }
 }
 
-__global__ void __launch_bounds__(OR_T)
+__global__ void __launch_bounds__(ROW_T)
 side_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
             const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
             const int32_t* __restrict__ ne, const float* __restrict__ da,
             const unsigned long long* __restrict__ best_b, int32_t* __restrict__ side) {
-  __shared__ RowTile tiles[OR_W];
+  __shared__ __align__(16) RowTile tiles[ROW_W];
+  __shared__ __align__(16) RefRows refs[ROW_W];
   RowTile& tile = tiles[warp_id()];
+  RefRows& ref = refs[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
@@ -199,7 +241,7 @@ side_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     if (p < npacked) { s = ns[p]; e = ne[p]; }
     const bool active = p < npacked && e - s > leaf;
     const int32_t row = active ? perm[p] : -1;
-    const float db = warp_row_d2(X, d, row, active ? perm[far_pos(best_b[s])] : 0, tile);
+    const float db = warp_row_d2(X, d, row, active ? perm[far_pos(best_b[s])] : 0, tile, ref);
     if (p < npacked) side[p] = active && da[p] > db ? 1 : 0;   // nearer to b: second half
   }
 }
@@ -245,78 +287,99 @@ __global__ void split_start_kernel(int64_t npacked, int leaf, const int32_t* __r
     flag[p] = (ns[p] == p && ne[p] - ns[p] > leaf) ? 1 : 0;
 }
 
-// Per split node and side: Σ x and the count.  A warp walks 64 consecutive positions; lane t owns
-// dimensions t, t+32, ...; partial sums go out with one atomic per (node, side, dimension) each
-// time the node changes along the walk.  acc layout per node: [2][d] sums, then [2] counts.
-constexpr int SUM_RUN = 64;
-constexpr int SUM_WARPS = OR_T / 32;
-constexpr int SUM_SLOT = 2 * 128 + 2;       // sums and counts of one node (d <= 128)
-__global__ void __launch_bounds__(OR_T)
+// Per split node and side: Σ x and the count.  Each warp takes a contiguous range of 32-position
+// tasks (consecutive tasks mostly lie in one node); lane t owns dimensions t, t+32, ... (PER of
+// them: d <= 32·PER) and keeps FP64 sums for the node it is in, handed on with one atomic per
+// (node, side, dimension) when the node changes.  A task whose active positions share one node
+// stages its 32 rows chunk by chunk and adds the columns from shared memory (in FP32 over the
+// task's rows, then into the FP64 sums); a task that straddles nodes adds row by row from global
+// memory.  At the end the warps of a block that finish in the same node combine in shared memory,
+// so at the top levels, where every warp is in one of a few nodes, a block issues one set of
+// atomics.  acc layout per node: [2][d] sums, then [2] counts.
+constexpr int SUM_SLOT = 2 * MSC_MAX_D + 2;
+template <int PER>
+__global__ void __launch_bounds__(ROW_T)
 side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
                 const int32_t* __restrict__ side, double* __restrict__ acc) {
-  // Runs that lie inside one node (almost all of them) are first combined across the warps of the
-  // block in shared memory, so that at the top levels, where every run belongs to the same one or
-  // two nodes, a block issues one set of atomics instead of one per warp.
-  __shared__ double part[SUM_WARPS][SUM_SLOT];
-  __shared__ int64_t part_node[SUM_WARPS];
+  __shared__ __align__(16) RowTile tiles[ROW_W];
+  __shared__ double part[ROW_W][SUM_SLOT];
+  __shared__ int64_t part_node[ROW_W];
+  RowTile& tile = tiles[warp_id()];
   const int lane = lane_id(), wib = warp_id();
-  const int64_t nruns = (npacked + SUM_RUN - 1) / SUM_RUN;
-  const int per = (d + 31) / 32;            // dimensions per lane (d <= 128)
-  for (int64_t rb = int64_t(blockIdx.x) * SUM_WARPS; rb < nruns;
-       rb += int64_t(gridDim.x) * SUM_WARPS) {          // block-uniform
-    const int64_t r = rb + wib;
-    double s0[4] = {0, 0, 0, 0}, s1[4] = {0, 0, 0, 0};
-    double c0 = 0, c1 = 0;
-    int64_t cur = -1;                        // node id being accumulated
-    bool flushed = false;
-    auto flush = [&]() {
-      if (cur < 0) return;
-      flushed = true;
-      double* a = acc + cur * (2 * d + 2);
-      for (int j = 0; j < per; ++j) {
-        const int t = lane + 32 * j;
-        if (t < d) {
-          if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
-          if (s1[j] != 0.0) atomicAdd(&a[d + t], s1[j]);
-        }
-        s0[j] = 0; s1[j] = 0;
-      }
-      if (lane == 0) {
-        if (c0 != 0) atomicAdd(&a[2 * d], c0);
-        if (c1 != 0) atomicAdd(&a[2 * d + 1], c1);
-      }
-      c0 = 0; c1 = 0;
-    };
-    if (r < nruns) {                         // warp-uniform
-      const int64_t p0 = r * SUM_RUN, p1 = min64(npacked, p0 + SUM_RUN);
-      // the run's node ids, rows and sides, one position per lane (two halves), then a walk that
-      // only loads row data (independent from position to position)
-      int32_t idh[2], rowh[2], sdh[2];
+  const int64_t ntask = (npacked + 31) / 32;
+  const int64_t nwarp = int64_t(gridDim.x) * ROW_W, gw = int64_t(blockIdx.x) * ROW_W + wib;
+  const int64_t t0 = ntask * gw / nwarp, t1 = ntask * (gw + 1) / nwarp;
+  double s0[PER], s1[PER];
 #pragma unroll
-      for (int hh = 0; hh < 2; ++hh) {
-        const int64_t p = p0 + 32 * hh + lane;
-        idh[hh] = -1; rowh[hh] = 0; sdh[hh] = 0;
-        if (p < p1) {
-          const int st = ns[p];
-          if (ne[p] - st > leaf) {
-            idh[hh] = int32_t(S[st]);
-            rowh[hh] = perm[p];
-            sdh[hh] = side[p];
+  for (int j = 0; j < PER; ++j) { s0[j] = 0.0; s1[j] = 0.0; }
+  double c0 = 0, c1 = 0;
+  int64_t cur = -1;                          // node id being accumulated
+  auto flush = [&]() {
+    if (cur < 0) return;
+    double* a = acc + cur * (2 * d + 2);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int t = lane + 32 * j;
+      if (t < d) {
+        if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
+        if (s1[j] != 0.0) atomicAdd(&a[d + t], s1[j]);
+      }
+      s0[j] = 0; s1[j] = 0;
+    }
+    if (lane == 0) {
+      if (c0 != 0) atomicAdd(&a[2 * d], c0);
+      if (c1 != 0) atomicAdd(&a[2 * d + 1], c1);
+    }
+    c0 = 0; c1 = 0;
+  };
+  for (int64_t tk = t0; tk < t1; ++tk) {     // warp-uniform
+    const int64_t p = tk * 32 + lane;
+    int64_t id = -1;
+    int32_t row = -1;
+    int sd = 0;
+    if (p < npacked) {
+      const int st = ns[p];
+      if (ne[p] - st > leaf) {
+        id = S[st];
+        row = perm[p];
+        sd = side[p];
+      }
+    }
+    const unsigned act = __ballot_sync(FULL, id >= 0);
+    if (act == 0) continue;
+    const int64_t id0 = __shfl_sync(FULL, id, __ffs(act) - 1);
+    if (__all_sync(FULL, id < 0 || id == id0)) {
+      if (id0 != cur) { flush(); cur = id0; }
+      const unsigned m1 = __ballot_sync(FULL, id >= 0 && sd != 0);
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        if (32 * j < d) {                    // warp-uniform
+          stage_rows(X, d, 32 * j, row, tile);
+          float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+          for (int r = 0; r < 32; ++r) {
+            const float v = tile[r][lane];
+            if ((m1 >> r) & 1u) f1 += v; else f0 += v;
           }
+          s0[j] += f0;
+          s1[j] += f1;
+          __syncwarp();
         }
       }
-#pragma unroll 4
-      for (int jj = 0; jj < SUM_RUN; ++jj) {
-        const int hh = jj >> 5;
-        const int32_t id = __shfl_sync(FULL, hh ? idh[1] : idh[0], jj & 31);
-        if (id < 0) continue;                // warp-uniform
-        const int32_t rw = __shfl_sync(FULL, hh ? rowh[1] : rowh[0], jj & 31);
-        const bool one = __shfl_sync(FULL, hh ? sdh[1] : sdh[0], jj & 31) != 0;
-        if (id != cur) { flush(); cur = id; }
+      c1 += __popc(m1);
+      c0 += __popc(act & ~m1);
+    } else {
+      for (int r = 0; r < 32; ++r) {
+        const int64_t idr = __shfl_sync(FULL, id, r);
+        if (idr < 0) continue;               // warp-uniform
+        const int32_t rw = __shfl_sync(FULL, row, r);
+        const bool one = __shfl_sync(FULL, sd, r) != 0;
+        if (idr != cur) { flush(); cur = idr; }
         const float* x = X + int64_t(rw) * d;
-        for (int j = 0; j < per; ++j) {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
           const int t = lane + 32 * j;
           if (t < d) {
             if (one) s1[j] += x[t]; else s0[j] += x[t];
@@ -325,62 +388,63 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
         if (one) c1 += 1.0; else c0 += 1.0;
       }
     }
-    // a run that met one node only hands its sums to the block; any other flushes its last node
-    int64_t slot_node = -1;
-    if (cur >= 0 && !flushed) {
-      slot_node = cur;
-      for (int j = 0; j < per; ++j) {
-        const int t = lane + 32 * j;
-        if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
-      }
-      if (lane == 0) { part[wib][2 * d] = c0; part[wib][2 * d + 1] = c1; }
-    } else {
-      flush();
+  }
+  // the last node's sums go to the block
+  if (cur >= 0) {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int t = lane + 32 * j;
+      if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
     }
-    if (lane == 0) part_node[wib] = slot_node;
-    __syncthreads();
-    if (wib == 0) {
-      // consecutive warps with the same node: one atomic per value per node
-      int w0 = 0;
-      while (w0 < SUM_WARPS) {
-        const int64_t nd = part_node[w0];
-        int w1 = w0 + 1;
-        while (w1 < SUM_WARPS && part_node[w1] == nd) ++w1;
-        if (nd >= 0) {
-          double* a = acc + nd * (2 * d + 2);
-          for (int t = lane; t < 2 * d + 2; t += 32) {
-            double v = 0.0;
-            for (int w = w0; w < w1; ++w) v += part[w][t];
-            if (v != 0.0) atomicAdd(&a[t], v);
-          }
+    if (lane == 0) { part[wib][2 * d] = c0; part[wib][2 * d + 1] = c1; }
+  }
+  if (lane == 0) part_node[wib] = cur;
+  __syncthreads();
+  if (wib == 0) {
+    // consecutive warps in the same node: one atomic per value per node
+    int w0 = 0;
+    while (w0 < ROW_W) {
+      const int64_t nd = part_node[w0];
+      int w1 = w0 + 1;
+      while (w1 < ROW_W && part_node[w1] == nd) ++w1;
+      if (nd >= 0) {
+        double* a = acc + nd * (2 * d + 2);
+        for (int t = lane; t < 2 * d + 2; t += 32) {
+          double v = 0.0;
+          for (int w = w0; w < w1; ++w) v += part[w][t];
+          if (v != 0.0) atomicAdd(&a[t], v);
         }
-        w0 = w1;
       }
+      w0 = w1;
     }
-    __syncthreads();
   }
 }
 
-// second assignment: the nearer of the two side means (ties to side 0); a side left empty by the
-// first assignment keeps it
-__global__ void __launch_bounds__(OR_T)
+// second assignment: the nearer of the two side means (ties to side 0), in FP32 with each mean
+// rounded once from its FP64 sum / count; a side left empty by the first assignment keeps it.  A
+// warp inside one node stages the two means once in ref.
+__global__ void __launch_bounds__(ROW_T)
 reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
                 const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
                 const double* __restrict__ acc, int32_t* __restrict__ side) {
-  __shared__ RowTile tiles[OR_W];
+  __shared__ __align__(16) RowTile tiles[ROW_W];
+  __shared__ __align__(16) RefRows refs[ROW_W];
   RowTile& tile = tiles[warp_id()];
+  RefRows& ref = refs[warp_id()];
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t b = blockIdx.x * int64_t(blockDim.x) + (threadIdx.x & ~31); b < npacked;
        b += stride) {
     const int64_t p = b + lane_id();
     const double* a = nullptr;
     double i0 = 0.0, i1 = 0.0;
+    int64_t slot = -1;
     int32_t row = -1;
     if (p < npacked) {
       const int st = ns[p];
       if (ne[p] - st > leaf) {
-        a = acc + S[st] * (2 * d + 2);
+        slot = S[st];
+        a = acc + slot * (2 * d + 2);
         const double n0 = a[2 * d], n1 = a[2 * d + 1];
         if (n0 != 0.0 && n1 != 0.0) {
           i0 = 1.0 / n0;
@@ -391,16 +455,45 @@ reassign_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
     }
     const unsigned act = __ballot_sync(FULL, row >= 0);
     if (act == 0) continue;                  // warp-uniform
-    double d0 = 0.0, d1 = 0.0;
+    const int src = __ffs(act) - 1;
+    const int64_t slot0 = __shfl_sync(FULL, slot, src);
+    const bool uni = __all_sync(FULL, row < 0 || slot == slot0);
+    if (uni) {
+      const double* a0 = acc + slot0 * (2 * d + 2);
+      const double j0 = __shfl_sync(FULL, i0, src), j1 = __shfl_sync(FULL, i1, src);
+      for (int t = lane_id(); t < MSC_MAX_D; t += 32) {
+        ref[0][t] = t < d ? float(a0[t] * j0) : 0.f;
+        ref[1][t] = t < d ? float(a0[d + t] * j1) : 0.f;
+      }
+      __syncwarp();
+    }
+    float d0 = 0.f, d1 = 0.f;
     for (int c = 0; c < d; c += 32) {
       stage_rows(X, d, c, row, tile);
       if (row >= 0) {
-        const int tn = min(32, d - c);
-        for (int j = 0; j < tn; ++j) {
-          const double v = tile[lane_id()][j];
-          const double u0 = v - a[c + j] * i0, u1 = v - a[d + c + j] * i1;
-          d0 += u0 * u0;
-          d1 += u1 * u1;
+        if (uni) {
+#pragma unroll
+          for (int j = 0; j < 32; j += 2) {
+            const float2 x = *reinterpret_cast<const float2*>(&tile[lane_id()][j]);
+            const float2 m0 = *reinterpret_cast<const float2*>(&ref[0][c + j]);
+            const float2 m1 = *reinterpret_cast<const float2*>(&ref[1][c + j]);
+            float u = x.x - m0.x;
+            d0 = fmaf(u, u, d0);
+            u = x.y - m0.y;
+            d0 = fmaf(u, u, d0);
+            u = x.x - m1.x;
+            d1 = fmaf(u, u, d1);
+            u = x.y - m1.y;
+            d1 = fmaf(u, u, d1);
+          }
+        } else {
+          const int tn = min(32, d - c);
+          for (int j = 0; j < tn; ++j) {
+            const float v = tile[lane_id()][j];
+            const float u0 = v - float(a[c + j] * i0), u1 = v - float(a[d + c + j] * i1);
+            d0 = fmaf(u0, u0, d0);
+            d1 = fmaf(u1, u1, d1);
+          }
         }
       }
       __syncwarp();
@@ -598,6 +691,17 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   int32_t* nstart = c.take<int32_t>(size_t(max_split_nodes(npacked, leaf)));
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ceil_div(npacked, OR_T),
                                                               int64_t(num_sms()) * 8)));
+  // the row passes: one wave of resident blocks each (a grid-stride grid of more blocks than the
+  // SMs hold ran a second, partly filled wave)
+  const int64_t wb = ceil_div(npacked, ROW_T);
+  const int g_far_a = resident_grid(far_a_kernel, ROW_T, 0, wb);
+  const int g_far_b = resident_grid(far_b_kernel, ROW_T, 0, wb);
+  const int g_side = resident_grid(side_kernel, ROW_T, 0, wb);
+  const int g_reassign = resident_grid(reassign_kernel, ROW_T, 0, wb);
+  const int64_t sb = ceil_div(ceil_div(npacked, 32), ROW_W);
+  const int g_sum1 = resident_grid(side_sum_kernel<1>, ROW_T, 0, sb);
+  const int g_sum2 = resident_grid(side_sum_kernel<2>, ROW_T, 0, sb);
+  const int g_sum4 = resident_grid(side_sum_kernel<4>, ROW_T, 0, sb);
   int lloyd_levels = LLOYD_LEVELS, lloyd_steps = LLOYD_STEPS;
   if (const char* e = std::getenv("MSC_B200_LLOYD_LEVELS")) lloyd_levels = std::max(0, std::atoi(e));
   if (const char* e = std::getenv("MSC_B200_LLOYD_STEPS")) lloyd_steps = std::max(0, std::atoi(e));
@@ -613,18 +717,23 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     d = (Xp && l >= proj_from) ? dp : d0;
     MSC_CUDA_TRY(cudaMemsetAsync(best_a, 0, sizeof(unsigned long long) * npacked, st));
     MSC_CUDA_TRY(cudaMemsetAsync(best_b, 0, sizeof(unsigned long long) * npacked, st));
-    far_a_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a);
+    far_a_kernel<<<g_far_a, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a);
     MSC_LAUNCH_CHECK();
-    far_b_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a, da, best_b);
+    far_b_kernel<<<g_far_b, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a, da, best_b);
     MSC_LAUNCH_CHECK();
-    side_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
+    side_kernel<<<g_side, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
     MSC_LAUNCH_CHECK();
     // one 2-means step: side means, then the nearer mean
     split_start_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, sc, ec, sflag);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
     MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-    side_sum_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    if (d <= 32)
+      side_sum_kernel<1><<<g_sum1, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    else if (d <= 64)
+      side_sum_kernel<2><<<g_sum2, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    else
+      side_sum_kernel<4><<<g_sum4, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
     MSC_LAUNCH_CHECK();
     if (l < lloyd_levels && lloyd_steps > 0 && (max_seg >> l) >= LLOYD_MIN_NODE) {
       node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
@@ -636,7 +745,7 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
           X, d, npacked, pc, ec, SN, nstart, acc, lloyd_steps, m_max);
       MSC_LAUNCH_CHECK();
     }
-    reassign_kernel<<<grid, OR_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side);
+    reassign_kernel<<<g_reassign, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, acc, side);
     MSC_LAUNCH_CHECK();
     MSC_TRY(scan_excl_i32(side, npacked, S, scratch, st));
     scatter_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, pc, sc, ec, side, S, pn, sn, en);
