@@ -420,6 +420,169 @@ side_sum_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
   }
 }
 
+// The first assignment and the side sums in one pass over the rows (d <= 32·PER, PER <= 2): a
+// warp stages a task's 32 rows whole (every 32-dimension chunk), takes each row's distance to b
+// (the same sum as warp_row_d2), writes the row's side (nearer to b: 1; as side_kernel), and adds
+// the columns of each side's rows from the same tiles.  Task ranges, node hand-off and the block
+// combine are those of side_sum_kernel.
+template <int PER>
+__global__ void __launch_bounds__(ROW_T)
+side_fused_kernel(const float* __restrict__ X, int d, int64_t npacked, int leaf,
+                  const int32_t* __restrict__ perm, const int32_t* __restrict__ ns,
+                  const int32_t* __restrict__ ne, const int64_t* __restrict__ S,
+                  const float* __restrict__ da, const unsigned long long* __restrict__ best_b,
+                  int32_t* __restrict__ side, double* __restrict__ acc) {
+  constexpr int SLOT = 2 * 32 * PER + 2;
+  __shared__ __align__(16) RowTile tiles[ROW_W][PER];
+  __shared__ __align__(16) float refs[ROW_W][32 * PER];
+  __shared__ double part[ROW_W][SLOT];
+  __shared__ int64_t part_node[ROW_W];
+  const int lane = lane_id(), wib = warp_id();
+  float* ref = refs[wib];
+  const int64_t ntask = (npacked + 31) / 32;
+  const int64_t nwarp = int64_t(gridDim.x) * ROW_W, gw = int64_t(blockIdx.x) * ROW_W + wib;
+  const int64_t t0 = ntask * gw / nwarp, t1 = ntask * (gw + 1) / nwarp;
+  double s0[PER], s1[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) { s0[j] = 0.0; s1[j] = 0.0; }
+  double c0 = 0, c1 = 0;
+  int64_t cur = -1;                          // node id being accumulated
+  auto flush = [&]() {
+    if (cur < 0) return;
+    double* a = acc + cur * (2 * d + 2);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int t = lane + 32 * j;
+      if (t < d) {
+        if (s0[j] != 0.0) atomicAdd(&a[t], s0[j]);
+        if (s1[j] != 0.0) atomicAdd(&a[d + t], s1[j]);
+      }
+      s0[j] = 0; s1[j] = 0;
+    }
+    if (lane == 0) {
+      if (c0 != 0) atomicAdd(&a[2 * d], c0);
+      if (c1 != 0) atomicAdd(&a[2 * d + 1], c1);
+    }
+    c0 = 0; c1 = 0;
+  };
+  for (int64_t tk = t0; tk < t1; ++tk) {     // warp-uniform
+    const int64_t p = tk * 32 + lane;
+    int64_t id = -1, other = 0;
+    int32_t row = -1;
+    if (p < npacked) {
+      const int st = ns[p];
+      if (ne[p] - st > leaf) {
+        id = S[st];
+        row = perm[p];
+        other = perm[far_pos(best_b[st])];
+      }
+    }
+    const unsigned act = __ballot_sync(FULL, id >= 0);
+    if (act == 0) {
+      if (p < npacked) side[p] = 0;
+      continue;
+    }
+    const int src = __ffs(act) - 1;
+    const int64_t id0 = __shfl_sync(FULL, id, src);
+    const bool uni = __all_sync(FULL, id < 0 || id == id0);
+#pragma unroll
+    for (int j = 0; j < PER; ++j)
+      if (32 * j < d) stage_rows(X, d, 32 * j, row, tiles[wib][j]);
+    float db = 0.f;
+    if (uni) {
+      const int64_t o0 = __shfl_sync(FULL, other, src);
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        const int t = lane + 32 * j;
+        ref[t] = t < d ? X[o0 * d + t] : 0.f;
+      }
+      __syncwarp();
+      if (row >= 0) {
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+          if (32 * j < d) db = chunk_d2(tiles[wib][j], ref, 32 * j, db);
+      }
+    } else if (row >= 0) {
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        if (32 * j < d) {
+          const float* y = X + other * d + 32 * j;
+          const int tn = min(32, d - 32 * j);
+          for (int jj = 0; jj < tn; ++jj) {
+            const float df = tiles[wib][j][lane][jj] - y[jj];
+            db = fmaf(df, df, db);
+          }
+        }
+      }
+    }
+    const int sd = (row >= 0 && da[p] > db) ? 1 : 0;
+    if (p < npacked) side[p] = sd;
+    const unsigned m1 = __ballot_sync(FULL, sd != 0);
+    if (uni) {
+      if (id0 != cur) { flush(); cur = id0; }
+#pragma unroll
+      for (int j = 0; j < PER; ++j) {
+        if (32 * j < d) {                    // warp-uniform
+          float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+          for (int r = 0; r < 32; ++r) {
+            const float v = tiles[wib][j][r][lane];
+            if ((m1 >> r) & 1u) f1 += v; else f0 += v;
+          }
+          s0[j] += f0;
+          s1[j] += f1;
+        }
+      }
+      c1 += __popc(m1);
+      c0 += __popc(act & ~m1);
+    } else {
+      for (int r = 0; r < 32; ++r) {
+        const int64_t idr = __shfl_sync(FULL, id, r);
+        if (idr < 0) continue;               // warp-uniform
+        const bool one = (m1 >> r) & 1u;
+        if (idr != cur) { flush(); cur = idr; }
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+          if (lane + 32 * j < d) {
+            const float v = tiles[wib][j][r][lane];
+            if (one) s1[j] += v; else s0[j] += v;
+          }
+        }
+        if (one) c1 += 1.0; else c0 += 1.0;
+      }
+    }
+    __syncwarp();                            // tiles and ref are restaged by the next task
+  }
+  // the last node's sums go to the block
+  if (cur >= 0) {
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int t = lane + 32 * j;
+      if (t < d) { part[wib][t] = s0[j]; part[wib][d + t] = s1[j]; }
+    }
+    if (lane == 0) { part[wib][2 * d] = c0; part[wib][2 * d + 1] = c1; }
+  }
+  if (lane == 0) part_node[wib] = cur;
+  __syncthreads();
+  if (wib == 0) {
+    int w0 = 0;
+    while (w0 < ROW_W) {
+      const int64_t nd = part_node[w0];
+      int w1 = w0 + 1;
+      while (w1 < ROW_W && part_node[w1] == nd) ++w1;
+      if (nd >= 0) {
+        double* a = acc + nd * (2 * d + 2);
+        for (int t = lane; t < 2 * d + 2; t += 32) {
+          double v = 0.0;
+          for (int w = w0; w < w1; ++w) v += part[w][t];
+          if (v != 0.0) atomicAdd(&a[t], v);
+        }
+      }
+      w0 = w1;
+    }
+  }
+}
+
 // second assignment: the nearer of the two side means (ties to side 0), in FP32 with each mean
 // rounded once from its FP64 sum / count; a side left empty by the first assignment keeps it.  A
 // warp inside one node stages the two means once in ref.
@@ -699,8 +862,8 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
   const int g_side = resident_grid(side_kernel, ROW_T, 0, wb);
   const int g_reassign = resident_grid(reassign_kernel, ROW_T, 0, wb);
   const int64_t sb = ceil_div(ceil_div(npacked, 32), ROW_W);
-  const int g_sum1 = resident_grid(side_sum_kernel<1>, ROW_T, 0, sb);
-  const int g_sum2 = resident_grid(side_sum_kernel<2>, ROW_T, 0, sb);
+  const int g_fused1 = resident_grid(side_fused_kernel<1>, ROW_T, 0, sb);
+  const int g_fused2 = resident_grid(side_fused_kernel<2>, ROW_T, 0, sb);
   const int g_sum4 = resident_grid(side_sum_kernel<4>, ROW_T, 0, sb);
   int lloyd_levels = LLOYD_LEVELS, lloyd_steps = LLOYD_STEPS;
   if (const char* e = std::getenv("MSC_B200_LLOYD_LEVELS")) lloyd_levels = std::max(0, std::atoi(e));
@@ -715,25 +878,29 @@ int launch_order(const float* X, int d, const SegDesc* seg, int nseg, int64_t np
     // the exact rows on the top levels, where a split separates clusters; the projected rows below
     X = (Xp && l >= proj_from) ? Xp : X0;
     d = (Xp && l >= proj_from) ? dp : d0;
+    // the level's split nodes and their ids (from the node bounds alone)
+    split_start_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, sc, ec, sflag);
+    MSC_LAUNCH_CHECK();
+    MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
+    MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
     MSC_CUDA_TRY(cudaMemsetAsync(best_a, 0, sizeof(unsigned long long) * npacked, st));
     MSC_CUDA_TRY(cudaMemsetAsync(best_b, 0, sizeof(unsigned long long) * npacked, st));
     far_a_kernel<<<g_far_a, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a);
     MSC_LAUNCH_CHECK();
     far_b_kernel<<<g_far_b, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, best_a, da, best_b);
     MSC_LAUNCH_CHECK();
-    side_kernel<<<g_side, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
-    MSC_LAUNCH_CHECK();
-    // one 2-means step: side means, then the nearer mean
-    split_start_kernel<<<grid, OR_T, 0, st>>>(npacked, leaf, sc, ec, sflag);
-    MSC_LAUNCH_CHECK();
-    MSC_TRY(scan_excl_i32(sflag, npacked, SN, scratch, st));
-    MSC_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * acc_elems, st));
-    if (d <= 32)
-      side_sum_kernel<1><<<g_sum1, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
-    else if (d <= 64)
-      side_sum_kernel<2><<<g_sum2, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
-    else
+    // the nearer of a and b, then the side sums for one 2-means step (one pass for d <= 64)
+    if (d <= 32) {
+      side_fused_kernel<1><<<g_fused1, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, da,
+                                                        best_b, side, acc);
+    } else if (d <= 64) {
+      side_fused_kernel<2><<<g_fused2, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, da,
+                                                        best_b, side, acc);
+    } else {
+      side_kernel<<<g_side, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, da, best_b, side);
+      MSC_LAUNCH_CHECK();
       side_sum_kernel<4><<<g_sum4, ROW_T, 0, st>>>(X, d, npacked, leaf, pc, sc, ec, SN, side, acc);
+    }
     MSC_LAUNCH_CHECK();
     if (l < lloyd_levels && lloyd_steps > 0 && (max_seg >> l) >= LLOYD_MIN_NODE) {
       node_start_kernel<<<grid, OR_T, 0, st>>>(npacked, sflag, SN, nstart);
